@@ -1,0 +1,866 @@
+/* CPU restatement (test oracle) of the AWFL Euler-3D ADER/WENO finite-volume step.
+ *
+ * TEST INFRASTRUCTURE ONLY -- see awfl_oracle.h. Every function names the reference
+ * lines it restates; arithmetic is written in the reference's evaluation order so that,
+ * compiled without FMA contraction against the same libm, results are bit-identical.
+ *
+ * Reference files (paths within mrnorman/awflCloud):
+ *   Spatial_euler3d_cons_expl_cart_fv_Agrid.h  ("Spatial" below)
+ *   WenoLimiter.h, TransformMatrices.h, Temporal_ader.h, Profiles.h, phys_params.h
+ */
+#define _GNU_SOURCE
+#include "awfl_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../awflcloud_b200/csrc/awfl_tables.h"
+
+#ifndef ORACLE_ORD
+#define ORACLE_ORD 5
+#endif
+#ifndef ORACLE_NGLL
+#define ORACLE_NGLL 3
+#endif
+
+#define ORD ORACLE_ORD
+#define NGLL ORACLE_NGLL
+#define NADER NGLL
+#define HS ((ORD - 1) / 2)
+#define NUMSTATE 5
+
+#if ORD == 5
+#define TBL(name) name##_o5
+#define TV_LO_N AWFL_TV_LO_O5_NTERM
+#define TV_HI_N AWFL_TV_HI_O5_NTERM
+#define TVS(part, name) awfl_tv_##part##_o5_##name
+#elif ORD == 9
+#define TBL(name) name##_o9
+#define TV_LO_N AWFL_TV_LO_O9_NTERM
+#define TV_HI_N AWFL_TV_HI_O9_NTERM
+#define TVS(part, name) awfl_tv_##part##_o9_##name
+#else
+#error "oracle supports ORD 5 (NGLL 3) and ORD 9 (NGLL 5)"
+#endif
+
+/* phys_params.h:4-10 */
+static const double GRAV = 9.81;
+static const double CP = 1004.;
+static const double RD = 287.;
+static const double P0 = 1.0e5;
+static const double C0 = 27.5629410929725921310572974482;
+static const double GAMMA = 1.40027894002789400278940027894;
+
+enum { idR = 0, idU = 1, idV = 2, idW = 3, idT = 4 };
+enum { BC_PERIODIC = 0, BC_WALL = 1 };
+enum { DATA_THERMAL = 1, DATA_COLLISION = 2, DATA_STRAKA = 3, DATA_IGW = 4 };
+
+struct oracle_ctx {
+  int nx, ny, nz;
+  double xlen, ylen, zlen, dx, dy, dz;
+  int bc[3];
+  int weno_scalars, weno_winds, sim2d, data_spec, dimswitch;
+  /* tables (Spatial:274-315) */
+  double recon[ORD][ORD][ORD];
+  double c2g[ORD][NGLL];   /* coefs_to_gll(col=s, row=ii) */
+  double s2g[ORD][NGLL];   /* sten_to_gll */
+  double deriv[NGLL][NGLL];
+  double idl[HS + 2];
+  double sigma;
+  double pts_ord[ORD], wts_ord[ORD], pts_ngll[NGLL], wts_ngll[NGLL];
+  /* hydrostatic background (Spatial:371-425) */
+  double *hyDensCells, *hyPressureCells, *hyThetaCells, *hyDensThetaCells; /* nz+2hs */
+  double *hyDensGLL, *hyPressureGLL, *hyThetaGLL, *hyDensThetaGLL;         /* nz*ngll */
+  /* scratch (Spatial:327-330) */
+  double *limits; /* (5,2,nz+1,ny+1,nx+1) */
+  double *flux;   /* (5,nz+1,ny+1,nx+1) */
+};
+
+/* ---------------------------------------------------------------- indexing */
+static inline long sidx(const oracle_ctx *c, int l, int k, int j, int i) {
+  return (((long)l * (c->nz + 2 * HS) + k) * (c->ny + 2 * HS) + j) * (c->nx + 2 * HS) + i;
+}
+static inline long tidx(const oracle_ctx *c, int l, int k, int j, int i) {
+  return (((long)l * c->nz + k) * c->ny + j) * c->nx + i;
+}
+static inline long lidx(const oracle_ctx *c, int l, int side, int k, int j, int i) {
+  return ((((long)l * 2 + side) * (c->nz + 1) + k) * (c->ny + 1) + j) * (c->nx + 1) + i;
+}
+static inline long fidx(const oracle_ctx *c, int l, int k, int j, int i) {
+  return (((long)l * (c->nz + 1) + k) * (c->ny + 1) + j) * (c->nx + 1) + i;
+}
+
+static inline double dmax(double a, double b) { return a > b ? a : b; }
+static inline double dmin(double a, double b) { return a < b ? a : b; }
+
+/* ---------------------------------------------------------------- WENO */
+/* TransformMatrices::coefs_to_tv: ordered quadratic form, c*(a*a) or (c*a_m)*a_q. */
+static double tv_eval(const double *a, int nterm, const int *m, const int *q, const double *cf) {
+  double r = 0;
+  for (int t = 0; t < nterm; t++) {
+    double term = (m[t] == q[t]) ? cf[t] * (a[q[t]] * a[q[t]]) : cf[t] * a[m[t]] * a[q[t]];
+    r = (t == 0) ? term : r + term;
+  }
+  return r;
+}
+static double tv_lo(const double *a) {
+  return tv_eval(a, TV_LO_N, TVS(lo, m), TVS(lo, q), TVS(lo, c));
+}
+static double tv_hi(const double *a) {
+  return tv_eval(a, TV_HI_N, TVS(hi, m), TVS(hi, q), TVS(hi, c));
+}
+
+/* WenoLimiter.h:20-25 */
+static void convexify(double *wts) {
+  double sum = 0.;
+  const double eps = 1.0e-20;
+  for (int i = 0; i < HS + 2; i++) sum += wts[i];
+  for (int i = 0; i < HS + 2; i++) wts[i] /= (sum + eps);
+}
+
+/* WenoLimiter.h:12-17 */
+static void map_weights(const double *idl, double *wts) {
+  for (int i = 0; i < HS + 2; i++) {
+    wts[i] = wts[i] * (idl[i] + idl[i] * idl[i] - 3. * idl[i] * wts[i] + wts[i] * wts[i]) /
+             (idl[i] * idl[i] + wts[i] * (1. - 2. * idl[i]));
+  }
+}
+
+/* WenoLimiter.h:28-90 (ord 5 and 9 rows) */
+static void weno_set_ideal_sigma(double *idl, double *sigma) {
+#if ORD == 5
+  *sigma = 0.73564225445964;
+  idl[0] = 1.; idl[1] = 73.564225445964; idl[2] = 1.; idl[3] = 1584.89319246111;
+#else
+  *sigma = 0.0288539981181442;
+  idl[0] = 1.; idl[1] = 2.15766927997459; idl[2] = 2.40224886796286;
+  idl[3] = 2.15766927997459; idl[4] = 1.; idl[5] = 1136.12697719888;
+#endif
+  convexify(idl);
+}
+
+/* WenoLimiter.h:93-172 */
+static void weno_coefs(const oracle_ctx *c, const double *u, double *aw) {
+  double tv[HS + 2], wts[HS + 2], a[HS + 2][ORD], lotmp[HS + 1], hitmp[ORD];
+  const double eps = 1.0e-20;
+  for (int j = 0; j < HS + 2; j++)
+    for (int i = 0; i < ORD; i++) a[j][i] = 0.;
+  for (int i = 0; i < HS + 1; i++)
+    for (int ii = 0; ii < HS + 1; ii++)
+      for (int s = 0; s < HS + 1; s++) a[i][ii] += c->recon[i][s][ii] * u[i + s];
+  for (int ii = 0; ii < ORD; ii++)
+    for (int s = 0; s < ORD; s++) a[HS + 1][ii] += c->recon[HS + 1][s][ii] * u[s];
+  for (int i = 0; i < HS + 1; i++)
+    for (int ii = 0; ii < HS + 1; ii++) a[HS + 1][ii] -= c->idl[i] * a[i][ii];
+  for (int ii = 0; ii < ORD; ii++) a[HS + 1][ii] /= c->idl[HS + 1];
+  for (int i = 0; i < HS + 1; i++) {
+    for (int ii = 0; ii < HS + 1; ii++) lotmp[ii] = a[i][ii];
+    tv[i] = tv_lo(lotmp);
+  }
+  for (int ii = 0; ii < ORD; ii++) hitmp[ii] = a[HS + 1][ii];
+  tv[HS + 1] = tv_hi(hitmp);
+  double lo_avg = 0.;
+  for (int i = 0; i < HS + 1; i++) lo_avg += tv[i];
+  lo_avg /= HS + 1;
+  tv[HS + 1] = lo_avg + (tv[HS + 1] - lo_avg) * c->sigma;
+  for (int i = 0; i < HS + 2; i++) wts[i] = c->idl[i] / (tv[i] * tv[i] + eps);
+  convexify(wts);
+  map_weights(c->idl, wts);
+  convexify(wts);
+  for (int i = 0; i < ORD; i++) aw[i] = 0.;
+  for (int i = 0; i < HS + 2; i++)
+    for (int ii = 0; ii < ORD; ii++) aw[ii] += wts[i] * a[i][ii];
+}
+
+/* Spatial:1800-1833 */
+static void reconstruct_gll(const oracle_ctx *c, const double *stencil, double *out, int doweno) {
+  if (doweno) {
+    double wc[ORD];
+    weno_coefs(c, stencil, wc);
+    for (int ii = 0; ii < NGLL; ii++) {
+      double tmp = 0;
+      for (int s = 0; s < ORD; s++) tmp += c->c2g[s][ii] * wc[s];
+      out[ii] = tmp;
+    }
+  } else {
+    for (int ii = 0; ii < NGLL; ii++) {
+      double tmp = 0;
+      for (int s = 0; s < ORD; s++) tmp += c->s2g[s][ii] * stencil[s];
+      out[ii] = tmp;
+    }
+  }
+}
+
+/* ---------------------------------------------------------------- ADER */
+/* Per-cell ADER arrays: q[v][kt][ii] for v = r, ru, rv, rw, rt; f[x][kt][ii] for the
+ * four normal-momentum flux products (normal*u, normal*v, normal*w, normal*t)/r, and the
+ * (rho*theta)^gamma series g. dir selects the normal momentum (1+dir). */
+typedef struct {
+  double q[NUMSTATE][NADER][NGLL];
+  double f[4][NADER][NGLL];
+  double g[NADER][NGLL];
+  double src[NADER][NGLL];
+} ader_t;
+
+/* diffTransformEulerConsX/Y/Z (Spatial:1837-1916, 1920-2000, 2004-2091). */
+static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, double dxd, int k) {
+  const int nm = 1 + dir; /* normal momentum index */
+  for (int kt = 1; kt < NADER; kt++)
+    for (int ii = 0; ii < NGLL; ii++) {
+      for (int x = 0; x < 4; x++) A->f[x][kt][ii] = 0;
+      A->g[kt][ii] = 0;
+    }
+  for (int kt = 0; kt < NADER - 1; kt++) {
+    for (int ii = 0; ii < NGLL; ii++) {
+      double dq[NUMSTATE] = {0, 0, 0, 0, 0};
+      for (int s = 0; s < NGLL; s++) {
+        double D = c->deriv[s][ii];
+        dq[idR] += D * (A->q[nm][kt][s]);
+        for (int v = 1; v <= 3; v++) {
+          if (v == nm) {
+            if (dir == 2 && kt == 0) {
+              dq[v] += D * (A->f[v - 1][kt][s] + C0 * A->g[kt][s] - c->hyPressureGLL[k * NGLL + s]);
+            } else if (kt == 0) {
+              dq[v] += D * (A->f[v - 1][kt][s] + C0 * A->g[kt][s]);
+            } else {
+              dq[v] += D * (A->f[v - 1][kt][s] + C0 * A->g[kt][s] / 2);
+            }
+          } else {
+            dq[v] += D * (A->f[v - 1][kt][s]);
+          }
+        }
+        dq[idT] += D * (A->f[3][kt][s]);
+      }
+      for (int v = 0; v < NUMSTATE; v++) A->q[v][kt + 1][ii] = -dq[v] / dxd / (kt + 1.);
+      if (dir == 2) {
+        A->q[idW][kt + 1][ii] = -dq[idW] / dxd / (kt + 1.) + A->src[kt][ii] / (kt + 1.);
+        if (c->bc[2] == BC_WALL) {
+          if (k == c->nz - 1) A->q[idW][kt + 1][NGLL - 1] = 0;
+          if (k == 0) A->q[idW][kt + 1][0] = 0;
+        }
+        A->src[kt + 1][ii] = -A->q[idR][kt + 1][ii] * GRAV;
+      }
+    }
+    for (int ii = 0; ii < NGLL; ii++) {
+      double tot[4] = {0, 0, 0, 0};
+      for (int ir = 0; ir <= kt + 1; ir++) {
+        for (int x = 0; x < 4; x++) {
+          int xv = x + 1; /* u->ru(1), v->rv(2), w->rw(3), t->rt(4) */
+          tot[x] += A->q[nm][ir][ii] * A->q[xv][kt + 1 - ir][ii] - A->q[idR][ir][ii] * A->f[x][kt + 1 - ir][ii];
+        }
+      }
+      for (int x = 0; x < 4; x++) A->f[x][kt + 1][ii] = tot[x] / A->q[idR][0][ii];
+      double tg = 0;
+      for (int ir = 0; ir <= kt; ir++) {
+        tg += (kt + 1. - ir) * (GAMMA * A->g[ir][ii] * A->q[idT][kt + 1 - ir][ii] -
+                                A->q[idT][ir][ii] * A->g[kt + 1 - ir][ii]);
+      }
+      A->g[kt + 1][ii] = (GAMMA * A->g[0][ii] * A->q[idT][kt + 1][ii] + tg / (kt + 1.)) / A->q[idT][0][ii];
+    }
+  }
+  for (int kt = 1; kt < NADER; kt++)
+    for (int ii = 0; ii < NGLL; ii++) A->g[kt][ii] /= 2;
+}
+
+/* compute_timeAvg_edges (Spatial:2153-2177): edge points only. */
+static void time_avg_edges(double dts[NADER][NGLL], double dt) {
+  double dtmult = dt;
+  for (int kt = 1; kt < NADER; kt++) {
+    dts[0][0] += dts[kt][0] * dtmult / (kt + 1.);
+    dts[0][NGLL - 1] += dts[kt][NGLL - 1] * dtmult / (kt + 1.);
+    dtmult *= dt;
+  }
+}
+
+/* compute_timeAvg (Spatial:2130-2138): all points. */
+static void time_avg_full(double dts[NADER][NGLL], double dt) {
+  double dtmult = dt;
+  for (int kt = 1; kt < NADER; kt++) {
+    for (int ii = 0; ii < NGLL; ii++) dts[0][ii] += dts[kt][ii] * dtmult / (kt + 1.);
+    dtmult *= dt;
+  }
+}
+
+/* ---------------------------------------------------------------- halos */
+/* Spatial:631-662 (x), 994-1025 (y), 1351-1382 (z). */
+static void fill_halos(const oracle_ctx *c, double *st, int dir) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  if (dir == 0) {
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int ii = 0; ii < HS; ii++)
+          for (int l = 0; l < NUMSTATE; l++) {
+            if (c->bc[0] == BC_PERIODIC) {
+              st[sidx(c, l, HS + k, HS + j, ii)] = st[sidx(c, l, HS + k, HS + j, nx + ii)];
+              st[sidx(c, l, HS + k, HS + j, HS + nx + ii)] = st[sidx(c, l, HS + k, HS + j, HS + ii)];
+            } else if (l == idU) {
+              st[sidx(c, l, HS + k, HS + j, ii)] = 0;
+              st[sidx(c, l, HS + k, HS + j, HS + nx + ii)] = 0;
+            } else {
+              st[sidx(c, l, HS + k, HS + j, ii)] = st[sidx(c, l, HS + k, HS + j, HS)];
+              st[sidx(c, l, HS + k, HS + j, HS + nx + ii)] = st[sidx(c, l, HS + k, HS + j, HS + nx - 1)];
+            }
+          }
+  } else if (dir == 1) {
+#pragma omp parallel for collapse(2)
+    for (int k = 0; k < nz; k++)
+      for (int i = 0; i < nx; i++)
+        for (int jj = 0; jj < HS; jj++)
+          for (int l = 0; l < NUMSTATE; l++) {
+            if (c->bc[1] == BC_PERIODIC) {
+              st[sidx(c, l, HS + k, jj, HS + i)] = st[sidx(c, l, HS + k, ny + jj, HS + i)];
+              st[sidx(c, l, HS + k, HS + ny + jj, HS + i)] = st[sidx(c, l, HS + k, HS + jj, HS + i)];
+            } else if (l == idV) {
+              st[sidx(c, l, HS + k, jj, HS + i)] = 0;
+              st[sidx(c, l, HS + k, HS + ny + jj, HS + i)] = 0;
+            } else {
+              st[sidx(c, l, HS + k, jj, HS + i)] = st[sidx(c, l, HS + k, HS, HS + i)];
+              st[sidx(c, l, HS + k, HS + ny + jj, HS + i)] = st[sidx(c, l, HS + k, HS + ny - 1, HS + i)];
+            }
+          }
+  } else {
+#pragma omp parallel for collapse(2)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        for (int kk = 0; kk < HS; kk++)
+          for (int l = 0; l < NUMSTATE; l++) {
+            if (c->bc[2] == BC_PERIODIC) {
+              st[sidx(c, l, kk, HS + j, HS + i)] = st[sidx(c, l, nz + kk, HS + j, HS + i)];
+              st[sidx(c, l, HS + nz + kk, HS + j, HS + i)] = st[sidx(c, l, HS + kk, HS + j, HS + i)];
+            } else if (l == idW) {
+              st[sidx(c, l, kk, HS + j, HS + i)] = 0;
+              st[sidx(c, l, HS + nz + kk, HS + j, HS + i)] = 0;
+            } else {
+              st[sidx(c, l, kk, HS + j, HS + i)] = st[sidx(c, l, HS, HS + j, HS + i)];
+              st[sidx(c, l, HS + nz + kk, HS + j, HS + i)] = st[sidx(c, l, HS + nz - 1, HS + j, HS + i)];
+            }
+          }
+  }
+}
+
+/* ---------------------------------------------------------------- tendencies */
+/* computeTendenciesX/Y/Z (Spatial:598-957, 961-1311, 1315-1697), one direction. */
+void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, double dt, int dir) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  const int nm = 1 + dir;
+  const double dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+  const int bc = c->bc[dir];
+
+  fill_halos(c, st, dir);
+
+  /* Reconstruct + ADER + time average; store cell-edge states (K2). */
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        ader_t A;
+        double stencil[ORD];
+        for (int v = 0; v < NUMSTATE; v++) {
+          for (int s = 0; s < ORD; s++) {
+            if (dir == 0) stencil[s] = st[sidx(c, v, HS + k, HS + j, i + s)];
+            else if (dir == 1) stencil[s] = st[sidx(c, v, HS + k, j + s, HS + i)];
+            else stencil[s] = st[sidx(c, v, k + s, HS + j, HS + i)];
+          }
+          int doweno = (v == idR || v == idT) ? c->weno_scalars : c->weno_winds;
+          reconstruct_gll(c, stencil, A.q[v][0], doweno);
+          if (v == idR) {
+            for (int ii = 0; ii < NGLL; ii++)
+              A.q[idR][0][ii] += (dir == 2) ? c->hyDensGLL[k * NGLL + ii] : c->hyDensCells[HS + k];
+          }
+          if (dir == 2 && v == idW && bc == BC_WALL) { /* Spatial:1413-1416 */
+            if (k == nz - 1) A.q[idW][0][NGLL - 1] = 0;
+            if (k == 0) A.q[idW][0][0] = 0;
+          }
+          if (v == idT) {
+            for (int ii = 0; ii < NGLL; ii++)
+              A.q[idT][0][ii] += (dir == 2) ? c->hyDensThetaGLL[k * NGLL + ii] : c->hyDensThetaCells[HS + k];
+          }
+        }
+        /* level-0 flux products (Spatial:704-715 and per-direction equivalents) */
+        double srcfill = 0;
+        for (int ii = 0; ii < NGLL; ii++) {
+          double r = A.q[idR][0][ii];
+          double u = A.q[idU][0][ii] / r;
+          double v = A.q[idV][0][ii] / r;
+          double w = A.q[idW][0][ii] / r;
+          double t = A.q[idT][0][ii] / r;
+          double vn = nm == 1 ? u : (nm == 2 ? v : w);
+          A.f[0][0][ii] = r * vn * u;
+          A.f[1][0][ii] = r * vn * v;
+          A.f[2][0][ii] = r * vn * w;
+          A.f[3][0][ii] = r * vn * t;
+          A.g[0][ii] = pow(r * t, GAMMA);
+          if (dir == 2) srcfill = -(A.q[idR][0][ii] - c->hyDensGLL[k * NGLL + ii]) * GRAV;
+        }
+        if (dir == 2) { /* SArray scalar assignment fills every entry (Spatial:1439) */
+          for (int kt = 0; kt < NADER; kt++)
+            for (int ii = 0; ii < NGLL; ii++) A.src[kt][ii] = srcfill;
+        }
+        if (NADER > 1) diff_transform(c, &A, dir, dxd, k);
+        for (int v = 0; v < NUMSTATE; v++) time_avg_edges(A.q[v], dt);
+        int kl = k, jl = j, il = i, kr = k, jr = j, ir = i;
+        if (dir == 0) ir = i + 1;
+        else if (dir == 1) jr = j + 1;
+        else kr = k + 1;
+        for (int v = 0; v < NUMSTATE; v++) {
+          c->limits[lidx(c, v, 1, kl, jl, il)] = A.q[v][0][0];
+          c->limits[lidx(c, v, 0, kr, jr, ir)] = A.q[v][0][NGLL - 1];
+        }
+        if (dir == 2) { /* gravity source (Spatial:1459-1499) */
+          time_avg_full(A.src, dt);
+          double src_avg = 0;
+          for (int ii = 0; ii < NGLL; ii++) src_avg += A.src[0][ii] * c->wts_ngll[ii];
+          tend[tidx(c, idR, k, j, i)] = 0;
+          tend[tidx(c, idU, k, j, i)] = 0;
+          tend[tidx(c, idV, k, j, i)] = 0;
+          tend[tidx(c, idW, k, j, i)] = src_avg;
+          tend[tidx(c, idT, k, j, i)] = 0;
+        }
+      }
+
+  /* Edge-value BCs (K3: Spatial:816-837, 1176-1197, 1557-1578). */
+  {
+    int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    int na = dir == 2 ? ny : nz;   /* outer */
+    int nb = dir == 0 ? ny : nx;   /* inner */
+    for (int a = 0; a < na; a++)
+      for (int b = 0; b < nb; b++)
+        for (int l = 0; l < NUMSTATE; l++) {
+          long i0, in, i0s1, ins0;
+#define LIM(side, f) (dir == 0 ? lidx(c, l, side, a, b, f) : (dir == 1 ? lidx(c, l, side, a, f, b) : lidx(c, l, side, f, a, b)))
+          i0 = LIM(0, 0); in = LIM(1, n); i0s1 = LIM(1, 0); ins0 = LIM(0, n);
+#undef LIM
+          if (bc == BC_PERIODIC) {
+            c->limits[i0] = c->limits[ins0];
+            c->limits[in] = c->limits[i0s1];
+          } else {
+            c->limits[i0] = c->limits[i0s1];
+            c->limits[in] = c->limits[ins0];
+          }
+        }
+  }
+
+  /* Upwind Riemann flux (K4: Spatial:842-902, 1202-1260, 1583-1644). */
+  {
+    int ek = nz + (dir == 2), ej = ny + (dir == 1), ei = nx + (dir == 0);
+#pragma omp parallel for collapse(3)
+    for (int k = 0; k < ek; k++)
+      for (int j = 0; j < ej; j++)
+        for (int i = 0; i < ei; i++) {
+          double qL[5], qR[5];
+          for (int l = 0; l < 5; l++) {
+            qL[l] = c->limits[lidx(c, l, 0, k, j, i)];
+            qR[l] = c->limits[lidx(c, l, 1, k, j, i)];
+          }
+          double r, vel[3], t;
+          r = 0.5 * (qL[0] + qR[0]);
+          if (dir == 1) { /* y: averages are NOT divided by density (Spatial:1210-1214) */
+            vel[0] = 0.5 * (qL[1] + qR[1]);
+            vel[1] = 0.5 * (qL[2] + qR[2]);
+            vel[2] = 0.5 * (qL[3] + qR[3]);
+            t = 0.5 * (qL[4] + qR[4]);
+          } else {
+            vel[0] = 0.5 * (qL[1] / qL[0] + qR[1] / qR[0]);
+            vel[1] = 0.5 * (qL[2] / qL[0] + qR[2] / qR[0]);
+            vel[2] = 0.5 * (qL[3] / qL[0] + qR[3] / qR[0]);
+            t = 0.5 * (qL[4] / qL[0] + qR[4] / qR[0]);
+          }
+          double p = C0 * pow(r * t, GAMMA);
+          double cs2 = GAMMA * p / r;
+          double cs = sqrt(cs2);
+          /* tangential indices in increasing order */
+          int ta = dir == 0 ? 1 : 0, tb = dir == 2 ? 1 : 2; /* velocity slots */
+          double vn = vel[dir], va = vel[ta], vb = vel[tb];
+          int qn = 1 + dir, qa = 1 + ta, qb = 1 + tb;
+          double w1, w2, w3;
+          if (vn > 0) {
+            w1 = qL[0] - qL[4] / t;
+            w2 = qL[qa] - va * qL[4] / t;
+            w3 = qL[qb] - vb * qL[4] / t;
+          } else {
+            w1 = qR[0] - qR[4] / t;
+            w2 = qR[qa] - va * qR[4] / t;
+            w3 = qR[qb] - vb * qR[4] / t;
+          }
+          double w5 = vn * qR[0] / (2 * cs) - qR[qn] / (2 * cs) + qR[4] / (2 * t);
+          double w6 = -vn * qL[0] / (2 * cs) + qL[qn] / (2 * cs) + qL[4] / (2 * t);
+          double q[5];
+          q[0] = w1 + w5 + w6;
+          q[qn] = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
+          q[qa] = w2 + va * w5 + va * w6;
+          q[qb] = w3 + vb * w5 + vb * w6;
+          q[4] = t * w5 + t * w6;
+          double F[5];
+          F[0] = q[qn];
+          F[qn] = q[qn] * q[qn] / q[0] + C0 * pow(q[4], GAMMA);
+          F[qa] = q[qn] * q[qa] / q[0];
+          F[qb] = q[qn] * q[qb] / q[0];
+          F[4] = q[qn] * q[4] / q[0];
+          if (dir == 2) {
+            if (k < nz) F[idW] -= c->hyPressureGLL[k * NGLL + 0];
+            if (k == nz) F[idW] -= c->hyPressureGLL[(nz - 1) * NGLL + NGLL - 1];
+          }
+          for (int l = 0; l < 5; l++) c->flux[fidx(c, l, k, j, i)] = F[l];
+        }
+  }
+
+  /* Flux divergence (K5: Spatial:940-956, 1298-1310, 1680-1696). */
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        for (int l = 0; l < NUMSTATE; l++) {
+          double fl = c->flux[fidx(c, l, k, j, i)];
+          double fr = dir == 0 ? c->flux[fidx(c, l, k, j, i + 1)]
+                    : (dir == 1 ? c->flux[fidx(c, l, k, j + 1, i)] : c->flux[fidx(c, l, k + 1, j, i)]);
+          long ti = tidx(c, l, k, j, i);
+          if (dir == 0) {
+            tend[ti] = (c->sim2d && l == idV) ? 0 : -(fr - fl) / dxd;
+          } else if (dir == 1) {
+            tend[ti] = -(fr - fl) / dxd;
+          } else {
+            if (c->sim2d && l == idV) tend[ti] = 0;
+            else tend[ti] += -(fr - fl) / dxd;
+          }
+        }
+}
+
+/* Spatial:565-594 */
+void oracle_compute_tendencies(oracle_ctx *c, double *st, double *tend, double dt, int split) {
+  int dir;
+  if (c->dimswitch) dir = split == 0 ? 0 : (split == 1 ? 1 : 2);
+  else dir = split == 0 ? 2 : (split == 1 ? 1 : 0);
+  if (dir == 1 && c->sim2d) {
+    long n = (long)NUMSTATE * c->nz * c->ny * c->nx;
+    for (long i = 0; i < n; i++) tend[i] = 0.;
+  } else {
+    oracle_compute_tendencies_dir(c, st, tend, dt, dir);
+  }
+  if (split == 2) c->dimswitch = !c->dimswitch;
+}
+
+/* Temporal_ader.h:63-65 */
+void oracle_apply(const oracle_ctx *c, double *st, const double *tend, double dt) {
+#pragma omp parallel for collapse(3)
+  for (int l = 0; l < NUMSTATE; l++)
+    for (int k = 0; k < c->nz; k++)
+      for (int j = 0; j < c->ny; j++)
+        for (int i = 0; i < c->nx; i++)
+          st[sidx(c, l, HS + k, HS + j, HS + i)] += dt * tend[tidx(c, l, k, j, i)];
+}
+
+/* Temporal_ader.h:48-72 */
+void oracle_time_step(oracle_ctx *c, double *st, double dt) {
+  long n = (long)NUMSTATE * c->nz * c->ny * c->nx;
+  double *tend = (double *)calloc((size_t)n, sizeof(double));
+  for (int spl = 0; spl < 3; spl++) {
+    oracle_compute_tendencies(c, st, tend, dt, spl);
+    oracle_apply(c, st, tend, dt);
+  }
+  free(tend);
+}
+
+int oracle_get_dimswitch(const oracle_ctx *c) { return c->dimswitch; }
+void oracle_set_dimswitch(oracle_ctx *c, int v) { c->dimswitch = v != 0; }
+
+/* ---------------------------------------------------------------- CFL */
+/* Spatial:159-187 */
+double oracle_compute_dt(const oracle_ctx *c, const double *st, double cfl) {
+  double best = INFINITY;
+  int first = 1;
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++) {
+        double r = st[sidx(c, idR, HS + k, HS + j, HS + i)] + c->hyDensCells[HS + k];
+        double u = st[sidx(c, idU, HS + k, HS + j, HS + i)] / r;
+        double v = st[sidx(c, idV, HS + k, HS + j, HS + i)] / r;
+        double w = st[sidx(c, idW, HS + k, HS + j, HS + i)] / r;
+        double t = (st[sidx(c, idT, HS + k, HS + j, HS + i)] + c->hyDensThetaCells[HS + k]) / r;
+        double p = C0 * pow(r * t, GAMMA);
+        double cs = sqrt(GAMMA * p / r);
+        double udt = cfl * c->dx / dmax(fabs(u - cs), fabs(u + cs));
+        double vdt = cfl * c->dy / dmax(fabs(v - cs), fabs(v + cs));
+        double wdt = cfl * c->dz / dmax(fabs(w - cs), fabs(w + cs));
+        double d = dmin(dmin(udt, vdt), wdt);
+        if (first || d < best) { best = d; first = 0; }
+      }
+  return best;
+}
+
+/* ---------------------------------------------------------------- profiles */
+/* Profiles.h:8-46 */
+static double const_theta_density(double t0, double z) {
+  double exner = 1. - GRAV * z / (CP * t0);
+  double p = pow(exner, CP / RD) * P0;
+  double rt = pow(p / C0, 1. / GAMMA);
+  return rt / t0;
+}
+static double const_theta_pressure(double t0, double z) {
+  double r = const_theta_density(t0, z);
+  return C0 * pow(r * t0, GAMMA);
+}
+static double bvf_pot_temp(double t0, double bvf, double z) { return t0 * exp(bvf * bvf * z / GRAV); }
+static double bvf_density(double t0, double bvf, double z) {
+  double t = bvf_pot_temp(t0, bvf, z);
+  double exner = 1. - GRAV * GRAV / (CP * bvf * bvf) * (t - t0) / (t * t0);
+  double p = pow(exner, CP / RD) * P0;
+  double rt = pow(p / C0, 1. / GAMMA);
+  return rt / t;
+}
+static double bvf_pressure(double t0, double bvf, double z) {
+  double t = bvf_pot_temp(t0, bvf, z);
+  double r = bvf_density(t0, bvf, z);
+  return C0 * pow(r * t, GAMMA);
+}
+/* Profiles.h:49-81 */
+static double ellipsoid_linear(double x, double y, double z, double x0, double y0, double z0,
+                               double xrad, double yrad, double zrad, double amp) {
+  double xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
+  double dist = sqrt(xn * xn + yn * yn + zn * zn);
+  return amp * dmax(1. - dist, 0.);
+}
+static double ellipsoid_cosine(double x, double y, double z, double x0, double y0, double z0,
+                               double xrad, double yrad, double zrad, double amp, double pwr) {
+  double val = 0;
+  double xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
+  double dist = sqrt(xn * xn + yn * yn + zn * zn);
+  if (dist <= 1.) val = amp * pow((cos(M_PI * dist) + 1) / 2, pwr);
+  return val;
+}
+static double igw_prof(double x, double y, double z, double x0, double y0, double hr, double zlen, double amp) {
+  double xn = (x - x0) / hr, yn = (y - y0) / hr;
+  return amp * sin(M_PI * z / zlen) / sqrt(1 + xn * xn + yn * yn);
+}
+
+/* Spatial:371-425 */
+static void init_background(oracle_ctx *c) {
+  const int nz = c->nz;
+  for (int k = 0; k < nz + 2 * HS; k++) {
+    c->hyDensCells[k] = 0; c->hyPressureCells[k] = 0; c->hyThetaCells[k] = 0; c->hyDensThetaCells[k] = 0;
+    for (int kk = 0; kk < ORD; kk++) {
+      double zloc = (k - HS + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+      double th, rh, ph;
+      if (c->data_spec == DATA_IGW) {
+        const double bvf = 0.01, t0 = 300;
+        th = bvf_pot_temp(t0, bvf, zloc); rh = bvf_density(t0, bvf, zloc); ph = bvf_pressure(t0, bvf, zloc);
+      } else {
+        th = 300; rh = const_theta_density(th, zloc); ph = const_theta_pressure(th, zloc);
+      }
+      double wt = c->wts_ord[kk];
+      c->hyDensCells[k] += rh * wt;
+      c->hyThetaCells[k] += th * wt;
+      c->hyDensThetaCells[k] += rh * th * wt;
+      c->hyPressureCells[k] += ph * wt;
+    }
+  }
+  for (int k = 0; k < nz; k++)
+    for (int kk = 0; kk < NGLL; kk++) {
+      double zloc = (k + 0.5) * c->dz + c->pts_ngll[kk] * c->dz;
+      double th, rh, ph;
+      if (c->data_spec == DATA_IGW) {
+        const double bvf = 0.01, t0 = 300;
+        th = bvf_pot_temp(t0, bvf, zloc); rh = bvf_density(t0, bvf, zloc); ph = bvf_pressure(t0, bvf, zloc);
+      } else {
+        th = 300; rh = const_theta_density(th, zloc); ph = const_theta_pressure(th, zloc);
+      }
+      c->hyDensGLL[k * NGLL + kk] = rh;
+      c->hyThetaGLL[k * NGLL + kk] = th;
+      c->hyDensThetaGLL[k * NGLL + kk] = rh * th;
+      c->hyPressureGLL[k * NGLL + kk] = ph;
+    }
+}
+
+/* Spatial:428-485 */
+void oracle_init_state(oracle_ctx *c, double *st) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        for (int l = 0; l < NUMSTATE; l++) st[sidx(c, l, HS + k, HS + j, HS + i)] = 0;
+        for (int kk = 0; kk < ORD; kk++)
+          for (int jj = 0; jj < ORD; jj++)
+            for (int ii = 0; ii < ORD; ii++) {
+              double zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+              double yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
+              double xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
+              double wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
+              long it = sidx(c, idT, HS + k, HS + j, HS + i);
+              if (c->data_spec == DATA_THERMAL) {
+                double th = 300, rh = const_theta_density(th, zloc);
+                double tp = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 2);
+                double t = th + tp;
+                st[it] += (rh * t - rh * th) * wt;
+              } else if (c->data_spec == DATA_COLLISION) {
+                double th = 300, rh = const_theta_density(th, zloc);
+                double tp = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 20);
+                tp += ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 8000, 2000, 2000, 2000, -20);
+                double t = th + tp;
+                st[it] += (rh * t - rh * th) * wt;
+              } else if (c->data_spec == DATA_STRAKA) {
+                double th = 300, rh = const_theta_density(th, zloc);
+                double tp = ellipsoid_cosine(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 3000, 4000, 2000, 2000, -15, 1);
+                double t = th + tp;
+                st[it] += (rh * t - rh * th) * wt;
+              } else if (c->data_spec == DATA_IGW) {
+                if (c->sim2d) yloc = c->ylen / 3;
+                const double t0 = 300, bvf = 0.01;
+                double rh = bvf_density(t0, bvf, zloc);
+                double th = bvf_pot_temp(t0, bvf, zloc);
+                double tp = igw_prof(xloc, yloc, zloc, c->xlen / 3, c->ylen / 3, 5000, c->zlen, 0.01);
+                double t = th + tp;
+                st[it] += (rh * t - rh * th) * wt;
+                st[sidx(c, idU, HS + k, HS + j, HS + i)] += 20 * rh * wt;
+                if (!c->sim2d) st[sidx(c, idV, HS + k, HS + j, HS + i)] += 20 * rh * wt;
+              }
+            }
+      }
+}
+
+void oracle_set_bubble(oracle_ctx *c, double *st, int shape, double x0, double y0, double z0,
+                       double xrad, double yrad, double zrad, double amp, double pwr) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        for (int l = 0; l < NUMSTATE; l++) st[sidx(c, l, HS + k, HS + j, HS + i)] = 0;
+        for (int kk = 0; kk < ORD; kk++)
+          for (int jj = 0; jj < ORD; jj++)
+            for (int ii = 0; ii < ORD; ii++) {
+              double zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+              double yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
+              double xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
+              double wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
+              double th = 300, rh = const_theta_density(th, zloc);
+              double tp = shape == 0 ? ellipsoid_linear(xloc, yloc, zloc, x0, y0, z0, xrad, yrad, zrad, amp)
+                                     : ellipsoid_cosine(xloc, yloc, zloc, x0, y0, z0, xrad, yrad, zrad, amp, pwr);
+              double t = th + tp;
+              st[sidx(c, idT, HS + k, HS + j, HS + i)] += (rh * t - rh * th) * wt;
+            }
+      }
+}
+
+static inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+void oracle_add_theta_noise(oracle_ctx *c, double *st, unsigned long long seed, double amp) {
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++) {
+        uint64_t idx = ((uint64_t)k * c->ny + j) * c->nx + i;
+        double u = (double)(splitmix64(seed * 0x100000001B3ULL + idx) >> 11) * (1.0 / 9007199254740992.0);
+        double n = (2.0 * u - 1.0) * amp;
+        st[sidx(c, idT, HS + k, HS + j, HS + i)] += c->hyDensCells[HS + k] * n;
+      }
+}
+
+/* ---------------------------------------------------------------- setup */
+/* matmul_cr: C(col,row) = sum_k A(k,row) * B(col,k), k ascending. */
+static void matmul_cr(const double *A, int K, int R, const double *B, int C, double *out) {
+  for (int cc = 0; cc < C; cc++)
+    for (int r = 0; r < R; r++) {
+      double tmp = 0;
+      for (int k = 0; k < K; k++) tmp += A[k * R + r] * B[cc * K + k];
+      out[cc * R + r] = tmp;
+    }
+}
+
+oracle_ctx *oracle_create(int nx, int ny, int nz, double xlen, double ylen, double zlen,
+                          int bc_x, int bc_y, int bc_z, int weno_scalars, int weno_winds,
+                          int data_spec) {
+  oracle_ctx *c = (oracle_ctx *)calloc(1, sizeof(oracle_ctx));
+  c->nx = nx; c->ny = ny; c->nz = nz;
+  c->xlen = xlen; c->ylen = ylen; c->zlen = zlen;
+  c->bc[0] = bc_x; c->bc[1] = bc_y; c->bc[2] = bc_z;
+  c->weno_scalars = weno_scalars; c->weno_winds = weno_winds;
+  c->sim2d = ny == 1;
+  c->data_spec = data_spec;
+  c->dimswitch = 1;
+  c->dx = xlen / nx; c->dy = ylen / ny; c->dz = zlen / nz;
+  /* Spatial:274-315 */
+  memcpy(c->recon, TBL(awfl_weno_recon), sizeof(c->recon));
+  memcpy(c->c2g, TBL(awfl_coefs_to_gll_lower), sizeof(c->c2g));
+  matmul_cr(TBL(awfl_coefs_to_gll_lower), ORD, NGLL, TBL(awfl_sten_to_coefs), ORD, &c->s2g[0][0]);
+  {
+    double tmp[NGLL * NGLL];
+#if ORD == 5
+    matmul_cr(awfl_coefs_to_deriv_n3_o5, NGLL, NGLL, awfl_gll_to_coefs_n3_o5, NGLL, tmp);
+    matmul_cr(awfl_coefs_to_gll_n3_o5, NGLL, NGLL, tmp, NGLL, &c->deriv[0][0]);
+#else
+    matmul_cr(awfl_coefs_to_deriv_n5_o9, NGLL, NGLL, awfl_gll_to_coefs_n5_o9, NGLL, tmp);
+    matmul_cr(awfl_coefs_to_gll_n5_o9, NGLL, NGLL, tmp, NGLL, &c->deriv[0][0]);
+#endif
+  }
+  memcpy(c->pts_ord, TBL(awfl_gll_pts_ord), sizeof(c->pts_ord));
+  memcpy(c->wts_ord, TBL(awfl_gll_wts_ord), sizeof(c->wts_ord));
+  memcpy(c->pts_ngll, TBL(awfl_gll_pts_ngll), sizeof(c->pts_ngll));
+  memcpy(c->wts_ngll, TBL(awfl_gll_wts_ngll), sizeof(c->wts_ngll));
+  weno_set_ideal_sigma(c->idl, &c->sigma);
+
+  int nzc = nz + 2 * HS;
+  c->hyDensCells = (double *)calloc(nzc, sizeof(double));
+  c->hyPressureCells = (double *)calloc(nzc, sizeof(double));
+  c->hyThetaCells = (double *)calloc(nzc, sizeof(double));
+  c->hyDensThetaCells = (double *)calloc(nzc, sizeof(double));
+  c->hyDensGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
+  c->hyPressureGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
+  c->hyThetaGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
+  c->hyDensThetaGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
+  c->limits = (double *)calloc((size_t)5 * 2 * (nz + 1) * (ny + 1) * (nx + 1), sizeof(double));
+  c->flux = (double *)calloc((size_t)5 * (nz + 1) * (ny + 1) * (nx + 1), sizeof(double));
+  init_background(c);
+  return c;
+}
+
+void oracle_destroy(oracle_ctx *c) {
+  if (!c) return;
+  free(c->hyDensCells); free(c->hyPressureCells); free(c->hyThetaCells); free(c->hyDensThetaCells);
+  free(c->hyDensGLL); free(c->hyPressureGLL); free(c->hyThetaGLL); free(c->hyDensThetaGLL);
+  free(c->limits); free(c->flux);
+  free(c);
+}
+
+int oracle_ord(void) { return ORD; }
+int oracle_ngll(void) { return NGLL; }
+int oracle_hs(void) { return HS; }
+long oracle_state_size(const oracle_ctx *c) {
+  return (long)NUMSTATE * (c->nz + 2 * HS) * (c->ny + 2 * HS) * (c->nx + 2 * HS);
+}
+
+void oracle_get_tables(const oracle_ctx *c, double *s2g, double *deriv, double *idl, double *sigma) {
+  memcpy(s2g, c->s2g, sizeof(c->s2g));
+  memcpy(deriv, c->deriv, sizeof(c->deriv));
+  memcpy(idl, c->idl, sizeof(c->idl));
+  *sigma = c->sigma;
+}
+
+void oracle_get_background(const oracle_ctx *c, double *dens_c, double *pres_c, double *theta_c,
+                           double *denstheta_c, double *dens_g, double *pres_g, double *theta_g,
+                           double *denstheta_g) {
+  int nzc = c->nz + 2 * HS;
+  memcpy(dens_c, c->hyDensCells, nzc * sizeof(double));
+  memcpy(pres_c, c->hyPressureCells, nzc * sizeof(double));
+  memcpy(theta_c, c->hyThetaCells, nzc * sizeof(double));
+  memcpy(denstheta_c, c->hyDensThetaCells, nzc * sizeof(double));
+  memcpy(dens_g, c->hyDensGLL, (size_t)c->nz * NGLL * sizeof(double));
+  memcpy(pres_g, c->hyPressureGLL, (size_t)c->nz * NGLL * sizeof(double));
+  memcpy(theta_g, c->hyThetaGLL, (size_t)c->nz * NGLL * sizeof(double));
+  memcpy(denstheta_g, c->hyDensThetaGLL, (size_t)c->nz * NGLL * sizeof(double));
+}
+
+double oracle_coefs_to_tv(const double *a, int n) {
+  if (n == HS + 1) return tv_lo(a);
+  return tv_hi(a);
+}
+
+void oracle_weno_coefs(const oracle_ctx *c, const double *stencil, double *coefs_out) {
+  weno_coefs(c, stencil, coefs_out);
+}

@@ -1,0 +1,122 @@
+"""Generate the golden fixtures in tests/golden/ by running the REFERENCE's own code.
+
+The reference (mrnorman/awflCloud) is C++ on the YAKL library, which is an absent
+submodule in its repository; ``oracle/Makefile`` builds its unmodified headers on
+project-written stand-ins for YAKL / yaml-cpp / netCDF into oracle/_ref/. This script
+drives that build through ``oracle.pyoracle.RefHarness`` and stores:
+
+* ``tables_o{5,9}.npz``  -- the constant tables the reference's init builds
+                            (Spatial_euler3d_cons_expl_cart_fv_Agrid.h:274-315);
+* ``probes_o{5,9}.npz``  -- coefs_to_tv and compute_weno_coefs on seeded inputs;
+* ``case_<name>.npz``    -- per configuration: background, initial state, CFL dt,
+                            tendencies of every split of steps 1-2, the state after
+                            each split of step 1 and after every step.
+
+Needs the reference sources (REF, default /root/reference) and g++ with OpenMP.
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle  # noqa: E402
+from oracle.pyoracle import RefHarness  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+SEED = 20261203
+
+# name: (ord, nx, ny, nz, bc, weno_scalars, weno_winds, data, bubble, noise, nsteps)
+BUBBLE_COS = (1, 10000.0, 10000.0, 2000.0, 2000.0, 2000.0, 2000.0, 3.0, 1.0)
+CASES = {
+    "o5_pw_thermal":     (5, 10, 8, 6, (0, 0, 1), True, True, "thermal", None, 0.01, 4),
+    "o5_walls":          (5, 10, 8, 6, (1, 1, 1), True, True, "thermal", None, 0.01, 3),
+    "o5_periodic":       (5, 10, 8, 6, (0, 0, 0), True, True, "thermal", None, 0.01, 3),
+    "o5_linear":         (5, 10, 8, 6, (0, 0, 1), False, False, "thermal", None, 0.01, 3),
+    "o5_mixedweno":      (5, 10, 8, 6, (0, 1, 1), False, True, "thermal", None, 0.01, 3),
+    "o5_sim2d":          (5, 12, 1, 8, (0, 0, 1), True, True, "thermal", None, 0.01, 3),
+    "o5_bubble_cos":     (5, 12, 12, 8, (0, 0, 1), True, True, "thermal", BUBBLE_COS, 0.01, 2),
+    "o5_igw":            (5, 10, 8, 6, (0, 0, 1), True, True, "igw", None, None, 2),
+    "o5_collision":      (5, 10, 8, 6, (0, 0, 1), True, True, "collision", None, None, 1),
+    "o5_straka":         (5, 10, 8, 6, (0, 0, 1), True, True, "straka", None, None, 1),
+    "o9_pw_thermal":     (9, 10, 8, 6, (0, 0, 1), True, True, "thermal", None, 0.01, 3),
+    "o9_walls_mixed":    (9, 10, 8, 6, (1, 1, 1), True, False, "thermal", None, 0.01, 2),
+}
+
+
+def make_case(name, spec):
+    ord_, nx, ny, nz, bc, ws, ww, data, bubble, noise, nsteps = spec
+    R = RefHarness(nx, ny, nz, bc=bc, weno_scalars=ws, weno_winds=ww, data=data, ord_=ord_)
+    R.init_state()
+    if bubble is not None:
+        R.set_bubble(*bubble)
+    if noise is not None:
+        R.add_theta_noise(SEED, noise)
+    out = {"config": np.array([ord_, nx, ny, nz, bc[0], bc[1], bc[2], int(ws), int(ww)]),
+           "data": np.array(data), "state0": R.get_state()}
+    if bubble is not None:
+        out["bubble"] = np.array(bubble, dtype=np.float64)
+    if noise is not None:
+        out["noise"] = np.array([SEED, noise], dtype=np.float64)
+    for k, v in R.background().items():
+        out[k] = v
+    dt = R.compute_dt(0.8)
+    out["dt"] = np.array(dt)
+    h = R.hs
+    for step in range(nsteps):
+        if step < 2:
+            for spl in range(3):
+                tend = R.compute_tendencies(dt, spl)
+                st = R.get_state()  # halos were filled in place
+                st[:, h:h + nz, h:h + ny, h:h + nx] += dt * tend
+                R.set_state(st)
+                out["tend_s%d_p%d" % (step, spl)] = tend
+                if step == 0:
+                    out["state_s0_p%d" % spl] = st
+        else:
+            R.time_step(dt)
+        out["state_s%d" % step] = R.get_state()
+    path = os.path.join(OUT, "case_%s.npz" % name)
+    np.savez_compressed(path, **out)
+    return path
+
+
+def make_tables(ord_):
+    R = RefHarness(10, 8, 6, ord_=ord_)
+    np.savez_compressed(os.path.join(OUT, "tables_o%d.npz" % ord_), **R.tables())
+
+
+def make_probes(ord_):
+    R = RefHarness(10, 8, 6, ord_=ord_)
+    rng = np.random.default_rng(SEED + ord_)
+    hs = (ord_ - 1) // 2
+    tv_lo_in = rng.standard_normal((64, hs + 1)) * 10.0 ** rng.integers(-6, 3, (64, 1))
+    tv_hi_in = rng.standard_normal((64, ord_)) * 10.0 ** rng.integers(-6, 3, (64, 1))
+    tv_lo = np.array([R.coefs_to_tv(a) for a in tv_lo_in])
+    tv_hi = np.array([R.coefs_to_tv(a) for a in tv_hi_in])
+    x = np.arange(ord_) - hs
+    sten = [np.zeros(ord_), np.ones(ord_), 1.0 + 0.1 * x, 0.3 * x ** 2 - x, (x > 0).astype(float),
+            np.where(x >= 1, 5.0, -2.0), 1e-9 * np.cos(x)]
+    sten += list(rng.standard_normal((57, ord_)) * 10.0 ** rng.integers(-8, 2, (57, 1)))
+    sten = np.array(sten)
+    weno = np.array([R.weno_coefs(s) for s in sten])
+    np.savez_compressed(os.path.join(OUT, "probes_o%d.npz" % ord_), tv_lo_in=tv_lo_in,
+                        tv_lo=tv_lo, tv_hi_in=tv_hi_in, tv_hi=tv_hi, weno_in=sten, weno=weno)
+
+
+def main():
+    pyoracle.build(ref=True)
+    for o in (5, 9):
+        make_tables(o)
+        make_probes(o)
+    for name, spec in CASES.items():
+        print("wrote", make_case(name, spec))
+
+
+if __name__ == "__main__":
+    main()
