@@ -1,0 +1,85 @@
+"""Build libawfl.so (the C-ABI library of include/awfl.h) for sm_100a with nvcc.
+
+Translation units and their numerics flags:
+  awfl_capi.cu  host code: -ffp-contract=off (init-time tables/background bit-identical
+                to the reference CPU build)
+  awfl_fp64.cu  FP64 kernels: --fmad=false (no contracted multiply-add, like the
+                reference CPU build)
+  awfl_fp32.cu  FP32 precision form (when present): contraction allowed
+
+The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
+source tree. ``python -m awflcloud_b200.build [--force]``.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SRC = os.path.join(HERE, "csrc")
+ROOT = os.path.dirname(HERE)
+LIBDIR = os.path.join(HERE, "lib")
+OBJDIR = os.path.join(HERE, "_build")
+LIB = os.path.join(LIBDIR, "libawfl.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
+          "-I" + SRC, "-I" + os.path.join(ROOT, "include")]
+UNITS = {
+    "awfl_capi.cu": ["--fmad=false"],
+    "awfl_fp64.cu": ["--fmad=false"],
+    "awfl_fp32.cu": ["--fmad=true"],
+}
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _deps(unit: str):
+    hdrs = [os.path.join(SRC, f) for f in os.listdir(SRC) if f.endswith((".h", ".cuh"))]
+    hdrs.append(os.path.join(ROOT, "include", "awfl.h"))
+    return [os.path.join(SRC, unit)] + hdrs
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = []
+    rebuilt = False
+    for unit, flags in UNITS.items():
+        src = os.path.join(SRC, unit)
+        if not os.path.exists(src):
+            continue
+        obj = os.path.join(OBJDIR, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _stale(obj, _deps(unit)):
+            cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
+            if ptxas_info:
+                cmd += ["-Xptxas", "-v"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
+            rebuilt = True
+    if rebuilt or force or _stale(LIB, objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_info="-v" in sys.argv)

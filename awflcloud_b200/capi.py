@@ -1,0 +1,231 @@
+"""ctypes bindings of the C ABI (include/awfl.h) and a thin context wrapper.
+
+The CUDA library libawfl.so is REQUIRED: importing this module on a machine without it
+raises. There is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libawfl.so")
+
+AWFL_OK = 0
+STATUS = {0: "AWFL_OK", -1: "AWFL_ERR_ARG", -2: "AWFL_ERR_CUDA", -3: "AWFL_ERR_NOMEM",
+          -4: "AWFL_ERR_STATE", -5: "AWFL_ERR_TIMEOUT", -6: "AWFL_ERR_NOT_BUILT"}
+BC = {"periodic": 0, "wall": 1}
+DATA = {"thermal": 1, "collision": 2, "straka": 3, "igw": 4}
+FP64, FP32 = 0, 1
+INIT_REFERENCE, INIT_BUBBLE = 0, 1
+
+
+class AwflConfig(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("xlen", ctypes.c_double), ("ylen", ctypes.c_double), ("zlen", ctypes.c_double),
+                ("bc_x", ctypes.c_int), ("bc_y", ctypes.c_int), ("bc_z", ctypes.c_int),
+                ("weno_scalars", ctypes.c_int), ("weno_winds", ctypes.c_int),
+                ("data_spec", ctypes.c_int), ("ord", ctypes.c_int), ("precision", ctypes.c_int)]
+
+
+class AwflInitSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("shape", ctypes.c_int),
+                ("x0", ctypes.c_double), ("y0", ctypes.c_double), ("z0", ctypes.c_double),
+                ("xrad", ctypes.c_double), ("yrad", ctypes.c_double), ("zrad", ctypes.c_double),
+                ("amp", ctypes.c_double), ("pwr", ctypes.c_double),
+                ("noise_amp", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong)]
+
+
+class AwflError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (STATUS.get(code, "?"), code, msg))
+        self.code = code
+
+
+_VP, _I, _D, _L = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
+_DP = ctypes.POINTER(ctypes.c_double)
+_SIGS = {
+    "awfl_create": (_I, [ctypes.POINTER(AwflConfig), _I, ctypes.POINTER(_VP)]),
+    "awfl_destroy": (_I, [_VP]),
+    "awfl_last_error": (ctypes.c_char_p, [_VP]),
+    "awfl_version": (ctypes.c_char_p, []),
+    "awfl_sizes": (_I, [_VP, ctypes.POINTER(_L), ctypes.POINTER(_L), ctypes.POINTER(_I)]),
+    "awfl_init_state": (_I, [_VP, _VP, ctypes.POINTER(AwflInitSpec), _VP]),
+    "awfl_cfl": (_I, [_VP, _VP, _D, _DP, _VP]),
+    "awfl_compute_tendencies": (_I, [_VP, _VP, _VP, _D, _I, _VP]),
+    "awfl_apply_tendencies": (_I, [_VP, _VP, _VP, _D, _VP]),
+    "awfl_split": (_I, [_VP, _VP, _D, _I, _VP]),
+    "awfl_step": (_I, [_VP, _VP, _D, _VP]),
+    "awfl_get_dimswitch": (_I, [_VP, ctypes.POINTER(_I)]),
+    "awfl_set_dimswitch": (_I, [_VP, _I]),
+    "awfl_get_tables": (_I, [_VP] + [_DP] * 10),
+    "awfl_get_background": (_I, [_VP] + [_DP] * 8),
+    "awfl_selftest_pow": (_I, [_VP, _D, _VP, _L, _I, _VP]),
+    "awfl_device_alloc": (_I, [ctypes.POINTER(_VP), _L]),
+    "awfl_device_free": (_I, [_VP]),
+    "awfl_copy_h2d": (_I, [_VP, _VP, _L, _VP]),
+    "awfl_copy_d2h": (_I, [_VP, _VP, _L, _VP]),
+    "awfl_memset_device": (_I, [_VP, _I, _L, _VP]),
+    "awfl_stream_synchronize": (_I, [_VP]),
+    "awfl_device_synchronize": (_I, []),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libawfl.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(LIB_PATH + " is missing: build it with python -m awflcloud_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(x):
+    """Device or host address of a torch tensor / numpy array / int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return x.ctypes.data
+
+
+def _stream(s):
+    if s is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except Exception:
+            pass
+        return None
+    return s if isinstance(s, int) else s.cuda_stream
+
+
+class Context:
+    """An awfl_ctx: one grid configuration on one device (device < 0: host-only)."""
+
+    def __init__(self, nx, ny, nz, xlen=20000.0, ylen=20000.0, zlen=10000.0,
+                 bc=("periodic", "periodic", "wall"), weno_scalars=True, weno_winds=True,
+                 data="thermal", ord_=5, precision=FP64, device=0):
+        self.L = lib()
+        bcv = [BC[b] if isinstance(b, str) else int(b) for b in bc]
+        self.cfg = AwflConfig(nx, ny, nz, xlen, ylen, zlen, bcv[0], bcv[1], bcv[2],
+                              int(weno_scalars), int(weno_winds),
+                              DATA[data] if isinstance(data, str) else int(data), ord_, precision)
+        h = _VP()
+        rc = self.L.awfl_create(ctypes.byref(self.cfg), device, ctypes.byref(h))
+        if rc != AWFL_OK:
+            raise AwflError(rc, self.L.awfl_last_error(None).decode())
+        self.h = h
+        self.ord = ord_
+        self.ngll = 3 if ord_ == 5 else 5
+        self.hs = (ord_ - 1) // 2
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.precision = precision
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.awfl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != AWFL_OK:
+            raise AwflError(rc, self.L.awfl_last_error(self.h).decode())
+
+    # ---- shapes
+    @property
+    def state_shape(self):
+        h = 2 * self.hs
+        return (5, self.nz + h, self.ny + h, self.nx + h)
+
+    @property
+    def tend_shape(self):
+        return (5, self.nz, self.ny, self.nx)
+
+    def new_state(self, **kw):
+        import torch
+        dt = torch.float64 if self.precision == FP64 else torch.float32
+        return torch.zeros(self.state_shape, dtype=dt, device="cuda:%d" % max(self.device, 0), **kw)
+
+    def new_tend(self):
+        import torch
+        dt = torch.float64 if self.precision == FP64 else torch.float32
+        return torch.zeros(self.tend_shape, dtype=dt, device="cuda:%d" % max(self.device, 0))
+
+    # ---- entry points
+    def init_state(self, state, kind=INIT_REFERENCE, shape=1, x0=10000.0, y0=10000.0, z0=2000.0,
+                   xrad=2000.0, yrad=2000.0, zrad=2000.0, amp=3.0, pwr=1.0, noise_amp=0.0,
+                   noise_seed=20261203, stream=None):
+        spec = AwflInitSpec(kind, shape, x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp, noise_seed)
+        self._check(self.L.awfl_init_state(self.h, _ptr(state), ctypes.byref(spec), _stream(stream)))
+
+    def cfl(self, state, cfl=0.8, stream=None):
+        out = ctypes.c_double()
+        self._check(self.L.awfl_cfl(self.h, _ptr(state), cfl, ctypes.byref(out), _stream(stream)))
+        return out.value
+
+    def compute_tendencies(self, state, tend, dt, d, stream=None):
+        self._check(self.L.awfl_compute_tendencies(self.h, _ptr(state), _ptr(tend), dt, d, _stream(stream)))
+
+    def apply_tendencies(self, state, tend, dt, stream=None):
+        self._check(self.L.awfl_apply_tendencies(self.h, _ptr(state), _ptr(tend), dt, _stream(stream)))
+
+    def split(self, state, dt, d, stream=None):
+        self._check(self.L.awfl_split(self.h, _ptr(state), dt, d, _stream(stream)))
+
+    def step(self, state, dt, stream=None):
+        self._check(self.L.awfl_step(self.h, _ptr(state), dt, _stream(stream)))
+
+    @property
+    def dimswitch(self):
+        v = _I()
+        self._check(self.L.awfl_get_dimswitch(self.h, ctypes.byref(v)))
+        return v.value
+
+    @dimswitch.setter
+    def dimswitch(self, value):
+        self._check(self.L.awfl_set_dimswitch(self.h, int(value)))
+
+    def tables(self):
+        import numpy as np
+        o, g, hs = self.ord, self.ngll, self.hs
+        arrs = [np.zeros(o ** 3), np.zeros(o * g), np.zeros(o * g), np.zeros(g * g), np.zeros(hs + 2),
+                np.zeros(1), np.zeros(o), np.zeros(o), np.zeros(g), np.zeros(g)]
+        self._check(self.L.awfl_get_tables(self.h, *[a.ctypes.data_as(_DP) for a in arrs]))
+        names = ["weno_recon", "coefs_to_gll", "sten_to_gll", "deriv", "idl", "sigma",
+                 "gll_pts_ord", "gll_wts_ord", "gll_pts_ngll", "gll_wts_ngll"]
+        return dict(zip(names, arrs))
+
+    def background(self):
+        import numpy as np
+        nzc = self.nz + 2 * self.hs
+        arrs = [np.zeros(nzc) for _ in range(4)] + [np.zeros(self.nz * self.ngll) for _ in range(4)]
+        self._check(self.L.awfl_get_background(self.h, *[a.ctypes.data_as(_DP) for a in arrs]))
+        names = ["hyDensCells", "hyPressureCells", "hyThetaCells", "hyDensThetaCells",
+                 "hyDensGLL", "hyPressureGLL", "hyThetaGLL", "hyDensThetaGLL"]
+        return dict(zip(names, arrs))
+
+
+def header_symbols(path=None):
+    """Function names declared in include/awfl.h."""
+    import re
+    path = path or os.path.join(os.path.dirname(HERE), "include", "awfl.h")
+    src = open(path).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*|void)\s*\*?\s*(awfl_\w+)\s*\(", src, re.M)))

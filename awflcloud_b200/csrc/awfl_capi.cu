@@ -1,0 +1,530 @@
+// C ABI (include/awfl.h) of the AWFL Euler-3D ADER/WENO step: context, tables, background,
+// argument checking, launches. Host code here is compiled with -ffp-contract=off so the
+// init-time tables and background are bit-identical to the reference's CPU arithmetic.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/awfl.h"
+#include "awfl_internal.h"
+#include "awfl_tables.h"
+
+using namespace awfl;
+
+#define AWFL_VERSION_STRING "awflcloud_b200 0.1.0 (sm_100a)"
+
+struct awfl_ctx {
+  awfl_config cfg;
+  int device = 0;
+  int hs = 0, ngll = 0, sim2d = 0, dimswitch = 1, nsm = 148;
+  double dx = 0, dy = 0, dz = 0;
+  // tables (Spatial:274-315)
+  std::vector<double> recon, c2g, s2g, deriv, idl, pts_ord, wts_ord, pts_ngll, wts_ngll;
+  double sigma = 0;
+  // hydrostatic background (Spatial:371-425)
+  std::vector<double> dens_c, pres_c, theta_c, denstheta_c, dens_g, pres_g, theta_g, denstheta_g;
+  double *d_bg = nullptr;  // device: dens_c | denstheta_c | dens_g | denstheta_g | pres_g
+  double *d_dens_c = nullptr, *d_denstheta_c = nullptr, *d_dens_g = nullptr, *d_denstheta_g = nullptr,
+         *d_pres_g = nullptr;
+  unsigned long long *d_cfl = nullptr;  // CFL reduction result (8 bytes)
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(awfl_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  else g_create_error = buf;
+  return code;
+}
+
+int cuda_fail(awfl_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, AWFL_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// phys_params.h:4-10
+const double kGRAV = 9.81, kCP = 1004., kRD = 287., kP0 = 1.0e5;
+const double kC0 = 27.5629410929725921310572974482;
+const double kGAMMA = 1.40027894002789400278940027894;
+
+// Profiles.h:8-46
+double const_theta_density(double t0, double z) {
+  double exner = 1. - kGRAV * z / (kCP * t0);
+  double p = pow(exner, kCP / kRD) * kP0;
+  double rt = pow(p / kC0, 1. / kGAMMA);
+  return rt / t0;
+}
+double const_theta_pressure(double t0, double z) {
+  double r = const_theta_density(t0, z);
+  return kC0 * pow(r * t0, kGAMMA);
+}
+double bvf_pot_temp(double t0, double bvf, double z) { return t0 * exp(bvf * bvf * z / kGRAV); }
+double bvf_density(double t0, double bvf, double z) {
+  double t = bvf_pot_temp(t0, bvf, z);
+  double exner = 1. - kGRAV * kGRAV / (kCP * bvf * bvf) * (t - t0) / (t * t0);
+  double p = pow(exner, kCP / kRD) * kP0;
+  double rt = pow(p / kC0, 1. / kGAMMA);
+  return rt / t;
+}
+double bvf_pressure(double t0, double bvf, double z) {
+  double t = bvf_pot_temp(t0, bvf, z);
+  double r = bvf_density(t0, bvf, z);
+  return kC0 * pow(r * t, kGAMMA);
+}
+
+// YAKL matmul_cr on (col,row) storage: out(c,r) = sum_k A(k,r)*B(c,k), k ascending.
+void matmul_cr(const double *A, int K, int R, const double *B, int C, double *out) {
+  for (int cc = 0; cc < C; cc++)
+    for (int r = 0; r < R; r++) {
+      double tmp = 0;
+      for (int k = 0; k < K; k++) tmp += A[k * R + r] * B[cc * K + k];
+      out[cc * R + r] = tmp;
+    }
+}
+
+// WenoLimiter.h:20-25, 28-90
+void convexify(double *w, int n) {
+  double sum = 0.;
+  const double eps = 1.0e-20;
+  for (int i = 0; i < n; i++) sum += w[i];
+  for (int i = 0; i < n; i++) w[i] /= (sum + eps);
+}
+void ideal_sigma(int ord, double *idl, double *sigma) {
+  if (ord == 5) {
+    *sigma = 0.73564225445964;
+    idl[0] = 1.; idl[1] = 73.564225445964; idl[2] = 1.; idl[3] = 1584.89319246111;
+  } else {
+    *sigma = 0.0288539981181442;
+    idl[0] = 1.; idl[1] = 2.15766927997459; idl[2] = 2.40224886796286;
+    idl[3] = 2.15766927997459; idl[4] = 1.; idl[5] = 1136.12697719888;
+  }
+  convexify(idl, (ord - 1) / 2 + 2);
+}
+
+void build_tables(awfl_ctx *c) {
+  const int o = c->cfg.ord, g = c->ngll, hs = c->hs;
+  const double *rec, *s2c, *c2gl, *g2c, *c2d, *c2gn, *po, *wo, *pn, *wn;
+  if (o == 5) {
+    rec = awfl_weno_recon_o5; s2c = awfl_sten_to_coefs_o5; c2gl = awfl_coefs_to_gll_lower_o5;
+    g2c = awfl_gll_to_coefs_n3_o5; c2d = awfl_coefs_to_deriv_n3_o5; c2gn = awfl_coefs_to_gll_n3_o5;
+    po = awfl_gll_pts_ord_o5; wo = awfl_gll_wts_ord_o5; pn = awfl_gll_pts_ngll_o5; wn = awfl_gll_wts_ngll_o5;
+  } else {
+    rec = awfl_weno_recon_o9; s2c = awfl_sten_to_coefs_o9; c2gl = awfl_coefs_to_gll_lower_o9;
+    g2c = awfl_gll_to_coefs_n5_o9; c2d = awfl_coefs_to_deriv_n5_o9; c2gn = awfl_coefs_to_gll_n5_o9;
+    po = awfl_gll_pts_ord_o9; wo = awfl_gll_wts_ord_o9; pn = awfl_gll_pts_ngll_o9; wn = awfl_gll_wts_ngll_o9;
+  }
+  c->recon.assign(rec, rec + o * o * o);
+  c->c2g.assign(c2gl, c2gl + o * g);
+  c->s2g.assign(o * g, 0.0);
+  matmul_cr(c2gl, o, g, s2c, o, c->s2g.data());  // sten_to_gll = matmul_cr(c2g_lower, s2c)
+  std::vector<double> tmp(g * g);
+  c->deriv.assign(g * g, 0.0);
+  matmul_cr(c2d, g, g, g2c, g, tmp.data());        // derivMatrix = matmul_cr(c2g, matmul_cr(c2d, g2c))
+  matmul_cr(c2gn, g, g, tmp.data(), g, c->deriv.data());
+  c->idl.assign(hs + 2, 0.0);
+  ideal_sigma(o, c->idl.data(), &c->sigma);
+  c->pts_ord.assign(po, po + o); c->wts_ord.assign(wo, wo + o);
+  c->pts_ngll.assign(pn, pn + g); c->wts_ngll.assign(wn, wn + g);
+}
+
+// Spatial:371-425 (hydrostatic background)
+void build_background(awfl_ctx *c) {
+  const int nz = c->cfg.nz, hs = c->hs, o = c->cfg.ord, g = c->ngll;
+  const bool igw = c->cfg.data_spec == AWFL_DATA_IGW;
+  c->dens_c.assign(nz + 2 * hs, 0.0); c->pres_c.assign(nz + 2 * hs, 0.0);
+  c->theta_c.assign(nz + 2 * hs, 0.0); c->denstheta_c.assign(nz + 2 * hs, 0.0);
+  for (int k = 0; k < nz + 2 * hs; k++) {
+    for (int kk = 0; kk < o; kk++) {
+      double zloc = (k - hs + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+      double th, rh, ph;
+      if (igw) {
+        const double bvf = 0.01, t0 = 300;
+        th = bvf_pot_temp(t0, bvf, zloc); rh = bvf_density(t0, bvf, zloc); ph = bvf_pressure(t0, bvf, zloc);
+      } else {
+        th = 300; rh = const_theta_density(th, zloc); ph = const_theta_pressure(th, zloc);
+      }
+      double wt = c->wts_ord[kk];
+      c->dens_c[k] += rh * wt;
+      c->theta_c[k] += th * wt;
+      c->denstheta_c[k] += rh * th * wt;
+      c->pres_c[k] += ph * wt;
+    }
+  }
+  c->dens_g.assign(nz * g, 0.0); c->pres_g.assign(nz * g, 0.0);
+  c->theta_g.assign(nz * g, 0.0); c->denstheta_g.assign(nz * g, 0.0);
+  for (int k = 0; k < nz; k++)
+    for (int kk = 0; kk < g; kk++) {
+      double zloc = (k + 0.5) * c->dz + c->pts_ngll[kk] * c->dz;
+      double th, rh, ph;
+      if (igw) {
+        const double bvf = 0.01, t0 = 300;
+        th = bvf_pot_temp(t0, bvf, zloc); rh = bvf_density(t0, bvf, zloc); ph = bvf_pressure(t0, bvf, zloc);
+      } else {
+        th = 300; rh = const_theta_density(th, zloc); ph = const_theta_pressure(th, zloc);
+      }
+      c->dens_g[k * g + kk] = rh;
+      c->theta_g[k * g + kk] = th;
+      c->denstheta_g[k * g + kk] = rh * th;
+      c->pres_g[k * g + kk] = ph;
+    }
+}
+
+std::mutex g_tab_mutex;
+unsigned g_tab_uploaded[256];  // per device: bit 0 = ord 5, bit 1 = ord 9
+
+int ensure_tables(awfl_ctx *c) {
+  std::lock_guard<std::mutex> lock(g_tab_mutex);
+  const int bit = c->cfg.ord == 5 ? 1 : 2;
+  if (c->device >= 0 && c->device < 256 && (g_tab_uploaded[c->device] & bit)) return AWFL_OK;
+  cudaError_t e;
+  if (c->cfg.ord == 5) {
+    Tables<5> t;
+    std::memcpy(t.recon, c->recon.data(), sizeof t.recon);
+    std::memcpy(t.c2g, c->c2g.data(), sizeof t.c2g);
+    std::memcpy(t.s2g, c->s2g.data(), sizeof t.s2g);
+    std::memcpy(t.deriv, c->deriv.data(), sizeof t.deriv);
+    std::memcpy(t.idl, c->idl.data(), sizeof t.idl);
+    t.sigma = c->sigma;
+    std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
+    e = upload_tables_fp64(5, &t, sizeof t);
+  } else {
+    Tables<9> t;
+    std::memcpy(t.recon, c->recon.data(), sizeof t.recon);
+    std::memcpy(t.c2g, c->c2g.data(), sizeof t.c2g);
+    std::memcpy(t.s2g, c->s2g.data(), sizeof t.s2g);
+    std::memcpy(t.deriv, c->deriv.data(), sizeof t.deriv);
+    std::memcpy(t.idl, c->idl.data(), sizeof t.idl);
+    t.sigma = c->sigma;
+    std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
+    e = upload_tables_fp64(9, &t, sizeof t);
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload of transform tables");
+  if (c->device >= 0 && c->device < 256) g_tab_uploaded[c->device] |= bit;
+  return AWFL_OK;
+}
+
+int set_device(awfl_ctx *c) {
+  if (c->device < 0) return fail(c, AWFL_ERR_ARG, "host-only context (created with device < 0) cannot run device work");
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGetDevice");
+  if (cur != c->device) {
+    e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+  }
+  return AWFL_OK;
+}
+
+SweepArgs sweep_args(awfl_ctx *c, void *state, void *tend, double dt, int dir, int mode) {
+  SweepArgs A;
+  A.state = (double *)state;
+  A.tend = (double *)tend;
+  A.nx = c->cfg.nx; A.ny = c->cfg.ny; A.nz = c->cfg.nz;
+  A.bc = dir == 0 ? c->cfg.bc_x : (dir == 1 ? c->cfg.bc_y : c->cfg.bc_z);
+  A.weno_s = c->cfg.weno_scalars; A.weno_w = c->cfg.weno_winds; A.sim2d = c->sim2d; A.mode = mode;
+  A.dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+  A.dt = dt;
+  A.dens_c = c->d_dens_c; A.denstheta_c = c->d_denstheta_c;
+  A.dens_g = c->d_dens_g; A.denstheta_g = c->d_denstheta_g; A.pres_g = c->d_pres_g;
+  return A;
+}
+
+bool bad_ptr(const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 7) != 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char *awfl_version(void) { return AWFL_VERSION_STRING; }
+
+const char *awfl_last_error(const awfl_ctx *ctx) {
+  if (!ctx) return g_create_error.c_str();
+  return ctx->err.c_str();
+}
+
+int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
+  if (!cfg || !out) return fail(nullptr, AWFL_ERR_ARG, "awfl_create: NULL argument");
+  *out = nullptr;
+  if (cfg->ord != 5 && cfg->ord != 9) return fail(nullptr, AWFL_ERR_ARG, "ord must be 5 or 9 (got %d)", cfg->ord);
+  if (cfg->precision != AWFL_FP64)
+    return fail(nullptr, AWFL_ERR_NOT_BUILT, "precision %d is not available in this build", cfg->precision);
+  const int hs = (cfg->ord - 1) / 2;
+  if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(nullptr, AWFL_ERR_ARG, "nx, ny, nz must be >= 1");
+  if (!(cfg->xlen > 0) || !(cfg->ylen > 0) || !(cfg->zlen > 0))
+    return fail(nullptr, AWFL_ERR_ARG, "xlen, ylen, zlen must be > 0");
+  const int bcs[3] = {cfg->bc_x, cfg->bc_y, cfg->bc_z};
+  const int ns[3] = {cfg->nx, cfg->ny, cfg->nz};
+  const char *nm[3] = {"x", "y", "z"};
+  for (int d = 0; d < 3; d++) {
+    if (bcs[d] != AWFL_BC_PERIODIC && bcs[d] != AWFL_BC_WALL)
+      return fail(nullptr, AWFL_ERR_ARG, "bc_%s must be periodic (0) or wall (1)", nm[d]);
+    const bool swept = !(d == 1 && cfg->ny == 1);
+    if (swept && bcs[d] == AWFL_BC_PERIODIC && ns[d] < hs)
+      return fail(nullptr, AWFL_ERR_ARG, "periodic n%s = %d is smaller than the halo width %d", nm[d], ns[d], hs);
+  }
+  if (cfg->data_spec < AWFL_DATA_THERMAL || cfg->data_spec > AWFL_DATA_IGW)
+    return fail(nullptr, AWFL_ERR_ARG, "data_spec must be 1..4");
+  long long cells = (long long)(cfg->nx + 2 * hs) * (cfg->ny + 2 * hs) * (cfg->nz + 2 * hs);
+  if (cells * 5 > (1LL << 40)) return fail(nullptr, AWFL_ERR_ARG, "grid too large");
+
+  awfl_ctx *c = new (std::nothrow) awfl_ctx();
+  if (!c) return fail(nullptr, AWFL_ERR_NOMEM, "host allocation failed");
+  c->cfg = *cfg;
+  c->device = device;
+  c->hs = hs;
+  c->ngll = cfg->ord == 5 ? 3 : 5;
+  c->sim2d = cfg->ny == 1;
+  c->dx = cfg->xlen / cfg->nx;
+  c->dy = cfg->ylen / cfg->ny;
+  c->dz = cfg->zlen / cfg->nz;
+  build_tables(c);
+  build_background(c);
+  if (device < 0) {  // host-only context: tables and background, no device resources
+    *out = c;
+    return AWFL_OK;
+  }
+
+  int rc = set_device(c);
+  if (rc) { g_create_error = c->err; delete c; return rc; }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->nsm = prop.multiProcessorCount;
+  rc = ensure_tables(c);
+  if (rc) { g_create_error = c->err; delete c; return rc; }
+  const int nz = cfg->nz, g = c->ngll;
+  const size_t nbg = (size_t)2 * (nz + 2 * hs) + (size_t)3 * nz * g;
+  cudaError_t e = cudaMalloc(&c->d_bg, nbg * sizeof(double) + 64);
+  if (e != cudaSuccess) { fail(nullptr, AWFL_ERR_NOMEM, "cudaMalloc background: %s", cudaGetErrorString(e)); delete c; return AWFL_ERR_NOMEM; }
+  c->d_dens_c = c->d_bg;
+  c->d_denstheta_c = c->d_dens_c + (nz + 2 * hs);
+  c->d_dens_g = c->d_denstheta_c + (nz + 2 * hs);
+  c->d_denstheta_g = c->d_dens_g + nz * g;
+  c->d_pres_g = c->d_denstheta_g + nz * g;
+  c->d_cfl = reinterpret_cast<unsigned long long *>(c->d_pres_g + nz * g);
+  std::vector<double> h;
+  h.reserve(nbg);
+  h.insert(h.end(), c->dens_c.begin(), c->dens_c.end());
+  h.insert(h.end(), c->denstheta_c.begin(), c->denstheta_c.end());
+  h.insert(h.end(), c->dens_g.begin(), c->dens_g.end());
+  h.insert(h.end(), c->denstheta_g.begin(), c->denstheta_g.end());
+  h.insert(h.end(), c->pres_g.begin(), c->pres_g.end());
+  e = cudaMemcpy(c->d_bg, h.data(), nbg * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cuda_fail(nullptr, e, "upload background"); g_create_error = "upload background: " + std::string(cudaGetErrorString(e)); cudaFree(c->d_bg); delete c; return AWFL_ERR_CUDA; }
+  *out = c;
+  return AWFL_OK;
+}
+
+int awfl_destroy(awfl_ctx *c) {
+  if (!c) return AWFL_OK;
+  if (c->d_bg && c->device >= 0) {
+    set_device(c);
+    cudaFree(c->d_bg);
+  }
+  delete c;
+  return AWFL_OK;
+}
+
+int awfl_sizes(const awfl_ctx *c, long *state_elems, long *tend_elems, int *hs) {
+  if (!c) return AWFL_ERR_ARG;
+  const int h = c->hs;
+  if (state_elems) *state_elems = 5L * (c->cfg.nz + 2 * h) * (c->cfg.ny + 2 * h) * (c->cfg.nx + 2 * h);
+  if (tend_elems) *tend_elems = 5L * c->cfg.nz * c->cfg.ny * c->cfg.nx;
+  if (hs) *hs = h;
+  return AWFL_OK;
+}
+
+int awfl_get_dimswitch(const awfl_ctx *c, int *value) {
+  if (!c || !value) return AWFL_ERR_ARG;
+  *value = c->dimswitch;
+  return AWFL_OK;
+}
+
+int awfl_set_dimswitch(awfl_ctx *c, int value) {
+  if (!c) return AWFL_ERR_ARG;
+  c->dimswitch = value != 0;
+  return AWFL_OK;
+}
+
+int awfl_init_state(awfl_ctx *c, void *d_state, const awfl_init_spec *spec, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_init_state: state pointer is NULL or misaligned");
+  if (spec && spec->kind != AWFL_INIT_REFERENCE && spec->kind != AWFL_INIT_BUBBLE)
+    return fail(c, AWFL_ERR_ARG, "awfl_init_state: unknown kind %d", spec->kind);
+  if (spec && spec->kind == AWFL_INIT_BUBBLE && c->cfg.data_spec == AWFL_DATA_IGW)
+    return fail(c, AWFL_ERR_ARG, "awfl_init_state: bubble initial data needs a constant-theta background");
+  int rc = set_device(c);
+  if (rc) return rc;
+  InitLaunch L;
+  std::memset(&L, 0, sizeof L);
+  L.state = d_state;
+  L.nx = c->cfg.nx; L.ny = c->cfg.ny; L.nz = c->cfg.nz; L.hs = c->hs; L.ord = c->cfg.ord;
+  L.dx = c->dx; L.dy = c->dy; L.dz = c->dz; L.xlen = c->cfg.xlen; L.ylen = c->cfg.ylen; L.zlen = c->cfg.zlen;
+  L.data_spec = c->cfg.data_spec; L.sim2d = c->sim2d;
+  if (spec) {
+    L.kind = spec->kind; L.shape = spec->shape;
+    L.x0 = spec->x0; L.y0 = spec->y0; L.z0 = spec->z0; L.xrad = spec->xrad; L.yrad = spec->yrad; L.zrad = spec->zrad;
+    L.amp = spec->amp; L.pwr = spec->pwr; L.noise_amp = spec->noise_amp; L.seed = spec->noise_seed;
+  }
+  L.dens_c = c->d_dens_c;
+  for (int m = 0; m < c->cfg.ord; m++) { L.pts[m] = c->pts_ord[m]; L.wts[m] = c->wts_ord[m]; }
+  cudaError_t e = launch_init_state_fp64(L, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "init_state kernel");
+  return AWFL_OK;
+}
+
+int awfl_cfl(awfl_ctx *c, const void *d_state, double cfl, double *h_dt, void *stream) {
+  if (!c || !h_dt) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_cfl: state pointer is NULL or misaligned");
+  if (!(cfl > 0)) return fail(c, AWFL_ERR_ARG, "awfl_cfl: cfl must be > 0");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  static const unsigned long long inf_bits = 0x7ff0000000000000ULL;
+  cudaError_t e = cudaMemcpyAsync(c->d_cfl, &inf_bits, sizeof inf_bits, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_cfl init");
+  e = launch_cfl_fp64((const double *)d_state, c->d_dens_c, c->d_denstheta_c, cfl, c->dx, c->dy, c->dz, c->cfg.nx,
+                      c->cfg.ny, c->cfg.nz, c->hs, c->nsm, c->d_cfl, st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cfl kernel");
+  unsigned long long bits = 0;
+  e = cudaMemcpyAsync(&bits, c->d_cfl, sizeof bits, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_cfl readback");
+  double dt;
+  std::memcpy(&dt, &bits, sizeof dt);
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(c, AWFL_ERR_STATE, "awfl_cfl: non-finite or non-positive time step (%g)", dt);
+  *h_dt = dt;
+  return AWFL_OK;
+}
+
+int awfl_compute_tendencies(awfl_ctx *c, void *d_state, void *d_tend, double dt, int dir, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
+  if (bad_ptr(d_state) || bad_ptr(d_tend)) return fail(c, AWFL_ERR_ARG, "state/tend pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e;
+  if (dir == 1 && c->sim2d) {  // Spatial:573-576: the Y tendency is zero in 2-D
+    e = cudaMemsetAsync(d_tend, 0, sizeof(double) * 5L * c->cfg.nz * c->cfg.ny * c->cfg.nx, st);
+  } else {
+    e = launch_sweep_fp64(c->cfg.ord, dir, sweep_args(c, d_state, d_tend, dt, dir, MODE_TEND), st);
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "compute_tendencies");
+  return AWFL_OK;
+}
+
+int awfl_apply_tendencies(awfl_ctx *c, void *d_state, const void *d_tend, double dt, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state) || bad_ptr(d_tend)) return fail(c, AWFL_ERR_ARG, "state/tend pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaError_t e = launch_apply_fp64((double *)d_state, (const double *)d_tend, dt, c->cfg.nx, c->cfg.ny, c->cfg.nz,
+                                    c->hs, c->nsm, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "apply_tendencies");
+  return AWFL_OK;
+}
+
+int awfl_split(awfl_ctx *c, void *d_state, double dt, int dir, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "state pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendency: the state is unchanged
+  cudaError_t e = launch_sweep_fp64(c->cfg.ord, dir, sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY),
+                                    (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "split");
+  return AWFL_OK;
+}
+
+int awfl_step(awfl_ctx *c, void *d_state, double dt, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  for (int spl = 0; spl < 3; spl++) {
+    const int dir = c->dimswitch ? spl : 2 - spl;
+    int rc = awfl_split(c, d_state, dt, dir, stream);
+    if (rc) return rc;
+  }
+  c->dimswitch = !c->dimswitch;
+  return AWFL_OK;
+}
+
+int awfl_get_tables(const awfl_ctx *c, double *weno_recon, double *coefs_to_gll, double *sten_to_gll, double *deriv,
+                    double *idl, double *sigma, double *gll_pts_ord, double *gll_wts_ord, double *gll_pts_ngll,
+                    double *gll_wts_ngll) {
+  if (!c) return AWFL_ERR_ARG;
+  auto cp = [](double *dst, const std::vector<double> &v) {
+    if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+  };
+  cp(weno_recon, c->recon); cp(coefs_to_gll, c->c2g); cp(sten_to_gll, c->s2g); cp(deriv, c->deriv);
+  cp(idl, c->idl);
+  if (sigma) *sigma = c->sigma;
+  cp(gll_pts_ord, c->pts_ord); cp(gll_wts_ord, c->wts_ord); cp(gll_pts_ngll, c->pts_ngll); cp(gll_wts_ngll, c->wts_ngll);
+  return AWFL_OK;
+}
+
+int awfl_get_background(const awfl_ctx *c, double *dens_c, double *pres_c, double *theta_c, double *denstheta_c,
+                        double *dens_g, double *pres_g, double *theta_g, double *denstheta_g) {
+  if (!c) return AWFL_ERR_ARG;
+  auto cp = [](double *dst, const std::vector<double> &v) {
+    if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+  };
+  cp(dens_c, c->dens_c); cp(pres_c, c->pres_c); cp(theta_c, c->theta_c); cp(denstheta_c, c->denstheta_c);
+  cp(dens_g, c->dens_g); cp(pres_g, c->pres_g); cp(theta_g, c->theta_g); cp(denstheta_g, c->denstheta_g);
+  return AWFL_OK;
+}
+
+int awfl_selftest_pow(const void *d_x, double y, void *d_out, long n, int mode, void *stream) {
+  if (n < 0 || mode < 0 || mode > 2 || (n > 0 && (bad_ptr(d_x) || bad_ptr(d_out)))) return AWFL_ERR_ARG;
+  cudaError_t e = launch_selftest_pow((const double *)d_x, y, (double *)d_out, n, mode, (cudaStream_t)stream);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+
+int awfl_device_alloc(void **d_ptr, long bytes) {
+  if (!d_ptr || bytes < 0) return AWFL_ERR_ARG;
+  cudaError_t e = cudaMalloc(d_ptr, bytes > 0 ? (size_t)bytes : 1);
+  if (e != cudaSuccess) { g_create_error = cudaGetErrorString(e); return AWFL_ERR_NOMEM; }
+  return AWFL_OK;
+}
+int awfl_device_free(void *d_ptr) {
+  cudaError_t e = cudaFree(d_ptr);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+int awfl_copy_h2d(void *d_dst, const void *h_src, long bytes, void *stream) {
+  if (bytes < 0) return AWFL_ERR_ARG;
+  cudaError_t e = cudaMemcpyAsync(d_dst, h_src, (size_t)bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+int awfl_copy_d2h(void *h_dst, const void *d_src, long bytes, void *stream) {
+  if (bytes < 0) return AWFL_ERR_ARG;
+  cudaError_t e = cudaMemcpyAsync(h_dst, d_src, (size_t)bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+int awfl_memset_device(void *d_ptr, int value, long bytes, void *stream) {
+  if (bytes < 0) return AWFL_ERR_ARG;
+  cudaError_t e = cudaMemsetAsync(d_ptr, value, (size_t)bytes, (cudaStream_t)stream);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+int awfl_stream_synchronize(void *stream) {
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+int awfl_device_synchronize(void) {
+  cudaError_t e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,341 @@
+// Device building blocks of the AWFL Euler-3D ADER/WENO step (FP64 parity path).
+//
+// Every function reproduces the arithmetic of the reference (mrnorman/awflCloud) in its
+// evaluation order; the file:line cited is the reference code restated:
+//   Spatial  = Spatial_euler3d_cons_expl_cart_fv_Agrid.h
+//   Weno     = WenoLimiter.h
+// The translation unit that includes this header is compiled with --fmad=false so that
+// no multiply-add is contracted, like the reference's CPU build, and every pow is the
+// correctly rounded pow_cr (awfl_pow.cuh), like glibc's.
+#pragma once
+
+#include <cstdint>
+
+#include "awfl_internal.h"
+#include "awfl_pow.cuh"
+#include "awfl_tv.h"
+
+namespace awfl {
+
+// Definitions: this header is included by exactly one translation unit (awfl_fp64.cu).
+__constant__ Tables<5> c_tab5;
+__constant__ Tables<9> c_tab9;
+
+template <int ORD> __device__ __forceinline__ const Tables<ORD> &tab();
+template <> __device__ __forceinline__ const Tables<5> &tab<5>() { return c_tab5; }
+template <> __device__ __forceinline__ const Tables<9> &tab<9>() { return c_tab9; }
+
+template <int N> __device__ __forceinline__ double tv_eval(const double *a);
+template <> __device__ __forceinline__ double tv_eval<3>(const double *a) { return awfl_tv_n3<double>(a); }
+template <> __device__ __forceinline__ double tv_eval<5>(const double *a) { return awfl_tv_n5<double>(a); }
+template <> __device__ __forceinline__ double tv_eval<9>(const double *a) { return awfl_tv_n9<double>(a); }
+
+// Weno:93-172 -- WENO polynomial coefficients of one ord-cell stencil.
+template <int ORD>
+__device__ __forceinline__ void weno_coefs(const double (&u)[ORD], double (&aw)[ORD]) {
+  constexpr int HS = (ORD - 1) / 2;
+  const Tables<ORD> &T = tab<ORD>();
+  const double eps = 1.0e-20;
+  double a[HS + 2][ORD];
+#pragma unroll
+  for (int j = 0; j < HS + 2; j++)
+#pragma unroll
+    for (int i = 0; i < ORD; i++) a[j][i] = 0.;
+#pragma unroll
+  for (int i = 0; i < HS + 1; i++)
+#pragma unroll
+    for (int ii = 0; ii < HS + 1; ii++)
+#pragma unroll
+      for (int s = 0; s < HS + 1; s++) a[i][ii] += T.recon[(i * ORD + s) * ORD + ii] * u[i + s];
+#pragma unroll
+  for (int ii = 0; ii < ORD; ii++)
+#pragma unroll
+    for (int s = 0; s < ORD; s++) a[HS + 1][ii] += T.recon[((HS + 1) * ORD + s) * ORD + ii] * u[s];
+#pragma unroll
+  for (int i = 0; i < HS + 1; i++)
+#pragma unroll
+    for (int ii = 0; ii < HS + 1; ii++) a[HS + 1][ii] -= T.idl[i] * a[i][ii];
+#pragma unroll
+  for (int ii = 0; ii < ORD; ii++) a[HS + 1][ii] /= T.idl[HS + 1];
+  double tv[HS + 2];
+#pragma unroll
+  for (int i = 0; i < HS + 1; i++) tv[i] = tv_eval<HS + 1>(a[i]);
+  tv[HS + 1] = tv_eval<ORD>(a[HS + 1]);
+  double lo_avg = 0.;
+#pragma unroll
+  for (int i = 0; i < HS + 1; i++) lo_avg += tv[i];
+  lo_avg /= HS + 1;
+  tv[HS + 1] = lo_avg + (tv[HS + 1] - lo_avg) * T.sigma;
+  double wts[HS + 2];
+#pragma unroll
+  for (int i = 0; i < HS + 2; i++) wts[i] = T.idl[i] / (tv[i] * tv[i] + eps);
+  // convexify (Weno:20-25)
+  {
+    double sum = 0.;
+#pragma unroll
+    for (int i = 0; i < HS + 2; i++) sum += wts[i];
+#pragma unroll
+    for (int i = 0; i < HS + 2; i++) wts[i] /= (sum + eps);
+  }
+  // map_weights (Weno:12-17)
+#pragma unroll
+  for (int i = 0; i < HS + 2; i++) {
+    const double d = T.idl[i];
+    wts[i] = wts[i] * (d + d * d - 3. * d * wts[i] + wts[i] * wts[i]) / (d * d + wts[i] * (1. - 2. * d));
+  }
+  {
+    double sum = 0.;
+#pragma unroll
+    for (int i = 0; i < HS + 2; i++) sum += wts[i];
+#pragma unroll
+    for (int i = 0; i < HS + 2; i++) wts[i] /= (sum + eps);
+  }
+#pragma unroll
+  for (int i = 0; i < ORD; i++) aw[i] = 0.;
+#pragma unroll
+  for (int i = 0; i < HS + 2; i++)
+#pragma unroll
+    for (int ii = 0; ii < ORD; ii++) aw[ii] += wts[i] * a[i][ii];
+}
+
+// Spatial:1800-1833 -- ord stencil averages -> ngll GLL point values.
+template <int ORD>
+__device__ __forceinline__ void reconstruct_gll(const double (&sten)[ORD],
+                                                double (&out)[OrdTraits<ORD>::NGLL], bool doweno) {
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  const Tables<ORD> &T = tab<ORD>();
+  if (doweno) {
+    double wc[ORD];
+    weno_coefs<ORD>(sten, wc);
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      double tmp = 0;
+#pragma unroll
+      for (int s = 0; s < ORD; s++) tmp += T.c2g[s * NG + ii] * wc[s];
+      out[ii] = tmp;
+    }
+  } else {
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      double tmp = 0;
+#pragma unroll
+      for (int s = 0; s < ORD; s++) tmp += T.s2g[s * NG + ii] * sten[s];
+      out[ii] = tmp;
+    }
+  }
+}
+
+// Reconstruction + ADER differential transform + edge time average of one cell
+// (the K2 kernels: Spatial:665-811 x, 1028-1171 y, 1385-1552 z; diffTransformEulerConsX/Y/Z
+// at Spatial:1837-2091; compute_timeAvg[_edges] at Spatial:2130-2177).
+// sten(v, s) returns stencil value s of variable v. kb is the k index of the cell (z) or of
+// the line (x, y). Outputs: the time-averaged left/right edge states and, for z, the
+// time-averaged, GLL-weighted gravity source.
+template <int ORD, int DIR, class Sten>
+__device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const SweepArgs &A,
+                                           double (&eL)[5], double (&eR)[5], double &src_avg) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int NA = NG;  // nAder = ngll (Temporal_ader.h:8)
+  constexpr int NM = 1 + DIR;  // normal momentum
+  const Tables<ORD> &T = tab<ORD>();
+
+  double q[5][NA][NG];
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    double s[ORD];
+#pragma unroll
+    for (int m = 0; m < ORD; m++) s[m] = sten(v, m);
+    const bool doweno = (v == idR || v == idT) ? A.weno_s : A.weno_w;
+    reconstruct_gll<ORD>(s, q[v][0], doweno);
+  }
+  // add hydrostasis back on (x/y: cell averages, Spatial:680,697; z: GLL values, :1400,:1421)
+#pragma unroll
+  for (int ii = 0; ii < NG; ii++) {
+    if (DIR == 2) {
+      q[idR][0][ii] += A.dens_g[kb * NG + ii];
+      q[idT][0][ii] += A.denstheta_g[kb * NG + ii];
+    } else {
+      q[idR][0][ii] += A.dens_c[HS + kb];
+      q[idT][0][ii] += A.denstheta_c[HS + kb];
+    }
+  }
+  if (DIR == 2 && A.bc == BC_WALL) {  // Spatial:1413-1416
+    if (kb == A.nz - 1) q[idW][0][NG - 1] = 0;
+    if (kb == 0) q[idW][0][0] = 0;
+  }
+  // level-0 flux products (Spatial:704-715 and y/z equivalents)
+  double f[4][NA][NG];
+  double g[NA][NG];
+  double srcfill = 0;
+#pragma unroll
+  for (int ii = 0; ii < NG; ii++) {
+    const double r = q[idR][0][ii];
+    const double u = q[idU][0][ii] / r;
+    const double v = q[idV][0][ii] / r;
+    const double w = q[idW][0][ii] / r;
+    const double t = q[idT][0][ii] / r;
+    const double vn = NM == 1 ? u : (NM == 2 ? v : w);
+    f[0][0][ii] = r * vn * u;
+    f[1][0][ii] = r * vn * v;
+    f[2][0][ii] = r * vn * w;
+    f[3][0][ii] = r * vn * t;
+    g[0][ii] = pow_cr(r * t, GAMMA);
+    if (DIR == 2) srcfill = -(q[idR][0][ii] - A.dens_g[kb * NG + ii]) * GRAV;
+  }
+  // The z source SArray is filled by a scalar assignment inside the kk loop, so every entry
+  // holds the kk = ngll-1 value (Spatial:1439).
+  double sr[NA][NG];
+#pragma unroll
+  for (int kt = 0; kt < NA; kt++)
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) sr[kt][ii] = srcfill;
+
+  // diffTransformEulerCons{X,Y,Z}
+#pragma unroll
+  for (int kt = 1; kt < NA; kt++)
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      f[0][kt][ii] = 0; f[1][kt][ii] = 0; f[2][kt][ii] = 0; f[3][kt][ii] = 0;
+      g[kt][ii] = 0;
+    }
+#pragma unroll
+  for (int kt = 0; kt < NA - 1; kt++) {
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      double dq[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+      for (int s = 0; s < NG; s++) {
+        const double D = T.deriv[s * NG + ii];
+        dq[idR] += D * (q[NM][kt][s]);
+#pragma unroll
+        for (int m = 1; m <= 3; m++) {
+          if (m == NM) {
+            if (DIR == 2 && kt == 0) {
+              dq[m] += D * (f[m - 1][kt][s] + C0 * g[kt][s] - A.pres_g[kb * NG + s]);
+            } else if (kt == 0) {
+              dq[m] += D * (f[m - 1][kt][s] + C0 * g[kt][s]);
+            } else {
+              dq[m] += D * (f[m - 1][kt][s] + C0 * g[kt][s] / 2);
+            }
+          } else {
+            dq[m] += D * (f[m - 1][kt][s]);
+          }
+        }
+        dq[idT] += D * (f[3][kt][s]);
+      }
+#pragma unroll
+      for (int m = 0; m < 5; m++) q[m][kt + 1][ii] = -dq[m] / A.dxd / (kt + 1.);
+      if (DIR == 2) {
+        q[idW][kt + 1][ii] = -dq[idW] / A.dxd / (kt + 1.) + sr[kt][ii] / (kt + 1.);
+        if (A.bc == BC_WALL) {
+          if (kb == A.nz - 1) q[idW][kt + 1][NG - 1] = 0;
+          if (kb == 0) q[idW][kt + 1][0] = 0;
+        }
+        sr[kt + 1][ii] = -q[idR][kt + 1][ii] * GRAV;
+      }
+    }
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      double tot[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int ir = 0; ir <= kt + 1; ir++) {
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+          tot[x] += q[NM][ir][ii] * q[x + 1][kt + 1 - ir][ii] - q[idR][ir][ii] * f[x][kt + 1 - ir][ii];
+      }
+#pragma unroll
+      for (int x = 0; x < 4; x++) f[x][kt + 1][ii] = tot[x] / q[idR][0][ii];
+      double tg = 0;
+#pragma unroll
+      for (int ir = 0; ir <= kt; ir++)
+        tg += (kt + 1. - ir) * (GAMMA * g[ir][ii] * q[idT][kt + 1 - ir][ii] - q[idT][ir][ii] * g[kt + 1 - ir][ii]);
+      g[kt + 1][ii] = (GAMMA * g[0][ii] * q[idT][kt + 1][ii] + tg / (kt + 1.)) / q[idT][0][ii];
+    }
+  }
+  // compute_timeAvg_edges (Spatial:2153-2177)
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    double l = q[v][0][0], r = q[v][0][NG - 1];
+    double dtmult = A.dt;
+#pragma unroll
+    for (int kt = 1; kt < NA; kt++) {
+      l += q[v][kt][0] * dtmult / (kt + 1.);
+      r += q[v][kt][NG - 1] * dtmult / (kt + 1.);
+      dtmult *= A.dt;
+    }
+    eL[v] = l;
+    eR[v] = r;
+  }
+  src_avg = 0;
+  if (DIR == 2) {  // compute_timeAvg (Spatial:2130-2138) + GLL quadrature (Spatial:1489-1496)
+    double dtmult = A.dt;
+#pragma unroll
+    for (int kt = 1; kt < NA; kt++) {
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) sr[0][ii] += sr[kt][ii] * dtmult / (kt + 1.);
+      dtmult *= A.dt;
+    }
+    double sa = 0;
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) sa += sr[0][ii] * T.wts[ii];
+    src_avg = sa;
+  }
+}
+
+// Upwind characteristic Riemann flux at one interface (K4: Spatial:842-902 x, 1202-1260 y,
+// 1583-1644 z). The y-direction averages are not divided by density (Spatial:1210-1214).
+// kf is the interface's k index (z only) for the hydrostatic pressure subtraction.
+template <int DIR, int NG>
+__device__ __forceinline__ void riemann(const double (&qL)[5], const double (&qR)[5], int kf,
+                                        const SweepArgs &A, double (&F)[5]) {
+  constexpr int TA = DIR == 0 ? 1 : 0;  // first tangential velocity slot
+  constexpr int TB = DIR == 2 ? 1 : 2;  // second tangential velocity slot
+  constexpr int QN = 1 + DIR, QA = 1 + TA, QB = 1 + TB;
+  const double r = 0.5 * (qL[0] + qR[0]);
+  double vel[3], t;
+  if (DIR == 1) {
+    vel[0] = 0.5 * (qL[1] + qR[1]);
+    vel[1] = 0.5 * (qL[2] + qR[2]);
+    vel[2] = 0.5 * (qL[3] + qR[3]);
+    t = 0.5 * (qL[4] + qR[4]);
+  } else {
+    vel[0] = 0.5 * (qL[1] / qL[0] + qR[1] / qR[0]);
+    vel[1] = 0.5 * (qL[2] / qL[0] + qR[2] / qR[0]);
+    vel[2] = 0.5 * (qL[3] / qL[0] + qR[3] / qR[0]);
+    t = 0.5 * (qL[4] / qL[0] + qR[4] / qR[0]);
+  }
+  const double p = C0 * pow_cr(r * t, GAMMA);
+  const double cs2 = GAMMA * p / r;
+  const double cs = sqrt(cs2);
+  const double vn = vel[DIR], va = vel[TA], vb = vel[TB];
+  double w1, w2, w3;
+  if (vn > 0) {
+    w1 = qL[0] - qL[4] / t;
+    w2 = qL[QA] - va * qL[4] / t;
+    w3 = qL[QB] - vb * qL[4] / t;
+  } else {
+    w1 = qR[0] - qR[4] / t;
+    w2 = qR[QA] - va * qR[4] / t;
+    w3 = qR[QB] - vb * qR[4] / t;
+  }
+  const double w5 = vn * qR[0] / (2 * cs) - qR[QN] / (2 * cs) + qR[4] / (2 * t);
+  const double w6 = -vn * qL[0] / (2 * cs) + qL[QN] / (2 * cs) + qL[4] / (2 * t);
+  double q[5];
+  q[0] = w1 + w5 + w6;
+  q[QN] = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
+  q[QA] = w2 + va * w5 + va * w6;
+  q[QB] = w3 + vb * w5 + vb * w6;
+  q[4] = t * w5 + t * w6;
+  F[0] = q[QN];
+  F[QN] = q[QN] * q[QN] / q[0] + C0 * pow_cr(q[4], GAMMA);
+  F[QA] = q[QN] * q[QA] / q[0];
+  F[QB] = q[QN] * q[QB] / q[0];
+  F[4] = q[QN] * q[4] / q[0];
+  if (DIR == 2) {  // Spatial:1628-1629
+    if (kf < A.nz) F[idW] -= A.pres_g[kf * NG + 0];
+    if (kf == A.nz) F[idW] -= A.pres_g[(A.nz - 1) * NG + NG - 1];
+  }
+}
+
+}  // namespace awfl

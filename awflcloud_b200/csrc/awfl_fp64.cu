@@ -1,0 +1,504 @@
+// FP64 kernels of the AWFL Euler-3D ADER/WENO step (the parity path), sm_100a.
+// Compiled with --fmad=false: no multiply-add contraction, matching the reference's CPU build.
+//
+// Kernel map (reference kernels it replaces, Spatial = Spatial_euler3d_cons_expl_cart_fv_Agrid.h):
+//   sweep_kernel<ORD,DIR>  K1 halo fill + K2 recon/ADER + K3 edge BCs + K4 Riemann +
+//                          K5 divergence (+ K6 apply when fused), one direction
+//                          (Spatial:631-957 x, 994-1310 y, 1351-1696 z; Temporal_ader.h:63-65)
+//   apply_kernel           K6 apply alone (Temporal_ader.h:63-65)
+//   cfl_kernel             K0 CFL time step (Spatial:169-183)
+//   init_state_kernel      K9 initial data quadrature (Spatial:428-485)
+#include <cuda_runtime.h>
+
+#include "awfl_device.cuh"
+#include "awfl_internal.h"
+
+namespace awfl {
+
+// ------------------------------------------------------------------------------------
+// The line sweep.
+//
+// A CTA owns W whole lines along the sweep direction DIR and marches along them in
+// chunks of C cells. Because no other CTA touches those lines, the tendency can be
+// applied in place (MODE_APPLY) with no race: every stencil value a chunk reads comes
+// from a shared-memory ring holding the ORIGINAL values of positions
+// [base-HS, base+C+HS), refilled one chunk ahead of the updates, and the first HS rows
+// (needed again by the periodic wrap at the end of the line) are saved before they are
+// overwritten.
+//
+// Per chunk: (A) store the prefetched ring rows; (B) reconstruct cells base..base+C-1
+// -> left/right edge states; (C) Riemann flux at their left faces (the left state of
+// the first face is carried from the previous chunk); (D) divergence and update of
+// cells base-1..base+C-2 (the last cell's right face is computed in the next chunk),
+// while the next chunk's rows are prefetched into registers. The last cell of the line
+// is finished after the loop.
+//
+// Boundary handling reproduces the reference's halo fill (Spatial:631-662 etc.) and
+// edge-value BCs (Spatial:816-837 etc.): periodic wraps; a wall copies the edge cell
+// with zero normal momentum, and its boundary face uses the interior state on both
+// sides. The halo values are also written to the state's halo cells, as the reference
+// does in place.
+// ------------------------------------------------------------------------------------
+template <int ORD, int DIR, int C, int W>
+__global__ void __launch_bounds__(C *W) sweep_kernel(SweepArgs A) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int R = 2 * C;  // ring length (power of two, >= C + 2*HS)
+  constexpr int NM = 1 + DIR;
+  static_assert((C & (C - 1)) == 0 && C >= 2 * HS, "chunk must be a power of two >= 2*HS");
+
+  __shared__ double ring[5][R * W];
+  __shared__ double sEL[5][C * W];
+  __shared__ double sER[5][(C + 1) * W];
+  __shared__ double sF[5][(C + 1) * W];
+  __shared__ double sSrc[DIR == 2 ? (C + 1) * W : 1];
+  __shared__ double sWrap[5][HS * W];
+  __shared__ double sEL0[5][W];
+
+  const int c = DIR == 0 ? threadIdx.x : threadIdx.y;  // position in chunk
+  const int w = DIR == 0 ? threadIdx.y : threadIdx.x;  // line within CTA
+
+  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  const long sx = 1, sy = nx + 2 * HS, sz = (long)(ny + 2 * HS) * sy, sv = (long)(nz + 2 * HS) * sz;
+  int L, kline = 0;
+  bool valid;
+  long lb;  // offset of (v=0, position 0 along DIR) of this line, halo-inclusive frame
+  long sd;  // stride along DIR
+  long tb;  // tendency offset of position 0
+  long tsd;
+  if (DIR == 0) {
+    const int k = blockIdx.y, j = blockIdx.x * W + w;
+    L = nx; valid = j < ny; kline = k;
+    lb = (HS + k) * sz + (HS + (valid ? j : 0)) * sy + HS * sx; sd = sx;
+    tb = ((long)k * ny + (valid ? j : 0)) * nx; tsd = 1;
+  } else if (DIR == 1) {
+    const int k = blockIdx.y, i = blockIdx.x * W + w;
+    L = ny; valid = i < nx; kline = k;
+    lb = (HS + k) * sz + HS * sy + HS + (valid ? i : 0); sd = sy;
+    tb = (long)k * ny * nx + (valid ? i : 0); tsd = nx;
+  } else {
+    const int j = blockIdx.y, i = blockIdx.x * W + w;
+    L = nz; valid = i < nx;
+    lb = HS * sz + (HS + j) * sy + HS + (valid ? i : 0); sd = sz;
+    tb = (long)j * nx + (valid ? i : 0); tsd = (long)ny * nx;
+  }
+  const long tv = (long)nz * ny * nx;
+  const bool periodic = A.bc == BC_PERIODIC;
+
+  auto G = [&](int v, int p) -> double { return A.state[lb + v * sv + p * sd]; };
+  auto ringAt = [&](int v, int p) -> double & {
+    const int s = p & (R - 1);
+    return DIR == 0 ? ring[v][w * R + s] : ring[v][s * W + w];
+  };
+  auto topval = [&](int v, int p, bool first) -> double {  // p >= L
+    const int q = p - L;
+    if (q >= HS) return 0.0;  // beyond the last cell's stencil: never read
+    if (periodic) return first ? G(v, q) : sWrap[v][q * W + w];
+    return v == NM ? 0.0 : G(v, L - 1);
+  };
+  auto stenIdx = [&](int v, int p) -> double { return ringAt(v, p); };
+
+  // ---- prologue: bottom halo, saved wrap rows, top halo; chunk-0 prefetch
+  if (valid && c < HS) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const double bot = periodic ? G(v, L + c - HS) : (v == NM ? 0.0 : G(v, 0));
+      const double orig = G(v, c);
+      const double top = periodic ? orig : (v == NM ? 0.0 : G(v, L - 1));
+      ringAt(v, c - HS) = bot;
+      ringAt(v, c) = orig;
+      sWrap[v][c * W + w] = orig;
+      A.state[lb + v * sv + (c - HS) * sd] = bot;
+      A.state[lb + v * sv + (L + c) * sd] = top;
+    }
+  }
+  double pre[5];
+  if (valid) {
+    const int p = HS + c;
+#pragma unroll
+    for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, true);
+  }
+  // periodic: the left state of face 0 is the right edge of cell L-1
+  if (valid && periodic && c == 0) {
+    auto wrapSten = [&](int v, int m) -> double {
+      int p = L - 1 - HS + m;
+      p %= L;
+      if (p < 0) p += L;
+      return G(v, p);
+    };
+    double eL[5], eR[5], sa;
+    cell_recon<ORD, DIR>(wrapSten, DIR == 2 ? L - 1 : kline, A, eL, eR, sa);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sER[v][0 * W + w] = eR[v];
+  }
+
+  const int nchunk = (L + C - 1) / C;
+  for (int t = 0; t < nchunk; t++) {
+    const int base = t * C;
+    const int nvalid = min(C, L - base);
+    if (valid) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) ringAt(v, base + HS + c) = pre[v];
+    }
+    __syncthreads();  // (A)
+    if (valid && c < nvalid) {
+      const int p = base + c;
+      auto sten = [&](int v, int m) -> double { return stenIdx(v, p - HS + m); };
+      double eL[5], eR[5], sa;
+      cell_recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa);
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        sEL[v][c * W + w] = eL[v];
+        sER[v][(c + 1) * W + w] = eR[v];
+      }
+      if (DIR == 2) sSrc[(c + 1) * W + w] = sa;
+      if (p == 0) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) sEL0[v][w] = eL[v];
+      }
+    }
+    __syncthreads();  // (B)
+    if (valid && c < nvalid) {
+      const int f = base + c;  // face index = left face of cell f
+      double qL[5], qR[5], F[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) qR[v] = sEL[v][c * W + w];
+#pragma unroll
+      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][c * W + w];
+      riemann<DIR, NG>(qL, qR, f, A, F);
+#pragma unroll
+      for (int v = 0; v < 5; v++) sF[v][(c + 1) * W + w] = F[v];
+    }
+    __syncthreads();  // (C)
+    if (valid && c < nvalid) {
+      const int cell = base + c - 1;
+      if (cell >= 0) {
+        const double sa = DIR == 2 ? sSrc[c * W + w] : 0.0;
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const double Fl = sF[v][c * W + w], Fr = sF[v][(c + 1) * W + w];
+          const double d = -(Fr - Fl) / A.dxd;
+          double tnd;
+          if (DIR == 0) tnd = (A.sim2d && v == idV) ? 0.0 : d;
+          else if (DIR == 1) tnd = d;
+          else tnd = (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;
+          if (A.mode == MODE_APPLY) {
+            A.state[lb + v * sv + cell * sd] = ringAt(v, cell) + A.dt * tnd;
+          } else {
+            A.tend[tb + v * tv + cell * tsd] = tnd;
+          }
+        }
+      }
+    }
+    if (valid && t + 1 < nchunk) {
+      const int p = base + C + HS + c;
+#pragma unroll
+      for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
+    }
+    __syncthreads();  // (D)
+    if (valid && c == 0) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        sER[v][w] = sER[v][nvalid * W + w];
+        sF[v][w] = sF[v][nvalid * W + w];
+      }
+      if (DIR == 2) sSrc[w] = sSrc[nvalid * W + w];
+    }
+  }
+  // ---- epilogue: face L and the last cell (same thread that wrote the carry)
+  if (valid && c == 0) {
+    double qL[5], qR[5], F[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      qL[v] = sER[v][w];
+      qR[v] = periodic ? sEL0[v][w] : qL[v];
+    }
+    riemann<DIR, NG>(qL, qR, L, A, F);
+    const int cell = L - 1;
+    const double sa = DIR == 2 ? sSrc[w] : 0.0;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const double Fl = sF[v][w], Fr = F[v];
+      const double d = -(Fr - Fl) / A.dxd;
+      double tnd;
+      if (DIR == 0) tnd = (A.sim2d && v == idV) ? 0.0 : d;
+      else if (DIR == 1) tnd = d;
+      else tnd = (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;
+      if (A.mode == MODE_APPLY) {
+        A.state[lb + v * sv + cell * sd] = ringAt(v, cell) + A.dt * tnd;
+      } else {
+        A.tend[tb + v * tv + cell * tsd] = tnd;
+      }
+    }
+  }
+}
+
+// Launch geometry per (ORD, DIR): lines are grouped W per CTA along the contiguous axis.
+template <int ORD, int DIR> struct SweepShape;
+template <> struct SweepShape<5, 0> { static constexpr int C = 32, W = 4; };
+template <> struct SweepShape<5, 1> { static constexpr int C = 4, W = 32; };
+template <> struct SweepShape<5, 2> { static constexpr int C = 4, W = 32; };
+template <> struct SweepShape<9, 0> { static constexpr int C = 32, W = 2; };
+template <> struct SweepShape<9, 1> { static constexpr int C = 8, W = 16; };
+template <> struct SweepShape<9, 2> { static constexpr int C = 8, W = 16; };
+
+template <int ORD, int DIR>
+static cudaError_t launch_sweep_t(const SweepArgs &A, cudaStream_t st) {
+  constexpr int C = SweepShape<ORD, DIR>::C, W = SweepShape<ORD, DIR>::W;
+  dim3 block(DIR == 0 ? C : W, DIR == 0 ? W : C);
+  dim3 grid;
+  if (DIR == 0) grid = dim3((A.ny + W - 1) / W, A.nz);
+  else if (DIR == 1) grid = dim3((A.nx + W - 1) / W, A.nz);
+  else grid = dim3((A.nx + W - 1) / W, A.ny);
+  sweep_kernel<ORD, DIR, C, W><<<grid, block, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
+  if (ord == 5) {
+    if (dir == 0) return launch_sweep_t<5, 0>(A, st);
+    if (dir == 1) return launch_sweep_t<5, 1>(A, st);
+    return launch_sweep_t<5, 2>(A, st);
+  }
+  if (dir == 0) return launch_sweep_t<9, 0>(A, st);
+  if (dir == 1) return launch_sweep_t<9, 1>(A, st);
+  return launch_sweep_t<9, 2>(A, st);
+}
+
+// ------------------------------------------------------------------------------------
+// K6 apply (Temporal_ader.h:63-65): state(l,hs+k,hs+j,hs+i) += dt * tend(l,k,j,i).
+// ------------------------------------------------------------------------------------
+__global__ void apply_kernel(double *state, const double *tend, double dt, int nx, int ny, int nz, int hs) {
+  const long n = 5L * nz * ny * nx;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+    long r = idx;
+    const int i = r % nx; r /= nx;
+    const int j = r % ny; r /= ny;
+    const int k = r % nz; r /= nz;
+    const int l = (int)r;
+    const long s = (((long)l * (nz + 2 * hs) + hs + k) * (ny + 2 * hs) + hs + j) * (nx + 2 * hs) + hs + i;
+    state[s] += dt * tend[idx];
+  }
+}
+
+cudaError_t launch_apply_fp64(double *state, const double *tend, double dt, int nx, int ny, int nz, int hs,
+                              int nsm, cudaStream_t st) {
+  const long n = 5L * nz * ny * nx;
+  long blocks = (n + 255) / 256;
+  const long cap = (long)nsm * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  apply_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, tend, dt, nx, ny, nz, hs);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// K0 CFL (Spatial:169-183): per-cell min(cfl*dx/max|u+-cs|, ...); block min in shared
+// memory, then an atomic min on the bit pattern (valid for non-negative doubles) into
+// *out, which the caller initialises to +inf.
+// ------------------------------------------------------------------------------------
+__global__ void cfl_kernel(const double *state, const double *dens_c, const double *denstheta_c,
+                           double cfl, double dx, double dy, double dz, int nx, int ny, int nz, int hs,
+                           unsigned long long *out) {
+  __shared__ double red[256];
+  double best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  const long n = (long)nz * ny * nx;
+  const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+    const int i = idx % nx;
+    const int j = (idx / nx) % ny;
+    const int k = idx / ((long)nx * ny);
+    const long s = (hs + k) * sz + (hs + j) * sy + hs + i;
+    const double r = state[s] + dens_c[hs + k];
+    const double u = state[s + sv] / r;
+    const double v = state[s + 2 * sv] / r;
+    const double w = state[s + 3 * sv] / r;
+    const double t = (state[s + 4 * sv] + denstheta_c[hs + k]) / r;
+    const double p = C0 * pow_cr(r * t, GAMMA);
+    const double cs = sqrt(GAMMA * p / r);
+    const double au = fabs(u - cs), bu = fabs(u + cs);
+    const double av = fabs(v - cs), bv = fabs(v + cs);
+    const double aw = fabs(w - cs), bw = fabs(w + cs);
+    const double udt = cfl * dx / (au > bu ? au : bu);
+    const double vdt = cfl * dy / (av > bv ? av : bv);
+    const double wdt = cfl * dz / (aw > bw ? aw : bw);
+    const double m1 = udt < vdt ? udt : vdt;
+    const double d = m1 < wdt ? m1 : wdt;
+    best = d < best ? d : best;
+  }
+  red[threadIdx.x] = best;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      const double o = red[threadIdx.x + s];
+      if (o < red[threadIdx.x]) red[threadIdx.x] = o;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicMin(out, (unsigned long long)__double_as_longlong(red[0]));
+}
+
+cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const double *denstheta_c, double cfl,
+                            double dx, double dy, double dz, int nx, int ny, int nz, int hs, int nsm,
+                            unsigned long long *d_out, cudaStream_t st) {
+  const long n = (long)nz * ny * nx;
+  long blocks = (n + 255) / 256;
+  const long cap = (long)nsm * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  cfl_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, dens_c, denstheta_c, cfl, dx, dy, dz, nx, ny, nz, hs, d_out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// K9 initial data (Spatial:428-485 and Profiles.h), one thread per cell.
+// ------------------------------------------------------------------------------------
+struct InitArgs {
+  double *state;
+  int nx, ny, nz, hs, ord;
+  double dx, dy, dz, xlen, ylen, zlen;
+  int data_spec, sim2d;
+  int kind, shape;
+  double x0, y0, z0, xrad, yrad, zrad, amp, pwr;
+  double noise_amp;
+  unsigned long long seed;
+  const double *dens_c;
+  double pts[9], wts[9];
+};
+
+__device__ double d_const_theta_density(double t0, double z) {  // Profiles.h:8-13
+  const double exner = 1. - GRAV * z / (1004. * t0);
+  const double p = pow_cr(exner, 1004. / 287.) * 1.0e5;
+  const double rt = pow_cr(p / C0, 1. / GAMMA);
+  return rt / t0;
+}
+__device__ double d_bvf_pot_temp(double t0, double bvf, double z) { return t0 * exp_cr(bvf * bvf * z / GRAV); }
+__device__ double d_bvf_density(double t0, double bvf, double z) {  // Profiles.h:31-37
+  const double t = d_bvf_pot_temp(t0, bvf, z);
+  const double exner = 1. - GRAV * GRAV / (1004. * bvf * bvf) * (t - t0) / (t * t0);
+  const double p = pow_cr(exner, 1004. / 287.) * 1.0e5;
+  const double rt = pow_cr(p / C0, 1. / GAMMA);
+  return rt / t;
+}
+__device__ double d_ellipsoid_linear(double x, double y, double z, double x0, double y0, double z0, double xrad,
+                                     double yrad, double zrad, double amp) {  // Profiles.h:49-57
+  const double xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
+  const double dist = sqrt(xn * xn + yn * yn + zn * zn);
+  const double m = 1. - dist;
+  return amp * (m > 0. ? m : 0.);
+}
+__device__ double d_ellipsoid_cosine(double x, double y, double z, double x0, double y0, double z0, double xrad,
+                                     double yrad, double zrad, double amp, double pwr) {  // Profiles.h:60-72
+  double val = 0;
+  const double xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
+  const double dist = sqrt(xn * xn + yn * yn + zn * zn);
+  if (dist <= 1.) val = amp * pow_cr((cos(3.14159265358979323846 * dist) + 1) / 2, pwr);
+  return val;
+}
+__device__ double d_igw(double x, double y, double z, double x0, double y0, double hr, double zlen,
+                        double amp) {  // Profiles.h:75-81
+  const double xn = (x - x0) / hr, yn = (y - y0) / hr;
+  return amp * sin(3.14159265358979323846 * z / zlen) / sqrt(1 + xn * xn + yn * yn);
+}
+__device__ __forceinline__ unsigned long long d_splitmix64(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+__global__ void init_state_kernel(InitArgs a) {
+  const long n = (long)a.nz * a.ny * a.nx;
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int i = idx % a.nx, j = (idx / a.nx) % a.ny, k = idx / ((long)a.nx * a.ny);
+  const int hs = a.hs;
+  const long sy = a.nx + 2 * hs, sz = (long)(a.ny + 2 * hs) * sy, sv = (long)(a.nz + 2 * hs) * sz;
+  const long s = (hs + k) * sz + (hs + j) * sy + hs + i;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int kk = 0; kk < a.ord; kk++)
+    for (int jj = 0; jj < a.ord; jj++)
+      for (int ii = 0; ii < a.ord; ii++) {
+        const double zloc = (k + 0.5) * a.dz + a.pts[kk] * a.dz;
+        double yloc = a.sim2d ? a.ylen / 2 : (j + 0.5) * a.dy + a.pts[jj] * a.dy;
+        const double xloc = (i + 0.5) * a.dx + a.pts[ii] * a.dx;
+        const double wt = a.wts[kk] * a.wts[jj] * a.wts[ii];
+        if (a.kind == 1) {
+          const double th = 300, rh = d_const_theta_density(th, zloc);
+          const double tp = a.shape == 0
+                                ? d_ellipsoid_linear(xloc, yloc, zloc, a.x0, a.y0, a.z0, a.xrad, a.yrad, a.zrad, a.amp)
+                                : d_ellipsoid_cosine(xloc, yloc, zloc, a.x0, a.y0, a.z0, a.xrad, a.yrad, a.zrad, a.amp, a.pwr);
+          const double t = th + tp;
+          acc[4] += (rh * t - rh * th) * wt;
+        } else if (a.data_spec == 1) {
+          const double th = 300, rh = d_const_theta_density(th, zloc);
+          const double tp = d_ellipsoid_linear(xloc, yloc, zloc, a.xlen / 2, a.ylen / 2, 2000, 2000, 2000, 2000, 2);
+          const double t = th + tp;
+          acc[4] += (rh * t - rh * th) * wt;
+        } else if (a.data_spec == 2) {
+          const double th = 300, rh = d_const_theta_density(th, zloc);
+          double tp = d_ellipsoid_linear(xloc, yloc, zloc, a.xlen / 2, a.ylen / 2, 2000, 2000, 2000, 2000, 20);
+          tp += d_ellipsoid_linear(xloc, yloc, zloc, a.xlen / 2, a.ylen / 2, 8000, 2000, 2000, 2000, -20);
+          const double t = th + tp;
+          acc[4] += (rh * t - rh * th) * wt;
+        } else if (a.data_spec == 3) {
+          const double th = 300, rh = d_const_theta_density(th, zloc);
+          const double tp = d_ellipsoid_cosine(xloc, yloc, zloc, a.xlen / 2, a.ylen / 2, 3000, 4000, 2000, 2000, -15, 1);
+          const double t = th + tp;
+          acc[4] += (rh * t - rh * th) * wt;
+        } else {
+          if (a.sim2d) yloc = a.ylen / 3;
+          const double t0 = 300, bvf = 0.01;
+          const double rh = d_bvf_density(t0, bvf, zloc);
+          const double th = d_bvf_pot_temp(t0, bvf, zloc);
+          const double tp = d_igw(xloc, yloc, zloc, a.xlen / 3, a.ylen / 3, 5000, a.zlen, 0.01);
+          const double t = th + tp;
+          acc[4] += (rh * t - rh * th) * wt;
+          acc[1] += 20 * rh * wt;
+          if (!a.sim2d) acc[2] += 20 * rh * wt;
+        }
+      }
+  if (a.noise_amp > 0) {
+    const unsigned long long cell = ((unsigned long long)k * a.ny + j) * a.nx + i;
+    const double u = (double)(d_splitmix64(a.seed * 0x100000001B3ULL + cell) >> 11) * (1.0 / 9007199254740992.0);
+    const double nz_ = (2.0 * u - 1.0) * a.noise_amp;
+    acc[4] += a.dens_c[hs + k] * nz_;
+  }
+#pragma unroll
+  for (int l = 0; l < 5; l++) a.state[s + l * sv] = acc[l];
+}
+
+cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st) {
+  InitArgs a;
+  a.state = (double *)L.state;
+  a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.hs = L.hs; a.ord = L.ord;
+  a.dx = L.dx; a.dy = L.dy; a.dz = L.dz; a.xlen = L.xlen; a.ylen = L.ylen; a.zlen = L.zlen;
+  a.data_spec = L.data_spec; a.sim2d = L.sim2d; a.kind = L.kind; a.shape = L.shape;
+  a.x0 = L.x0; a.y0 = L.y0; a.z0 = L.z0; a.xrad = L.xrad; a.yrad = L.yrad; a.zrad = L.zrad;
+  a.amp = L.amp; a.pwr = L.pwr; a.noise_amp = L.noise_amp; a.seed = L.seed; a.dens_c = L.dens_c;
+  for (int m = 0; m < 9; m++) { a.pts[m] = m < L.ord ? L.pts[m] : 0; a.wts[m] = m < L.ord ? L.wts[m] : 0; }
+  const long n = (long)L.nz * L.ny * L.nx;
+  init_state_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// Device math self-test: out[i] = pow(x[i], y) by the library's pow_cr (mode 0) or by
+// the CUDA math library (mode 1); exp_cr(x[i]) (mode 2).
+__global__ void selftest_pow_kernel(const double *x, double y, double *out, long n, int mode) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = mode == 0 ? pow_cr(x[i], y) : (mode == 1 ? pow(x[i], y) : exp_cr(x[i]));
+}
+
+cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  selftest_pow_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(x, y, out, n, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t upload_tables_fp64(int ord, const void *tab, size_t bytes) {
+  if (ord == 5) return cudaMemcpyToSymbol(c_tab5, tab, bytes);
+  return cudaMemcpyToSymbol(c_tab9, tab, bytes);
+}
+
+}  // namespace awfl

@@ -1,0 +1,71 @@
+// Internal declarations shared by the library's translation units (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace awfl {
+
+// phys_params.h:4-10
+constexpr double GRAV = 9.81;
+constexpr double C0 = 27.5629410929725921310572974482;
+constexpr double GAMMA = 1.40027894002789400278940027894;
+
+enum { idR = 0, idU = 1, idV = 2, idW = 3, idT = 4 };
+enum { BC_PERIODIC = 0, BC_WALL = 1 };
+enum { MODE_TEND = 0, MODE_APPLY = 1 };
+
+template <int ORD> struct OrdTraits;
+template <> struct OrdTraits<5> { static constexpr int NGLL = 3; };
+template <> struct OrdTraits<9> { static constexpr int NGLL = 5; };
+
+// Constant tables (Spatial:274-315), one set per order, uploaded once per device.
+template <int ORD> struct Tables {
+  static constexpr int HS = (ORD - 1) / 2;
+  static constexpr int NG = OrdTraits<ORD>::NGLL;
+  double recon[ORD * ORD * ORD];  // weno_sten_to_coefs(i, s, ii)
+  double c2g[ORD * NG];            // coefs_to_gll(s, ii)
+  double s2g[ORD * NG];            // sten_to_gll(s, ii)
+  double deriv[NG * NG];          // derivMatrix(s, ii)
+  double idl[HS + 2];
+  double sigma;
+  double wts[NG];                 // gllWts_ngll
+};
+
+// Per-line constants of one sweep.
+struct SweepArgs {
+  double *state;   // (5, nz+2hs, ny+2hs, nx+2hs)
+  double *tend;    // (5, nz, ny, nx) for MODE_TEND
+  int nx, ny, nz;
+  int bc;          // BC along the sweep direction
+  int weno_s, weno_w, sim2d, mode;
+  double dxd;      // dx, dy or dz
+  double dt;
+  const double *dens_c, *denstheta_c;             // hyDensCells, hyDensThetaCells (nz+2hs)
+  const double *dens_g, *denstheta_g, *pres_g;    // hyDensGLL, hyDensThetaGLL, hyPressureGLL (nz*ngll)
+};
+
+
+struct InitLaunch {
+  void *state;
+  int nx, ny, nz, hs, ord;
+  double dx, dy, dz, xlen, ylen, zlen;
+  int data_spec, sim2d, kind, shape;
+  double x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp;
+  unsigned long long seed;
+  const double *dens_c;
+  double pts[9], wts[9];
+};
+
+// FP64 translation unit (awfl_fp64.cu)
+cudaError_t upload_tables_fp64(int ord, const void *tab, size_t bytes);
+cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st);
+cudaError_t launch_apply_fp64(double *state, const double *tend, double dt, int nx, int ny, int nz, int hs,
+                              int nsm, cudaStream_t st);
+cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const double *denstheta_c, double cfl,
+                            double dx, double dy, double dz, int nx, int ny, int nz, int hs, int nsm,
+                            unsigned long long *d_out, cudaStream_t st);
+cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st);
+cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st);
+
+}  // namespace awfl

@@ -276,12 +276,96 @@ def emit_header() -> str:
     return "".join(out)
 
 
+def emit_tv_header() -> str:
+    """C++ (host + device) evaluators of coefs_to_tv, one straight-line function per n,
+    in the reference's term order; templated on the arithmetic type."""
+    out = ["// GENERATED by awflcloud_b200/gen_tables.py -- do not edit by hand.\n",
+           "// coefs_to_tv(n) evaluators: r = c0*(a_q*a_q); r = r + (c*a_m)*a_q ... in the\n",
+           "// reference's term order (TransformMatrices.h coefs_to_tv).\n",
+           "#pragma once\n\n",
+           "#if defined(__CUDACC__)\n#define AWFL_TV_HD __host__ __device__ __forceinline__\n",
+           "#else\n#define AWFL_TV_HD inline\n#endif\n\n"]
+    done = set()
+    for ordv, _ in ORDS:
+        hs = (ordv - 1) // 2
+        for n in (hs + 1, ordv):
+            if n in done:
+                continue
+            done.add(n)
+            out.append("template <class T> AWFL_TV_HD T awfl_tv_n%d(const T *a) {\n" % n)
+            for t, (m, q, c) in enumerate(tv_terms(n)):
+                lit = "T(%s)" % hexlit(to_double(c))
+                term = ("%s * (a[%d] * a[%d])" % (lit, q, q)) if m == q else ("%s * a[%d] * a[%d]" % (lit, m, q))
+                out.append(("  T r = %s;\n" % term) if t == 0 else ("  r = r + %s;\n" % term))
+            out.append("  return r;\n}\n\n")
+    return "".join(out)
+
+
+def _split_bits(x, bits):
+    """x rounded to ``bits`` significant bits (so that small-integer multiples are exact)."""
+    return _round_mant(mp.mpf(x), bits)
+
+
+def emit_pow_header() -> str:
+    """Tables of the correctly rounded pow (csrc/awfl_pow.cuh):
+    log: for j in 0..127, inv_j = double(1 / (1 + (j + 1/2)/128)) and -ln(inv_j) as a
+    double-double; exp: 2^(j/64) for j in 0..63 as double-doubles; ln2 split as
+    L2HI (42 bits) + L2LO, and ln2/64 split as E1 (36 bits) + E2."""
+    out = ["// GENERATED by awflcloud_b200/gen_tables.py -- do not edit by hand.\n",
+           "// Tables for awfl_pow.cuh (values exact to 256 bits before rounding).\n",
+           "#pragma once\n\n",
+           "#ifdef __CUDACC__\n#define AWFL_POW_TABLE __device__ const double\n",
+           "#else\n#define AWFL_POW_TABLE static const double\n#endif\n\n"]
+    inv, th, tl = [], [], []
+    for j in range(128):
+        c = 1 + (mp.mpf(j) + HALF) / 128
+        iv = float(_round_mant(1 / c, 53))
+        lv = -mp.log(mp.mpf(iv))
+        hi = float(_round_mant(lv, 53))
+        lo = float(_round_mant(lv - mp.mpf(hi), 53))
+        inv.append(iv); th.append(hi); tl.append(lo)
+    e2h, e2l = [], []
+    for j in range(64):
+        v = mp.mpf(2) ** (mp.mpf(j) / 64)
+        hi = float(_round_mant(v, 53))
+        lo = float(_round_mant(v - mp.mpf(hi), 53))
+        e2h.append(hi); e2l.append(lo)
+    ln2 = mp.log(2)
+    l2hi = float(_split_bits(ln2, 42))
+    l2lo = float(_round_mant(ln2 - mp.mpf(l2hi), 53))
+    q = ln2 / 64
+    e1 = float(_split_bits(q, 36))
+    e2 = float(_round_mant(q - mp.mpf(e1), 53))
+    inv64 = float(_round_mant(64 / ln2, 53))
+
+    def arr(name, vals):
+        return "AWFL_POW_TABLE %s[%d] = {%s};\n" % (name, len(vals), ", ".join(hexlit(v) for v in vals))
+
+    out.append(arr("awfl_pow_log_inv", inv))
+    out.append(arr("awfl_pow_log_hi", th))
+    out.append(arr("awfl_pow_log_lo", tl))
+    out.append(arr("awfl_pow_exp_hi", e2h))
+    out.append(arr("awfl_pow_exp_lo", e2l))
+    out.append("#define AWFL_POW_L2HI %s\n#define AWFL_POW_L2LO %s\n" % (hexlit(l2hi), hexlit(l2lo)))
+    out.append("#define AWFL_POW_E1 %s\n#define AWFL_POW_E2 %s\n#define AWFL_POW_INV_E %s\n"
+               % (hexlit(e1), hexlit(e2), hexlit(inv64)))
+    return "".join(out)
+
+
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     path = os.path.join(here, "csrc", "awfl_tables.h")
     os.makedirs(os.path.dirname(path), exist_ok=True)
     with open(path, "w") as f:
         f.write(emit_header())
+    print("wrote", path)
+    path = os.path.join(here, "csrc", "awfl_tv.h")
+    with open(path, "w") as f:
+        f.write(emit_tv_header())
+    print("wrote", path)
+    path = os.path.join(here, "csrc", "awfl_pow_tables.h")
+    with open(path, "w") as f:
+        f.write(emit_pow_header())
     print("wrote", path)
 
 

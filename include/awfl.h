@@ -1,0 +1,152 @@
+/* awfl.h -- C ABI of the B200-native AWFL Euler-3D ADER/WENO finite-volume step.
+ *
+ * This is the boundary that replaces the reference's YAKL parallel_for kernels behind its
+ * Spatial/Temporal operator interface (mrnorman/awflCloud):
+ *   Spatial_euler3d_cons_expl_cart_fv_Agrid.h (the spatial operator, "Spatial" below)
+ *   Temporal_ader.h                            (the ADER time stepper)
+ * The C++ drop-in headers in awflcloud_b200/dropin/ implement that interface on top of
+ * these entry points; any other host (ctypes, JNI, cgo) can bind them directly.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only. Device pointers are CUDA device addresses; streams
+ *     are passed as void* (a cudaStream_t; NULL = the legacy default stream).
+ *   - State arrays are C-order (5, nz+2hs, ny+2hs, nx+2hs), x fastest, variables
+ *     (rho', rho*u, rho*v, rho*w, (rho*theta)') -- Spatial:129-131, :69-73.
+ *     Tendency arrays are C-order (5, nz, ny, nx) -- Spatial:141-143.
+ *   - Element type is double for AWFL_FP64 contexts and float for AWFL_FP32 contexts.
+ *   - Every function returns AWFL_OK (0) or a negative awfl_status; nothing throws
+ *     across the ABI. awfl_last_error() gives the message of the last failure.
+ *   - A context is used by one host thread at a time; all work is ordered on the
+ *     stream passed in. Separate contexts are independent.
+ */
+#ifndef AWFL_H
+#define AWFL_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AWFL_OK = 0,
+  AWFL_ERR_ARG = -1,       /* invalid argument or unsupported configuration */
+  AWFL_ERR_CUDA = -2,      /* a CUDA runtime call failed */
+  AWFL_ERR_NOMEM = -3,     /* device allocation failed */
+  AWFL_ERR_STATE = -4,     /* device-side check failed (NaN / non-positive density) */
+  AWFL_ERR_TIMEOUT = -5,   /* a bounded device wait gave up */
+  AWFL_ERR_NOT_BUILT = -6  /* the requested variant is not compiled into this library */
+} awfl_status;
+
+enum { AWFL_BC_PERIODIC = 0, AWFL_BC_WALL = 1 };           /* Spatial:80-81 */
+enum { AWFL_FP64 = 0, AWFL_FP32 = 1 };
+enum { AWFL_DATA_THERMAL = 1, AWFL_DATA_COLLISION = 2,      /* Spatial:83-86 */
+       AWFL_DATA_STRAKA = 3, AWFL_DATA_IGW = 4 };
+enum { AWFL_DIR_X = 0, AWFL_DIR_Y = 1, AWFL_DIR_Z = 2 };
+
+/* The YAML keys read by Spatial::init (Spatial:197-272) plus the compile-time order
+ * (const.h:21-27: ord in {5, 9}, ngll = 3 or 5) and the arithmetic precision. */
+typedef struct {
+  int nx, ny, nz;
+  double xlen, ylen, zlen;
+  int bc_x, bc_y, bc_z;
+  int weno_scalars, weno_winds;
+  int data_spec;   /* selects the hydrostatic background: constant theta, or constant
+                      Brunt-Vaisala frequency for AWFL_DATA_IGW (Spatial:371-425) */
+  int ord;         /* 5 or 9 */
+  int precision;   /* AWFL_FP64 or AWFL_FP32 */
+} awfl_config;
+
+/* Initial-data recipe for awfl_init_state. kind AWFL_INIT_REFERENCE reproduces
+ * Spatial::initState for the context's data_spec (Spatial:428-485); AWFL_INIT_BUBBLE
+ * replaces the theta perturbation by an ellipsoid (shape 0 linear / 1 cosine, Profiles.h
+ * 49-72) integrated with the same ord^3 GLL quadrature. noise_amp > 0 then adds seeded
+ * uniform theta noise n in [-amp, amp) as state(rho*theta) += hyDensCells(k) * n, where
+ * n = 2*u-1 times amp, u = top 53 bits of splitmix64(seed*0x100000001B3 + cell)/2^53,
+ * cell = (k*ny + j)*nx + i. */
+enum { AWFL_INIT_REFERENCE = 0, AWFL_INIT_BUBBLE = 1 };
+typedef struct {
+  int kind;
+  int shape;
+  double x0, y0, z0, xrad, yrad, zrad, amp, pwr;
+  double noise_amp;
+  unsigned long long noise_seed;
+} awfl_init_spec;
+
+typedef struct awfl_ctx awfl_ctx;
+
+/* Spatial::init (Spatial:192-340) + the background of Spatial::initState (:371-425):
+ * validates the configuration, builds the transform tables and the hydrostatic
+ * background on `device`, uploads them. device < 0 makes a host-only context: tables and
+ * background are built (awfl_get_tables / awfl_get_background work) but every entry point
+ * that runs device work returns AWFL_ERR_ARG. */
+int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out);
+int awfl_destroy(awfl_ctx *ctx);
+const char *awfl_last_error(const awfl_ctx *ctx);
+/* Library version string (never NULL). */
+const char *awfl_version(void);
+
+/* Sizes (elements) of the state (with halos) and tendency arrays; the halo width hs. */
+int awfl_sizes(const awfl_ctx *ctx, long *state_elems, long *tend_elems, int *hs);
+
+/* Spatial::initState (Spatial:345-500) on the device; writes the interior of d_state. */
+int awfl_init_state(awfl_ctx *ctx, void *d_state, const awfl_init_spec *spec, void *stream);
+
+/* Spatial::computeTimeStep without the caching (Spatial:159-187): the acoustic CFL time
+ * step, min over all cells, returned in *h_dt (synchronises the stream). */
+int awfl_cfl(awfl_ctx *ctx, const void *d_state, double cfl, double *h_dt, void *stream);
+
+/* Spatial::computeTendenciesX/Y/Z for dir = 0/1/2 (Spatial:598-957, 961-1311,
+ * 1315-1697): fills the dir-halos of d_state in place (as the reference does) and writes
+ * the dt-time-averaged tendencies to d_tend. The interior of d_state is not modified. */
+int awfl_compute_tendencies(awfl_ctx *ctx, void *d_state, void *d_tend, double dt, int dir,
+                            void *stream);
+
+/* Temporal_ader's apply (Temporal_ader.h:63-65): state(l,hs+k,hs+j,hs+i) += dt*tend(l,k,j,i). */
+int awfl_apply_tendencies(awfl_ctx *ctx, void *d_state, const void *d_tend, double dt,
+                          void *stream);
+
+/* One split fused: compute_tendencies(dir) followed by apply_tendencies, in one kernel,
+ * without a tendency array. Same results as the two calls. */
+int awfl_split(awfl_ctx *ctx, void *d_state, double dt, int dir, void *stream);
+
+/* Temporal_ader::timeStep (Temporal_ader.h:48-72): three fused splits in the order
+ * X,Y,Z or Z,Y,X (the reference's dimSwitch, Spatial:568-593, kept in the context and
+ * flipped after every step). sim2d (ny == 1) skips the Y split, whose tendency the
+ * reference sets to zero. */
+int awfl_step(awfl_ctx *ctx, void *d_state, double dt, void *stream);
+
+/* The dimSwitch flag of the context (1 = next step runs X,Y,Z). */
+int awfl_get_dimswitch(const awfl_ctx *ctx, int *value);
+int awfl_set_dimswitch(awfl_ctx *ctx, int value);
+
+/* Host views of the tables and background the context built, for verification:
+ * weno_recon (ord^3), coefs_to_gll (ord*ngll), sten_to_gll (ord*ngll), deriv (ngll^2),
+ * idl (hs+2), sigma (1), gll points/weights (ord, ord, ngll, ngll); hydrostatic cells
+ * (4 x (nz+2hs): dens, pressure, theta, dens*theta) and GLL (4 x nz*ngll). Any pointer
+ * may be NULL. Host-only; needs no GPU work. */
+int awfl_get_tables(const awfl_ctx *ctx, double *weno_recon, double *coefs_to_gll,
+                    double *sten_to_gll, double *deriv, double *idl, double *sigma,
+                    double *gll_pts_ord, double *gll_wts_ord, double *gll_pts_ngll,
+                    double *gll_wts_ngll);
+int awfl_get_background(const awfl_ctx *ctx, double *dens_c, double *pres_c, double *theta_c,
+                        double *denstheta_c, double *dens_g, double *pres_g, double *theta_g,
+                        double *denstheta_g);
+
+/* Diagnostic: the FP64 path's device math on n doubles (device pointers). mode 0:
+ * out = pow(x, y) by the library's correctly rounded pow (the one every FP64 kernel uses
+ * in place of the reference's glibc pow); mode 1: the CUDA math library's pow, for
+ * comparison; mode 2: the library's correctly rounded exp(x) (y ignored). */
+int awfl_selftest_pow(const void *d_x, double y, void *d_out, long n, int mode, void *stream);
+
+/* Device memory helpers for hosts that do not link the CUDA runtime themselves. */
+int awfl_device_alloc(void **d_ptr, long bytes);
+int awfl_device_free(void *d_ptr);
+int awfl_copy_h2d(void *d_dst, const void *h_src, long bytes, void *stream);
+int awfl_copy_d2h(void *h_dst, const void *d_src, long bytes, void *stream);
+int awfl_memset_device(void *d_ptr, int value, long bytes, void *stream);
+int awfl_stream_synchronize(void *stream);
+int awfl_device_synchronize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AWFL_H */

@@ -18,6 +18,19 @@
 
 #include "../awflcloud_b200/csrc/awfl_tables.h"
 
+/* ORACLE_CR_POW builds the variant whose pow calls in the time step and the CFL time step
+ * are correctly rounded (awfl_pow_cr.h) instead of glibc's, like the GPU FP64 kernels.
+ * The hydrostatic profiles (init-time, computed on the host by the library as well) keep
+ * glibc's pow/exp. */
+#ifdef ORACLE_CR_POW
+#include "awfl_pow_cr.h"
+#define OPOW(x, y) awfl_test_pow_cr((x), (y))
+#define OEXP(x) awfl_test_exp_cr((x))
+#else
+#define OPOW(x, y) pow((x), (y))
+#define OEXP(x) exp((x))
+#endif
+
 #ifndef ORACLE_ORD
 #define ORACLE_ORD 5
 #endif
@@ -392,7 +405,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
           A.f[1][0][ii] = r * vn * v;
           A.f[2][0][ii] = r * vn * w;
           A.f[3][0][ii] = r * vn * t;
-          A.g[0][ii] = pow(r * t, GAMMA);
+          A.g[0][ii] = OPOW(r * t, GAMMA);
           if (dir == 2) srcfill = -(A.q[idR][0][ii] - c->hyDensGLL[k * NGLL + ii]) * GRAV;
         }
         if (dir == 2) { /* SArray scalar assignment fills every entry (Spatial:1439) */
@@ -468,7 +481,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
             vel[2] = 0.5 * (qL[3] / qL[0] + qR[3] / qR[0]);
             t = 0.5 * (qL[4] / qL[0] + qR[4] / qR[0]);
           }
-          double p = C0 * pow(r * t, GAMMA);
+          double p = C0 * OPOW(r * t, GAMMA);
           double cs2 = GAMMA * p / r;
           double cs = sqrt(cs2);
           /* tangential indices in increasing order */
@@ -495,7 +508,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
           q[4] = t * w5 + t * w6;
           double F[5];
           F[0] = q[qn];
-          F[qn] = q[qn] * q[qn] / q[0] + C0 * pow(q[4], GAMMA);
+          F[qn] = q[qn] * q[qn] / q[0] + C0 * OPOW(q[4], GAMMA);
           F[qa] = q[qn] * q[qa] / q[0];
           F[qb] = q[qn] * q[qb] / q[0];
           F[4] = q[qn] * q[4] / q[0];
@@ -579,7 +592,7 @@ double oracle_compute_dt(const oracle_ctx *c, const double *st, double cfl) {
         double v = st[sidx(c, idV, HS + k, HS + j, HS + i)] / r;
         double w = st[sidx(c, idW, HS + k, HS + j, HS + i)] / r;
         double t = (st[sidx(c, idT, HS + k, HS + j, HS + i)] + c->hyDensThetaCells[HS + k]) / r;
-        double p = C0 * pow(r * t, GAMMA);
+        double p = C0 * OPOW(r * t, GAMMA);
         double cs = sqrt(GAMMA * p / r);
         double udt = cfl * c->dx / dmax(fabs(u - cs), fabs(u + cs));
         double vdt = cfl * c->dy / dmax(fabs(v - cs), fabs(v + cs));

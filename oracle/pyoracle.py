@@ -35,16 +35,16 @@ def build(ref: bool = False) -> None:
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
-def oracle_path(ord_: int) -> str:
-    return os.path.join(HERE, "liboracle_o%d.so" % ord_)
+def oracle_path(ord_: int, crpow: bool = False) -> str:
+    return os.path.join(HERE, "liboracle_o%d%s.so" % (ord_, "_crpow" if crpow else ""))
 
 
-def ref_path(ord_: int) -> str:
-    return os.path.join(HERE, "_ref", "libawflref_o%d.so" % ord_)
+def ref_path(ord_: int, crpow: bool = False) -> str:
+    return os.path.join(HERE, "_ref", "libawflref_o%d%s.so" % (ord_, "_crpow" if crpow else ""))
 
 
-def ref_available(ord_: int = 5) -> bool:
-    return os.path.exists(ref_path(ord_))
+def ref_available(ord_: int = 5, crpow: bool = False) -> bool:
+    return os.path.exists(ref_path(ord_, crpow))
 
 
 class _Grid:
@@ -77,9 +77,10 @@ class Oracle(_Grid):
     _libs: dict = {}
 
     @classmethod
-    def lib(cls, ord_):
-        if ord_ not in cls._libs:
-            path = oracle_path(ord_)
+    def lib(cls, ord_, crpow=False):
+        key = (ord_, crpow)
+        if key not in cls._libs:
+            path = oracle_path(ord_, crpow)
             if not os.path.exists(path):
                 build()
             L = ctypes.CDLL(path)
@@ -105,13 +106,14 @@ class Oracle(_Grid):
             L.oracle_coefs_to_tv.restype = _D
             L.oracle_coefs_to_tv.argtypes = [_DP, _I]
             L.oracle_weno_coefs.argtypes = [_VP, _DP, _DP]
-            cls._libs[ord_] = L
-        return cls._libs[ord_]
+            cls._libs[key] = L
+        return cls._libs[key]
 
     def __init__(self, nx, ny, nz, xlen=20000.0, ylen=20000.0, zlen=10000.0, bc=(0, 0, 1),
-                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5):
+                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5, crpow=False):
+        """crpow: the variant with correctly rounded pow/exp in place of glibc's."""
         super().__init__(ord_, nx, ny, nz)
-        self.L = self.lib(ord_)
+        self.L = self.lib(ord_, crpow)
         self.h = self.L.oracle_create(nx, ny, nz, xlen, ylen, zlen, bc[0], bc[1], bc[2],
                                       int(weno_scalars), int(weno_winds), DATA_SPECS[data])
 
@@ -183,9 +185,10 @@ class RefHarness(_Grid):
     _libs: dict = {}
 
     @classmethod
-    def lib(cls, ord_):
-        if ord_ not in cls._libs:
-            path = ref_path(ord_)
+    def lib(cls, ord_, crpow=False):
+        key = (ord_, crpow)
+        if key not in cls._libs:
+            path = ref_path(ord_, crpow)
             if not os.path.exists(path):
                 raise FileNotFoundError(path + " (build with: make -C oracle ref)")
             L = ctypes.CDLL(path)
@@ -211,13 +214,15 @@ class RefHarness(_Grid):
             L.awflref_coefs_to_tv.restype = _D
             L.awflref_coefs_to_tv.argtypes = [_DP, _I]
             L.awflref_weno_coefs.argtypes = [_VP, _DP, _DP]
-            cls._libs[ord_] = L
-        return cls._libs[ord_]
+            cls._libs[key] = L
+        return cls._libs[key]
 
     def __init__(self, nx, ny, nz, xlen=20000.0, ylen=20000.0, zlen=10000.0, bc=(0, 0, 1),
-                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5):
+                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5, crpow=False):
+        """crpow: the reference's code with its pow/exp calls bound to a correctly rounded
+        implementation instead of glibc's."""
         super().__init__(ord_, nx, ny, nz)
-        self.L = self.lib(ord_)
+        self.L = self.lib(ord_, crpow)
         self.h = self.L.awflref_create(nx, ny, nz, xlen, ylen, zlen, bc[0], bc[1], bc[2],
                                        int(weno_scalars), int(weno_winds), data.encode())
         if not self.h:

@@ -10,9 +10,23 @@
 // The only arithmetic written here (not in the reference) is the BASELINE initial-data
 // extension: a cosine-squared bubble and seeded white theta noise, both integrated with
 // the same ord^3 GLL quadrature as Spatial...h:428-485.
+#ifdef AWFL_REF_CR_POW
+// Variant: the reference's own headers with the pow calls of the spatial operator (time
+// step and CFL) bound to a correctly rounded implementation (oracle/awfl_pow_cr.h) instead
+// of glibc's. const.h (hence <cmath>) and Profiles.h are included first, so the
+// hydrostatic profiles keep glibc's pow/exp and only the operator's call sites see the
+// macro.
+#include "const.h"
+#include "Profiles.h"
+#include "awfl_pow_cr.h"
+#define pow(a, b) awfl_test_pow_cr((a), (b))
+#endif
 #include "const.h"
 #include "Spatial_euler3d_cons_expl_cart_fv_Agrid.h"
 #include "Temporal_ader.h"
+#ifdef AWFL_REF_CR_POW
+#undef pow
+#endif
 
 #include <cstdint>
 #include <cstdio>

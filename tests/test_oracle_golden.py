@@ -102,3 +102,49 @@ def test_derived_tables(ord_):
     # derivMatrix: exact-math tables vs the reference's Sage literals, which carry
     # 129-bit round-off (gll_to_coefs<5>(2,1) = -2.35e-38 where the exact value is 0).
     assert np.max(np.abs(mine["deriv"] - t["deriv"])) <= 1e-37
+
+
+@pytest.mark.skipif(not __import__("oracle.pyoracle", fromlist=["x"]).ref_available(5, True),
+                    reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("ord_,bc,ws", [(5, (0, 0, 1), True), (5, (1, 1, 0), False), (9, (0, 0, 1), True)])
+def test_crpow_oracle_equals_crpow_reference(ord_, bc, ws):
+    """The oracle variant with a correctly rounded pow/exp is bit-identical to the
+    reference's own code built with the same pow/exp (oracle/_ref/*_crpow.so)."""
+    from oracle.pyoracle import RefHarness
+    n = (12, 10, 8)
+    R = RefHarness(*n, bc=bc, weno_scalars=ws, ord_=ord_, crpow=True)
+    O = Oracle(*n, bc=bc, weno_scalars=ws, ord_=ord_, crpow=True)
+    R.init_state()
+    R.set_bubble(1, 10000.0, 10000.0, 2000.0, 2500.0, 2500.0, 2500.0, 3.0, 1.0)
+    R.add_theta_noise(7, 0.01)
+    st = O.new_state()
+    O.init_state(st)
+    O.set_bubble(st, 1, 10000.0, 10000.0, 2000.0, 2500.0, 2500.0, 2500.0, 3.0, 1.0)
+    O.add_theta_noise(st, 7, 0.01)
+    assert np.array_equal(st, R.get_state())
+    dt = R.compute_dt(0.4)
+    assert O.compute_dt(st, 0.4) == dt
+    for _ in range(4):
+        R.time_step(dt)
+        O.time_step(st, dt)
+    assert np.array_equal(st, R.get_state())
+
+
+def test_glibc_pow_rounding_spread():
+    """The reference's sensitivity to last-bit pow rounding: glibc pow vs a correctly
+    rounded pow, same code, 32x32x16 bubble + noise, 20 steps. Documents the size of the
+    spread the FP64 GPU parity tolerance against the glibc build is based on."""
+    res = []
+    for cr in (False, True):
+        O = Oracle(32, 32, 16, crpow=cr)
+        st = O.new_state()
+        O.init_state(st)
+        O.set_bubble(st, 1, 10000.0, 10000.0, 2000.0, 2000.0, 2000.0, 2000.0, 3.0, 1.0)
+        O.add_theta_noise(st, 20261203, 0.01)
+        dt = O.compute_dt(st, 0.8)
+        for _ in range(20):
+            O.time_step(st, dt)
+        res.append(st[:, 2:-2, 2:-2, 2:-2])
+    spread = [np.linalg.norm(res[0][v] - res[1][v]) / np.linalg.norm(res[1][v]) for v in range(5)]
+    assert max(spread) > 0          # glibc's pow is not correctly rounded everywhere
+    assert max(spread) < 5e-12      # ... but only in the last bit
