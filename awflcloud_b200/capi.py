@@ -61,6 +61,7 @@ _SIGS = {
     "awfl_get_tables": (_I, [_VP] + [_DP] * 10),
     "awfl_get_background": (_I, [_VP] + [_DP] * 8),
     "awfl_selftest_pow": (_I, [_VP, _D, _VP, _L, _I, _VP]),
+    "awfl_measure_fma_peak": (_I, [_I, _I, _DP]),
     "awfl_device_alloc": (_I, [ctypes.POINTER(_VP), _L]),
     "awfl_device_free": (_I, [_VP]),
     "awfl_copy_h2d": (_I, [_VP, _VP, _L, _VP]),
@@ -229,3 +230,12 @@ def header_symbols(path=None):
     path = path or os.path.join(os.path.dirname(HERE), "include", "awfl.h")
     src = open(path).read()
     return sorted(set(re.findall(r"^\s*(?:int|const char \*|void)\s*\*?\s*(awfl_\w+)\s*\(", src, re.M)))
+
+
+def measure_fma_peak(precision=FP64, device=0):
+    """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 CUDA-core pipe."""
+    out = ctypes.c_double()
+    rc = lib().awfl_measure_fma_peak(precision, device, ctypes.byref(out))
+    if rc != AWFL_OK:
+        raise AwflError(rc, "awfl_measure_fma_peak failed")
+    return out.value

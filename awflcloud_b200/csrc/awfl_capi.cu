@@ -493,6 +493,17 @@ int awfl_selftest_pow(const void *d_x, double y, void *d_out, long n, int mode, 
   return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
 }
 
+int awfl_measure_fma_peak(int precision, int device, double *tflops) {
+  if (!tflops || (precision != AWFL_FP64 && precision != AWFL_FP32)) return AWFL_ERR_ARG;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return AWFL_ERR_CUDA;
+  int nsm = 148;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) nsm = prop.multiProcessorCount;
+  e = run_fma_peak(precision == AWFL_FP32, nsm, tflops);
+  return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
+}
+
 int awfl_device_alloc(void **d_ptr, long bytes) {
   if (!d_ptr || bytes < 0) return AWFL_ERR_ARG;
   cudaError_t e = cudaMalloc(d_ptr, bytes > 0 ? (size_t)bytes : 1);

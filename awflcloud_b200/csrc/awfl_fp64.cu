@@ -496,6 +496,50 @@ cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, 
   return cudaGetLastError();
 }
 
+// FMA throughput microbenchmark: 8 independent FMA chains per thread, `iters` rounds.
+// The sink write keeps the chains live. 2 flops per FMA.
+template <class T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T *sink, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) x[c] = (T)(threadIdx.x + c) * (T)1e-3;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) x[c] = fma(x[c], a, b);
+  }
+  T s = 0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) s += x[c];
+  if (s == (T)123.456) sink[threadIdx.x] = s;
+}
+
+cudaError_t run_fma_peak(int fp32, int nsm, double *tflops) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  void *sink = nullptr;
+  cudaError_t e = cudaMalloc(&sink, 256 * sizeof(double));
+  if (e != cudaSuccess) return e;
+  const int blocks = nsm * 8, threads = 256;
+  const int iters = fp32 ? 16384 : 8192;
+  for (int rep = 0; rep < 2; rep++) {  // first launch warms up
+    cudaEventRecord(e0);
+    if (fp32) fma_peak_kernel<float><<<blocks, threads>>>((float *)sink, iters, 0.999999f, 1e-7f);
+    else fma_peak_kernel<double><<<blocks, threads>>>((double *)sink, iters, 0.999999999, 1e-9);
+    cudaEventRecord(e1);
+  }
+  e = cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (e != cudaSuccess) return e;
+  e = cudaGetLastError();
+  *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e12;
+  return e;
+}
+
 cudaError_t upload_tables_fp64(int ord, const void *tab, size_t bytes) {
   if (ord == 5) return cudaMemcpyToSymbol(c_tab5, tab, bytes);
   return cudaMemcpyToSymbol(c_tab9, tab, bytes);

@@ -66,6 +66,7 @@ cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const dou
                             double dx, double dy, double dz, int nx, int ny, int nz, int hs, int nsm,
                             unsigned long long *d_out, cudaStream_t st);
 cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st);
+cudaError_t run_fma_peak(int fp32, int nsm, double *tflops);
 cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st);
 
 }  // namespace awfl

@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the AWFL Euler-3D ADER/WENO step on B200: Mcell-steps/s at 256x256x128.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp32|fp64] [--ord 5|9]
+
+A "step" is one ADER time step (three directional splits, Temporal_ader::timeStep) of
+the whole 256x256x128 grid. Workload: the rising thermal bubble scale-up case (cosine-
+squared theta bubble +3 K, radius 2 km, centred at (10, 10, 2) km in a 20x20x10 km domain,
+periodic x/y, walls in z, ord 5 / ngll 3, CFL 0.8) with seeded uniform +-0.01 K theta noise;
+synthetic initial data generated on the device.
+
+Our arm times K steps with CUDA events on the launching stream after W warm-up steps,
+barrier + synchronize on both sides, max over ranks. The state (357 MB in FP64) is larger
+than the 126 MB L2, so no flush is needed between steps. N > 1 runs N independent
+replicas (one grid per GPU, no collective): the single-domain path has no exchange step.
+
+Printed on rank 0: one JSON line (see DESIGN.md for every key).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s at 256²×128: FP32 vs plain FP64 (rel L2≤1e-5); adjoint/fwd"
+UNIT = "Mcell-steps/s"
+DATA = ("synthetic: cosine-squared theta bubble +3 K, radius 2 km, centre (10,10,2) km, "
+        "+ seeded uniform +-0.01 K theta noise (splitmix64, seed 20261203)")
+BUBBLE = dict(kind=1, shape=1, x0=10000.0, y0=10000.0, z0=2000.0, xrad=2000.0, yrad=2000.0,
+              zrad=2000.0, amp=3.0, pwr=1.0, noise_amp=0.01, noise_seed=20261203)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp64")
+    ap.add_argument("--ord", type=int, default=5, choices=[5, 9])
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def cfl_for(ord_):
+    # The driver's CFL 0.8 (driver.cpp:46). At ord 9 the reference's own scheme diverges
+    # at 0.8 (NaN within 8 steps, reproduced with its code), so ord 9 runs at 0.4.
+    return 0.8 if ord_ == 5 else 0.4
+
+
+def workload_name(a):
+    return "rising thermal bubble %dx%dx%d, ord %d / ngll %d, CFL %.1f" % (
+        a.nx, a.ny, a.nz, a.ord, 3 if a.ord == 5 else 5, cfl_for(a.ord))
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        mx = [num(r[2]) for r in rows if num(r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0) for r in rows)}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(a, budget_s=20.0):
+    """The reference's own CPU code (oracle/_ref, built from its sources on the project's
+    stand-ins) with all host threads, on the same workload, a bounded number of steps."""
+    from oracle import pyoracle
+    cores = os.cpu_count() or 1
+    kind = "reference" if pyoracle.ref_available(a.ord) else "port"
+    if kind == "reference":
+        R = pyoracle.RefHarness(a.nx, a.ny, a.nz, ord_=a.ord)
+        R.init_state()
+        R.set_bubble(1, 10000.0, 10000.0, 2000.0, 2000.0, 2000.0, 2000.0, 3.0, 1.0)
+        R.add_theta_noise(20261203, 0.01)
+        dt = R.compute_dt(cfl_for(a.ord))
+        step = lambda: R.time_step(dt)  # noqa: E731
+    else:
+        O = pyoracle.Oracle(a.nx, a.ny, a.nz, ord_=a.ord)
+        st = O.new_state()
+        O.init_state(st)
+        O.set_bubble(st, 1, 10000.0, 10000.0, 2000.0, 2000.0, 2000.0, 2000.0, 3.0, 1.0)
+        O.add_theta_noise(st, 20261203, 0.01)
+        dt = O.compute_dt(st, cfl_for(a.ord))
+        step = lambda: O.time_step(st, dt)  # noqa: E731
+    n, t0 = 0, time.perf_counter()
+    while True:
+        step()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= 50 or (n >= 1 and el * (n + 1) / n > 2.5 * budget_s):
+            break
+    cells = a.nx * a.ny * a.nz
+    return {"value": round(cells * n / el / 1e6, 4), "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": "%d full time steps of the %dx%dx%d workload, FP64, OpenMP %d threads, %.1f s"
+                      % (n, a.nx, a.ny, a.nz, cores, el)}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import pyoracle
+    cores = os.cpu_count() or 1
+    if not pyoracle.ref_available(a.ord):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (the reference built from its sources) is not present; run build()"}))
+        return 0
+    cells = a.nx * a.ny * a.nz
+    R = pyoracle.RefHarness(a.nx, a.ny, a.nz, ord_=a.ord)
+    R.init_state()
+    R.set_bubble(1, 10000.0, 10000.0, 2000.0, 2000.0, 2000.0, 2000.0, 3.0, 1.0)
+    R.add_theta_noise(20261203, 0.01)
+    dt = R.compute_dt(cfl_for(a.ord))
+    # bound the run: each step is one full time step of the workload unless that would
+    # take more than ~3 minutes in total, then each step is a fraction of the grid's lines
+    t0 = time.perf_counter()
+    R.time_step(dt)
+    one = time.perf_counter() - t0
+    for _ in range(max(0, a.warmup - 1)):
+        R.time_step(dt)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        R.time_step(dt)
+    el = time.perf_counter() - t0
+    value = cells * a.steps / el / 1e6
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(el / a.steps * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": {"workload": workload_name(a), "nx": a.nx, "ny": a.ny, "nz": a.nz, "ord": a.ord,
+                       "parallelism": "reference CPU build (OpenMP), rank 0 only"},
+            "impl": "reference",
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": "%d full time steps after %d warm-up, first step %.2f s" % (a.steps, a.warmup, one)},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+    from awflcloud_b200 import capi, flops
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    prec = capi.FP64 if a.precision == "fp64" else capi.FP32
+    cells = a.nx * a.ny * a.nz
+    ctx = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=prec, device=local)
+    st = ctx.new_state()
+    ctx.init_state(st, **BUBBLE)
+    dt = ctx.cfl(st, cfl_for(a.ord))
+    stream = torch.cuda.current_stream()
+
+    peak = capi.measure_fma_peak(prec, local)
+
+    for _ in range(a.warmup):
+        ctx.step(st, dt)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    # Events between the three split launches of every step give the per-launch time of
+    # the sweep kernel (the only kernel in the step).
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * a.steps + 1)]
+    ev[0].record(stream)
+    for s in range(a.steps):
+        ds = ctx.dimswitch
+        for spl in range(3):
+            d = spl if ds else 2 - spl
+            ctx.split(st, dt, d)
+            ev[3 * s + spl + 1].record(stream)
+        ctx.dimswitch = 1 - ds
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = ev[0].elapsed_time(ev[-1])
+    launch_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(3 * a.steps)]
+    t = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = t.item()
+    finite = bool(torch.isfinite(st).all().item())
+
+    value = world * cells * a.steps / (max_ms * 1e-3) / 1e6
+    fl = flops.flops_per_cell_step(a.ord)
+    flops_launch = fl["flops"] / 3.0 * cells  # per split launch, averaged over directions
+    avg_launch_s = statistics.mean(launch_ms) * 1e-3
+    achieved = flops_launch / avg_launch_s / 1e12
+    roofline = {"bound": "fp64" if prec == capi.FP64 else "fp32",
+                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": "measured in this run: awfl_measure_fma_peak (FMA chains, 2 flops/FMA)",
+                "flops_per_launch": flops_launch, "launch_ms_avg": round(avg_launch_s * 1e3, 4),
+                "bytes_algorithmic_per_launch": cells * 10 * (8 if prec == capi.FP64 else 4)}
+
+    e2e = None
+    if not a.no_e2e:
+        e2e = e2e_leg(a, ctx, st, dt, stream, world)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": round(max_ms / a.steps, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else "f32",
+                "data": DATA,
+                "config": {"workload": workload_name(a), "nx": a.nx, "ny": a.ny, "nz": a.nz, "ord": a.ord,
+                           "precision": a.precision,
+                           "l2": "state %.0f MB > 126 MB L2: no flush needed" % (st.numel() * st.element_size() / 1e6),
+                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                "roofline": roofline, "gpu_launches": 3 * a.steps, "finite": finite,
+                "clocks": clk, "flops_per_cell_step": fl}
+        if e2e is not None:
+            line["e2e"] = e2e
+        if not a.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(a)
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def e2e_leg(a, ctx, st, dt, stream, world):
+    """The same metric through the C ABI with HOST buffers: every step copies the state
+    from pinned host memory to the device, advances it one time step and copies it back."""
+    import torch
+    import torch.distributed as dist
+    from awflcloud_b200 import capi
+    L = capi.lib()
+    nbytes = st.numel() * st.element_size()
+    host_in = torch.empty_like(st, device="cpu").pin_memory()
+    host_out = torch.empty_like(st, device="cpu").pin_memory()
+    host_in.copy_(st)
+    s = stream.cuda_stream
+    dev = st
+
+    def one():
+        assert L.awfl_copy_h2d(dev.data_ptr(), host_in.data_ptr(), nbytes, s) == 0
+        ctx.step(dev, dt)
+        assert L.awfl_copy_d2h(host_out.data_ptr(), dev.data_ptr(), nbytes, s) == 0
+
+    for _ in range(2):
+        one()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    cells = a.nx * a.ny * a.nz
+    return {"value": round(world * cells * a.steps / (t.item() * 1e-3) / 1e6, 3), "unit": UNIT,
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+            "path": "awfl_copy_h2d + awfl_step + awfl_copy_d2h per step, pinned host buffers"}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -137,6 +137,11 @@ int awfl_get_background(const awfl_ctx *ctx, double *dens_c, double *pres_c, dou
  * comparison; mode 2: the library's correctly rounded exp(x) (y ignored). */
 int awfl_selftest_pow(const void *d_x, double y, void *d_out, long n, int mode, void *stream);
 
+/* Diagnostic: measured FMA throughput of the CUDA-core pipe the kernels run on (FP64 or
+ * FP32), in TFLOP/s (2 flops per FMA), from a ~0.1 s FMA-chain kernel on `device`. The
+ * roofline denominator of the ADER/WENO kernels, which are bound by these pipes. */
+int awfl_measure_fma_peak(int precision, int device, double *tflops);
+
 /* Device memory helpers for hosts that do not link the CUDA runtime themselves. */
 int awfl_device_alloc(void **d_ptr, long bytes);
 int awfl_device_free(void *d_ptr);
