@@ -6,6 +6,7 @@ Translation units and their numerics flags:
   awfl_fp64.cu  FP64 kernels: --fmad=false (no contracted multiply-add, like the
                 reference CPU build)
   awfl_fp32.cu  FP32 precision form (when present): contraction allowed
+  awfl_noalloc.cu  allocation-free CFL variant: --fmad=false (same arithmetic as awfl_cfl)
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
 source tree. ``python -m awflcloud_b200.build [--force]``.
@@ -31,6 +32,7 @@ UNITS = {
     "awfl_capi.cu": ["--fmad=false"],
     "awfl_fp64.cu": ["--fmad=false"],
     "awfl_fp32.cu": ["--fmad=true"],
+    "awfl_noalloc.cu": ["--fmad=false"],
 }
 
 

@@ -62,6 +62,7 @@ _SIGS = {
     "awfl_get_background": (_I, [_VP] + [_DP] * 8),
     "awfl_selftest_pow": (_I, [_VP, _D, _VP, _L, _I, _VP]),
     "awfl_measure_fma_peak": (_I, [_I, _I, _DP]),
+    "awfl_cfl_noalloc": (_I, [ctypes.POINTER(AwflConfig), _VP, _VP, _VP, _D, _DP, _VP]),
     "awfl_device_alloc": (_I, [ctypes.POINTER(_VP), _L]),
     "awfl_device_free": (_I, [_VP]),
     "awfl_copy_h2d": (_I, [_VP, _VP, _L, _VP]),

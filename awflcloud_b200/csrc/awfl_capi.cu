@@ -53,6 +53,13 @@ int fail(awfl_ctx *c, int code, const char *fmt, ...) {
   return code;
 }
 
+}  // namespace
+
+// Error message for entry points that have no context (read by awfl_last_error(NULL)).
+void awfl::set_unbound_error(const char *msg) { g_create_error = msg; }
+
+namespace {
+
 int cuda_fail(awfl_ctx *c, cudaError_t e, const char *what) {
   return fail(c, AWFL_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }

@@ -57,6 +57,9 @@ struct InitLaunch {
   double pts[9], wts[9];
 };
 
+// Error message for entry points without a context (awfl_capi.cu).
+void set_unbound_error(const char *msg);
+
 // FP64 translation unit (awfl_fp64.cu)
 cudaError_t upload_tables_fp64(int ord, const void *tab, size_t bytes);
 cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st);

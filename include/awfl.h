@@ -131,6 +131,22 @@ int awfl_get_background(const awfl_ctx *ctx, double *dens_c, double *pres_c, dou
                         double *denstheta_c, double *dens_g, double *pres_g, double *theta_g,
                         double *denstheta_g);
 
+/* Allocation-free CFL time step. No counterpart in the reference: it is an extra entry
+ * point for callers that cannot call cudaMalloc -- hosts whose device memory all comes
+ * from their own arena or pool and must not be allocated behind their back, or loops that
+ * cannot afford the device synchronisation an allocation may cause. It needs no context
+ * and allocates nothing: the caller passes the FP64 state and the device copies of the
+ * hydrostatic cell averages hyDensCells and hyDensThetaCells (nz+2hs each, as returned by
+ * awfl_get_background), and the reduction runs in a static device array of the library
+ * (512 KiB per GPU that loads it, held until exit). Result: the same value as awfl_cfl.
+ * Limits: FP64 only; nx*ny*nz <= 16,777,216 cells, larger grids are rejected with
+ * AWFL_ERR_ARG (use awfl_cfl). The first call on each device looks up the array's device
+ * address; make that first call before any stream capture. Every call shares the one
+ * array: calls that overlap on the GPU (other streams, other host threads) race.
+ * Synchronises `stream`. Errors are reported by awfl_last_error(NULL). */
+int awfl_cfl_noalloc(const awfl_config *cfg, const void *d_state, const void *d_hy_dens_cells,
+                     const void *d_hy_denstheta_cells, double cfl, double *h_dt, void *stream);
+
 /* Diagnostic: the FP64 path's device math on n doubles (device pointers). mode 0:
  * out = pow(x, y) by the library's correctly rounded pow (the one every FP64 kernel uses
  * in place of the reference's glibc pow); mode 1: the CUDA math library's pow, for
