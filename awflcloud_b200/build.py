@@ -5,7 +5,7 @@ Translation units and their numerics flags:
                 to the reference CPU build)
   awfl_fp64.cu  FP64 kernels: --fmad=false (no contracted multiply-add, like the
                 reference CPU build)
-  awfl_fp32.cu  FP32 precision form (when present): contraction allowed
+  awfl_fp32.cu  FP32 precision form: contraction, approximate division/sqrt, flush-to-zero
   awfl_noalloc.cu  allocation-free CFL variant: --fmad=false (same arithmetic as awfl_cfl)
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
@@ -31,7 +31,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 UNITS = {
     "awfl_capi.cu": ["--fmad=false"],
     "awfl_fp64.cu": ["--fmad=false"],
-    "awfl_fp32.cu": ["--fmad=true"],
+    "awfl_fp32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "awfl_noalloc.cu": ["--fmad=false"],
 }
 

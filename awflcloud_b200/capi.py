@@ -154,8 +154,10 @@ class Context:
     # ---- shapes
     @property
     def state_shape(self):
+        """FP64: (5, nz+2hs, ny+2hs, nx+2hs). FP32: (10, ...) -- the value plane (5
+        variables) followed by the Kahan compensation plane."""
         h = 2 * self.hs
-        return (5, self.nz + h, self.ny + h, self.nx + h)
+        return (5 if self.precision == FP64 else 10, self.nz + h, self.ny + h, self.nx + h)
 
     @property
     def tend_shape(self):
@@ -171,29 +173,51 @@ class Context:
         dt = torch.float64 if self.precision == FP64 else torch.float32
         return torch.zeros(self.tend_shape, dtype=dt, device="cuda:%d" % max(self.device, 0))
 
+    # ---- argument checks (the C ABI cannot see allocation sizes)
+    def _dtype(self):
+        import torch
+        return torch.float64 if self.precision == FP64 else torch.float32
+
+    def _check_buf(self, x, shape, what):
+        if isinstance(x, int) or x is None:
+            return  # raw device address: the caller vouches for its size
+        import math
+        need = math.prod(shape)
+        if x.numel() < need or not x.is_contiguous() or x.dtype != self._dtype() or not x.is_cuda:
+            raise ValueError("%s must be a contiguous CUDA %s tensor with >= %d elements (got %s %s %s)"
+                             % (what, self._dtype(), need, tuple(x.shape), x.dtype, x.device))
+
+    def _st(self, x):
+        self._check_buf(x, self.state_shape, "state")
+        return _ptr(x)
+
+    def _td(self, x):
+        self._check_buf(x, self.tend_shape, "tendency")
+        return _ptr(x)
+
     # ---- entry points
     def init_state(self, state, kind=INIT_REFERENCE, shape=1, x0=10000.0, y0=10000.0, z0=2000.0,
                    xrad=2000.0, yrad=2000.0, zrad=2000.0, amp=3.0, pwr=1.0, noise_amp=0.0,
                    noise_seed=20261203, stream=None):
         spec = AwflInitSpec(kind, shape, x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp, noise_seed)
-        self._check(self.L.awfl_init_state(self.h, _ptr(state), ctypes.byref(spec), _stream(stream)))
+        self._check(self.L.awfl_init_state(self.h, self._st(state), ctypes.byref(spec), _stream(stream)))
 
     def cfl(self, state, cfl=0.8, stream=None):
         out = ctypes.c_double()
-        self._check(self.L.awfl_cfl(self.h, _ptr(state), cfl, ctypes.byref(out), _stream(stream)))
+        self._check(self.L.awfl_cfl(self.h, self._st(state), cfl, ctypes.byref(out), _stream(stream)))
         return out.value
 
     def compute_tendencies(self, state, tend, dt, d, stream=None):
-        self._check(self.L.awfl_compute_tendencies(self.h, _ptr(state), _ptr(tend), dt, d, _stream(stream)))
+        self._check(self.L.awfl_compute_tendencies(self.h, self._st(state), self._td(tend), dt, d, _stream(stream)))
 
     def apply_tendencies(self, state, tend, dt, stream=None):
-        self._check(self.L.awfl_apply_tendencies(self.h, _ptr(state), _ptr(tend), dt, _stream(stream)))
+        self._check(self.L.awfl_apply_tendencies(self.h, self._st(state), self._td(tend), dt, _stream(stream)))
 
     def split(self, state, dt, d, stream=None):
-        self._check(self.L.awfl_split(self.h, _ptr(state), dt, d, _stream(stream)))
+        self._check(self.L.awfl_split(self.h, self._st(state), dt, d, _stream(stream)))
 
     def step(self, state, dt, stream=None):
-        self._check(self.L.awfl_step(self.h, _ptr(state), dt, _stream(stream)))
+        self._check(self.L.awfl_step(self.h, self._st(state), dt, _stream(stream)))
 
     @property
     def dimswitch(self):

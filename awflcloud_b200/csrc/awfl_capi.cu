@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/awfl.h"
+#include "awfl_fp32_args.h"
 #include "awfl_internal.h"
 #include "awfl_tables.h"
 
@@ -35,6 +36,9 @@ struct awfl_ctx {
   double *d_dens_c = nullptr, *d_denstheta_c = nullptr, *d_dens_g = nullptr, *d_denstheta_g = nullptr,
          *d_pres_g = nullptr;
   unsigned long long *d_cfl = nullptr;  // CFL reduction result (8 bytes)
+  // FP32 form: FP32 copies of FP64 background constants (awfl_fp32_args.h)
+  float *d_bg32 = nullptr;
+  Bg32 bg32{};
   std::string err;
 };
 
@@ -221,8 +225,74 @@ int ensure_tables(awfl_ctx *c) {
     e = upload_tables_fp64(9, &t, sizeof t);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "upload of transform tables");
+  e = upload_tables_fp32(c->cfg.ord, c->recon.data(), c->c2g.data(), c->s2g.data(), c->deriv.data(), c->idl.data(),
+                         c->sigma, c->wts_ngll.data());
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload of FP32 transform tables");
   if (c->device >= 0 && c->device < 256) g_tab_uploaded[c->device] |= bit;
   return AWFL_OK;
+}
+
+// FP32 background constants from the FP64 background (awfl_fp32_args.h): rows (nz+2hs) of
+// rho_h, (rho theta)_h, its inverse and C0*(rho theta)_h^gamma; the same per GLL point and
+// per z face. The top GLL point of cell k and the bottom point of cell k+1 are the same
+// height, so both take the face value.
+int build_bg32(awfl_ctx *c) {
+  const int nz = c->cfg.nz, hs = c->hs, g = c->ngll;
+  const size_t nr = nz + 2 * hs, ng = (size_t)nz * g, nf = nz + 1;
+  std::vector<float> h(4 * (nr + ng + nf));
+  float *rho_c = h.data(), *rt_c = rho_c + nr, *irt_c = rt_c + nr, *p_c = irt_c + nr;
+  float *rho_g = p_c + nr, *rt_g = rho_g + ng, *irt_g = rt_g + ng, *p_g = irt_g + ng;
+  float *rho_f = p_g + ng, *rt_f = rho_f + nf, *irt_f = rt_f + nf, *p_f = irt_f + nf;
+  for (size_t k = 0; k < nr; k++) {
+    rho_c[k] = (float)c->dens_c[k];
+    rt_c[k] = (float)c->denstheta_c[k];
+    irt_c[k] = (float)(1.0 / c->denstheta_c[k]);
+    p_c[k] = (float)(kC0 * pow(c->denstheta_c[k], kGAMMA));
+  }
+  for (int f = 0; f <= nz; f++) {
+    const size_t i = f < nz ? (size_t)f * g : (size_t)(nz - 1) * g + (g - 1);
+    rho_f[f] = (float)c->dens_g[i];
+    rt_f[f] = (float)c->denstheta_g[i];
+    irt_f[f] = (float)(1.0 / c->denstheta_g[i]);
+    p_f[f] = (float)c->pres_g[i];
+  }
+  for (int k = 0; k < nz; k++)
+    for (int s = 0; s < g; s++) {
+      const size_t i = (size_t)k * g + s;
+      if (s == 0 || s == g - 1) {
+        const int f = s == 0 ? k : k + 1;
+        rho_g[i] = rho_f[f]; rt_g[i] = rt_f[f]; irt_g[i] = irt_f[f]; p_g[i] = p_f[f];
+      } else {
+        rho_g[i] = (float)c->dens_g[i];
+        rt_g[i] = (float)c->denstheta_g[i];
+        irt_g[i] = (float)(1.0 / c->denstheta_g[i]);
+        p_g[i] = (float)c->pres_g[i];
+      }
+    }
+  cudaError_t e = cudaMalloc(&c->d_bg32, h.size() * sizeof(float));
+  if (e != cudaSuccess) return fail(c, AWFL_ERR_NOMEM, "cudaMalloc FP32 background: %s", cudaGetErrorString(e));
+  e = cudaMemcpy(c->d_bg32, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload FP32 background");
+  float *d = c->d_bg32;
+  auto at = [&](float *hp) { return d + (hp - h.data()); };
+  c->bg32 = Bg32{at(rho_c), at(rt_c), at(irt_c), at(p_c), at(rho_g), at(rt_g), at(irt_g), at(p_g),
+                 at(rho_f), at(rt_f), at(irt_f), at(p_f)};
+  return AWFL_OK;
+}
+
+SweepArgs32 sweep_args32(awfl_ctx *c, void *state, void *tend, double dt, int dir, int mode) {
+  SweepArgs32 A;
+  const long n = 5L * (c->cfg.nz + 2 * c->hs) * (c->cfg.ny + 2 * c->hs) * (c->cfg.nx + 2 * c->hs);
+  A.state = (float *)state;
+  A.comp = (float *)state + n;
+  A.tend = (float *)tend;
+  A.nx = c->cfg.nx; A.ny = c->cfg.ny; A.nz = c->cfg.nz;
+  A.bc = dir == 0 ? c->cfg.bc_x : (dir == 1 ? c->cfg.bc_y : c->cfg.bc_z);
+  A.weno_s = c->cfg.weno_scalars; A.weno_w = c->cfg.weno_winds; A.sim2d = c->sim2d; A.mode = mode;
+  A.inv_dxd = (float)(1.0 / (dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz)));
+  A.dt = (float)dt;
+  A.bg = c->bg32;
+  return A;
 }
 
 int set_device(awfl_ctx *c) {
@@ -253,6 +323,12 @@ SweepArgs sweep_args(awfl_ctx *c, void *state, void *tend, double dt, int dir, i
 
 bool bad_ptr(const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 7) != 0; }
 
+bool fp32(const awfl_ctx *c) { return c->cfg.precision == AWFL_FP32; }
+
+long state_plane(const awfl_ctx *c) {
+  return 5L * (c->cfg.nz + 2 * c->hs) * (c->cfg.ny + 2 * c->hs) * (c->cfg.nx + 2 * c->hs);
+}
+
 }  // namespace
 
 extern "C" {
@@ -268,7 +344,7 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   if (!cfg || !out) return fail(nullptr, AWFL_ERR_ARG, "awfl_create: NULL argument");
   *out = nullptr;
   if (cfg->ord != 5 && cfg->ord != 9) return fail(nullptr, AWFL_ERR_ARG, "ord must be 5 or 9 (got %d)", cfg->ord);
-  if (cfg->precision != AWFL_FP64)
+  if (cfg->precision != AWFL_FP64 && cfg->precision != AWFL_FP32)
     return fail(nullptr, AWFL_ERR_NOT_BUILT, "precision %d is not available in this build", cfg->precision);
   const int hs = (cfg->ord - 1) / 2;
   if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(nullptr, AWFL_ERR_ARG, "nx, ny, nz must be >= 1");
@@ -331,6 +407,10 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   h.insert(h.end(), c->pres_g.begin(), c->pres_g.end());
   e = cudaMemcpy(c->d_bg, h.data(), nbg * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cuda_fail(nullptr, e, "upload background"); g_create_error = "upload background: " + std::string(cudaGetErrorString(e)); cudaFree(c->d_bg); delete c; return AWFL_ERR_CUDA; }
+  if (cfg->precision == AWFL_FP32) {
+    rc = build_bg32(c);
+    if (rc) { g_create_error = c->err; cudaFree(c->d_bg); if (c->d_bg32) cudaFree(c->d_bg32); delete c; return rc; }
+  }
   *out = c;
   return AWFL_OK;
 }
@@ -340,6 +420,7 @@ int awfl_destroy(awfl_ctx *c) {
   if (c->d_bg && c->device >= 0) {
     set_device(c);
     cudaFree(c->d_bg);
+    if (c->d_bg32) cudaFree(c->d_bg32);
   }
   delete c;
   return AWFL_OK;
@@ -348,7 +429,8 @@ int awfl_destroy(awfl_ctx *c) {
 int awfl_sizes(const awfl_ctx *c, long *state_elems, long *tend_elems, int *hs) {
   if (!c) return AWFL_ERR_ARG;
   const int h = c->hs;
-  if (state_elems) *state_elems = 5L * (c->cfg.nz + 2 * h) * (c->cfg.ny + 2 * h) * (c->cfg.nx + 2 * h);
+  // FP32 contexts: value plane followed by the Kahan compensation plane
+  if (state_elems) *state_elems = (fp32(c) ? 2L : 1L) * 5L * (c->cfg.nz + 2 * h) * (c->cfg.ny + 2 * h) * (c->cfg.nx + 2 * h);
   if (tend_elems) *tend_elems = 5L * c->cfg.nz * c->cfg.ny * c->cfg.nx;
   if (hs) *hs = h;
   return AWFL_OK;
@@ -378,6 +460,10 @@ int awfl_init_state(awfl_ctx *c, void *d_state, const awfl_init_spec *spec, void
   InitLaunch L;
   std::memset(&L, 0, sizeof L);
   L.state = d_state;
+  if (fp32(c)) {
+    L.state32 = (float *)d_state;
+    L.comp32 = (float *)d_state + state_plane(c);
+  }
   L.nx = c->cfg.nx; L.ny = c->cfg.ny; L.nz = c->cfg.nz; L.hs = c->hs; L.ord = c->cfg.ord;
   L.dx = c->dx; L.dy = c->dy; L.dz = c->dz; L.xlen = c->cfg.xlen; L.ylen = c->cfg.ylen; L.zlen = c->cfg.zlen;
   L.data_spec = c->cfg.data_spec; L.sim2d = c->sim2d;
@@ -403,8 +489,12 @@ int awfl_cfl(awfl_ctx *c, const void *d_state, double cfl, double *h_dt, void *s
   static const unsigned long long inf_bits = 0x7ff0000000000000ULL;
   cudaError_t e = cudaMemcpyAsync(c->d_cfl, &inf_bits, sizeof inf_bits, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_fail(c, e, "awfl_cfl init");
-  e = launch_cfl_fp64((const double *)d_state, c->d_dens_c, c->d_denstheta_c, cfl, c->dx, c->dy, c->dz, c->cfg.nx,
-                      c->cfg.ny, c->cfg.nz, c->hs, c->nsm, c->d_cfl, st);
+  if (fp32(c))
+    e = launch_cfl_fp32((const float *)d_state, c->d_dens_c, c->d_denstheta_c, cfl, c->dx, c->dy, c->dz, c->cfg.nx,
+                        c->cfg.ny, c->cfg.nz, c->hs, c->nsm, c->d_cfl, st);
+  else
+    e = launch_cfl_fp64((const double *)d_state, c->d_dens_c, c->d_denstheta_c, cfl, c->dx, c->dy, c->dz, c->cfg.nx,
+                        c->cfg.ny, c->cfg.nz, c->hs, c->nsm, c->d_cfl, st);
   if (e != cudaSuccess) return cuda_fail(c, e, "cfl kernel");
   unsigned long long bits = 0;
   e = cudaMemcpyAsync(&bits, c->d_cfl, sizeof bits, cudaMemcpyDeviceToHost, st);
@@ -426,7 +516,9 @@ int awfl_compute_tendencies(awfl_ctx *c, void *d_state, void *d_tend, double dt,
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
   if (dir == 1 && c->sim2d) {  // Spatial:573-576: the Y tendency is zero in 2-D
-    e = cudaMemsetAsync(d_tend, 0, sizeof(double) * 5L * c->cfg.nz * c->cfg.ny * c->cfg.nx, st);
+    e = cudaMemsetAsync(d_tend, 0, (fp32(c) ? sizeof(float) : sizeof(double)) * 5L * c->cfg.nz * c->cfg.ny * c->cfg.nx, st);
+  } else if (fp32(c)) {
+    e = launch_sweep_fp32(c->cfg.ord, dir, sweep_args32(c, d_state, d_tend, dt, dir, MODE_TEND), st);
   } else {
     e = launch_sweep_fp64(c->cfg.ord, dir, sweep_args(c, d_state, d_tend, dt, dir, MODE_TEND), st);
   }
@@ -439,8 +531,13 @@ int awfl_apply_tendencies(awfl_ctx *c, void *d_state, const void *d_tend, double
   if (bad_ptr(d_state) || bad_ptr(d_tend)) return fail(c, AWFL_ERR_ARG, "state/tend pointer is NULL or misaligned");
   int rc = set_device(c);
   if (rc) return rc;
-  cudaError_t e = launch_apply_fp64((double *)d_state, (const double *)d_tend, dt, c->cfg.nx, c->cfg.ny, c->cfg.nz,
-                                    c->hs, c->nsm, (cudaStream_t)stream);
+  cudaError_t e;
+  if (fp32(c))
+    e = launch_apply_fp32((float *)d_state, (float *)d_state + state_plane(c), (const float *)d_tend, (float)dt,
+                          c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs, c->nsm, (cudaStream_t)stream);
+  else
+    e = launch_apply_fp64((double *)d_state, (const double *)d_tend, dt, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs,
+                          c->nsm, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "apply_tendencies");
   return AWFL_OK;
 }
@@ -452,8 +549,11 @@ int awfl_split(awfl_ctx *c, void *d_state, double dt, int dir, void *stream) {
   int rc = set_device(c);
   if (rc) return rc;
   if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendency: the state is unchanged
-  cudaError_t e = launch_sweep_fp64(c->cfg.ord, dir, sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY),
-                                    (cudaStream_t)stream);
+  cudaError_t e = fp32(c)
+                      ? launch_sweep_fp32(c->cfg.ord, dir, sweep_args32(c, d_state, nullptr, dt, dir, MODE_APPLY),
+                                          (cudaStream_t)stream)
+                      : launch_sweep_fp64(c->cfg.ord, dir, sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY),
+                                          (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "split");
   return AWFL_OK;
 }

@@ -2,8 +2,8 @@
 // Compiled with --fmad=false: no multiply-add contraction, matching the reference's CPU build.
 //
 // Kernel map (reference kernels it replaces, Spatial = Spatial_euler3d_cons_expl_cart_fv_Agrid.h):
-//   sweep_kernel<ORD,DIR>  K1 halo fill + K2 recon/ADER + K3 edge BCs + K4 Riemann +
-//                          K5 divergence (+ K6 apply when fused), one direction
+//   sweep_kernel<P64,ORD,DIR>  (awfl_sweep.cuh) K1 halo fill + K2 recon/ADER + K3 edge BCs +
+//                          K4 Riemann + K5 divergence (+ K6 apply when fused), one direction
 //                          (Spatial:631-957 x, 994-1310 y, 1351-1696 z; Temporal_ader.h:63-65)
 //   apply_kernel           K6 apply alone (Temporal_ader.h:63-65)
 //   cfl_kernel             K0 CFL time step (Spatial:169-183)
@@ -12,257 +12,46 @@
 
 #include "awfl_device.cuh"
 #include "awfl_internal.h"
+#include "awfl_sweep.cuh"
 
 namespace awfl {
 
 // ------------------------------------------------------------------------------------
-// The line sweep.
-//
-// A CTA owns W whole lines along the sweep direction DIR and marches along them in
-// chunks of C cells. Because no other CTA touches those lines, the tendency can be
-// applied in place (MODE_APPLY) with no race: every stencil value a chunk reads comes
-// from a shared-memory ring holding the ORIGINAL values of positions
-// [base-HS, base+C+HS), refilled one chunk ahead of the updates, and the first HS rows
-// (needed again by the periodic wrap at the end of the line) are saved before they are
-// overwritten.
-//
-// Per chunk: (A) store the prefetched ring rows; (B) reconstruct cells base..base+C-1
-// -> left/right edge states; (C) Riemann flux at their left faces (the left state of
-// the first face is carried from the previous chunk); (D) divergence and update of
-// cells base-1..base+C-2 (the last cell's right face is computed in the next chunk),
-// while the next chunk's rows are prefetched into registers. The last cell of the line
-// is finished after the loop.
-//
-// Boundary handling reproduces the reference's halo fill (Spatial:631-662 etc.) and
-// edge-value BCs (Spatial:816-837 etc.): periodic wraps; a wall copies the edge cell
-// with zero normal momentum, and its boundary face uses the interior state on both
-// sides. The halo values are also written to the state's halo cells, as the reference
-// does in place.
+// FP64 physics policy of the line sweep (awfl_sweep.cuh): the reference's arithmetic.
 // ------------------------------------------------------------------------------------
-template <int ORD, int DIR, int C, int W>
-__global__ void __launch_bounds__(C *W) sweep_kernel(SweepArgs A) {
-  constexpr int HS = (ORD - 1) / 2;
-  constexpr int NG = OrdTraits<ORD>::NGLL;
-  constexpr int R = 2 * C;  // ring length (power of two, >= C + 2*HS)
-  constexpr int NM = 1 + DIR;
-  static_assert((C & (C - 1)) == 0 && C >= 2 * HS, "chunk must be a power of two >= 2*HS");
+struct P64 {
+  using Real = double;
+  using Args = SweepArgs;
 
-  __shared__ double ring[5][R * W];
-  __shared__ double sEL[5][C * W];
-  __shared__ double sER[5][(C + 1) * W];
-  __shared__ double sF[5][(C + 1) * W];
-  __shared__ double sSrc[DIR == 2 ? (C + 1) * W : 1];
-  __shared__ double sWrap[5][HS * W];
-  __shared__ double sEL0[5][W];
-
-  const int c = DIR == 0 ? threadIdx.x : threadIdx.y;  // position in chunk
-  const int w = DIR == 0 ? threadIdx.y : threadIdx.x;  // line within CTA
-
-  const int nx = A.nx, ny = A.ny, nz = A.nz;
-  const long sx = 1, sy = nx + 2 * HS, sz = (long)(ny + 2 * HS) * sy, sv = (long)(nz + 2 * HS) * sz;
-  int L, kline = 0;
-  bool valid;
-  long lb;  // offset of (v=0, position 0 along DIR) of this line, halo-inclusive frame
-  long sd;  // stride along DIR
-  long tb;  // tendency offset of position 0
-  long tsd;
-  if (DIR == 0) {
-    const int k = blockIdx.y, j = blockIdx.x * W + w;
-    L = nx; valid = j < ny; kline = k;
-    lb = (HS + k) * sz + (HS + (valid ? j : 0)) * sy + HS * sx; sd = sx;
-    tb = ((long)k * ny + (valid ? j : 0)) * nx; tsd = 1;
-  } else if (DIR == 1) {
-    const int k = blockIdx.y, i = blockIdx.x * W + w;
-    L = ny; valid = i < nx; kline = k;
-    lb = (HS + k) * sz + HS * sy + HS + (valid ? i : 0); sd = sy;
-    tb = (long)k * ny * nx + (valid ? i : 0); tsd = nx;
-  } else {
-    const int j = blockIdx.y, i = blockIdx.x * W + w;
-    L = nz; valid = i < nx;
-    lb = HS * sz + (HS + j) * sy + HS + (valid ? i : 0); sd = sz;
-    tb = (long)j * nx + (valid ? i : 0); tsd = (long)ny * nx;
-  }
-  const long tv = (long)nz * ny * nx;
-  const bool periodic = A.bc == BC_PERIODIC;
-
-  auto G = [&](int v, int p) -> double { return A.state[lb + v * sv + p * sd]; };
-  auto ringAt = [&](int v, int p) -> double & {
-    const int s = p & (R - 1);
-    return DIR == 0 ? ring[v][w * R + s] : ring[v][s * W + w];
-  };
-  auto topval = [&](int v, int p, bool first) -> double {  // p >= L
-    const int q = p - L;
-    if (q >= HS) return 0.0;  // beyond the last cell's stencil: never read
-    if (periodic) return first ? G(v, q) : sWrap[v][q * W + w];
-    return v == NM ? 0.0 : G(v, L - 1);
-  };
-  auto stenIdx = [&](int v, int p) -> double { return ringAt(v, p); };
-
-  // ---- prologue: bottom halo, saved wrap rows, top halo; chunk-0 prefetch
-  if (valid && c < HS) {
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      const double bot = periodic ? G(v, L + c - HS) : (v == NM ? 0.0 : G(v, 0));
-      const double orig = G(v, c);
-      const double top = periodic ? orig : (v == NM ? 0.0 : G(v, L - 1));
-      ringAt(v, c - HS) = bot;
-      ringAt(v, c) = orig;
-      sWrap[v][c * W + w] = orig;
-      A.state[lb + v * sv + (c - HS) * sd] = bot;
-      A.state[lb + v * sv + (L + c) * sd] = top;
-    }
-  }
-  double pre[5];
-  if (valid) {
-    const int p = HS + c;
-#pragma unroll
-    for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, true);
-  }
-  // periodic: the left state of face 0 is the right edge of cell L-1
-  if (valid && periodic && c == 0) {
-    auto wrapSten = [&](int v, int m) -> double {
-      int p = L - 1 - HS + m;
-      p %= L;
-      if (p < 0) p += L;
-      return G(v, p);
-    };
-    double eL[5], eR[5], sa;
-    cell_recon<ORD, DIR>(wrapSten, DIR == 2 ? L - 1 : kline, A, eL, eR, sa);
-#pragma unroll
-    for (int v = 0; v < 5; v++) sER[v][0 * W + w] = eR[v];
+  template <int ORD, int DIR, class S>
+  static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],
+                                               double (&eR)[5], double &src) {
+    cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
   }
 
-  const int nchunk = (L + C - 1) / C;
-  for (int t = 0; t < nchunk; t++) {
-    const int base = t * C;
-    const int nvalid = min(C, L - base);
-    if (valid) {
-#pragma unroll
-      for (int v = 0; v < 5; v++) ringAt(v, base + HS + c) = pre[v];
-    }
-    __syncthreads();  // (A)
-    if (valid && c < nvalid) {
-      const int p = base + c;
-      auto sten = [&](int v, int m) -> double { return stenIdx(v, p - HS + m); };
-      double eL[5], eR[5], sa;
-      cell_recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa);
-#pragma unroll
-      for (int v = 0; v < 5; v++) {
-        sEL[v][c * W + w] = eL[v];
-        sER[v][(c + 1) * W + w] = eR[v];
-      }
-      if (DIR == 2) sSrc[(c + 1) * W + w] = sa;
-      if (p == 0) {
-#pragma unroll
-        for (int v = 0; v < 5; v++) sEL0[v][w] = eL[v];
-      }
-    }
-    __syncthreads();  // (B)
-    if (valid && c < nvalid) {
-      const int f = base + c;  // face index = left face of cell f
-      double qL[5], qR[5], F[5];
-#pragma unroll
-      for (int v = 0; v < 5; v++) qR[v] = sEL[v][c * W + w];
-#pragma unroll
-      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][c * W + w];
-      riemann<DIR, NG>(qL, qR, f, A, F);
-#pragma unroll
-      for (int v = 0; v < 5; v++) sF[v][(c + 1) * W + w] = F[v];
-    }
-    __syncthreads();  // (C)
-    if (valid && c < nvalid) {
-      const int cell = base + c - 1;
-      if (cell >= 0) {
-        const double sa = DIR == 2 ? sSrc[c * W + w] : 0.0;
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-          const double Fl = sF[v][c * W + w], Fr = sF[v][(c + 1) * W + w];
-          const double d = -(Fr - Fl) / A.dxd;
-          double tnd;
-          if (DIR == 0) tnd = (A.sim2d && v == idV) ? 0.0 : d;
-          else if (DIR == 1) tnd = d;
-          else tnd = (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;
-          if (A.mode == MODE_APPLY) {
-            A.state[lb + v * sv + cell * sd] = ringAt(v, cell) + A.dt * tnd;
-          } else {
-            A.tend[tb + v * tv + cell * tsd] = tnd;
-          }
-        }
-      }
-    }
-    if (valid && t + 1 < nchunk) {
-      const int p = base + C + HS + c;
-#pragma unroll
-      for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
-    }
-    __syncthreads();  // (D)
-    if (valid && c == 0) {
-#pragma unroll
-      for (int v = 0; v < 5; v++) {
-        sER[v][w] = sER[v][nvalid * W + w];
-        sF[v][w] = sF[v][nvalid * W + w];
-      }
-      if (DIR == 2) sSrc[w] = sSrc[nvalid * W + w];
-    }
+  template <int DIR, int NG>
+  static __device__ __forceinline__ void flux(const double (&qL)[5], const double (&qR)[5], int kf, const Args &A,
+                                              double (&F)[5]) {
+    riemann<DIR, NG>(qL, qR, kf, A, F);
   }
-  // ---- epilogue: face L and the last cell (same thread that wrote the carry)
-  if (valid && c == 0) {
-    double qL[5], qR[5], F[5];
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      qL[v] = sER[v][w];
-      qR[v] = periodic ? sEL0[v][w] : qL[v];
-    }
-    riemann<DIR, NG>(qL, qR, L, A, F);
-    const int cell = L - 1;
-    const double sa = DIR == 2 ? sSrc[w] : 0.0;
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      const double Fl = sF[v][w], Fr = F[v];
-      const double d = -(Fr - Fl) / A.dxd;
-      double tnd;
-      if (DIR == 0) tnd = (A.sim2d && v == idV) ? 0.0 : d;
-      else if (DIR == 1) tnd = d;
-      else tnd = (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;
-      if (A.mode == MODE_APPLY) {
-        A.state[lb + v * sv + cell * sd] = ringAt(v, cell) + A.dt * tnd;
-      } else {
-        A.tend[tb + v * tv + cell * tsd] = tnd;
-      }
-    }
+
+  // K5 divergence (Spatial:940-956, 1298-1310, 1680-1696): z adds onto the gravity source.
+  template <int DIR>
+  static __device__ __forceinline__ double tendency(int v, double Fl, double Fr, double sa, const Args &A) {
+    const double d = -(Fr - Fl) / A.dxd;
+    if (DIR == 0) return (A.sim2d && v == idV) ? 0.0 : d;
+    if (DIR == 1) return d;
+    return (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;
   }
-}
 
-// Launch geometry per (ORD, DIR): lines are grouped W per CTA along the contiguous axis.
-template <int ORD, int DIR> struct SweepShape;
-template <> struct SweepShape<5, 0> { static constexpr int C = 32, W = 4; };
-template <> struct SweepShape<5, 1> { static constexpr int C = 4, W = 32; };
-template <> struct SweepShape<5, 2> { static constexpr int C = 4, W = 32; };
-template <> struct SweepShape<9, 0> { static constexpr int C = 32, W = 2; };
-template <> struct SweepShape<9, 1> { static constexpr int C = 8, W = 16; };
-template <> struct SweepShape<9, 2> { static constexpr int C = 8, W = 16; };
-
-template <int ORD, int DIR>
-static cudaError_t launch_sweep_t(const SweepArgs &A, cudaStream_t st) {
-  constexpr int C = SweepShape<ORD, DIR>::C, W = SweepShape<ORD, DIR>::W;
-  dim3 block(DIR == 0 ? C : W, DIR == 0 ? W : C);
-  dim3 grid;
-  if (DIR == 0) grid = dim3((A.ny + W - 1) / W, A.nz);
-  else if (DIR == 1) grid = dim3((A.nx + W - 1) / W, A.nz);
-  else grid = dim3((A.nx + W - 1) / W, A.ny);
-  sweep_kernel<ORD, DIR, C, W><<<grid, block, 0, st>>>(A);
-  return cudaGetLastError();
-}
+  // K6 apply (Temporal_ader.h:63-65)
+  static __device__ __forceinline__ void apply(const Args &A, long g, double orig, double tnd) {
+    A.state[g] = orig + A.dt * tnd;
+  }
+};
 
 cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
-  if (ord == 5) {
-    if (dir == 0) return launch_sweep_t<5, 0>(A, st);
-    if (dir == 1) return launch_sweep_t<5, 1>(A, st);
-    return launch_sweep_t<5, 2>(A, st);
-  }
-  if (dir == 0) return launch_sweep_t<9, 0>(A, st);
-  if (dir == 1) return launch_sweep_t<9, 1>(A, st);
-  return launch_sweep_t<9, 2>(A, st);
+  return launch_sweep_any<P64>(ord, dir, A, st);
 }
 
 // ------------------------------------------------------------------------------------
@@ -355,6 +144,7 @@ cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const dou
 // ------------------------------------------------------------------------------------
 struct InitArgs {
   double *state;
+  float *state32, *comp32;
   int nx, ny, nz, hs, ord;
   double dx, dy, dz, xlen, ylen, zlen;
   int data_spec, sim2d;
@@ -464,13 +254,23 @@ __global__ void init_state_kernel(InitArgs a) {
     const double nz_ = (2.0 * u - 1.0) * a.noise_amp;
     acc[4] += a.dens_c[hs + k] * nz_;
   }
+  if (a.state32) {  // FP32 context: value plane and a zeroed Kahan plane
 #pragma unroll
-  for (int l = 0; l < 5; l++) a.state[s + l * sv] = acc[l];
+    for (int l = 0; l < 5; l++) {
+      a.state32[s + l * sv] = (float)acc[l];
+      a.comp32[s + l * sv] = 0.f;
+    }
+  } else {
+#pragma unroll
+    for (int l = 0; l < 5; l++) a.state[s + l * sv] = acc[l];
+  }
 }
 
 cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st) {
   InitArgs a;
   a.state = (double *)L.state;
+  a.state32 = L.state32;
+  a.comp32 = L.comp32;
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.hs = L.hs; a.ord = L.ord;
   a.dx = L.dx; a.dy = L.dy; a.dz = L.dz; a.xlen = L.xlen; a.ylen = L.ylen; a.zlen = L.zlen;
   a.data_spec = L.data_spec; a.sim2d = L.sim2d; a.kind = L.kind; a.shape = L.shape;

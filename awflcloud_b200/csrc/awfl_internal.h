@@ -48,6 +48,7 @@ struct SweepArgs {
 
 struct InitLaunch {
   void *state;
+  float *state32, *comp32;  // FP32 contexts: value and Kahan planes (state unused)
   int nx, ny, nz, hs, ord;
   double dx, dy, dz, xlen, ylen, zlen;
   int data_spec, sim2d, kind, shape;
@@ -56,6 +57,17 @@ struct InitLaunch {
   const double *dens_c;
   double pts[9], wts[9];
 };
+
+// FP32 form (awfl_fp32.cu)
+struct SweepArgs32;
+cudaError_t launch_sweep_fp32(int ord, int dir, const SweepArgs32 &A, cudaStream_t st);
+cudaError_t launch_apply_fp32(float *state, float *comp, const float *tend, float dt, int nx, int ny, int nz, int hs,
+                              int nsm, cudaStream_t st);
+cudaError_t launch_cfl_fp32(const float *state, const double *dens_c, const double *denstheta_c, double cfl, double dx,
+                            double dy, double dz, int nx, int ny, int nz, int hs, int nsm, unsigned long long *d_out,
+                            cudaStream_t st);
+cudaError_t upload_tables_fp32(int ord, const double *recon, const double *c2g, const double *s2g,
+                               const double *deriv, const double *idl, double sigma, const double *wts);
 
 // Error message for entry points without a context (awfl_capi.cu).
 void set_unbound_error(const char *msg);

@@ -1,0 +1,248 @@
+// The line-sweep kernel skeleton shared by the FP64 and FP32 forms.
+//
+// A CTA owns W whole lines along the sweep direction DIR and marches along them in
+// chunks of C cells. Because no other CTA touches those lines, the tendency can be
+// applied in place (MODE_APPLY) with no race: every stencil value a chunk reads comes
+// from a shared-memory ring holding the ORIGINAL values of positions
+// [base-HS, base+C+HS), refilled one chunk ahead of the updates, and the first HS rows
+// (needed again by the periodic wrap at the end of the line) are saved before they are
+// overwritten.
+//
+// Per chunk: (A) store the prefetched ring rows; (B) reconstruct cells base..base+C-1
+// -> left/right edge states; (C) Riemann flux at their left faces (the left state of
+// the first face is carried from the previous chunk); (D) divergence and update of
+// cells base-1..base+C-2 (the last cell's right face is computed in the next chunk),
+// while the next chunk's rows are prefetched into registers. The last cell of the line
+// is finished after the loop.
+//
+// Boundary handling reproduces the reference's halo fill (Spatial_euler3d_cons_expl_
+// cart_fv_Agrid.h:631-662, 994-1025, 1351-1382) and edge-value BCs (:816-837, 1176-1197,
+// 1557-1578): periodic wraps; a wall copies the edge cell with zero normal momentum, and
+// its boundary face uses the interior state on both sides. The halo values are also
+// written to the state's halo cells, as the reference does in place.
+//
+// The physics policy P supplies the element type, the per-cell reconstruction (+ADER +
+// time average), the face flux, the tendency and the in-place update:
+//   using Real; using Args;                         Args has state/tend/nx/ny/nz/bc/mode/sim2d
+//   template <int ORD, int DIR, class S> recon(sten, kb, A, eL[5], eR[5], src)
+//   template <int DIR, int NG>            flux(qL[5], qR[5], kf, A, F[5])
+//   template <int DIR>                    tendency(v, Fl, Fr, src, A) -> Real
+//   apply(A, gidx, orig, tnd)             state[gidx] = orig "+" dt*tnd (MODE_APPLY)
+#pragma once
+
+#include "awfl_internal.h"
+
+namespace awfl {
+
+template <class P, int ORD, int DIR, int C, int W>
+__global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
+  using Real = typename P::Real;
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int R = 2 * C;  // ring length (power of two, >= C + 2*HS)
+  constexpr int NM = 1 + DIR;
+  static_assert((C & (C - 1)) == 0 && C >= 2 * HS, "chunk must be a power of two >= 2*HS");
+
+  __shared__ Real ring[5][R * W];
+  __shared__ Real sEL[5][C * W];
+  __shared__ Real sER[5][(C + 1) * W];
+  __shared__ Real sF[5][(C + 1) * W];
+  __shared__ Real sSrc[DIR == 2 ? (C + 1) * W : 1];
+  __shared__ Real sWrap[5][HS * W];
+  __shared__ Real sEL0[5][W];
+
+  const int c = DIR == 0 ? threadIdx.x : threadIdx.y;  // position in chunk
+  const int w = DIR == 0 ? threadIdx.y : threadIdx.x;  // line within CTA
+
+  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  const long sx = 1, sy = nx + 2 * HS, sz = (long)(ny + 2 * HS) * sy, sv = (long)(nz + 2 * HS) * sz;
+  int L, kline = 0;
+  bool valid;
+  long lb;  // offset of (v=0, position 0 along DIR) of this line, halo-inclusive frame
+  long sd;  // stride along DIR
+  long tb;  // tendency offset of position 0
+  long tsd;
+  if (DIR == 0) {
+    const int k = blockIdx.y, j = blockIdx.x * W + w;
+    L = nx; valid = j < ny; kline = k;
+    lb = (HS + k) * sz + (HS + (valid ? j : 0)) * sy + HS * sx; sd = sx;
+    tb = ((long)k * ny + (valid ? j : 0)) * nx; tsd = 1;
+  } else if (DIR == 1) {
+    const int k = blockIdx.y, i = blockIdx.x * W + w;
+    L = ny; valid = i < nx; kline = k;
+    lb = (HS + k) * sz + HS * sy + HS + (valid ? i : 0); sd = sy;
+    tb = (long)k * ny * nx + (valid ? i : 0); tsd = nx;
+  } else {
+    const int j = blockIdx.y, i = blockIdx.x * W + w;
+    L = nz; valid = i < nx;
+    lb = HS * sz + (HS + j) * sy + HS + (valid ? i : 0); sd = sz;
+    tb = (long)j * nx + (valid ? i : 0); tsd = (long)ny * nx;
+  }
+  const long tv = (long)nz * ny * nx;
+  const bool periodic = A.bc == BC_PERIODIC;
+
+  auto G = [&](int v, int p) -> Real { return A.state[lb + v * sv + p * sd]; };
+  auto ringAt = [&](int v, int p) -> Real & {
+    const int s = p & (R - 1);
+    return DIR == 0 ? ring[v][w * R + s] : ring[v][s * W + w];
+  };
+  auto topval = [&](int v, int p, bool first) -> Real {  // p >= L
+    const int q = p - L;
+    if (q >= HS) return Real(0);  // beyond the last cell's stencil: never read
+    if (periodic) return first ? G(v, q) : sWrap[v][q * W + w];
+    return v == NM ? Real(0) : G(v, L - 1);
+  };
+  auto finish = [&](int cell, const Real *Fl, const Real *Fr, Real sa) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const Real tnd = P::template tendency<DIR>(v, Fl[v], Fr[v], sa, A);
+      if (A.mode == MODE_APPLY) P::apply(A, lb + v * sv + cell * sd, ringAt(v, cell), tnd);
+      else A.tend[tb + v * tv + cell * tsd] = tnd;
+    }
+  };
+
+  // ---- prologue: bottom halo, saved wrap rows, top halo; chunk-0 prefetch
+  if (valid && c < HS) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const Real bot = periodic ? G(v, L + c - HS) : (v == NM ? Real(0) : G(v, 0));
+      const Real orig = G(v, c);
+      const Real top = periodic ? orig : (v == NM ? Real(0) : G(v, L - 1));
+      ringAt(v, c - HS) = bot;
+      ringAt(v, c) = orig;
+      sWrap[v][c * W + w] = orig;
+      A.state[lb + v * sv + (c - HS) * sd] = bot;
+      A.state[lb + v * sv + (L + c) * sd] = top;
+    }
+  }
+  Real pre[5];
+  if (valid) {
+    const int p = HS + c;
+#pragma unroll
+    for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, true);
+  }
+  // periodic: the left state of face 0 is the right edge of cell L-1
+  if (valid && periodic && c == 0) {
+    auto wrapSten = [&](int v, int m) -> Real {
+      int p = L - 1 - HS + m;
+      p %= L;
+      if (p < 0) p += L;
+      return G(v, p);
+    };
+    Real eL[5], eR[5], sa;
+    P::template recon<ORD, DIR>(wrapSten, DIR == 2 ? L - 1 : kline, A, eL, eR, sa);
+#pragma unroll
+    for (int v = 0; v < 5; v++) sER[v][0 * W + w] = eR[v];
+  }
+
+  const int nchunk = (L + C - 1) / C;
+  for (int t = 0; t < nchunk; t++) {
+    const int base = t * C;
+    const int nvalid = min(C, L - base);
+    if (valid) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) ringAt(v, base + HS + c) = pre[v];
+    }
+    __syncthreads();  // (A)
+    if (valid && c < nvalid) {
+      const int p = base + c;
+      auto sten = [&](int v, int m) -> Real { return ringAt(v, p - HS + m); };
+      Real eL[5], eR[5], sa;
+      P::template recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa);
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        sEL[v][c * W + w] = eL[v];
+        sER[v][(c + 1) * W + w] = eR[v];
+      }
+      if (DIR == 2) sSrc[(c + 1) * W + w] = sa;
+      if (p == 0) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) sEL0[v][w] = eL[v];
+      }
+    }
+    __syncthreads();  // (B)
+    if (valid && c < nvalid) {
+      const int f = base + c;  // face index = left face of cell f
+      Real qL[5], qR[5], F[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) qR[v] = sEL[v][c * W + w];
+#pragma unroll
+      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][c * W + w];
+      P::template flux<DIR, NG>(qL, qR, f, A, F);
+#pragma unroll
+      for (int v = 0; v < 5; v++) sF[v][(c + 1) * W + w] = F[v];
+    }
+    __syncthreads();  // (C)
+    if (valid && c < nvalid) {
+      const int cell = base + c - 1;
+      if (cell >= 0) {
+        Real Fl[5], Fr[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          Fl[v] = sF[v][c * W + w];
+          Fr[v] = sF[v][(c + 1) * W + w];
+        }
+        finish(cell, Fl, Fr, DIR == 2 ? sSrc[c * W + w] : Real(0));
+      }
+    }
+    if (valid && t + 1 < nchunk) {
+      const int p = base + C + HS + c;
+#pragma unroll
+      for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
+    }
+    __syncthreads();  // (D)
+    if (valid && c == 0) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        sER[v][w] = sER[v][nvalid * W + w];
+        sF[v][w] = sF[v][nvalid * W + w];
+      }
+      if (DIR == 2) sSrc[w] = sSrc[nvalid * W + w];
+    }
+  }
+  // ---- epilogue: face L and the last cell (same thread that wrote the carry)
+  if (valid && c == 0) {
+    Real qL[5], qR[5], F[5], Fl[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      qL[v] = sER[v][w];
+      qR[v] = periodic ? sEL0[v][w] : qL[v];
+      Fl[v] = sF[v][w];
+    }
+    P::template flux<DIR, NG>(qL, qR, L, A, F);
+    finish(L - 1, Fl, F, DIR == 2 ? sSrc[w] : Real(0));
+  }
+}
+
+template <int ORD, int DIR> struct SweepShape;
+template <> struct SweepShape<5, 0> { static constexpr int C = 32, W = 4; };
+template <> struct SweepShape<5, 1> { static constexpr int C = 4, W = 32; };
+template <> struct SweepShape<5, 2> { static constexpr int C = 4, W = 32; };
+template <> struct SweepShape<9, 0> { static constexpr int C = 32, W = 2; };
+template <> struct SweepShape<9, 1> { static constexpr int C = 8, W = 16; };
+template <> struct SweepShape<9, 2> { static constexpr int C = 8, W = 16; };
+
+template <class P, int ORD, int DIR, int C = SweepShape<ORD, DIR>::C, int W = SweepShape<ORD, DIR>::W>
+cudaError_t launch_sweep_t(const typename P::Args &A, cudaStream_t st) {
+  dim3 block(DIR == 0 ? C : W, DIR == 0 ? W : C);
+  dim3 grid;
+  if (DIR == 0) grid = dim3((A.ny + W - 1) / W, A.nz);
+  else if (DIR == 1) grid = dim3((A.nx + W - 1) / W, A.nz);
+  else grid = dim3((A.nx + W - 1) / W, A.ny);
+  sweep_kernel<P, ORD, DIR, C, W><<<grid, block, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+template <class P>
+cudaError_t launch_sweep_any(int ord, int dir, const typename P::Args &A, cudaStream_t st) {
+  if (ord == 5) {
+    if (dir == 0) return launch_sweep_t<P, 5, 0>(A, st);
+    if (dir == 1) return launch_sweep_t<P, 5, 1>(A, st);
+    return launch_sweep_t<P, 5, 2>(A, st);
+  }
+  if (dir == 0) return launch_sweep_t<P, 9, 0>(A, st);
+  if (dir == 1) return launch_sweep_t<P, 9, 1>(A, st);
+  return launch_sweep_t<P, 9, 2>(A, st);
+}
+
+}  // namespace awfl

@@ -14,6 +14,10 @@
  *     (rho', rho*u, rho*v, rho*w, (rho*theta)') -- Spatial:129-131, :69-73.
  *     Tendency arrays are C-order (5, nz, ny, nx) -- Spatial:141-143.
  *   - Element type is double for AWFL_FP64 contexts and float for AWFL_FP32 contexts.
+ *     An FP32 state buffer holds two such planes back to back: the values, then the Kahan
+ *     compensation of the stage updates (zeroed by awfl_init_state); awfl_sizes reports
+ *     the total. The library cannot see allocation sizes: buffers must be at least that
+ *     large.
  *   - Every function returns AWFL_OK (0) or a negative awfl_status; nothing throws
  *     across the ABI. awfl_last_error() gives the message of the last failure.
  *   - A context is used by one host thread at a time; all work is ordered on the

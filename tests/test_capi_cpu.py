@@ -65,3 +65,13 @@ def test_background_matches_reference(case):
     c = capi.Context(nx, ny, nz, ord_=ord_, data=str(g["data"]), device=-1)
     for k, v in c.background().items():
         assert np.array_equal(v, g[k]), k
+
+
+def test_wrapper_rejects_wrong_buffers_before_any_device_call():
+    import torch
+    c = capi.Context(10, 8, 6, precision=capi.FP32, device=-1)
+    assert c.state_shape[0] == 10  # values + Kahan compensation plane
+    with pytest.raises(ValueError):
+        c.step(torch.zeros((5,) + c.state_shape[1:], dtype=torch.float32), 0.1)  # one plane only, on the CPU
+    with pytest.raises(ValueError):
+        c.step(torch.zeros(c.state_shape, dtype=torch.float64), 0.1)  # wrong dtype
