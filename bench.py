@@ -10,8 +10,10 @@ squared theta bubble +3 K, radius 2 km, centred at (10, 10, 2) km in a 20x20x10 
 periodic x/y, walls in z, ord 5 / ngll 3, CFL 0.8) with seeded uniform +-0.01 K theta noise;
 synthetic initial data generated on the device.
 
-Our arm times K steps with CUDA events on the launching stream after W warm-up steps,
-barrier + synchronize on both sides, max over ranks. The state (357 MB in FP64) is larger
+Our arm times K steps of the FP32 precision form (the headline `value`) and of the plain
+FP64 path (`fp64`), each with CUDA events on the launching stream after W warm-up steps,
+barrier + synchronize on both sides, max over ranks, and reports the FP32-vs-FP64 relative
+L2 after 100 steps. The state (357 MB in FP64) is larger
 than the 126 MB L2, so no flush is needed between steps. N > 1 runs N independent
 replicas (one grid per GPU, no collective): the single-domain path has no exchange step.
 
@@ -46,13 +48,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp64")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--ord", type=int, default=5, choices=[5, 9])
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--ny", type=int, default=256)
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the FP64 comparison arm and the 100-step accuracy check")
     return ap.parse_args()
 
 
@@ -205,10 +209,95 @@ def run_reference(a):
 
 
 # ----------------------------------------------------------------------------- our arm
-def run_ours(a):
+def time_form(a, prec, local, world, clocks=None):
+    """Time K fused steps of one precision form; per-launch CUDA events on the stream."""
     import torch
     import torch.distributed as dist
     from awflcloud_b200 import capi, flops
+    cells = a.nx * a.ny * a.nz
+    ctx = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=prec, device=local)
+    st = ctx.new_state()
+    ctx.init_state(st, **BUBBLE)
+    dt = ctx.cfl(st, cfl_for(a.ord))
+    stream = torch.cuda.current_stream()
+    peak = capi.measure_fma_peak(prec, local)
+    for _ in range(a.warmup):
+        ctx.step(st, dt)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.start()
+    # Events between the three split launches of every step give the per-launch time of
+    # the sweep kernel (the only kernel in the step).
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * a.steps + 1)]
+    ev[0].record(stream)
+    for s in range(a.steps):
+        ds = ctx.dimswitch
+        for spl in range(3):
+            ctx.split(st, dt, spl if ds else 2 - spl)
+            ev[3 * s + spl + 1].record(stream)
+        ctx.dimswitch = 1 - ds
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks is not None else None
+    total_ms = ev[0].elapsed_time(ev[-1])
+    launch_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(3 * a.steps)]
+    t = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = t.item()
+    fl = flops.flops_per_cell_step(a.ord)
+    flops_launch = fl["flops"] / 3.0 * cells  # per split launch, averaged over directions
+    avg_launch_s = statistics.mean(launch_ms) * 1e-3
+    achieved = flops_launch / avg_launch_s / 1e12
+    esz = 8 if prec == capi.FP64 else 4
+    roofline = {"bound": "fp64" if prec == capi.FP64 else "fp32",
+                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4), "traffic": TRAFFIC.get((prec, a.ord)),
+                "peak_source": "measured in this run: awfl_measure_fma_peak (FMA chains, 2 flops/FMA)",
+                "flops_per_launch": flops_launch, "launch_ms_avg": round(avg_launch_s * 1e3, 4),
+                "bytes_algorithmic_per_launch": cells * 10 * esz * (1 if prec == capi.FP64 else 2)}
+    return {"ctx": ctx, "state": st, "dt": dt, "value": world * cells * a.steps / (max_ms * 1e-3) / 1e6,
+            "ms_per_step": max_ms / a.steps, "roofline": roofline, "clocks": clk, "flops": fl,
+            "finite": bool(torch.isfinite(st).all().item())}
+
+
+# DRAM bytes per sweep launch (read + write), from ncu on the 256x256x128 workload
+# (profiles/sweep_kernel_256x256x128.md).
+TRAFFIC = {(0, 5): 630_000_000}
+
+
+def rel_l2_after(a, steps, local):
+    """FP32 form vs FP64 path after `steps` steps from the same initial data: relative L2
+    per variable (interior cells)."""
+    import torch
+    from awflcloud_b200 import capi
+    c64 = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=capi.FP64, device=local)
+    c32 = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=capi.FP32, device=local)
+    s64, s32 = c64.new_state(), c32.new_state()
+    c64.init_state(s64, **BUBBLE)
+    c32.init_state(s32, **BUBBLE)
+    dt = c64.cfl(s64, cfl_for(a.ord))
+    for _ in range(steps):
+        c64.step(s64, dt)
+        c32.step(s32, dt)
+    h = c64.hs
+    out = []
+    for v in range(5):
+        x = s32[v, h:-h, h:-h, h:-h].double()
+        y = s64[v, h:-h, h:-h, h:-h]
+        out.append((torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)).item())
+    return out
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+    from awflcloud_b200 import capi
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -217,76 +306,30 @@ def run_ours(a):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    prec = capi.FP64 if a.precision == "fp64" else capi.FP32
-    cells = a.nx * a.ny * a.nz
-    ctx = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=prec, device=local)
-    st = ctx.new_state()
-    ctx.init_state(st, **BUBBLE)
-    dt = ctx.cfl(st, cfl_for(a.ord))
-    stream = torch.cuda.current_stream()
-
-    peak = capi.measure_fma_peak(prec, local)
-
-    for _ in range(a.warmup):
-        ctx.step(st, dt)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-
-    clocks = ClockSampler(local)
-    clocks.start()
-    # Events between the three split launches of every step give the per-launch time of
-    # the sweep kernel (the only kernel in the step).
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * a.steps + 1)]
-    ev[0].record(stream)
-    for s in range(a.steps):
-        ds = ctx.dimswitch
-        for spl in range(3):
-            d = spl if ds else 2 - spl
-            ctx.split(st, dt, d)
-            ev[3 * s + spl + 1].record(stream)
-        ctx.dimswitch = 1 - ds
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    total_ms = ev[0].elapsed_time(ev[-1])
-    launch_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(3 * a.steps)]
-    t = torch.tensor([total_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = t.item()
-    finite = bool(torch.isfinite(st).all().item())
-
-    value = world * cells * a.steps / (max_ms * 1e-3) / 1e6
-    fl = flops.flops_per_cell_step(a.ord)
-    flops_launch = fl["flops"] / 3.0 * cells  # per split launch, averaged over directions
-    avg_launch_s = statistics.mean(launch_ms) * 1e-3
-    achieved = flops_launch / avg_launch_s / 1e12
-    roofline = {"bound": "fp64" if prec == capi.FP64 else "fp32",
-                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "peak_source": "measured in this run: awfl_measure_fma_peak (FMA chains, 2 flops/FMA)",
-                "flops_per_launch": flops_launch, "launch_ms_avg": round(avg_launch_s * 1e3, 4),
-                "bytes_algorithmic_per_launch": cells * 10 * (8 if prec == capi.FP64 else 4)}
-
-    e2e = None
-    if not a.no_e2e:
-        e2e = e2e_leg(a, ctx, st, dt, stream, world)
+    main_prec = capi.FP32 if a.precision == "fp32" else capi.FP64
+    main = time_form(a, main_prec, local, world, clocks=ClockSampler(local))
+    other = time_form(a, capi.FP64, local, world) if (main_prec == capi.FP32 and not a.no_compare) else None
+    e2e = None if a.no_e2e else e2e_leg(a, main["ctx"], main["state"], main["dt"], torch.cuda.current_stream(), world)
 
     if rank == 0:
-        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
-                "warmup": a.warmup, "ms_per_step": round(max_ms / a.steps, 4), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == capi.FP64 else "f32",
-                "data": DATA,
+        line = {"metric": METRIC, "value": round(main["value"], 3), "unit": UNIT, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(main["ms_per_step"], 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if main_prec == capi.FP64 else "f32", "data": DATA,
                 "config": {"workload": workload_name(a), "nx": a.nx, "ny": a.ny, "nz": a.nz, "ord": a.ord,
                            "precision": a.precision,
-                           "l2": "state %.0f MB > 126 MB L2: no flush needed" % (st.numel() * st.element_size() / 1e6),
+                           "l2": "state %.0f MB > 126 MB L2: no flush needed"
+                                 % (main["state"].numel() * main["state"].element_size() / 1e6),
                            "parallelism": "replicas" if world > 1 else "single GPU"},
-                "roofline": roofline, "gpu_launches": 3 * a.steps, "finite": finite,
-                "clocks": clk, "flops_per_cell_step": fl}
+                "roofline": main["roofline"], "gpu_launches": 3 * a.steps, "finite": main["finite"],
+                "clocks": main["clocks"], "flops_per_cell_step": main["flops"]}
+        if other is not None:
+            line["fp64"] = {"value": round(other["value"], 3), "ms_per_step": round(other["ms_per_step"], 4),
+                            "roofline": other["roofline"], "finite": other["finite"]}
+            line["fp32_over_fp64"] = round(main["value"] / other["value"], 3)
+            errs = rel_l2_after(a, 100, local)
+            line["rel_l2_vs_fp64_after_100_steps"] = {"rho": errs[0], "rho_u": errs[1], "rho_v": errs[2],
+                                                      "rho_w": errs[3], "rho_theta": errs[4]}
         if e2e is not None:
             line["e2e"] = e2e
         if not a.no_cpu_baseline and world == 1:
