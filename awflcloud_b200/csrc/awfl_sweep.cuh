@@ -11,8 +11,8 @@
 // Per chunk: (A) store the prefetched ring rows; (B) reconstruct cells base..base+C-1
 // -> left/right edge states; (C) Riemann flux at their left faces (the left state of
 // the first face is carried from the previous chunk); (D) divergence and update of
-// cells base-1..base+C-2 (the last cell's right face is computed in the next chunk),
-// while the next chunk's rows are prefetched into registers. The last cell of the line
+// cells base-1..base+C-2 (the last cell's right face is computed in the next chunk).
+// The next chunk's rows are loaded into registers at the start of each chunk. The last cell of the line
 // is finished after the loop.
 //
 // Boundary handling reproduces the reference's halo fill (Spatial_euler3d_cons_expl_
@@ -42,9 +42,13 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
   constexpr int R = 2 * C;  // ring length (power of two, >= C + 2*HS)
   constexpr int NM = 1 + DIR;
   static_assert((C & (C - 1)) == 0 && C >= 2 * HS, "chunk must be a power of two >= 2*HS");
+  // When to load the next chunk's rows: before the reconstruction (its latency hidden
+  // behind it, at the cost of 5 live registers) for the z sweep, whose loads stride over
+  // whole planes; after the updates for x and y, where occupancy matters more (measured).
+  constexpr bool EARLY_PREFETCH = DIR == 2;
 
   __shared__ Real ring[5][R * W];
-  __shared__ Real sEL[5][C * W];
+  __shared__ Real sEL[5][(C + 1) * W];
   __shared__ Real sER[5][(C + 1) * W];
   __shared__ Real sF[5][(C + 1) * W];
   __shared__ Real sSrc[DIR == 2 ? (C + 1) * W : 1];
@@ -53,6 +57,8 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
 
   const int c = DIR == 0 ? threadIdx.x : threadIdx.y;  // position in chunk
   const int w = DIR == 0 ? threadIdx.y : threadIdx.x;  // line within CTA
+  // edge/flux slot (0..C) of this line: consecutive threads of a warp hit consecutive words
+  auto E = [&](int slot) { return DIR == 0 ? w * (C + 1) + slot : slot * W + w; };
 
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   const long sx = 1, sy = nx + 2 * HS, sz = (long)(ny + 2 * HS) * sy, sv = (long)(nz + 2 * HS) * sz;
@@ -132,7 +138,7 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
     Real eL[5], eR[5], sa;
     P::template recon<ORD, DIR>(wrapSten, DIR == 2 ? L - 1 : kline, A, eL, eR, sa);
 #pragma unroll
-    for (int v = 0; v < 5; v++) sER[v][0 * W + w] = eR[v];
+    for (int v = 0; v < 5; v++) sER[v][E(0)] = eR[v];
   }
 
   const int nchunk = (L + C - 1) / C;
@@ -144,6 +150,13 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
       for (int v = 0; v < 5; v++) ringAt(v, base + HS + c) = pre[v];
     }
     __syncthreads();  // (A)
+    // next chunk's rows (stored into the ring at the next (A); the updates of this chunk
+    // never reach them)
+    if (EARLY_PREFETCH && valid && t + 1 < nchunk) {
+      const int p = base + C + HS + c;
+#pragma unroll
+      for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
+    }
     if (valid && c < nvalid) {
       const int p = base + c;
       auto sten = [&](int v, int m) -> Real { return ringAt(v, p - HS + m); };
@@ -151,10 +164,10 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
       P::template recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
-        sEL[v][c * W + w] = eL[v];
-        sER[v][(c + 1) * W + w] = eR[v];
+        sEL[v][E(c)] = eL[v];
+        sER[v][E(c + 1)] = eR[v];
       }
-      if (DIR == 2) sSrc[(c + 1) * W + w] = sa;
+      if (DIR == 2) sSrc[E(c + 1)] = sa;
       if (p == 0) {
 #pragma unroll
         for (int v = 0; v < 5; v++) sEL0[v][w] = eL[v];
@@ -165,12 +178,12 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
       const int f = base + c;  // face index = left face of cell f
       Real qL[5], qR[5], F[5];
 #pragma unroll
-      for (int v = 0; v < 5; v++) qR[v] = sEL[v][c * W + w];
+      for (int v = 0; v < 5; v++) qR[v] = sEL[v][E(c)];
 #pragma unroll
-      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][c * W + w];
+      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][E(c)];
       P::template flux<DIR, NG>(qL, qR, f, A, F);
 #pragma unroll
-      for (int v = 0; v < 5; v++) sF[v][(c + 1) * W + w] = F[v];
+      for (int v = 0; v < 5; v++) sF[v][E(c + 1)] = F[v];
     }
     __syncthreads();  // (C)
     if (valid && c < nvalid) {
@@ -179,13 +192,13 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
         Real Fl[5], Fr[5];
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          Fl[v] = sF[v][c * W + w];
-          Fr[v] = sF[v][(c + 1) * W + w];
+          Fl[v] = sF[v][E(c)];
+          Fr[v] = sF[v][E(c + 1)];
         }
-        finish(cell, Fl, Fr, DIR == 2 ? sSrc[c * W + w] : Real(0));
+        finish(cell, Fl, Fr, DIR == 2 ? sSrc[E(c)] : Real(0));
       }
     }
-    if (valid && t + 1 < nchunk) {
+    if (!EARLY_PREFETCH && valid && t + 1 < nchunk) {
       const int p = base + C + HS + c;
 #pragma unroll
       for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
@@ -194,10 +207,10 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
     if (valid && c == 0) {
 #pragma unroll
       for (int v = 0; v < 5; v++) {
-        sER[v][w] = sER[v][nvalid * W + w];
-        sF[v][w] = sF[v][nvalid * W + w];
+        sER[v][E(0)] = sER[v][E(nvalid)];
+        sF[v][E(0)] = sF[v][E(nvalid)];
       }
-      if (DIR == 2) sSrc[w] = sSrc[nvalid * W + w];
+      if (DIR == 2) sSrc[E(0)] = sSrc[E(nvalid)];
     }
   }
   // ---- epilogue: face L and the last cell (same thread that wrote the carry)
@@ -205,12 +218,12 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
     Real qL[5], qR[5], F[5], Fl[5];
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-      qL[v] = sER[v][w];
+      qL[v] = sER[v][E(0)];
       qR[v] = periodic ? sEL0[v][w] : qL[v];
-      Fl[v] = sF[v][w];
+      Fl[v] = sF[v][E(0)];
     }
     P::template flux<DIR, NG>(qL, qR, L, A, F);
-    finish(L - 1, Fl, F, DIR == 2 ? sSrc[w] : Real(0));
+    finish(L - 1, Fl, F, DIR == 2 ? sSrc[E(0)] : Real(0));
   }
 }
 
