@@ -1,0 +1,104 @@
+"""The reference's own driver.cpp, compiled unchanged against the drop-in operator headers
+(awflcloud_b200/dropin/) and libawfl.so, run end to end from a YAML input on the GPU.
+
+The binary is built where the reference sources are present (build()); it then travels
+with the tree. The driver's final output (outFile *.bin: raw FP64 state) is compared with
+the CPU oracle advanced through the same sequence of time steps (the driver clips the last
+step to simTime, driver.cpp:45-48).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from oracle.pyoracle import Oracle  # noqa: E402
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "awflcloud_b200", "dropin", "bin", "driver_o5")
+
+
+def _yaml(path, out, sim_time, extra=""):
+    with open(path, "w") as f:
+        f.write("""---
+simTime  : %r
+nx       : 32
+ny       : 24
+nz       : 16
+xlen     : 20000
+ylen     : 20000
+zlen     : 10000
+bc_x   : periodic
+bc_y   : wall
+bc_z   : wall
+weno_scalars : true
+weno_winds   : true
+initData : thermal
+outFile  : %s
+outFreq  : %r
+perturb: false
+%s""" % (sim_time, out, sim_time, extra))
+
+
+def _oracle_run(sim_time):
+    O = Oracle(32, 24, 16, bc=(0, 1, 1), crpow=True)
+    st = O.new_state()
+    O.init_state(st)
+    dt0 = O.compute_dt(st, 0.8)
+    etime, n = 0.0, 0
+    while etime < sim_time:  # driver.cpp:45-48
+        dt = dt0
+        if etime + dt > sim_time:
+            dt = sim_time - etime
+        O.time_step(st, dt)
+        etime += dt
+        n += 1
+    return st, dt0, n
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _needs_binary():
+    if not os.path.exists(BIN):
+        pytest.skip("drop-in driver not built (needs the reference sources at build time)")
+
+
+def _run(tmp_path, extra=""):
+    O = Oracle(32, 24, 16, bc=(0, 1, 1), crpow=True)
+    st = O.new_state()
+    O.init_state(st)
+    sim_time = 3.5 * O.compute_dt(st, 0.8)
+    inp, out = str(tmp_path / "in.yaml"), str(tmp_path / "state.bin")
+    _yaml(inp, out, sim_time, extra)
+    p = subprocess.run([BIN, inp], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    assert "Walltime:" in p.stdout
+    got = np.fromfile(out, dtype=np.float64).reshape(O.state_shape)
+    ref, dt0, n = _oracle_run(sim_time)
+    assert n == 4
+    assert ("dt: %g" % dt0)[:8] in p.stdout.replace("dt: ", "dt: ")
+    return got, ref
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_reference_driver_fp64(tmp_path):
+    got, ref = _run(tmp_path)
+    # initial data: the library's device quadrature (correctly rounded pow) against the
+    # oracle's glibc profiles -> last-bit differences, then the same arithmetic
+    for v in range(5):
+        assert _rel(got[v], ref[v]) <= 5e-12, v
+
+
+def test_reference_driver_fp32(tmp_path):
+    got, ref = _run(tmp_path, "precision : fp32\n")
+    h = 2
+    for v in range(5):
+        a, b = got[v, h:-h, h:-h, h:-h], ref[v, h:-h, h:-h, h:-h]
+        if np.abs(b).max() == 0:
+            assert np.abs(a).max() < 1e-6
+        else:
+            assert _rel(a, b) <= 1e-5, (v, _rel(a, b))
