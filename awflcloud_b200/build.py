@@ -7,6 +7,8 @@ Translation units and their numerics flags:
                 reference CPU build)
   awfl_fp32.cu  FP32 precision form: contraction, approximate division/sqrt, flush-to-zero
   awfl_noalloc.cu  allocation-free CFL variant: --fmad=false (same arithmetic as awfl_cfl)
+  awfl_adjoint.cu  tangent-linear sweep: --fmad=false (its value part replays the FP64 path)
+  awfl_adjrev.cu   adjoint reverse sweeps: --fmad=true (a derivative, not a replay)
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
 source tree. ``python -m awflcloud_b200.build [--force]``.
@@ -33,6 +35,8 @@ UNITS = {
     "awfl_fp64.cu": ["--fmad=false"],
     "awfl_fp32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "awfl_noalloc.cu": ["--fmad=false"],
+    "awfl_adjoint.cu": ["--fmad=false"],
+    "awfl_adjrev.cu": ["--fmad=true"],
 }
 
 

@@ -56,6 +56,9 @@ _SIGS = {
     "awfl_apply_tendencies": (_I, [_VP, _VP, _VP, _D, _VP]),
     "awfl_split": (_I, [_VP, _VP, _D, _I, _VP]),
     "awfl_step": (_I, [_VP, _VP, _D, _VP]),
+    "awfl_step_tlm": (_I, [_VP, _VP, _D, _VP]),
+    "awfl_step_adjoint": (_I, [_VP, _VP, _VP, _I, _D, _VP]),
+    "awfl_adjoint_tape_bytes": (_I, [_VP, _I, ctypes.POINTER(_L)]),
     "awfl_get_dimswitch": (_I, [_VP, ctypes.POINTER(_I)]),
     "awfl_set_dimswitch": (_I, [_VP, _I]),
     "awfl_get_tables": (_I, [_VP] + [_DP] * 10),
@@ -218,6 +221,24 @@ class Context:
 
     def step(self, state, dt, stream=None):
         self._check(self.L.awfl_step(self.h, self._st(state), dt, _stream(stream)))
+
+    def step_tlm(self, state_tangent, dt, stream=None):
+        """One tangent-linear step; state_tangent = (state plane, tangent plane), FP64."""
+        shp = (2 * self.state_shape[0],) + self.state_shape[1:]
+        self._check_buf(state_tangent, shp, "state+tangent")
+        self._check(self.L.awfl_step_tlm(self.h, _ptr(state_tangent), dt, _stream(stream)))
+
+    def step_adjoint(self, state_ckpt, lam, nsteps, dt, stream=None):
+        """lam <- (d S_{n+nsteps} / d S_n)^T lam, S_n = state_ckpt (not modified), with the
+        context's dimswitch holding its value at the checkpoint (unchanged on return)."""
+        self._check_buf(state_ckpt, self.state_shape, "checkpoint state")
+        self._check_buf(lam, self.state_shape, "adjoint")
+        self._check(self.L.awfl_step_adjoint(self.h, _ptr(state_ckpt), _ptr(lam), int(nsteps), dt, _stream(stream)))
+
+    def adjoint_tape_bytes(self, nsteps):
+        out = _L()
+        self._check(self.L.awfl_adjoint_tape_bytes(self.h, int(nsteps), ctypes.byref(out)))
+        return out.value
 
     @property
     def dimswitch(self):

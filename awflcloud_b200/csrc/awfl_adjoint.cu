@@ -1,0 +1,61 @@
+// Differentiation form of the FP64 step: the tangent-linear sweep (forward mode, Dual
+// scalars through the same templated FP64 code) and the hand-written discrete adjoint.
+// Compiled with --fmad=false like the FP64 path.
+#include <cuda_runtime.h>
+
+#include "awfl_device.cuh"
+#include "awfl_dual.cuh"
+#include "awfl_internal.h"
+#include "awfl_sweep.cuh"
+
+namespace awfl {
+
+// ------------------------------------------------------------------------------------
+// Tangent-linear policy: the FP64 arithmetic on Dual numbers. The state buffer holds the
+// value plane and, A.plane elements further, the tangent plane; both advance together.
+// The time step dt is a fixed parameter (not differentiated).
+// ------------------------------------------------------------------------------------
+struct PTLM {
+  using Real = Dual;
+  static constexpr int kWdiv = 2;
+  using Args = SweepArgs;
+
+  template <int ORD, int DIR, class S>
+  static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, Dual (&eL)[5], Dual (&eR)[5],
+                                               Dual &src) {
+    cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
+  }
+  template <int DIR, int NG>
+  static __device__ __forceinline__ void flux(const Dual (&qL)[5], const Dual (&qR)[5], int kf, const Args &A,
+                                              Dual (&F)[5]) {
+    riemann<DIR, NG>(qL, qR, kf, A, F);
+  }
+  template <int DIR>
+  static __device__ __forceinline__ Dual tendency(int v, Dual Fl, Dual Fr, Dual sa, const Args &A) {
+    const Dual d = -(Fr - Fl) / A.dxd;
+    if (DIR == 0) return (A.sim2d && v == idV) ? Dual(0.0) : d;
+    if (DIR == 1) return d;
+    return (A.sim2d && v == idV) ? Dual(0.0) : (v == idW ? sa : Dual(0.0)) + d;
+  }
+  static __device__ __forceinline__ void apply(const Args &A, long g, Dual orig, Dual tnd) {
+    A.state[g] = orig.v + A.dt * tnd.v;
+    A.state[g + A.plane] = orig.d + A.dt * tnd.d;
+  }
+  static __device__ __forceinline__ Dual load(const Args &A, long g) { return Dual(A.state[g], A.state[g + A.plane]); }
+  static __device__ __forceinline__ void store(const Args &A, long g, Dual x) {
+    A.state[g] = x.v;
+    A.state[g + A.plane] = x.d;
+  }
+  static __device__ __forceinline__ void store_tend(const Args &A, long g, Dual x) { A.tend[g] = x.d; }
+};
+
+cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
+  return launch_sweep_any<PTLM>(ord, dir, A, st);
+}
+
+cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes) {
+  if (ord == 5) return cudaMemcpyToSymbol(c_tab5, tab, bytes);
+  return cudaMemcpyToSymbol(c_tab9, tab, bytes);
+}
+
+}  // namespace awfl

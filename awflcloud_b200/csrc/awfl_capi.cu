@@ -15,6 +15,7 @@
 
 #include "../../include/awfl.h"
 #include "awfl_fp32_args.h"
+#include "awfl_adj_split.h"
 #include "awfl_internal.h"
 #include "awfl_tables.h"
 
@@ -39,6 +40,11 @@ struct awfl_ctx {
   // FP32 form: FP32 copies of FP64 background constants (awfl_fp32_args.h)
   float *d_bg32 = nullptr;
   Bg32 bg32{};
+  // discrete adjoint: split-start states of the recomputed window, and reverse scratch
+  double *d_tape = nullptr;
+  size_t tape_bytes = 0;
+  double *d_adj = nullptr;
+  size_t adj_bytes = 0;
   std::string err;
 };
 
@@ -213,6 +219,8 @@ int ensure_tables(awfl_ctx *c) {
     t.sigma = c->sigma;
     std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
     e = upload_tables_fp64(5, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_adj(5, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_adjrev(5, &t, sizeof t);
   } else {
     Tables<9> t;
     std::memcpy(t.recon, c->recon.data(), sizeof t.recon);
@@ -223,6 +231,8 @@ int ensure_tables(awfl_ctx *c) {
     t.sigma = c->sigma;
     std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
     e = upload_tables_fp64(9, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_adj(9, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_adjrev(9, &t, sizeof t);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "upload of transform tables");
   e = upload_tables_fp32(c->cfg.ord, c->recon.data(), c->c2g.data(), c->s2g.data(), c->deriv.data(), c->idl.data(),
@@ -316,6 +326,7 @@ SweepArgs sweep_args(awfl_ctx *c, void *state, void *tend, double dt, int dir, i
   A.weno_s = c->cfg.weno_scalars; A.weno_w = c->cfg.weno_winds; A.sim2d = c->sim2d; A.mode = mode;
   A.dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
   A.dt = dt;
+  A.plane = 0;
   A.dens_c = c->d_dens_c; A.denstheta_c = c->d_denstheta_c;
   A.dens_g = c->d_dens_g; A.denstheta_g = c->d_denstheta_g; A.pres_g = c->d_pres_g;
   return A;
@@ -421,6 +432,8 @@ int awfl_destroy(awfl_ctx *c) {
     set_device(c);
     cudaFree(c->d_bg);
     if (c->d_bg32) cudaFree(c->d_bg32);
+    if (c->d_tape) cudaFree(c->d_tape);
+    if (c->d_adj) cudaFree(c->d_adj);
   }
   delete c;
   return AWFL_OK;
@@ -566,6 +579,123 @@ int awfl_step(awfl_ctx *c, void *d_state, double dt, void *stream) {
     if (rc) return rc;
   }
   c->dimswitch = !c->dimswitch;
+  return AWFL_OK;
+}
+
+int awfl_step_tlm(awfl_ctx *c, void *d_state_tangent, double dt, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (fp32(c)) return fail(c, AWFL_ERR_ARG, "awfl_step_tlm needs an FP64 context");
+  if (bad_ptr(d_state_tangent)) return fail(c, AWFL_ERR_ARG, "state pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  for (int spl = 0; spl < 3; spl++) {
+    const int dir = c->dimswitch ? spl : 2 - spl;
+    if (dir == 1 && c->sim2d) continue;
+    SweepArgs A = sweep_args(c, d_state_tangent, nullptr, dt, dir, MODE_APPLY);
+    A.plane = state_plane(c);
+    cudaError_t e = launch_sweep_tlm(c->cfg.ord, dir, A, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "step_tlm");
+  }
+  c->dimswitch = !c->dimswitch;
+  return AWFL_OK;
+}
+
+namespace {
+
+// Grows a device buffer owned by the context (contents are not kept).
+int ensure_buffer(awfl_ctx *c, double **buf, size_t *have, size_t need, const char *what) {
+  if (*have >= need) return AWFL_OK;
+  if (*buf) {
+    cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+  }
+  cudaError_t e = cudaMalloc(buf, need);
+  if (e != cudaSuccess) {
+    *buf = nullptr;
+    cudaGetLastError();
+    return fail(c, AWFL_ERR_NOMEM, "cudaMalloc %s (%zu bytes): %s", what, need, cudaGetErrorString(e));
+  }
+  *have = need;
+  return AWFL_OK;
+}
+
+}  // namespace
+
+int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
+  if (!c || nsteps < 0 || !bytes) return AWFL_ERR_ARG;
+  const long nspl = (c->sim2d ? 2L : 3L) * nsteps;
+  const long ncell = (long)c->cfg.nx * c->cfg.ny * c->cfg.nz;
+  const long nface = (long)(c->cfg.nx + 1) * (c->cfg.ny + 1) * (c->cfg.nz + 1);
+  *bytes = (long)sizeof(double) * (nspl * state_plane(c) + 10L * ncell + 10L * nface + 5L * c->cfg.ord * ncell);
+  return AWFL_OK;
+}
+
+int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int nsteps, double dt, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (fp32(c)) return fail(c, AWFL_ERR_ARG, "awfl_step_adjoint needs an FP64 context");
+  if (bad_ptr(d_state_ckpt) || bad_ptr(d_lambda)) return fail(c, AWFL_ERR_ARG, "state or lambda pointer is NULL or misaligned");
+  if (d_state_ckpt == d_lambda) return fail(c, AWFL_ERR_ARG, "state and lambda must be distinct buffers");
+  if (nsteps < 0) return fail(c, AWFL_ERR_ARG, "nsteps must be >= 0");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, AWFL_ERR_ARG, "dt must be positive and finite");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nx = c->cfg.nx, ny = c->cfg.ny, nz = c->cfg.nz, ord = c->cfg.ord;
+  const long plane = state_plane(c);
+  const long ncell = (long)nx * ny * nz;
+  const long nface = (long)(nx + 1) * (ny + 1) * (nz + 1);
+  // split order of the window: dimSwitch as the context holds it now (its value at the
+  // checkpoint), flipped after every step
+  std::vector<int> dirs;
+  int ds = c->dimswitch;
+  for (int n = 0; n < nsteps; n++) {
+    for (int spl = 0; spl < 3; spl++) {
+      const int dir = ds ? spl : 2 - spl;
+      if (dir == 1 && c->sim2d) continue;
+      dirs.push_back(dir);
+    }
+    ds = !ds;
+  }
+  const long nspl = (long)dirs.size();
+  if (nspl > 0) {
+    rc = ensure_buffer(c, &c->d_tape, &c->tape_bytes, sizeof(double) * (size_t)(nspl * plane), "adjoint tape");
+    if (rc) return rc;
+    rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes, sizeof(double) * (size_t)(10 * ncell + 10 * nface + 5L * ord * ncell),
+                       "adjoint scratch");
+    if (rc) return rc;
+  }
+  // forward recomputation: tape[s] = state at the start of split s
+  cudaError_t e = cudaSuccess;
+  for (long s = 0; s < nspl && e == cudaSuccess; s++) {
+    double *dst = c->d_tape + s * plane;
+    const double *src = s == 0 ? (const double *)d_state_ckpt : dst - plane;
+    e = cudaMemcpyAsync(dst, src, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && s > 0) e = launch_sweep_fp64(ord, dirs[s - 1], sweep_args(c, dst, nullptr, dt, dirs[s - 1], MODE_APPLY), st);
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "adjoint forward recomputation");
+  // reverse sweeps, last split first
+  for (long s = nspl - 1; s >= 0 && e == cudaSuccess; s--) {
+    const int dir = dirs[s];
+    adj::SplitArgs A{};
+    A.state = c->d_tape + s * plane;
+    A.edges = c->d_adj;
+    A.lq = c->d_adj + 10 * ncell;
+    A.ls = c->d_adj + 10 * ncell + 10 * nface;
+    A.lam = (double *)d_lambda;
+    A.nx = nx; A.ny = ny; A.nz = nz; A.hs = c->hs;
+    A.sim2d = c->sim2d;
+    A.ca.nz = nz;
+    A.ca.bc = dir == 0 ? c->cfg.bc_x : (dir == 1 ? c->cfg.bc_y : c->cfg.bc_z);
+    A.ca.weno_s = c->cfg.weno_scalars; A.ca.weno_w = c->cfg.weno_winds;
+    A.ca.dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+    A.ca.dt = dt;
+    A.ca.dens_c = c->d_dens_c; A.ca.denstheta_c = c->d_denstheta_c;
+    A.ca.dens_g = c->d_dens_g; A.ca.denstheta_g = c->d_denstheta_g; A.ca.pres_g = c->d_pres_g;
+    e = launch_adjoint_split(ord, dir, A, 1, c->nsm, st);
+  }
+  if (e == cudaSuccess) e = launch_zero_halo((double *)d_lambda, nx, ny, nz, c->hs, c->nsm, st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "adjoint reverse sweep");
   return AWFL_OK;
 }
 

@@ -17,26 +17,30 @@
 
 namespace awfl {
 
-// Definitions: this header is included by exactly one translation unit (awfl_fp64.cu).
-__constant__ Tables<5> c_tab5;
-__constant__ Tables<9> c_tab9;
+// One copy per translation unit that includes this header (awfl_fp64.cu, awfl_adjoint.cu);
+// each is uploaded by that unit's upload function.
+static __constant__ Tables<5> c_tab5;
+static __constant__ Tables<9> c_tab9;
 
 template <int ORD> __device__ __forceinline__ const Tables<ORD> &tab();
 template <> __device__ __forceinline__ const Tables<5> &tab<5>() { return c_tab5; }
 template <> __device__ __forceinline__ const Tables<9> &tab<9>() { return c_tab9; }
 
-template <int N> __device__ __forceinline__ double tv_eval(const double *a);
-template <> __device__ __forceinline__ double tv_eval<3>(const double *a) { return awfl_tv_n3<double>(a); }
-template <> __device__ __forceinline__ double tv_eval<5>(const double *a) { return awfl_tv_n5<double>(a); }
-template <> __device__ __forceinline__ double tv_eval<9>(const double *a) { return awfl_tv_n9<double>(a); }
+// The scalar type Sc is double for the FP64 path and Dual (awfl_dual.cuh) for the
+// tangent-linear sweep; both evaluate the same expressions in the same order.
+template <int N, class Sc> __device__ __forceinline__ Sc tv_eval(const Sc *a) {
+  if constexpr (N == 3) return awfl_tv_n3<Sc>(a);
+  else if constexpr (N == 5) return awfl_tv_n5<Sc>(a);
+  else return awfl_tv_n9<Sc>(a);
+}
 
 // Weno:93-172 -- WENO polynomial coefficients of one ord-cell stencil.
-template <int ORD>
-__device__ __forceinline__ void weno_coefs(const double (&u)[ORD], double (&aw)[ORD]) {
+template <int ORD, class Sc>
+__device__ __forceinline__ void weno_coefs(const Sc (&u)[ORD], Sc (&aw)[ORD]) {
   constexpr int HS = (ORD - 1) / 2;
   const Tables<ORD> &T = tab<ORD>();
   const double eps = 1.0e-20;
-  double a[HS + 2][ORD];
+  Sc a[HS + 2][ORD];
 #pragma unroll
   for (int j = 0; j < HS + 2; j++)
 #pragma unroll
@@ -57,21 +61,21 @@ __device__ __forceinline__ void weno_coefs(const double (&u)[ORD], double (&aw)[
     for (int ii = 0; ii < HS + 1; ii++) a[HS + 1][ii] -= T.idl[i] * a[i][ii];
 #pragma unroll
   for (int ii = 0; ii < ORD; ii++) a[HS + 1][ii] /= T.idl[HS + 1];
-  double tv[HS + 2];
+  Sc tv[HS + 2];
 #pragma unroll
   for (int i = 0; i < HS + 1; i++) tv[i] = tv_eval<HS + 1>(a[i]);
   tv[HS + 1] = tv_eval<ORD>(a[HS + 1]);
-  double lo_avg = 0.;
+  Sc lo_avg = 0.;
 #pragma unroll
   for (int i = 0; i < HS + 1; i++) lo_avg += tv[i];
   lo_avg /= HS + 1;
   tv[HS + 1] = lo_avg + (tv[HS + 1] - lo_avg) * T.sigma;
-  double wts[HS + 2];
+  Sc wts[HS + 2];
 #pragma unroll
   for (int i = 0; i < HS + 2; i++) wts[i] = T.idl[i] / (tv[i] * tv[i] + eps);
   // convexify (Weno:20-25)
   {
-    double sum = 0.;
+    Sc sum = 0.;
 #pragma unroll
     for (int i = 0; i < HS + 2; i++) sum += wts[i];
 #pragma unroll
@@ -84,7 +88,7 @@ __device__ __forceinline__ void weno_coefs(const double (&u)[ORD], double (&aw)[
     wts[i] = wts[i] * (d + d * d - 3. * d * wts[i] + wts[i] * wts[i]) / (d * d + wts[i] * (1. - 2. * d));
   }
   {
-    double sum = 0.;
+    Sc sum = 0.;
 #pragma unroll
     for (int i = 0; i < HS + 2; i++) sum += wts[i];
 #pragma unroll
@@ -99,17 +103,17 @@ __device__ __forceinline__ void weno_coefs(const double (&u)[ORD], double (&aw)[
 }
 
 // Spatial:1800-1833 -- ord stencil averages -> ngll GLL point values.
-template <int ORD>
-__device__ __forceinline__ void reconstruct_gll(const double (&sten)[ORD],
-                                                double (&out)[OrdTraits<ORD>::NGLL], bool doweno) {
+template <int ORD, class Sc>
+__device__ __forceinline__ void reconstruct_gll(const Sc (&sten)[ORD], Sc (&out)[OrdTraits<ORD>::NGLL],
+                                                bool doweno) {
   constexpr int NG = OrdTraits<ORD>::NGLL;
   const Tables<ORD> &T = tab<ORD>();
   if (doweno) {
-    double wc[ORD];
+    Sc wc[ORD];
     weno_coefs<ORD>(sten, wc);
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      double tmp = 0;
+      Sc tmp = 0;
 #pragma unroll
       for (int s = 0; s < ORD; s++) tmp += T.c2g[s * NG + ii] * wc[s];
       out[ii] = tmp;
@@ -117,7 +121,7 @@ __device__ __forceinline__ void reconstruct_gll(const double (&sten)[ORD],
   } else {
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      double tmp = 0;
+      Sc tmp = 0;
 #pragma unroll
       for (int s = 0; s < ORD; s++) tmp += T.s2g[s * NG + ii] * sten[s];
       out[ii] = tmp;
@@ -131,19 +135,19 @@ __device__ __forceinline__ void reconstruct_gll(const double (&sten)[ORD],
 // sten(v, s) returns stencil value s of variable v. kb is the k index of the cell (z) or of
 // the line (x, y). Outputs: the time-averaged left/right edge states and, for z, the
 // time-averaged, GLL-weighted gravity source.
-template <int ORD, int DIR, class Sten>
-__device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const SweepArgs &A,
-                                           double (&eL)[5], double (&eR)[5], double &src_avg) {
+template <int ORD, int DIR, class Sten, class Sc>
+__device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const SweepArgs &A, Sc (&eL)[5], Sc (&eR)[5],
+                                           Sc &src_avg) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
   constexpr int NA = NG;  // nAder = ngll (Temporal_ader.h:8)
   constexpr int NM = 1 + DIR;  // normal momentum
   const Tables<ORD> &T = tab<ORD>();
 
-  double q[5][NA][NG];
+  Sc q[5][NA][NG];
 #pragma unroll
   for (int v = 0; v < 5; v++) {
-    double s[ORD];
+    Sc s[ORD];
 #pragma unroll
     for (int m = 0; m < ORD; m++) s[m] = sten(v, m);
     const bool doweno = (v == idR || v == idT) ? A.weno_s : A.weno_w;
@@ -165,17 +169,17 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
     if (kb == 0) q[idW][0][0] = 0;
   }
   // level-0 flux products (Spatial:704-715 and y/z equivalents)
-  double f[4][NA][NG];
-  double g[NA][NG];
-  double srcfill = 0;
+  Sc f[4][NA][NG];
+  Sc g[NA][NG];
+  Sc srcfill = 0;
 #pragma unroll
   for (int ii = 0; ii < NG; ii++) {
-    const double r = q[idR][0][ii];
-    const double u = q[idU][0][ii] / r;
-    const double v = q[idV][0][ii] / r;
-    const double w = q[idW][0][ii] / r;
-    const double t = q[idT][0][ii] / r;
-    const double vn = NM == 1 ? u : (NM == 2 ? v : w);
+    const Sc r = q[idR][0][ii];
+    const Sc u = q[idU][0][ii] / r;
+    const Sc v = q[idV][0][ii] / r;
+    const Sc w = q[idW][0][ii] / r;
+    const Sc t = q[idT][0][ii] / r;
+    const Sc vn = NM == 1 ? u : (NM == 2 ? v : w);
     f[0][0][ii] = r * vn * u;
     f[1][0][ii] = r * vn * v;
     f[2][0][ii] = r * vn * w;
@@ -185,7 +189,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
   }
   // The z source SArray is filled by a scalar assignment inside the kk loop, so every entry
   // holds the kk = ngll-1 value (Spatial:1439).
-  double sr[NA][NG];
+  Sc sr[NA][NG];
 #pragma unroll
   for (int kt = 0; kt < NA; kt++)
 #pragma unroll
@@ -203,7 +207,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
   for (int kt = 0; kt < NA - 1; kt++) {
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      double dq[5] = {0, 0, 0, 0, 0};
+      Sc dq[5] = {0., 0., 0., 0., 0.};
 #pragma unroll
       for (int s = 0; s < NG; s++) {
         const double D = T.deriv[s * NG + ii];
@@ -237,7 +241,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
     }
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      double tot[4] = {0, 0, 0, 0};
+      Sc tot[4] = {0., 0., 0., 0.};
 #pragma unroll
       for (int ir = 0; ir <= kt + 1; ir++) {
 #pragma unroll
@@ -246,7 +250,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
       }
 #pragma unroll
       for (int x = 0; x < 4; x++) f[x][kt + 1][ii] = tot[x] / q[idR][0][ii];
-      double tg = 0;
+      Sc tg = 0.;
 #pragma unroll
       for (int ir = 0; ir <= kt; ir++)
         tg += (kt + 1. - ir) * (GAMMA * g[ir][ii] * q[idT][kt + 1 - ir][ii] - q[idT][ir][ii] * g[kt + 1 - ir][ii]);
@@ -256,7 +260,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
   // compute_timeAvg_edges (Spatial:2153-2177)
 #pragma unroll
   for (int v = 0; v < 5; v++) {
-    double l = q[v][0][0], r = q[v][0][NG - 1];
+    Sc l = q[v][0][0], r = q[v][0][NG - 1];
     double dtmult = A.dt;
 #pragma unroll
     for (int kt = 1; kt < NA; kt++) {
@@ -267,7 +271,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
     eL[v] = l;
     eR[v] = r;
   }
-  src_avg = 0;
+  src_avg = 0.;
   if (DIR == 2) {  // compute_timeAvg (Spatial:2130-2138) + GLL quadrature (Spatial:1489-1496)
     double dtmult = A.dt;
 #pragma unroll
@@ -276,7 +280,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
       for (int ii = 0; ii < NG; ii++) sr[0][ii] += sr[kt][ii] * dtmult / (kt + 1.);
       dtmult *= A.dt;
     }
-    double sa = 0;
+    Sc sa = 0.;
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) sa += sr[0][ii] * T.wts[ii];
     src_avg = sa;
@@ -286,14 +290,14 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
 // Upwind characteristic Riemann flux at one interface (K4: Spatial:842-902 x, 1202-1260 y,
 // 1583-1644 z). The y-direction averages are not divided by density (Spatial:1210-1214).
 // kf is the interface's k index (z only) for the hydrostatic pressure subtraction.
-template <int DIR, int NG>
-__device__ __forceinline__ void riemann(const double (&qL)[5], const double (&qR)[5], int kf,
-                                        const SweepArgs &A, double (&F)[5]) {
+template <int DIR, int NG, class Sc>
+__device__ __forceinline__ void riemann(const Sc (&qL)[5], const Sc (&qR)[5], int kf, const SweepArgs &A,
+                                        Sc (&F)[5]) {
   constexpr int TA = DIR == 0 ? 1 : 0;  // first tangential velocity slot
   constexpr int TB = DIR == 2 ? 1 : 2;  // second tangential velocity slot
   constexpr int QN = 1 + DIR, QA = 1 + TA, QB = 1 + TB;
-  const double r = 0.5 * (qL[0] + qR[0]);
-  double vel[3], t;
+  const Sc r = 0.5 * (qL[0] + qR[0]);
+  Sc vel[3], t;
   if (DIR == 1) {
     vel[0] = 0.5 * (qL[1] + qR[1]);
     vel[1] = 0.5 * (qL[2] + qR[2]);
@@ -305,11 +309,11 @@ __device__ __forceinline__ void riemann(const double (&qL)[5], const double (&qR
     vel[2] = 0.5 * (qL[3] / qL[0] + qR[3] / qR[0]);
     t = 0.5 * (qL[4] / qL[0] + qR[4] / qR[0]);
   }
-  const double p = C0 * pow_cr(r * t, GAMMA);
-  const double cs2 = GAMMA * p / r;
-  const double cs = sqrt(cs2);
-  const double vn = vel[DIR], va = vel[TA], vb = vel[TB];
-  double w1, w2, w3;
+  const Sc p = C0 * pow_cr(r * t, GAMMA);
+  const Sc cs2 = GAMMA * p / r;
+  const Sc cs = sqrt(cs2);
+  const Sc vn = vel[DIR], va = vel[TA], vb = vel[TB];
+  Sc w1, w2, w3;
   if (vn > 0) {
     w1 = qL[0] - qL[4] / t;
     w2 = qL[QA] - va * qL[4] / t;
@@ -319,9 +323,9 @@ __device__ __forceinline__ void riemann(const double (&qL)[5], const double (&qR
     w2 = qR[QA] - va * qR[4] / t;
     w3 = qR[QB] - vb * qR[4] / t;
   }
-  const double w5 = vn * qR[0] / (2 * cs) - qR[QN] / (2 * cs) + qR[4] / (2 * t);
-  const double w6 = -vn * qL[0] / (2 * cs) + qL[QN] / (2 * cs) + qL[4] / (2 * t);
-  double q[5];
+  const Sc w5 = vn * qR[0] / (2. * cs) - qR[QN] / (2. * cs) + qR[4] / (2. * t);
+  const Sc w6 = -vn * qL[0] / (2. * cs) + qL[QN] / (2. * cs) + qL[4] / (2. * t);
+  Sc q[5];
   q[0] = w1 + w5 + w6;
   q[QN] = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
   q[QA] = w2 + va * w5 + va * w6;

@@ -404,6 +404,7 @@ __device__ __forceinline__ void riemann32(const float (&qL)[5], const float (&qR
 
 struct P32 {
   using Real = float;
+  static constexpr int kWdiv = 1;
   using Args = SweepArgs32;
 
   template <int ORD, int DIR, class S>
@@ -430,6 +431,9 @@ struct P32 {
     A.comp[g] = __fsub_rn(__fsub_rn(t, orig), y);
     A.state[g] = t;
   }
+  static __device__ __forceinline__ float load(const Args &A, long g) { return A.state[g]; }
+  static __device__ __forceinline__ void store(const Args &A, long g, float x) { A.state[g] = x; }
+  static __device__ __forceinline__ void store_tend(const Args &A, long g, float x) { A.tend[g] = x; }
 };
 
 cudaError_t launch_sweep_fp32(int ord, int dir, const SweepArgs32 &A, cudaStream_t st) {

@@ -21,6 +21,7 @@ namespace awfl {
 // ------------------------------------------------------------------------------------
 struct P64 {
   using Real = double;
+  static constexpr int kWdiv = 1;
   using Args = SweepArgs;
 
   template <int ORD, int DIR, class S>
@@ -48,11 +49,16 @@ struct P64 {
   static __device__ __forceinline__ void apply(const Args &A, long g, double orig, double tnd) {
     A.state[g] = orig + A.dt * tnd;
   }
+  static __device__ __forceinline__ double load(const Args &A, long g) { return A.state[g]; }
+  static __device__ __forceinline__ void store(const Args &A, long g, double x) { A.state[g] = x; }
+  static __device__ __forceinline__ void store_tend(const Args &A, long g, double x) { A.tend[g] = x; }
 };
 
 cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
   return launch_sweep_any<P64>(ord, dir, A, st);
 }
+
+
 
 // ------------------------------------------------------------------------------------
 // K6 apply (Temporal_ader.h:63-65): state(l,hs+k,hs+j,hs+i) += dt * tend(l,k,j,i).

@@ -6,6 +6,10 @@
 
 namespace awfl {
 
+namespace adj {
+struct SplitArgs;
+}
+
 // phys_params.h:4-10
 constexpr double GRAV = 9.81;
 constexpr double C0 = 27.5629410929725921310572974482;
@@ -36,6 +40,7 @@ template <int ORD> struct Tables {
 struct SweepArgs {
   double *state;   // (5, nz+2hs, ny+2hs, nx+2hs)
   double *tend;    // (5, nz, ny, nx) for MODE_TEND
+  long plane;      // tangent-linear sweep: offset of the tangent plane in state (else 0)
   int nx, ny, nz;
   int bc;          // BC along the sweep direction
   int weno_s, weno_w, sim2d, mode;
@@ -75,6 +80,13 @@ void set_unbound_error(const char *msg);
 // FP64 translation unit (awfl_fp64.cu)
 cudaError_t upload_tables_fp64(int ord, const void *tab, size_t bytes);
 cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st);
+// Differentiation TU (awfl_adjoint.cu)
+cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t st);
+cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes);
+// Adjoint reverse sweeps (awfl_adjrev.cu)
+cudaError_t launch_adjoint_split(int ord, int dir, const adj::SplitArgs &A, int need_edges, int nsm, cudaStream_t st);
+cudaError_t launch_zero_halo(double *lam, int nx, int ny, int nz, int hs, int nsm, cudaStream_t st);
+cudaError_t upload_tables_adjrev(int ord, const void *tab, size_t bytes);
 cudaError_t launch_apply_fp64(double *state, const double *tend, double dt, int nx, int ny, int nz, int hs,
                               int nsm, cudaStream_t st);
 cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const double *denstheta_c, double cfl,

@@ -28,6 +28,8 @@
 //   template <int DIR, int NG>            flux(qL[5], qR[5], kf, A, F[5])
 //   template <int DIR>                    tendency(v, Fl, Fr, src, A) -> Real
 //   apply(A, gidx, orig, tnd)             state[gidx] = orig "+" dt*tnd (MODE_APPLY)
+//   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
+//   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
 #pragma once
 
 #include "awfl_internal.h"
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
   const long tv = (long)nz * ny * nx;
   const bool periodic = A.bc == BC_PERIODIC;
 
-  auto G = [&](int v, int p) -> Real { return A.state[lb + v * sv + p * sd]; };
+  auto G = [&](int v, int p) -> Real { return P::load(A, lb + v * sv + p * sd); };
   auto ringAt = [&](int v, int p) -> Real & {
     const int s = p & (R - 1);
     return DIR == 0 ? ring[v][w * R + s] : ring[v][s * W + w];
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
     for (int v = 0; v < 5; v++) {
       const Real tnd = P::template tendency<DIR>(v, Fl[v], Fr[v], sa, A);
       if (A.mode == MODE_APPLY) P::apply(A, lb + v * sv + cell * sd, ringAt(v, cell), tnd);
-      else A.tend[tb + v * tv + cell * tsd] = tnd;
+      else P::store_tend(A, tb + v * tv + cell * tsd, tnd);
     }
   };
 
@@ -117,8 +119,8 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
       ringAt(v, c - HS) = bot;
       ringAt(v, c) = orig;
       sWrap[v][c * W + w] = orig;
-      A.state[lb + v * sv + (c - HS) * sd] = bot;
-      A.state[lb + v * sv + (L + c) * sd] = top;
+      P::store(A, lb + v * sv + (c - HS) * sd, bot);
+      P::store(A, lb + v * sv + (L + c) * sd, top);
     }
   }
   Real pre[5];
@@ -235,7 +237,10 @@ template <> struct SweepShape<9, 0> { static constexpr int C = 32, W = 2; };
 template <> struct SweepShape<9, 1> { static constexpr int C = 8, W = 16; };
 template <> struct SweepShape<9, 2> { static constexpr int C = 8, W = 16; };
 
-template <class P, int ORD, int DIR, int C = SweepShape<ORD, DIR>::C, int W = SweepShape<ORD, DIR>::W>
+// Policies with wider elements (P::kWdiv > 1) use fewer lines per CTA to stay within the
+// 48 KB of static shared memory.
+template <class P, int ORD, int DIR, int C = SweepShape<ORD, DIR>::C,
+          int W = (SweepShape<ORD, DIR>::W / P::kWdiv > 0 ? SweepShape<ORD, DIR>::W / P::kWdiv : 1)>
 cudaError_t launch_sweep_t(const typename P::Args &A, cudaStream_t st) {
   dim3 block(DIR == 0 ? C : W, DIR == 0 ? W : C);
   dim3 grid;

@@ -298,6 +298,18 @@ def emit_tv_header() -> str:
                 term = ("%s * (a[%d] * a[%d])" % (lit, q, q)) if m == q else ("%s * a[%d] * a[%d]" % (lit, m, q))
                 out.append(("  T r = %s;\n" % term) if t == 0 else ("  r = r + %s;\n" % term))
             out.append("  return r;\n}\n\n")
+    # gradients for the discrete adjoint: g[m] += lam * d(tv)/d(a[m])
+    out.append("// Gradients of the quadratic forms above: g[m] += lam * d tv / d a[m].\n")
+    for n in sorted(done):
+        out.append("template <class T> AWFL_TV_HD void awfl_tv_grad_n%d(const T *a, T lam, T *g) {\n" % n)
+        for m, q, c in tv_terms(n):
+            if m == q:
+                out.append("  g[%d] += lam * (T(%s) * a[%d]);\n" % (q, hexlit(2 * to_double(c)), q))
+            else:
+                lit = hexlit(to_double(c))
+                out.append("  g[%d] += lam * (T(%s) * a[%d]);\n" % (m, lit, q))
+                out.append("  g[%d] += lam * (T(%s) * a[%d]);\n" % (q, lit, m))
+        out.append("}\n\n")
     return "".join(out)
 
 

@@ -118,6 +118,29 @@ int awfl_split(awfl_ctx *ctx, void *d_state, double dt, int dir, void *stream);
  * reference sets to zero. */
 int awfl_step(awfl_ctx *ctx, void *d_state, double dt, void *stream);
 
+/* Tangent-linear time step (FP64 contexts): d_state_tangent holds two FP64 state planes,
+ * the state then a perturbation direction. The state advances exactly like awfl_step
+ * (bit-identical) and the second plane becomes the derivative of the new state along the
+ * direction (forward-mode differentiation of the same arithmetic; dt is held fixed).
+ * Flips dimSwitch like awfl_step. */
+int awfl_step_tlm(awfl_ctx *ctx, void *d_state_tangent, double dt, void *stream);
+
+/* Discrete adjoint of nsteps time steps (FP64 contexts; no counterpart in the reference,
+ * whose time loop is Temporal_ader.h:48-72). d_state_ckpt is the state at the start of
+ * the window (a checkpoint; not modified) and the context's dimSwitch must hold its value
+ * at that checkpoint (awfl_set_dimswitch); it is left unchanged. On entry d_lambda holds
+ * the adjoint of the state after the nsteps steps (dJ/dS_end), on return the adjoint of
+ * the checkpoint state (dJ/dS_ckpt), dt held fixed. Halo entries of d_lambda are ignored
+ * on entry and zero on return. The window is recomputed forward from the checkpoint and
+ * its split-start states kept on a device tape owned by the context (see
+ * awfl_adjoint_tape_bytes); a caller checkpointing every k steps calls this once per
+ * segment, last segment first. Stream-ordered on `stream`. */
+int awfl_step_adjoint(awfl_ctx *ctx, const void *d_state_ckpt, void *d_lambda, int nsteps, double dt,
+                      void *stream);
+
+/* Device memory awfl_step_adjoint holds for a window of nsteps steps (tape + scratch). */
+int awfl_adjoint_tape_bytes(const awfl_ctx *ctx, int nsteps, long *bytes);
+
 /* The dimSwitch flag of the context (1 = next step runs X,Y,Z). */
 int awfl_get_dimswitch(const awfl_ctx *ctx, int *value);
 int awfl_set_dimswitch(awfl_ctx *ctx, int value);
