@@ -276,30 +276,38 @@ struct CellFwd {
   double sr[NA][NG];
 };
 
+// Level 0 of one cell: GLL values of the five variables, hydrostasis added back, the
+// wall's zero normal momentum at a z boundary point.
 template <int ORD, int DIR>
-AWFL_AHD void cell_fwd(const Tables<ORD> &T, const double (&sten)[5][ORD], int kb, const CellArgs &A,
-                       CellFwd<ORD, DIR> &X) {
+AWFL_AHD void cell_level0(const Tables<ORD> &T, const double (&sten)[5][ORD], int kb, const CellArgs &A,
+                          double (&q0)[5][OrdTraits<ORD>::NGLL]) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
-  constexpr int NA = NG;
-  constexpr int NM = 1 + DIR;
   AWFL_UNROLL for (int v = 0; v < 5; v++) {
     const bool doweno = (v == idR || v == idT) ? A.weno_s : A.weno_w;
-    gll_fwd<ORD>(T, sten[v], doweno, X.q[v][0]);
+    gll_fwd<ORD>(T, sten[v], doweno, q0[v]);
   }
   AWFL_UNROLL for (int ii = 0; ii < NG; ii++) {
     if (DIR == 2) {
-      X.q[idR][0][ii] += A.dens_g[kb * NG + ii];
-      X.q[idT][0][ii] += A.denstheta_g[kb * NG + ii];
+      q0[idR][ii] += A.dens_g[kb * NG + ii];
+      q0[idT][ii] += A.denstheta_g[kb * NG + ii];
     } else {
-      X.q[idR][0][ii] += A.dens_c[HS + kb];
-      X.q[idT][0][ii] += A.denstheta_c[HS + kb];
+      q0[idR][ii] += A.dens_c[HS + kb];
+      q0[idT][ii] += A.denstheta_c[HS + kb];
     }
   }
+  if (DIR == 2 && A.bc == BC_WALL && kb == A.nz - 1) q0[idW][NG - 1] = 0.;
+  if (DIR == 2 && A.bc == BC_WALL && kb == 0) q0[idW][0] = 0.;
+}
+
+// ADER differential transform of one cell from its level 0 (X.q[v][0][ii] set on entry).
+template <int ORD, int DIR>
+AWFL_AHD void cell_dt(const Tables<ORD> &T, int kb, const CellArgs &A, CellFwd<ORD, DIR> &X) {
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int NA = NG;
+  constexpr int NM = 1 + DIR;
   const bool wtop = DIR == 2 && A.bc == BC_WALL && kb == A.nz - 1;
   const bool wbot = DIR == 2 && A.bc == BC_WALL && kb == 0;
-  if (wtop) X.q[idW][0][NG - 1] = 0.;
-  if (wbot) X.q[idW][0][0] = 0.;
   AWFL_UNROLL for (int ii = 0; ii < NG; ii++) {
     const double rr = 1. / X.q[idR][0][ii];
     const double mn = X.q[NM][0][ii] * rr;
@@ -355,6 +363,17 @@ AWFL_AHD void cell_fwd(const Tables<ORD> &T, const double (&sten)[5][ORD], int k
   }
 }
 
+template <int ORD, int DIR>
+AWFL_AHD void cell_fwd(const Tables<ORD> &T, const double (&sten)[5][ORD], int kb, const CellArgs &A,
+                       CellFwd<ORD, DIR> &X) {
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  double q0[5][NG];
+  cell_level0<ORD, DIR>(T, sten, kb, A, q0);
+  AWFL_UNROLL for (int v = 0; v < 5; v++)
+    AWFL_UNROLL for (int ii = 0; ii < NG; ii++) X.q[v][0][ii] = q0[v][ii];
+  cell_dt<ORD, DIR>(T, kb, A, X);
+}
+
 // Edges (and z source) of a forward cell record.
 template <int ORD, int DIR>
 AWFL_AHD void cell_edges(const Tables<ORD> &T, const CellFwd<ORD, DIR> &X, double dt, double (&eL)[5],
@@ -385,16 +404,17 @@ AWFL_AHD void cell_edges(const Tables<ORD> &T, const CellFwd<ORD, DIR> &X, doubl
 }
 
 // ---------------------------------------------------------------------------------------
-// Reverse of one cell: (leL, leR, lsrc) -> lsten += d(eL, eR, src)/d(sten)^T (...).
+// Reverse of one cell
 // ---------------------------------------------------------------------------------------
+// Reverse of the ADER part: (leL, leR, lsrc) -> lq0, the adjoint of the level-0 values
+// (after hydrostasis; zero at a wall's zeroed boundary point). X from cell_dt.
 template <int ORD, int DIR>
-AWFL_AHD void cell_vjp(const Tables<ORD> &T, const double (&sten)[5][ORD], int kb, const CellArgs &A,
-                       const double (&leL)[5], const double (&leR)[5], double lsrc, double (&lsten)[5][ORD]) {
+AWFL_AHD void cell_dt_vjp(const Tables<ORD> &T, int kb, const CellArgs &A, const CellFwd<ORD, DIR> &X,
+                          const double (&leL)[5], const double (&leR)[5], double lsrc,
+                          double (&lq0)[5][OrdTraits<ORD>::NGLL]) {
   constexpr int NG = OrdTraits<ORD>::NGLL;
   constexpr int NA = NG;
   constexpr int NM = 1 + DIR;
-  CellFwd<ORD, DIR> X;
-  cell_fwd<ORD, DIR>(T, sten, kb, A, X);
   const bool wtop = DIR == 2 && A.bc == BC_WALL && kb == A.nz - 1;
   const bool wbot = DIR == 2 && A.bc == BC_WALL && kb == 0;
 
@@ -498,9 +518,22 @@ AWFL_AHD void cell_vjp(const Tables<ORD> &T, const double (&sten)[5][ORD], int k
   }
   if (wtop) lq[idW][0][NG - 1] = 0.;
   if (wbot) lq[idW][0][0] = 0.;
+  AWFL_UNROLL for (int v = 0; v < 5; v++)
+    AWFL_UNROLL for (int ii = 0; ii < NG; ii++) lq0[v][ii] = lq[v][0][ii];
+}
+
+// Reverse of one whole cell: (leL, leR, lsrc) -> lsten += d(eL, eR, src)/d(sten)^T (...).
+template <int ORD, int DIR>
+AWFL_AHD void cell_vjp(const Tables<ORD> &T, const double (&sten)[5][ORD], int kb, const CellArgs &A,
+                       const double (&leL)[5], const double (&leR)[5], double lsrc, double (&lsten)[5][ORD]) {
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  CellFwd<ORD, DIR> X;
+  cell_fwd<ORD, DIR>(T, sten, kb, A, X);
+  double lq0[5][NG];
+  cell_dt_vjp<ORD, DIR>(T, kb, A, X, leL, leR, lsrc, lq0);
   AWFL_UNROLL for (int v = 0; v < 5; v++) {
     const bool doweno = (v == idR || v == idT) ? A.weno_s : A.weno_w;
-    gll_vjp<ORD>(T, sten[v], doweno, lq[v][0], lsten[v]);
+    gll_vjp<ORD>(T, sten[v], doweno, lq0[v], lsten[v]);
   }
 }
 

@@ -9,14 +9,19 @@
 //   periodic end the far edge, at a wall the near edge on both sides
 //   -> state += dt * (-(F_right - F_left) / dx (+ source on rho*w for z)).
 // Its adjoint maps lam (adjoint of the state after the split) to the adjoint before it:
-//   edges    recompute eL, eR of every cell (the linearisation point)
+//   edges    recompute the level-0 GLL values q0 and the edges eL, eR of every cell
+//            (the linearisation point)
 //   face     lF = dt/dx (lam_right_cell - lam_left_cell) -> (lqL, lqR) per face
-//   cell     (lqR of the left face, lqL of the right face, dt*lam_w) -> per-cell adjoint
-//            of the ORD stencil values
+//   cell_dt  (lqR of the left face, lqL of the right face, dt*lam_w) -> ADER reverse from
+//            q0 -> lq0, the adjoint of the level-0 values
+//   weno     per (cell, variable): lq0 -> reconstruction reverse -> adjoint of the ORD
+//            stencil values
 //   gather   lam += sum of the stencil adjoints that read this cell (through the halo
 //            mapping), so no two threads write the same word and the result is
 //            independent of the launch order
-// Each function handles one index of its own grid: cells (nz*ny*nx) or faces along DIR.
+// Each function handles one index of its own grid: cells (nz*ny*nx), faces along DIR, or
+// (variable, cell) pairs. Splitting the cell reverse in two keeps the register footprint
+// of each kernel small.
 #pragma once
 
 #include "awfl_adj.h"
@@ -30,6 +35,8 @@ struct SplitArgs {
   double *lam;          // adjoint, state layout: in = after the split, out = before it
   double *lq;           // 10 planes of nface: lqL[v], lqR[v]
   double *ls;           // 5*ORD planes of ncell: adjoint of stencil slot m of variable v
+  double *q0;           // 5*NGLL planes of ncell: level-0 values (after hydrostasis)
+  double *lq0;          // 5*NGLL planes of ncell: their adjoint
   int nx, ny, nz, hs;
   int sim2d;
   CellArgs ca;          // bc (along DIR), weno switches, dxd, dt, background
@@ -101,6 +108,9 @@ template <int ORD, int DIR> AWFL_AHD void split_edges(const Tables<ORD> &T, cons
     A.edges[v * n + c] = eL[v];
     A.edges[(5 + v) * n + c] = eR[v];
   }
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  AWFL_UNROLL for (int v = 0; v < 5; v++)
+    AWFL_UNROLL for (int ii = 0; ii < NG; ii++) A.q0[(v * NG + ii) * n + c] = X.q[v][0][ii];
 }
 
 // ---- one face: flux adjoint from the two neighbouring cells' lam, then Riemann reverse
@@ -160,10 +170,9 @@ template <int DIR> AWFL_AHD void split_face(const SplitArgs &A, long idx) {
   }
 }
 
-// ---- one cell: edge adjoints from its faces, then the reconstruction reverse
-template <int ORD, int DIR> AWFL_AHD void split_cell(const Tables<ORD> &T, const SplitArgs &A, long c) {
-  constexpr int HS = (ORD - 1) / 2;
-  constexpr int NM = 1 + DIR;
+// ---- one cell: edge adjoints from its faces, then the ADER reverse from q0
+template <int ORD, int DIR> AWFL_AHD void split_cell_dt(const Tables<ORD> &T, const SplitArgs &A, long c) {
+  constexpr int NG = OrdTraits<ORD>::NGLL;
   int i, j, k;
   decode_cell(A, c, i, j, k);
   const int L = line_len<DIR>(A);
@@ -185,12 +194,35 @@ template <int ORD, int DIR> AWFL_AHD void split_cell(const Tables<ORD> &T, const
     AWFL_UNROLL for (int v = 0; v < 5; v++) leR[v] += periodic ? A.lq[v * nf + f0] : A.lq[(5 + v) * nf + fL];
   }
   const double lsrc = DIR == 2 ? A.ca.dt * A.lam[sidx(A, idW, i, j, k)] : 0.;
-  double sten[5][ORD];
+  const long n = ncell_of(A);
+  CellFwd<ORD, DIR> X;
+  AWFL_UNROLL for (int v = 0; v < 5; v++)
+    AWFL_UNROLL for (int ii = 0; ii < NG; ii++) X.q[v][0][ii] = A.q0[(v * NG + ii) * n + c];
+  cell_dt<ORD, DIR>(T, k, A.ca, X);
+  double lq0[5][NG];
+  cell_dt_vjp<ORD, DIR>(T, k, A.ca, X, leL, leR, lsrc, lq0);
+  AWFL_UNROLL for (int v = 0; v < 5; v++)
+    AWFL_UNROLL for (int ii = 0; ii < NG; ii++) A.lq0[(v * NG + ii) * n + c] = lq0[v][ii];
+}
+
+// ---- one (variable, cell): the reconstruction reverse of that variable's stencil
+template <int ORD, int DIR> AWFL_AHD void split_weno(const Tables<ORD> &T, const SplitArgs &A, long idx) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int NM = 1 + DIR;
+  const long n = ncell_of(A);
+  const int v = (int)(idx / n);
+  const long c = idx - v * n;
+  int i, j, k;
+  decode_cell(A, c, i, j, k);
+  const int L = line_len<DIR>(A);
+  const int p = DIR == 0 ? i : (DIR == 1 ? j : k);
+  double sten[ORD];
   AWFL_UNROLL for (int m = 0; m < ORD; m++) {
     int q = p - HS + m;
     bool zero_n = false;
     if (q < 0 || q >= L) {
-      if (periodic) {
+      if (A.ca.bc == BC_PERIODIC) {
         q %= L;
         if (q < 0) q += L;
       } else {
@@ -200,15 +232,14 @@ template <int ORD, int DIR> AWFL_AHD void split_cell(const Tables<ORD> &T, const
     }
     int ii, jj, kk;
     at<DIR>(i, j, k, q, ii, jj, kk);
-    AWFL_UNROLL for (int v = 0; v < 5; v++) sten[v][m] = (zero_n && v == NM) ? 0. : A.state[sidx(A, v, ii, jj, kk)];
+    sten[m] = (zero_n && v == NM) ? 0. : A.state[sidx(A, v, ii, jj, kk)];
   }
-  double ls[5][ORD];
-  AWFL_UNROLL for (int v = 0; v < 5; v++)
-    AWFL_UNROLL for (int m = 0; m < ORD; m++) ls[v][m] = 0.;
-  cell_vjp<ORD, DIR>(T, sten, k, A.ca, leL, leR, lsrc, ls);
-  const long n = ncell_of(A);
-  AWFL_UNROLL for (int v = 0; v < 5; v++)
-    AWFL_UNROLL for (int m = 0; m < ORD; m++) A.ls[(v * ORD + m) * n + c] = ls[v][m];
+  double lq0[NG], ls[ORD];
+  AWFL_UNROLL for (int ii = 0; ii < NG; ii++) lq0[ii] = A.lq0[(v * NG + ii) * n + c];
+  AWFL_UNROLL for (int m = 0; m < ORD; m++) ls[m] = 0.;
+  const bool doweno = (v == idR || v == idT) ? A.ca.weno_s : A.ca.weno_w;
+  gll_vjp<ORD>(T, sten, doweno, lq0, ls);
+  AWFL_UNROLL for (int m = 0; m < ORD; m++) A.ls[(v * ORD + m) * n + c] = ls[m];
 }
 
 // ---- one cell: lam += every stencil adjoint that read this cell

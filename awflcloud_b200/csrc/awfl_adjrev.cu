@@ -1,11 +1,13 @@
 // Reverse sweeps of the discrete adjoint (FP64), sm_100a.
 //
-// One directional split's adjoint runs as four grid-stride kernels over the per-thread
+// One directional split's adjoint runs as five grid-stride kernels over the per-thread
 // functions of awfl_adj_split.h:
-//   adj_edges_kernel   cell   recompute the edge states (the linearisation point)
-//   adj_face_kernel    face   flux adjoint -> Riemann reverse -> (lqL, lqR)
-//   adj_cell_kernel    cell   edge adjoints -> reconstruction/ADER reverse -> stencil adjoints
-//   adj_gather_kernel  cell   lam += the stencil adjoints that read the cell (deterministic)
+//   adj_edges_kernel   cell        recompute level-0 values and edges (linearisation point)
+//   adj_face_kernel    face        flux adjoint -> Riemann reverse -> (lqL, lqR)
+//   adj_cell_kernel    cell        edge adjoints -> ADER reverse -> level-0 adjoints
+//   adj_weno_kernel    var x cell  level-0 adjoints -> WENO reverse -> stencil adjoints
+//   adj_gather_kernel  cell        lam += the stencil adjoints that read the cell
+//                                  (deterministic)
 // The arithmetic is plain FP64 with contracted multiply-adds; it is a derivative, not a
 // replay of the reference's rounding.
 #include <cuda_runtime.h>
@@ -39,7 +41,13 @@ template <int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_face_kerne
 template <int ORD, int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_cell_kernel(adj::SplitArgs A) {
   const long n = adj::ncell_of(A);
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
-    adj::split_cell<ORD, DIR>(atab<ORD>(), A, c);
+    adj::split_cell_dt<ORD, DIR>(atab<ORD>(), A, c);
+}
+
+template <int ORD, int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_weno_kernel(adj::SplitArgs A) {
+  const long n = 5 * adj::ncell_of(A);
+  for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < n; x += (long)gridDim.x * blockDim.x)
+    adj::split_weno<ORD, DIR>(atab<ORD>(), A, x);
 }
 
 template <int ORD, int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_gather_kernel(adj::SplitArgs A) {
@@ -72,6 +80,7 @@ static cudaError_t split_t(const adj::SplitArgs &A, int need_edges, int nsm, cud
   if (need_edges) adj_edges_kernel<ORD, DIR><<<grid_for(n, nsm), kAdjThreads, 0, st>>>(A);
   adj_face_kernel<DIR><<<grid_for(nf, nsm), kAdjThreads, 0, st>>>(A);
   adj_cell_kernel<ORD, DIR><<<grid_for(n, nsm), kAdjThreads, 0, st>>>(A);
+  adj_weno_kernel<ORD, DIR><<<grid_for(5 * n, nsm), kAdjThreads, 0, st>>>(A);
   adj_gather_kernel<ORD, DIR><<<grid_for(n, nsm), kAdjThreads, 0, st>>>(A);
   return cudaGetLastError();
 }

@@ -627,7 +627,8 @@ int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
   const long nspl = (c->sim2d ? 2L : 3L) * nsteps;
   const long ncell = (long)c->cfg.nx * c->cfg.ny * c->cfg.nz;
   const long nface = (long)(c->cfg.nx + 1) * (c->cfg.ny + 1) * (c->cfg.nz + 1);
-  *bytes = (long)sizeof(double) * (nspl * state_plane(c) + 10L * ncell + 10L * nface + 5L * c->cfg.ord * ncell);
+  *bytes = (long)sizeof(double) *
+           (nspl * state_plane(c) + 10L * ncell + 10L * nface + 5L * (c->cfg.ord + 2L * c->ngll) * ncell);
   return AWFL_OK;
 }
 
@@ -661,7 +662,8 @@ int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int
   if (nspl > 0) {
     rc = ensure_buffer(c, &c->d_tape, &c->tape_bytes, sizeof(double) * (size_t)(nspl * plane), "adjoint tape");
     if (rc) return rc;
-    rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes, sizeof(double) * (size_t)(10 * ncell + 10 * nface + 5L * ord * ncell),
+    rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes,
+                       sizeof(double) * (size_t)(10 * ncell + 10 * nface + 5L * (ord + 2L * c->ngll) * ncell),
                        "adjoint scratch");
     if (rc) return rc;
   }
@@ -682,6 +684,8 @@ int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int
     A.edges = c->d_adj;
     A.lq = c->d_adj + 10 * ncell;
     A.ls = c->d_adj + 10 * ncell + 10 * nface;
+    A.q0 = A.ls + 5L * ord * ncell;
+    A.lq0 = A.q0 + 5L * c->ngll * ncell;
     A.lam = (double *)d_lambda;
     A.nx = nx; A.ny = ny; A.nz = nz; A.hs = c->hs;
     A.sim2d = c->sim2d;

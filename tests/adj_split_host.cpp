@@ -1,5 +1,5 @@
 // Host driver of the per-thread adjoint functions (awfl_adj_split.h): runs the edges,
-// face, cell and gather passes of one split as plain loops, so that tests can check the
+// face, cell_dt, weno and gather passes of one split as plain loops, so that tests can check the
 // split adjoint, halo mapping included, against finite differences of the oracle's split
 // without a GPU, and its forward recomputation against the oracle's tendencies. Built as a
 // shared library by tests/test_adjoint_host.py.
@@ -22,13 +22,17 @@ template <int ORD> static void unpack(const double *t, Tables<ORD> &T) {
 
 template <int ORD, int DIR> static void run(const Tables<ORD> &T, adj::SplitArgs &A) {
   const long n = adj::ncell_of(A), nf = adj::nface_of<DIR>(A);
-  std::vector<double> edges(10 * n), lq(10 * nf), ls(5L * ORD * n);
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  std::vector<double> edges(10 * n), lq(10 * nf), ls(5L * ORD * n), q0(5L * NG * n), lq0(5L * NG * n);
   A.edges = edges.data();
   A.lq = lq.data();
   A.ls = ls.data();
+  A.q0 = q0.data();
+  A.lq0 = lq0.data();
   for (long c = 0; c < n; c++) adj::split_edges<ORD, DIR>(T, A, c);
   for (long f = 0; f < nf; f++) adj::split_face<DIR>(A, f);
-  for (long c = 0; c < n; c++) adj::split_cell<ORD, DIR>(T, A, c);
+  for (long c = 0; c < n; c++) adj::split_cell_dt<ORD, DIR>(T, A, c);
+  for (long x = 0; x < 5 * n; x++) adj::split_weno<ORD, DIR>(T, A, x);
   for (long c = 0; c < n; c++) adj::split_gather<ORD, DIR>(A, c);
 }
 
@@ -39,8 +43,10 @@ template <int ORD, int DIR> static void forward(const Tables<ORD> &T, adj::Split
   const long n = adj::ncell_of(A);
   const int L = adj::line_len<DIR>(A);
   const bool periodic = A.ca.bc == BC_PERIODIC;
-  std::vector<double> edges(10 * n), src(n, 0.);
+  constexpr int NG_ = OrdTraits<ORD>::NGLL;
+  std::vector<double> edges(10 * n), src(n, 0.), q0(5L * NG_ * n);
   A.edges = edges.data();
+  A.q0 = q0.data();
   for (long c = 0; c < n; c++) adj::split_edges<ORD, DIR>(T, A, c);
   if (DIR == 2) {  // source: recompute per cell
     for (long c = 0; c < n; c++) {
