@@ -13,7 +13,8 @@ synthetic initial data generated on the device.
 Our arm times K steps of the FP32 precision form (the headline `value`) and of the plain
 FP64 path (`fp64`), each with CUDA events on the launching stream after W warm-up steps,
 barrier + synchronize on both sides, max over ranks, and reports the FP32-vs-FP64 relative
-L2 after 100 steps. The state (357 MB in FP64) is larger
+L2 after 100 steps, and the cost of the discrete adjoint against the forward step
+(`adjoint`, FP64 at 128x128x64, 200 steps, checkpoint every 20). The state (357 MB in FP64) is larger
 than the 126 MB L2, so no flush is needed between steps. N > 1 runs N independent
 replicas (one grid per GPU, no collective): the single-domain path has no exchange step.
 
@@ -55,6 +56,9 @@ def parse():
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
+    ap.add_argument("--adj-steps", type=int, default=200)
+    ap.add_argument("--adj-ckpt", type=int, default=20)
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison arm and the 100-step accuracy check")
     return ap.parse_args()
@@ -294,6 +298,61 @@ def rel_l2_after(a, steps, local):
     return out
 
 
+def adjoint_leg(a, local):
+    """Cost of the discrete adjoint against the forward step (FP64, ord 5, 128x128x64,
+    same bubble): the forward pass of a gradient computation (adj_steps steps, a state
+    checkpoint every adj_ckpt steps) and its backward pass (awfl_step_adjoint once per
+    segment, last segment first, each recomputing its segment from the checkpoint), both
+    timed with CUDA events on the stream."""
+    import torch
+    from awflcloud_b200 import capi
+    n = (128, 128, 64)
+    ctx = capi.Context(*n, ord_=5, precision=capi.FP64, device=local)
+    s0 = ctx.new_state()
+    ctx.init_state(s0, **BUBBLE)
+    dt = ctx.cfl(s0, 0.8)
+    nseg = (a.adj_steps + a.adj_ckpt - 1) // a.adj_ckpt
+    ckpts = [torch.empty_like(s0) for _ in range(nseg)]
+    lam = torch.empty_like(s0)
+    stream = torch.cuda.current_stream()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def forward():
+        s = s0.clone()
+        ctx.dimswitch = 1
+        ds = []
+        for k in range(a.adj_steps):
+            if k % a.adj_ckpt == 0:
+                ckpts[k // a.adj_ckpt].copy_(s)
+                ds.append(ctx.dimswitch)
+            ctx.step(s, dt)
+        return s, ds
+
+    def backward(sN, ds):
+        lam.copy_(sN)  # dJ/dS_end for J = 1/2 |S_end|^2
+        for g in range(nseg - 1, -1, -1):
+            ctx.dimswitch = ds[g]
+            ctx.step_adjoint(ckpts[g], lam, min(a.adj_ckpt, a.adj_steps - g * a.adj_ckpt), dt)
+
+    sN, ds = forward()  # warm-up (and tape allocation)
+    backward(sN, ds)
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    sN, ds = forward()
+    e[1].record(stream)
+    backward(sN, ds)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    fwd_ms, adj_ms = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    return {"workload": "rising bubble 128x128x64, ord 5, FP64, %d steps, checkpoint every %d"
+                        % (a.adj_steps, a.adj_ckpt),
+            "fwd_ms_per_step": round(fwd_ms / a.adj_steps, 4), "adj_ms_per_step": round(adj_ms / a.adj_steps, 4),
+            "adj_over_fwd": round(adj_ms / fwd_ms, 3),
+            "tape_bytes": ctx.adjoint_tape_bytes(a.adj_ckpt),
+            "finite": bool(torch.isfinite(lam).all().item()),
+            "note": "backward = recomputation of every segment from its checkpoint + reverse sweeps"}
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -332,6 +391,8 @@ def run_ours(a):
                                                       "rho_w": errs[3], "rho_theta": errs[4]}
         if e2e is not None:
             line["e2e"] = e2e
+        if not a.no_adjoint:
+            line["adjoint"] = adjoint_leg(a, local)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a)
         print(json.dumps(line))
