@@ -9,6 +9,9 @@ Translation units and their numerics flags:
   awfl_noalloc.cu  allocation-free CFL variant: --fmad=false (same arithmetic as awfl_cfl)
   awfl_adjoint.cu  tangent-linear sweep: --fmad=false (its value part replays the FP64 path)
   awfl_adjrev.cu   adjoint reverse sweeps: --fmad=true (a derivative, not a replay)
+  awfl_ens32.cu    ensemble persistent sweeps, FP32 form: the awfl_fp32.cu flags
+  awfl_ens64.cu    ensemble persistent sweeps, FP64 path: --fmad=false
+  awfl_ensemble.cu ensemble host side: work lists, CUDA graph, autotuner (host code only)
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
 source tree. ``python -m awflcloud_b200.build [--force]``.
@@ -37,6 +40,9 @@ UNITS = {
     "awfl_noalloc.cu": ["--fmad=false"],
     "awfl_adjoint.cu": ["--fmad=false"],
     "awfl_adjrev.cu": ["--fmad=true"],
+    "awfl_ens32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
+    "awfl_ens64.cu": ["--fmad=false"],
+    "awfl_ensemble.cu": [],
 }
 
 

@@ -66,6 +66,20 @@ _SIGS = {
     "awfl_selftest_pow": (_I, [_VP, _D, _VP, _L, _I, _VP]),
     "awfl_measure_fma_peak": (_I, [_I, _I, _DP]),
     "awfl_cfl_noalloc": (_I, [ctypes.POINTER(AwflConfig), _VP, _VP, _VP, _D, _DP, _VP]),
+    "awfl_ensemble_create": (_I, [ctypes.POINTER(AwflConfig), _I, _I, ctypes.POINTER(_VP)]),
+    "awfl_ensemble_destroy": (_I, [_VP]),
+    "awfl_ensemble_last_error": (ctypes.c_char_p, [_VP]),
+    "awfl_ensemble_size": (_I, [_VP, ctypes.POINTER(_I)]),
+    "awfl_ensemble_member": (_I, [_VP, _I, ctypes.POINTER(_VP)]),
+    "awfl_ensemble_bind": (_I, [_VP, _I, _VP, _D]),
+    "awfl_ensemble_step": (_I, [_VP, _I, _VP]),
+    "awfl_ensemble_tune": (_I, [_VP, _I, _VP]),
+    "awfl_ensemble_num_shapes": (_I, [_VP, _I, ctypes.POINTER(_I)]),
+    "awfl_ensemble_tuning": (_I, [_VP, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
+    "awfl_ensemble_get_shape": (_I, [_VP, _I] + [ctypes.POINTER(_I)] * 4),
+    "awfl_ensemble_set_shape": (_I, [_VP, _I, _I]),
+    "awfl_ensemble_get_dimswitch": (_I, [_VP, ctypes.POINTER(_I)]),
+    "awfl_ensemble_set_dimswitch": (_I, [_VP, _I]),
     "awfl_device_alloc": (_I, [ctypes.POINTER(_VP), _L]),
     "awfl_device_free": (_I, [_VP]),
     "awfl_copy_h2d": (_I, [_VP, _VP, _L, _VP]),
@@ -139,10 +153,26 @@ class Context:
         self.precision = precision
         self.device = device
 
+    @classmethod
+    def _borrow(cls, handle, cfg, device):
+        """A Context view of a member context owned by an ensemble (not destroyed here)."""
+        self = cls.__new__(cls)
+        self.L = lib()
+        self.cfg = cfg
+        self.h = handle
+        self.ord = cfg.ord
+        self.ngll = 3 if cfg.ord == 5 else 5
+        self.hs = (cfg.ord - 1) // 2
+        self.nx, self.ny, self.nz = cfg.nx, cfg.ny, cfg.nz
+        self.precision = cfg.precision
+        self.device = device
+        self._owned = False
+        return self
+
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and getattr(self, "_owned", True):
             self.L.awfl_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -268,6 +298,104 @@ class Context:
         names = ["hyDensCells", "hyPressureCells", "hyThetaCells", "hyDensThetaCells",
                  "hyDensGLL", "hyPressureGLL", "hyThetaGLL", "hyDensThetaGLL"]
         return dict(zip(names, arrs))
+
+
+class Ensemble:
+    """An awfl_ensemble: members with their own configurations advanced together by one
+    persistent kernel per split stage (replayed from a CUDA graph)."""
+
+    def __init__(self, configs, device=0):
+        """configs: a list of dicts of Context keyword arguments (nx, ny, nz, xlen, ...,
+        ord_, precision); every member must share ord_ and precision."""
+        self.L = lib()
+        arr = (AwflConfig * len(configs))()
+        self.members = []
+        for i, kw in enumerate(configs):
+            kw = dict(kw)
+            bc = kw.pop("bc", ("periodic", "periodic", "wall"))
+            bcv = [BC[b] if isinstance(b, str) else int(b) for b in bc]
+            data = kw.pop("data", "thermal")
+            arr[i] = AwflConfig(kw["nx"], kw["ny"], kw["nz"], kw.get("xlen", 20000.0), kw.get("ylen", 20000.0),
+                                kw.get("zlen", 10000.0), bcv[0], bcv[1], bcv[2], int(kw.get("weno_scalars", True)),
+                                int(kw.get("weno_winds", True)), DATA[data] if isinstance(data, str) else int(data),
+                                kw.get("ord_", 5), kw.get("precision", FP64))
+        h = _VP()
+        rc = self.L.awfl_ensemble_create(arr, len(configs), device, ctypes.byref(h))
+        if rc != AWFL_OK:
+            raise AwflError(rc, self.L.awfl_ensemble_last_error(None).decode())
+        self.h = h
+        self.device = device
+        for i in range(len(configs)):
+            c = _VP()
+            self._check(self.L.awfl_ensemble_member(self.h, i, ctypes.byref(c)))
+            self.members.append(Context._borrow(c, arr[i], device))
+        self.states = [None] * len(configs)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.h = None  # owned by the ensemble
+            self.L.awfl_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != AWFL_OK:
+            raise AwflError(rc, self.L.awfl_ensemble_last_error(self.h).decode())
+
+    def __len__(self):
+        return len(self.members)
+
+    def bind(self, i, state, dt):
+        self.members[i]._check_buf(state, self.members[i].state_shape, "state")
+        self.states[i] = state  # keep the buffer alive while bound
+        self._check(self.L.awfl_ensemble_bind(self.h, i, _ptr(state), float(dt)))
+
+    def step(self, nsteps=1, stream=None):
+        self._check(self.L.awfl_ensemble_step(self.h, int(nsteps), _stream(stream)))
+
+    def tune(self, reps=3, stream=None):
+        self._check(self.L.awfl_ensemble_tune(self.h, int(reps), _stream(stream)))
+        return self.tuning()
+
+    def tuning(self):
+        """Per direction: list of (chunk, lines, ms per launch) of every candidate shape."""
+        out = []
+        for d in range(3):
+            n = _I()
+            self._check(self.L.awfl_ensemble_num_shapes(self.h, d, ctypes.byref(n)))
+            rows = []
+            for i in range(n.value):
+                c, w, ms = _I(), _I(), ctypes.c_float()
+                self._check(self.L.awfl_ensemble_tuning(self.h, d, i, ctypes.byref(c), ctypes.byref(w),
+                                                        ctypes.byref(ms)))
+                rows.append((c.value, w.value, ms.value))
+            out.append(rows)
+        return out
+
+    def shape(self, d):
+        """(shape index, chunk, lines, persistent grid) in use for direction d."""
+        v = [_I() for _ in range(4)]
+        self._check(self.L.awfl_ensemble_get_shape(self.h, d, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def set_shape(self, d, i):
+        self._check(self.L.awfl_ensemble_set_shape(self.h, d, int(i)))
+
+    @property
+    def dimswitch(self):
+        v = _I()
+        self._check(self.L.awfl_ensemble_get_dimswitch(self.h, ctypes.byref(v)))
+        return v.value
+
+    @dimswitch.setter
+    def dimswitch(self, value):
+        self._check(self.L.awfl_ensemble_set_dimswitch(self.h, int(value)))
 
 
 def header_symbols(path=None):

@@ -221,6 +221,7 @@ int ensure_tables(awfl_ctx *c) {
     e = upload_tables_fp64(5, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adj(5, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adjrev(5, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_ens64(5, &t, sizeof t);
   } else {
     Tables<9> t;
     std::memcpy(t.recon, c->recon.data(), sizeof t.recon);
@@ -233,10 +234,14 @@ int ensure_tables(awfl_ctx *c) {
     e = upload_tables_fp64(9, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adj(9, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adjrev(9, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_ens64(9, &t, sizeof t);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "upload of transform tables");
   e = upload_tables_fp32(c->cfg.ord, c->recon.data(), c->c2g.data(), c->s2g.data(), c->deriv.data(), c->idl.data(),
                          c->sigma, c->wts_ngll.data());
+  if (e == cudaSuccess)
+    e = upload_tables_ens32(c->cfg.ord, c->recon.data(), c->c2g.data(), c->s2g.data(), c->deriv.data(),
+                            c->idl.data(), c->sigma, c->wts_ngll.data());
   if (e != cudaSuccess) return cuda_fail(c, e, "upload of FP32 transform tables");
   if (c->device >= 0 && c->device < 256) g_tab_uploaded[c->device] |= bit;
   return AWFL_OK;
@@ -341,6 +346,25 @@ long state_plane(const awfl_ctx *c) {
 }
 
 }  // namespace
+
+// Accessors for the library's other host translation unit (awfl_ensemble.cu).
+namespace awfl {
+namespace host {
+const awfl_config &ctx_cfg(const awfl_ctx *c) { return c->cfg; }
+int ctx_hs(const awfl_ctx *c) { return c->hs; }
+int ctx_sim2d(const awfl_ctx *c) { return c->sim2d; }
+int ctx_nsm(const awfl_ctx *c) { return c->nsm; }
+int ctx_device(const awfl_ctx *c) { return c->device; }
+int ctx_set_device(awfl_ctx *c) { return set_device(c); }
+long ctx_state_elems(const awfl_ctx *c) { return (fp32(c) ? 2L : 1L) * state_plane(c); }
+SweepArgs ctx_sweep_args64(awfl_ctx *c, void *state, double dt, int dir) {
+  return sweep_args(c, state, nullptr, dt, dir, MODE_APPLY);
+}
+SweepArgs32 ctx_sweep_args32(awfl_ctx *c, void *state, double dt, int dir) {
+  return sweep_args32(c, state, nullptr, dt, dir, MODE_APPLY);
+}
+}  // namespace host
+}  // namespace awfl
 
 extern "C" {
 

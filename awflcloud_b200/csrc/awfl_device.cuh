@@ -289,7 +289,8 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
 
 // Upwind characteristic Riemann flux at one interface (K4: Spatial:842-902 x, 1202-1260 y,
 // 1583-1644 z). The y-direction averages are not divided by density (Spatial:1210-1214).
-// kf is the interface's k index (z only) for the hydrostatic pressure subtraction.
+// kf is the interface's k index for the z hydrostatic pressure subtraction (x, y: the
+// line's k, unused).
 template <int DIR, int NG, class Sc>
 __device__ __forceinline__ void riemann(const Sc (&qL)[5], const Sc (&qR)[5], int kf, const SweepArgs &A,
                                         Sc (&F)[5]) {

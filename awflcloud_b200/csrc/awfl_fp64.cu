@@ -10,49 +10,10 @@
 //   init_state_kernel      K9 initial data quadrature (Spatial:428-485)
 #include <cuda_runtime.h>
 
-#include "awfl_device.cuh"
 #include "awfl_internal.h"
-#include "awfl_sweep.cuh"
+#include "awfl_p64.cuh"
 
 namespace awfl {
-
-// ------------------------------------------------------------------------------------
-// FP64 physics policy of the line sweep (awfl_sweep.cuh): the reference's arithmetic.
-// ------------------------------------------------------------------------------------
-struct P64 {
-  using Real = double;
-  static constexpr int kWdiv = 1;
-  using Args = SweepArgs;
-
-  template <int ORD, int DIR, class S>
-  static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],
-                                               double (&eR)[5], double &src) {
-    cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
-  }
-
-  template <int DIR, int NG>
-  static __device__ __forceinline__ void flux(const double (&qL)[5], const double (&qR)[5], int kf, const Args &A,
-                                              double (&F)[5]) {
-    riemann<DIR, NG>(qL, qR, kf, A, F);
-  }
-
-  // K5 divergence (Spatial:940-956, 1298-1310, 1680-1696): z adds onto the gravity source.
-  template <int DIR>
-  static __device__ __forceinline__ double tendency(int v, double Fl, double Fr, double sa, const Args &A) {
-    const double d = -(Fr - Fl) / A.dxd;
-    if (DIR == 0) return (A.sim2d && v == idV) ? 0.0 : d;
-    if (DIR == 1) return d;
-    return (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;
-  }
-
-  // K6 apply (Temporal_ader.h:63-65)
-  static __device__ __forceinline__ void apply(const Args &A, long g, double orig, double tnd) {
-    A.state[g] = orig + A.dt * tnd;
-  }
-  static __device__ __forceinline__ double load(const Args &A, long g) { return A.state[g]; }
-  static __device__ __forceinline__ void store(const Args &A, long g, double x) { A.state[g] = x; }
-  static __device__ __forceinline__ void store_tend(const Args &A, long g, double x) { A.tend[g] = x; }
-};
 
 cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
   return launch_sweep_any<P64>(ord, dir, A, st);

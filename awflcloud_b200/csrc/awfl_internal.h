@@ -9,6 +9,9 @@ namespace awfl {
 namespace adj {
 struct SplitArgs;
 }
+template <class Args> struct EnsList;
+struct SweepArgs32;
+struct SweepArgs;
 
 // phys_params.h:4-10
 constexpr double GRAV = 9.81;
@@ -73,6 +76,16 @@ cudaError_t launch_cfl_fp32(const float *state, const double *dens_c, const doub
                             cudaStream_t st);
 cudaError_t upload_tables_fp32(int ord, const double *recon, const double *c2g, const double *s2g,
                                const double *deriv, const double *idl, double sigma, const double *wts);
+
+// Ensemble sweeps (awfl_ens32.cu, awfl_ens64.cu): launch (occ == nullptr) or query the
+// occupancy of tile shape `shape` (awfl_ens.cuh).
+cudaError_t ens_run_fp32(int ord, int dir, int shape, const EnsList<SweepArgs32> *E, int grid, int *occ,
+                         cudaStream_t st);
+cudaError_t ens_run_fp64(int ord, int dir, int shape, const EnsList<SweepArgs> *E, int grid, int *occ,
+                         cudaStream_t st);
+cudaError_t upload_tables_ens32(int ord, const double *recon, const double *c2g, const double *s2g,
+                                const double *deriv, const double *idl, double sigma, const double *wts);
+cudaError_t upload_tables_ens64(int ord, const void *tab, size_t bytes);
 
 // Error message for entry points without a context (awfl_capi.cu).
 void set_unbound_error(const char *msg);

@@ -26,6 +26,7 @@
 //   using Real; using Args;                         Args has state/tend/nx/ny/nz/bc/mode/sim2d
 //   template <int ORD, int DIR, class S> recon(sten, kb, A, eL[5], eR[5], src)
 //   template <int DIR, int NG>            flux(qL[5], qR[5], kf, A, F[5])
+//                                          (kf: the face's k for z, the line's k for x, y)
 //   template <int DIR>                    tendency(v, Fl, Fr, src, A) -> Real
 //   apply(A, gidx, orig, tnd)             state[gidx] = orig "+" dt*tnd (MODE_APPLY)
 //   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
@@ -36,8 +37,9 @@
 
 namespace awfl {
 
+// One CTA's tile: lines bx*W .. bx*W+W-1 of plane `by` (x, y sweeps: by = k; z: by = j).
 template <class P, int ORD, int DIR, int C, int W>
-__global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
+__device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int bx, const int by) {
   using Real = typename P::Real;
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
@@ -71,17 +73,17 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
   long tb;  // tendency offset of position 0
   long tsd;
   if (DIR == 0) {
-    const int k = blockIdx.y, j = blockIdx.x * W + w;
+    const int k = by, j = bx * W + w;
     L = nx; valid = j < ny; kline = k;
     lb = (HS + k) * sz + (HS + (valid ? j : 0)) * sy + HS * sx; sd = sx;
     tb = ((long)k * ny + (valid ? j : 0)) * nx; tsd = 1;
   } else if (DIR == 1) {
-    const int k = blockIdx.y, i = blockIdx.x * W + w;
+    const int k = by, i = bx * W + w;
     L = ny; valid = i < nx; kline = k;
     lb = (HS + k) * sz + HS * sy + HS + (valid ? i : 0); sd = sy;
     tb = (long)k * ny * nx + (valid ? i : 0); tsd = nx;
   } else {
-    const int j = blockIdx.y, i = blockIdx.x * W + w;
+    const int j = by, i = bx * W + w;
     L = nz; valid = i < nx;
     lb = HS * sz + (HS + j) * sy + HS + (valid ? i : 0); sd = sz;
     tb = (long)j * nx + (valid ? i : 0); tsd = (long)ny * nx;
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
       for (int v = 0; v < 5; v++) qR[v] = sEL[v][E(c)];
 #pragma unroll
       for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][E(c)];
-      P::template flux<DIR, NG>(qL, qR, f, A, F);
+      P::template flux<DIR, NG>(qL, qR, DIR == 2 ? f : kline, A, F);
 #pragma unroll
       for (int v = 0; v < 5; v++) sF[v][E(c + 1)] = F[v];
     }
@@ -224,9 +226,14 @@ __global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
       qR[v] = periodic ? sEL0[v][w] : qL[v];
       Fl[v] = sF[v][E(0)];
     }
-    P::template flux<DIR, NG>(qL, qR, L, A, F);
+    P::template flux<DIR, NG>(qL, qR, DIR == 2 ? L : kline, A, F);
     finish(L - 1, Fl, F, DIR == 2 ? sSrc[E(0)] : Real(0));
   }
+}
+
+template <class P, int ORD, int DIR, int C, int W>
+__global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
+  sweep_tile<P, ORD, DIR, C, W>(A, blockIdx.x, blockIdx.y);
 }
 
 template <int ORD, int DIR> struct SweepShape;

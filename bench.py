@@ -13,8 +13,9 @@ synthetic initial data generated on the device.
 Our arm times K steps of the FP32 precision form (the headline `value`) and of the plain
 FP64 path (`fp64`), each with CUDA events on the launching stream after W warm-up steps,
 barrier + synchronize on both sides, max over ranks, and reports the FP32-vs-FP64 relative
-L2 after 100 steps, and the cost of the discrete adjoint against the forward step
-(`adjoint`, FP64 at 128x128x64, 200 steps, checkpoint every 20). The state (357 MB in FP64) is larger
+L2 after 100 steps, the cost of the discrete adjoint against the forward step
+(`adjoint`, FP64 at 128x128x64, 200 steps, checkpoint every 20), and the batching form
+(`ensemble`: 64 FP32 members of uneven sizes, 50 steps, persistent kernels in a CUDA graph). The state (357 MB in FP64) is larger
 than the 126 MB L2, so no flush is needed between steps. N > 1 runs N independent
 replicas (one grid per GPU, no collective): the single-domain path has no exchange step.
 
@@ -59,6 +60,9 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost leg")
     ap.add_argument("--adj-steps", type=int, default=200)
     ap.add_argument("--adj-ckpt", type=int, default=20)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble (batching) leg")
+    ap.add_argument("--ens-members", type=int, default=64)
+    ap.add_argument("--ens-steps", type=int, default=50)
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison arm and the 100-step accuracy check")
     return ap.parse_args()
@@ -353,6 +357,67 @@ def adjoint_leg(a, local):
             "note": "backward = recomputation of every segment from its checkpoint + reverse sweeps"}
 
 
+ENS_SIZES = ((32, 32, 32), (64, 64, 32), (96, 96, 48), (128, 128, 64))
+
+
+def ensemble_leg(a, local):
+    """Batching form: ens_members FP32 ord-5 members with seeded sizes from ENS_SIZES and
+    seeded bubbles (centre x, y in [5, 15] km, z in [1.5, 3] km, amp in [1, 4] K, radius in
+    [1, 3] km), advanced ens_steps steps by the ensemble (one persistent kernel per split
+    stage, two steps per CUDA-graph replay, autotuned tile shapes), against the same
+    members stepped one after another through awfl_step."""
+    import numpy as np
+    import torch
+    from awflcloud_b200 import capi
+    rng = np.random.default_rng(20261203)
+    picks = rng.integers(0, len(ENS_SIZES), size=a.ens_members)
+    cfgs = [dict(nx=ENS_SIZES[p][0], ny=ENS_SIZES[p][1], nz=ENS_SIZES[p][2], precision=capi.FP32, ord_=5)
+            for p in picks]
+    E = capi.Ensemble(cfgs, device=local)
+    states, dts = [], []
+    for i, m in enumerate(E.members):
+        s = m.new_state()
+        r = float(rng.uniform(1000.0, 3000.0))
+        m.init_state(s, kind=1, shape=1, x0=float(rng.uniform(5e3, 15e3)), y0=float(rng.uniform(5e3, 15e3)),
+                     z0=float(rng.uniform(1.5e3, 3e3)), xrad=r, yrad=r, zrad=r, amp=float(rng.uniform(1, 4)),
+                     pwr=1.0, noise_amp=0.01, noise_seed=20261203 + i)
+        dt = m.cfl(s, 0.8)
+        E.bind(i, s, dt)
+        states.append(s)
+        dts.append(dt)
+    cells = sum(c["nx"] * c["ny"] * c["nz"] for c in cfgs)
+    stream = torch.cuda.current_stream()
+    table = E.tune(reps=3, stream=stream)
+    E.step(2, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    E.step(a.ens_steps, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ens_ms = e0.elapsed_time(e1)
+    # the same members, one context at a time (3 launches per member per step)
+    for i, m in enumerate(E.members):
+        m.step(states[i], dts[i])
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(a.ens_steps):
+        for i, m in enumerate(E.members):
+            m.step(states[i], dts[i])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    counts = {"%dx%dx%d" % s: int((picks == k).sum()) for k, s in enumerate(ENS_SIZES)}
+    return {"workload": "%d FP32 ord-5 members, %d steps, sizes %s" % (a.ens_members, a.ens_steps, counts),
+            "value": round(cells * a.ens_steps / (ens_ms * 1e-3) / 1e6, 3), "unit": UNIT,
+            "ms_per_step": round(ens_ms / a.ens_steps, 4),
+            "sequential_value": round(cells * a.ens_steps / (seq_ms * 1e-3) / 1e6, 3),
+            "speedup_vs_sequential": round(seq_ms / ens_ms, 3),
+            "tuned_shapes": [{"dir": "xyz"[d], "chunk": E.shape(d)[1], "lines": E.shape(d)[2], "grid": E.shape(d)[3],
+                              "candidates_ms": [[c, w, round(ms, 4)] for c, w, ms in table[d]]} for d in range(3)],
+            "gpu_launches_per_step": 3, "finite": all(bool(torch.isfinite(s).all().item()) for s in states)}
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -393,6 +458,8 @@ def run_ours(a):
             line["e2e"] = e2e
         if not a.no_adjoint:
             line["adjoint"] = adjoint_leg(a, local)
+        if not a.no_ensemble:
+            line["ensemble"] = ensemble_leg(a, local)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a)
         print(json.dumps(line))

@@ -194,6 +194,39 @@ int awfl_memset_device(void *d_ptr, int value, long bytes, void *stream);
 int awfl_stream_synchronize(void *stream);
 int awfl_device_synchronize(void);
 
+/* ---- Ensemble (batching) form: no counterpart in the reference ----------------------
+ * An ensemble advances many independent members (each its own awfl_config: grid size,
+ * domain, boundary conditions; all with the same precision and ord) together: per split
+ * stage one persistent kernel covers the tiles of every member, and pairs of time steps
+ * replay a CUDA graph. An FP64 member's result is bit-identical to awfl_step on its own
+ * context; an FP32 member's agrees to FP32 rounding (multiply-add contraction may be
+ * placed differently in the persistent kernel). The ensemble owns the member contexts (awfl_ensemble_member lends them for
+ * awfl_init_state, awfl_cfl, ...); the caller owns the state buffers it binds. */
+typedef struct awfl_ensemble awfl_ensemble;
+
+int awfl_ensemble_create(const awfl_config *cfgs, int nmembers, int device, awfl_ensemble **ens);
+int awfl_ensemble_destroy(awfl_ensemble *ens);
+const char *awfl_ensemble_last_error(const awfl_ensemble *ens);
+int awfl_ensemble_size(const awfl_ensemble *ens, int *nmembers);
+int awfl_ensemble_member(awfl_ensemble *ens, int i, awfl_ctx **ctx);
+/* Member i advances d_state (awfl_sizes elements of its context) with time step dt. */
+int awfl_ensemble_bind(awfl_ensemble *ens, int i, void *d_state, double dt);
+/* nsteps time steps of every member (dimSwitch kept by the ensemble, flipped per step). */
+int awfl_ensemble_step(awfl_ensemble *ens, int nsteps, void *stream);
+/* Autotuner: times `reps` launches of every candidate tile shape of each direction on
+ * scratch copies of the bound states (the bound states are not advanced) and keeps the
+ * fastest; synchronizes `stream`. */
+int awfl_ensemble_tune(awfl_ensemble *ens, int reps, void *stream);
+int awfl_ensemble_num_shapes(const awfl_ensemble *ens, int dir, int *n);
+/* Candidate i of direction dir: chunk length, lines per CTA, and the tuner's ms per
+ * launch (negative before tuning). */
+int awfl_ensemble_tuning(const awfl_ensemble *ens, int dir, int i, int *chunk, int *lines, float *ms);
+/* Shape in use for direction dir (index, chunk, lines, persistent grid size). */
+int awfl_ensemble_get_shape(const awfl_ensemble *ens, int dir, int *shape, int *chunk, int *lines, int *grid);
+int awfl_ensemble_set_shape(awfl_ensemble *ens, int dir, int shape);
+int awfl_ensemble_get_dimswitch(const awfl_ensemble *ens, int *value);
+int awfl_ensemble_set_dimswitch(awfl_ensemble *ens, int value);
+
 #ifdef __cplusplus
 }
 #endif
