@@ -18,7 +18,10 @@ namespace awfl {
 struct PTLM {
   using Real = Dual;
   static constexpr int kWdiv = 2;
+  static constexpr bool kAsyncRing = false;
   using Args = SweepArgs;
+  struct Aux {};
+  static __device__ __forceinline__ void load_aux(const Args &, long, long, Aux &) {}
 
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, Dual (&eL)[5], Dual (&eR)[5],
@@ -37,7 +40,7 @@ struct PTLM {
     if (DIR == 1) return d;
     return (A.sim2d && v == idV) ? Dual(0.0) : (v == idW ? sa : Dual(0.0)) + d;
   }
-  static __device__ __forceinline__ void apply(const Args &A, long g, Dual orig, Dual tnd) {
+  static __device__ __forceinline__ void apply(const Args &A, long g, Dual orig, Dual tnd, const Aux &, int) {
     A.state[g] = orig.v + A.dt * tnd.v;
     A.state[g + A.plane] = orig.d + A.dt * tnd.d;
   }

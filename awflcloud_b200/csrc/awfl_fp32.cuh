@@ -410,7 +410,16 @@ __device__ __forceinline__ void riemann32(const float (&qL)[5], const float (&qR
 struct P32 {
   using Real = float;
   static constexpr int kWdiv = 1;
+  static constexpr bool kAsyncRing = true;
   using Args = SweepArgs32;
+  // the Kahan compensations of the cell's five variables, loaded before the reconstruction
+  struct Aux {
+    float c[5];
+  };
+  static __device__ __forceinline__ void load_aux(const Args &A, long g0, long sv, Aux &aux) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) aux.c[v] = A.comp[g0 + v * sv];
+  }
 
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, float (&eL)[5], float (&eR)[5],
@@ -430,8 +439,8 @@ struct P32 {
     return (A.sim2d && v == idV) ? 0.f : (v == idW ? sa + d : d);
   }
   // Kahan-compensated stage update: s += dt*tnd with the running compensation c.
-  static __device__ __forceinline__ void apply(const Args &A, long g, float orig, float tnd) {
-    const float y = A.dt * tnd - A.comp[g];
+  static __device__ __forceinline__ void apply(const Args &A, long g, float orig, float tnd, const Aux &aux, int v) {
+    const float y = A.dt * tnd - aux.c[v];
     const float t = orig + y;
     A.comp[g] = __fsub_rn(__fsub_rn(t, orig), y);
     A.state[g] = t;

@@ -15,7 +15,10 @@ namespace awfl {
 struct P64 {
   using Real = double;
   static constexpr int kWdiv = 1;
+  static constexpr bool kAsyncRing = false;
   using Args = SweepArgs;
+  struct Aux {};
+  static __device__ __forceinline__ void load_aux(const Args &, long, long, Aux &) {}
 
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],
@@ -39,7 +42,7 @@ struct P64 {
   }
 
   // K6 apply (Temporal_ader.h:63-65)
-  static __device__ __forceinline__ void apply(const Args &A, long g, double orig, double tnd) {
+  static __device__ __forceinline__ void apply(const Args &A, long g, double orig, double tnd, const Aux &, int) {
     A.state[g] = orig + A.dt * tnd;
   }
   static __device__ __forceinline__ double load(const Args &A, long g) { return A.state[g]; }

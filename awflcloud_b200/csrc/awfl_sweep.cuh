@@ -28,7 +28,10 @@
 //   template <int DIR, int NG>            flux(qL[5], qR[5], kf, A, F[5])
 //                                          (kf: the face's k for z, the line's k for x, y)
 //   template <int DIR>                    tendency(v, Fl, Fr, src, A) -> Real
-//   apply(A, gidx, orig, tnd)             state[gidx] = orig "+" dt*tnd (MODE_APPLY)
+//   struct Aux; load_aux(A, g0, sv, aux)   per-cell inputs of the update (variable v at
+//                                          g0 + v*sv), loaded a reconstruction ahead
+//   apply(A, gidx, orig, tnd, aux, v)      state[gidx] = orig "+" dt*tnd (MODE_APPLY)
+//   kAsyncRing                             next-chunk rows by cp.async into a 4C ring
 //   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
 //   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
 #pragma once
@@ -37,19 +40,32 @@
 
 namespace awfl {
 
+// Asynchronous global -> shared copy of one element (cp.async, sm_80+; 4 or 8 bytes).
+template <class T> __device__ __forceinline__ void cp_async_row(T *dst_smem, const T *src_gmem) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async of 4 or 8 bytes");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src_gmem), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // One CTA's tile: lines bx*W .. bx*W+W-1 of plane `by` (x, y sweeps: by = k; z: by = j).
 template <class P, int ORD, int DIR, int C, int W>
 __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int bx, const int by) {
   using Real = typename P::Real;
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
-  constexpr int R = 2 * C;  // ring length (power of two, >= C + 2*HS)
+  // Next-chunk rows: policies with kAsyncRing copy them global -> shared with cp.async one
+  // chunk ahead (issued before the reconstruction, no registers held), which needs a ring
+  // of 4C so that the rows in flight never share a slot with rows still being read;
+  // otherwise they are loaded into registers and stored at the next chunk's start.
+  constexpr bool ASYNC = P::kAsyncRing;
+  constexpr int R = ASYNC ? 4 * C : 2 * C;  // ring length (power of two, >= C + 2*HS)
   constexpr int NM = 1 + DIR;
   static_assert((C & (C - 1)) == 0 && C >= 2 * HS, "chunk must be a power of two >= 2*HS");
-  // When to load the next chunk's rows: before the reconstruction (its latency hidden
+  // Register path: load the next chunk's rows before the reconstruction (latency hidden
   // behind it, at the cost of 5 live registers) for the z sweep, whose loads stride over
   // whole planes; after the updates for x and y, where occupancy matters more (measured).
-  constexpr bool EARLY_PREFETCH = DIR == 2;
+  constexpr bool EARLY_PREFETCH = !ASYNC && DIR == 2;
 
   __shared__ Real ring[5][R * W];
   __shared__ Real sEL[5][(C + 1) * W];
@@ -102,12 +118,19 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
     if (periodic) return first ? G(v, q) : sWrap[v][q * W + w];
     return v == NM ? Real(0) : G(v, L - 1);
   };
-  auto finish = [&](int cell, const Real *Fl, const Real *Fr, Real sa) {
+  auto finish = [&](int cell, const Real *Fl, const Real *Fr, Real sa, const typename P::Aux &aux) {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       const Real tnd = P::template tendency<DIR>(v, Fl[v], Fr[v], sa, A);
-      if (A.mode == MODE_APPLY) P::apply(A, lb + v * sv + cell * sd, ringAt(v, cell), tnd);
+      if (A.mode == MODE_APPLY) P::apply(A, lb + v * sv + cell * sd, ringAt(v, cell), tnd, aux, v);
       else P::store_tend(A, tb + v * tv + cell * tsd, tnd);
+    }
+  };
+  // a row value into its ring slot: asynchronously when it is a load of an interior cell
+  auto stage = [&](int v, int p, bool first) {
+    if constexpr (ASYNC) {
+      if (p < L) cp_async_row(&ringAt(v, p), &A.state[lb + v * sv + p * sd]);
+      else ringAt(v, p) = topval(v, p, first);
     }
   };
 
@@ -125,11 +148,16 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       P::store(A, lb + v * sv + (L + c) * sd, top);
     }
   }
-  Real pre[5];
+  Real pre[ASYNC ? 1 : 5];
   if (valid) {
     const int p = HS + c;
+    if constexpr (ASYNC) {
 #pragma unroll
-    for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, true);
+      for (int v = 0; v < 5; v++) stage(v, p, true);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, true);
+    }
   }
   // periodic: the left state of face 0 is the right edge of cell L-1
   if (valid && periodic && c == 0) {
@@ -149,11 +177,22 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   for (int t = 0; t < nchunk; t++) {
     const int base = t * C;
     const int nvalid = min(C, L - base);
-    if (valid) {
+    if constexpr (ASYNC) {
+      cp_async_wait_all();  // this thread's rows of the chunk have landed
+    } else if (valid) {
 #pragma unroll
       for (int v = 0; v < 5; v++) ringAt(v, base + HS + c) = pre[v];
     }
     __syncthreads();  // (A)
+    if constexpr (ASYNC) {  // the next chunk's rows, a chunk ahead
+      if (valid && t + 1 < nchunk) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) stage(v, base + C + HS + c, false);
+      }
+    }
+    // the compensation (or other per-cell input) of the cell this thread updates below
+    typename P::Aux aux;
+    if (valid && c < nvalid && base + c >= 1 && A.mode == MODE_APPLY) P::load_aux(A, lb + (base + c - 1) * sd, sv, aux);
     // next chunk's rows (stored into the ring at the next (A); the updates of this chunk
     // never reach them)
     if (EARLY_PREFETCH && valid && t + 1 < nchunk) {
@@ -199,10 +238,10 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
           Fl[v] = sF[v][E(c)];
           Fr[v] = sF[v][E(c + 1)];
         }
-        finish(cell, Fl, Fr, DIR == 2 ? sSrc[E(c)] : Real(0));
+        finish(cell, Fl, Fr, DIR == 2 ? sSrc[E(c)] : Real(0), aux);
       }
     }
-    if (!EARLY_PREFETCH && valid && t + 1 < nchunk) {
+    if (!ASYNC && !EARLY_PREFETCH && valid && t + 1 < nchunk) {
       const int p = base + C + HS + c;
 #pragma unroll
       for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
@@ -227,7 +266,9 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       Fl[v] = sF[v][E(0)];
     }
     P::template flux<DIR, NG>(qL, qR, DIR == 2 ? L : kline, A, F);
-    finish(L - 1, Fl, F, DIR == 2 ? sSrc[E(0)] : Real(0));
+    typename P::Aux aux;
+    if (A.mode == MODE_APPLY) P::load_aux(A, lb + (L - 1) * sd, sv, aux);
+    finish(L - 1, Fl, F, DIR == 2 ? sSrc[E(0)] : Real(0), aux);
   }
 }
 
