@@ -28,7 +28,7 @@ template <class Args> struct EnsList {
 };
 
 template <class P, int ORD, int DIR, int C, int W>
-__global__ void __launch_bounds__(C *W) ens_sweep_kernel(EnsList<typename P::Args> E) {
+__global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) ens_sweep_kernel(EnsList<typename P::Args> E) {
   __shared__ typename P::Args sA;
   for (long t = blockIdx.x; t < E.total; t += gridDim.x) {
     int lo = 0, hi = E.n - 1;

@@ -411,6 +411,7 @@ struct P32 {
   using Real = float;
   static constexpr int kWdiv = 1;
   static constexpr bool kAsyncRing = true;
+  static constexpr int min_blocks(int) { return 1; }  // forcing more CTAs per SM measured slower
   using Args = SweepArgs32;
   // the Kahan compensations of the cell's five variables, loaded before the reconstruction
   struct Aux {

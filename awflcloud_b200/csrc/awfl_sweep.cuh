@@ -32,6 +32,7 @@
 //                                          g0 + v*sv), loaded a reconstruction ahead
 //   apply(A, gidx, orig, tnd, aux, v)      state[gidx] = orig "+" dt*tnd (MODE_APPLY)
 //   kAsyncRing                             next-chunk rows by cp.async into a 4C ring
+//   min_blocks(ORD)                        CTAs per SM the register budget must allow
 //   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
 //   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
 #pragma once
@@ -273,7 +274,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 }
 
 template <class P, int ORD, int DIR, int C, int W>
-__global__ void __launch_bounds__(C *W) sweep_kernel(typename P::Args A) {
+__global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) sweep_kernel(typename P::Args A) {
   sweep_tile<P, ORD, DIR, C, W>(A, blockIdx.x, blockIdx.y);
 }
 
