@@ -12,6 +12,7 @@
 #include "awfl_oracle.h"
 
 #include <math.h>
+#include <tgmath.h> /* pow/exp/sqrt/... follow the argument type (oreal) */
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -22,6 +23,9 @@
  * are correctly rounded (awfl_pow_cr.h) instead of glibc's, like the GPU FP64 kernels.
  * The hydrostatic profiles (init-time, computed on the host by the library as well) keep
  * glibc's pow/exp. */
+#if defined(ORACLE_CR_POW) && defined(ORACLE_LONG_DOUBLE)
+#error "ORACLE_CR_POW is a double-precision variant"
+#endif
 #ifdef ORACLE_CR_POW
 #include "awfl_pow_cr.h"
 #define OPOW(x, y) awfl_test_pow_cr((x), (y))
@@ -59,12 +63,12 @@
 #endif
 
 /* phys_params.h:4-10 */
-static const double GRAV = 9.81;
-static const double CP = 1004.;
-static const double RD = 287.;
-static const double P0 = 1.0e5;
-static const double C0 = 27.5629410929725921310572974482;
-static const double GAMMA = 1.40027894002789400278940027894;
+static const oreal GRAV = 9.81;
+static const oreal CP = 1004.;
+static const oreal RD = 287.;
+static const oreal P0 = 1.0e5;
+static const oreal C0 = 27.5629410929725921310572974482;
+static const oreal GAMMA = 1.40027894002789400278940027894;
 
 enum { idR = 0, idU = 1, idV = 2, idW = 3, idT = 4 };
 enum { BC_PERIODIC = 0, BC_WALL = 1 };
@@ -72,23 +76,23 @@ enum { DATA_THERMAL = 1, DATA_COLLISION = 2, DATA_STRAKA = 3, DATA_IGW = 4 };
 
 struct oracle_ctx {
   int nx, ny, nz;
-  double xlen, ylen, zlen, dx, dy, dz;
+  oreal xlen, ylen, zlen, dx, dy, dz;
   int bc[3];
   int weno_scalars, weno_winds, sim2d, data_spec, dimswitch;
   /* tables (Spatial:274-315) */
-  double recon[ORD][ORD][ORD];
-  double c2g[ORD][NGLL];   /* coefs_to_gll(col=s, row=ii) */
-  double s2g[ORD][NGLL];   /* sten_to_gll */
-  double deriv[NGLL][NGLL];
-  double idl[HS + 2];
-  double sigma;
-  double pts_ord[ORD], wts_ord[ORD], pts_ngll[NGLL], wts_ngll[NGLL];
+  oreal recon[ORD][ORD][ORD];
+  oreal c2g[ORD][NGLL];   /* coefs_to_gll(col=s, row=ii) */
+  oreal s2g[ORD][NGLL];   /* sten_to_gll */
+  oreal deriv[NGLL][NGLL];
+  oreal idl[HS + 2];
+  oreal sigma;
+  oreal pts_ord[ORD], wts_ord[ORD], pts_ngll[NGLL], wts_ngll[NGLL];
   /* hydrostatic background (Spatial:371-425) */
-  double *hyDensCells, *hyPressureCells, *hyThetaCells, *hyDensThetaCells; /* nz+2hs */
-  double *hyDensGLL, *hyPressureGLL, *hyThetaGLL, *hyDensThetaGLL;         /* nz*ngll */
+  oreal *hyDensCells, *hyPressureCells, *hyThetaCells, *hyDensThetaCells; /* nz+2hs */
+  oreal *hyDensGLL, *hyPressureGLL, *hyThetaGLL, *hyDensThetaGLL;         /* nz*ngll */
   /* scratch (Spatial:327-330) */
-  double *limits; /* (5,2,nz+1,ny+1,nx+1) */
-  double *flux;   /* (5,nz+1,ny+1,nx+1) */
+  oreal *limits; /* (5,2,nz+1,ny+1,nx+1) */
+  oreal *flux;   /* (5,nz+1,ny+1,nx+1) */
 };
 
 /* ---------------------------------------------------------------- indexing */
@@ -105,36 +109,36 @@ static inline long fidx(const oracle_ctx *c, int l, int k, int j, int i) {
   return (((long)l * (c->nz + 1) + k) * (c->ny + 1) + j) * (c->nx + 1) + i;
 }
 
-static inline double dmax(double a, double b) { return a > b ? a : b; }
-static inline double dmin(double a, double b) { return a < b ? a : b; }
+static inline oreal dmax(oreal a, oreal b) { return a > b ? a : b; }
+static inline oreal dmin(oreal a, oreal b) { return a < b ? a : b; }
 
 /* ---------------------------------------------------------------- WENO */
 /* TransformMatrices::coefs_to_tv: ordered quadratic form, c*(a*a) or (c*a_m)*a_q. */
-static double tv_eval(const double *a, int nterm, const int *m, const int *q, const double *cf) {
-  double r = 0;
+static oreal tv_eval(const oreal *a, int nterm, const int *m, const int *q, const double *cf) {
+  oreal r = 0;
   for (int t = 0; t < nterm; t++) {
-    double term = (m[t] == q[t]) ? cf[t] * (a[q[t]] * a[q[t]]) : cf[t] * a[m[t]] * a[q[t]];
+    oreal term = (m[t] == q[t]) ? cf[t] * (a[q[t]] * a[q[t]]) : cf[t] * a[m[t]] * a[q[t]];
     r = (t == 0) ? term : r + term;
   }
   return r;
 }
-static double tv_lo(const double *a) {
+static oreal tv_lo(const oreal *a) {
   return tv_eval(a, TV_LO_N, TVS(lo, m), TVS(lo, q), TVS(lo, c));
 }
-static double tv_hi(const double *a) {
+static oreal tv_hi(const oreal *a) {
   return tv_eval(a, TV_HI_N, TVS(hi, m), TVS(hi, q), TVS(hi, c));
 }
 
 /* WenoLimiter.h:20-25 */
-static void convexify(double *wts) {
-  double sum = 0.;
-  const double eps = 1.0e-20;
+static void convexify(oreal *wts) {
+  oreal sum = 0.;
+  const oreal eps = 1.0e-20;
   for (int i = 0; i < HS + 2; i++) sum += wts[i];
   for (int i = 0; i < HS + 2; i++) wts[i] /= (sum + eps);
 }
 
 /* WenoLimiter.h:12-17 */
-static void map_weights(const double *idl, double *wts) {
+static void map_weights(const oreal *idl, oreal *wts) {
   for (int i = 0; i < HS + 2; i++) {
     wts[i] = wts[i] * (idl[i] + idl[i] * idl[i] - 3. * idl[i] * wts[i] + wts[i] * wts[i]) /
              (idl[i] * idl[i] + wts[i] * (1. - 2. * idl[i]));
@@ -142,7 +146,7 @@ static void map_weights(const double *idl, double *wts) {
 }
 
 /* WenoLimiter.h:28-90 (ord 5 and 9 rows) */
-static void weno_set_ideal_sigma(double *idl, double *sigma) {
+static void weno_set_ideal_sigma(oreal *idl, oreal *sigma) {
 #if ORD == 5
   *sigma = 0.73564225445964;
   idl[0] = 1.; idl[1] = 73.564225445964; idl[2] = 1.; idl[3] = 1584.89319246111;
@@ -155,9 +159,9 @@ static void weno_set_ideal_sigma(double *idl, double *sigma) {
 }
 
 /* WenoLimiter.h:93-172 */
-static void weno_coefs(const oracle_ctx *c, const double *u, double *aw) {
-  double tv[HS + 2], wts[HS + 2], a[HS + 2][ORD], lotmp[HS + 1], hitmp[ORD];
-  const double eps = 1.0e-20;
+static void weno_coefs(const oracle_ctx *c, const oreal *u, oreal *aw) {
+  oreal tv[HS + 2], wts[HS + 2], a[HS + 2][ORD], lotmp[HS + 1], hitmp[ORD];
+  const oreal eps = 1.0e-20;
   for (int j = 0; j < HS + 2; j++)
     for (int i = 0; i < ORD; i++) a[j][i] = 0.;
   for (int i = 0; i < HS + 1; i++)
@@ -174,7 +178,7 @@ static void weno_coefs(const oracle_ctx *c, const double *u, double *aw) {
   }
   for (int ii = 0; ii < ORD; ii++) hitmp[ii] = a[HS + 1][ii];
   tv[HS + 1] = tv_hi(hitmp);
-  double lo_avg = 0.;
+  oreal lo_avg = 0.;
   for (int i = 0; i < HS + 1; i++) lo_avg += tv[i];
   lo_avg /= HS + 1;
   tv[HS + 1] = lo_avg + (tv[HS + 1] - lo_avg) * c->sigma;
@@ -188,18 +192,18 @@ static void weno_coefs(const oracle_ctx *c, const double *u, double *aw) {
 }
 
 /* Spatial:1800-1833 */
-static void reconstruct_gll(const oracle_ctx *c, const double *stencil, double *out, int doweno) {
+static void reconstruct_gll(const oracle_ctx *c, const oreal *stencil, oreal *out, int doweno) {
   if (doweno) {
-    double wc[ORD];
+    oreal wc[ORD];
     weno_coefs(c, stencil, wc);
     for (int ii = 0; ii < NGLL; ii++) {
-      double tmp = 0;
+      oreal tmp = 0;
       for (int s = 0; s < ORD; s++) tmp += c->c2g[s][ii] * wc[s];
       out[ii] = tmp;
     }
   } else {
     for (int ii = 0; ii < NGLL; ii++) {
-      double tmp = 0;
+      oreal tmp = 0;
       for (int s = 0; s < ORD; s++) tmp += c->s2g[s][ii] * stencil[s];
       out[ii] = tmp;
     }
@@ -211,14 +215,14 @@ static void reconstruct_gll(const oracle_ctx *c, const double *stencil, double *
  * four normal-momentum flux products (normal*u, normal*v, normal*w, normal*t)/r, and the
  * (rho*theta)^gamma series g. dir selects the normal momentum (1+dir). */
 typedef struct {
-  double q[NUMSTATE][NADER][NGLL];
-  double f[4][NADER][NGLL];
-  double g[NADER][NGLL];
-  double src[NADER][NGLL];
+  oreal q[NUMSTATE][NADER][NGLL];
+  oreal f[4][NADER][NGLL];
+  oreal g[NADER][NGLL];
+  oreal src[NADER][NGLL];
 } ader_t;
 
 /* diffTransformEulerConsX/Y/Z (Spatial:1837-1916, 1920-2000, 2004-2091). */
-static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, double dxd, int k) {
+static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, oreal dxd, int k) {
   const int nm = 1 + dir; /* normal momentum index */
   for (int kt = 1; kt < NADER; kt++)
     for (int ii = 0; ii < NGLL; ii++) {
@@ -227,9 +231,9 @@ static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, double dxd, 
     }
   for (int kt = 0; kt < NADER - 1; kt++) {
     for (int ii = 0; ii < NGLL; ii++) {
-      double dq[NUMSTATE] = {0, 0, 0, 0, 0};
+      oreal dq[NUMSTATE] = {0, 0, 0, 0, 0};
       for (int s = 0; s < NGLL; s++) {
-        double D = c->deriv[s][ii];
+        oreal D = c->deriv[s][ii];
         dq[idR] += D * (A->q[nm][kt][s]);
         for (int v = 1; v <= 3; v++) {
           if (v == nm) {
@@ -257,7 +261,7 @@ static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, double dxd, 
       }
     }
     for (int ii = 0; ii < NGLL; ii++) {
-      double tot[4] = {0, 0, 0, 0};
+      oreal tot[4] = {0, 0, 0, 0};
       for (int ir = 0; ir <= kt + 1; ir++) {
         for (int x = 0; x < 4; x++) {
           int xv = x + 1; /* u->ru(1), v->rv(2), w->rw(3), t->rt(4) */
@@ -265,7 +269,7 @@ static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, double dxd, 
         }
       }
       for (int x = 0; x < 4; x++) A->f[x][kt + 1][ii] = tot[x] / A->q[idR][0][ii];
-      double tg = 0;
+      oreal tg = 0;
       for (int ir = 0; ir <= kt; ir++) {
         tg += (kt + 1. - ir) * (GAMMA * A->g[ir][ii] * A->q[idT][kt + 1 - ir][ii] -
                                 A->q[idT][ir][ii] * A->g[kt + 1 - ir][ii]);
@@ -278,8 +282,8 @@ static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, double dxd, 
 }
 
 /* compute_timeAvg_edges (Spatial:2153-2177): edge points only. */
-static void time_avg_edges(double dts[NADER][NGLL], double dt) {
-  double dtmult = dt;
+static void time_avg_edges(oreal dts[NADER][NGLL], oreal dt) {
+  oreal dtmult = dt;
   for (int kt = 1; kt < NADER; kt++) {
     dts[0][0] += dts[kt][0] * dtmult / (kt + 1.);
     dts[0][NGLL - 1] += dts[kt][NGLL - 1] * dtmult / (kt + 1.);
@@ -288,8 +292,8 @@ static void time_avg_edges(double dts[NADER][NGLL], double dt) {
 }
 
 /* compute_timeAvg (Spatial:2130-2138): all points. */
-static void time_avg_full(double dts[NADER][NGLL], double dt) {
-  double dtmult = dt;
+static void time_avg_full(oreal dts[NADER][NGLL], oreal dt) {
+  oreal dtmult = dt;
   for (int kt = 1; kt < NADER; kt++) {
     for (int ii = 0; ii < NGLL; ii++) dts[0][ii] += dts[kt][ii] * dtmult / (kt + 1.);
     dtmult *= dt;
@@ -298,7 +302,7 @@ static void time_avg_full(double dts[NADER][NGLL], double dt) {
 
 /* ---------------------------------------------------------------- halos */
 /* Spatial:631-662 (x), 994-1025 (y), 1351-1382 (z). */
-static void fill_halos(const oracle_ctx *c, double *st, int dir) {
+static void fill_halos(const oracle_ctx *c, oreal *st, int dir) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
   if (dir == 0) {
 #pragma omp parallel for collapse(2)
@@ -356,10 +360,10 @@ static void fill_halos(const oracle_ctx *c, double *st, int dir) {
 
 /* ---------------------------------------------------------------- tendencies */
 /* computeTendenciesX/Y/Z (Spatial:598-957, 961-1311, 1315-1697), one direction. */
-void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, double dt, int dir) {
+void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal dt, int dir) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
   const int nm = 1 + dir;
-  const double dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+  const oreal dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
   const int bc = c->bc[dir];
 
   fill_halos(c, st, dir);
@@ -370,7 +374,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++) {
         ader_t A;
-        double stencil[ORD];
+        oreal stencil[ORD];
         for (int v = 0; v < NUMSTATE; v++) {
           for (int s = 0; s < ORD; s++) {
             if (dir == 0) stencil[s] = st[sidx(c, v, HS + k, HS + j, i + s)];
@@ -393,14 +397,14 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
           }
         }
         /* level-0 flux products (Spatial:704-715 and per-direction equivalents) */
-        double srcfill = 0;
+        oreal srcfill = 0;
         for (int ii = 0; ii < NGLL; ii++) {
-          double r = A.q[idR][0][ii];
-          double u = A.q[idU][0][ii] / r;
-          double v = A.q[idV][0][ii] / r;
-          double w = A.q[idW][0][ii] / r;
-          double t = A.q[idT][0][ii] / r;
-          double vn = nm == 1 ? u : (nm == 2 ? v : w);
+          oreal r = A.q[idR][0][ii];
+          oreal u = A.q[idU][0][ii] / r;
+          oreal v = A.q[idV][0][ii] / r;
+          oreal w = A.q[idW][0][ii] / r;
+          oreal t = A.q[idT][0][ii] / r;
+          oreal vn = nm == 1 ? u : (nm == 2 ? v : w);
           A.f[0][0][ii] = r * vn * u;
           A.f[1][0][ii] = r * vn * v;
           A.f[2][0][ii] = r * vn * w;
@@ -424,7 +428,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
         }
         if (dir == 2) { /* gravity source (Spatial:1459-1499) */
           time_avg_full(A.src, dt);
-          double src_avg = 0;
+          oreal src_avg = 0;
           for (int ii = 0; ii < NGLL; ii++) src_avg += A.src[0][ii] * c->wts_ngll[ii];
           tend[tidx(c, idR, k, j, i)] = 0;
           tend[tidx(c, idU, k, j, i)] = 0;
@@ -463,12 +467,12 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
     for (int k = 0; k < ek; k++)
       for (int j = 0; j < ej; j++)
         for (int i = 0; i < ei; i++) {
-          double qL[5], qR[5];
+          oreal qL[5], qR[5];
           for (int l = 0; l < 5; l++) {
             qL[l] = c->limits[lidx(c, l, 0, k, j, i)];
             qR[l] = c->limits[lidx(c, l, 1, k, j, i)];
           }
-          double r, vel[3], t;
+          oreal r, vel[3], t;
           r = 0.5 * (qL[0] + qR[0]);
           if (dir == 1) { /* y: averages are NOT divided by density (Spatial:1210-1214) */
             vel[0] = 0.5 * (qL[1] + qR[1]);
@@ -481,14 +485,14 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
             vel[2] = 0.5 * (qL[3] / qL[0] + qR[3] / qR[0]);
             t = 0.5 * (qL[4] / qL[0] + qR[4] / qR[0]);
           }
-          double p = C0 * OPOW(r * t, GAMMA);
-          double cs2 = GAMMA * p / r;
-          double cs = sqrt(cs2);
+          oreal p = C0 * OPOW(r * t, GAMMA);
+          oreal cs2 = GAMMA * p / r;
+          oreal cs = sqrt(cs2);
           /* tangential indices in increasing order */
           int ta = dir == 0 ? 1 : 0, tb = dir == 2 ? 1 : 2; /* velocity slots */
-          double vn = vel[dir], va = vel[ta], vb = vel[tb];
+          oreal vn = vel[dir], va = vel[ta], vb = vel[tb];
           int qn = 1 + dir, qa = 1 + ta, qb = 1 + tb;
-          double w1, w2, w3;
+          oreal w1, w2, w3;
           if (vn > 0) {
             w1 = qL[0] - qL[4] / t;
             w2 = qL[qa] - va * qL[4] / t;
@@ -498,15 +502,15 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
             w2 = qR[qa] - va * qR[4] / t;
             w3 = qR[qb] - vb * qR[4] / t;
           }
-          double w5 = vn * qR[0] / (2 * cs) - qR[qn] / (2 * cs) + qR[4] / (2 * t);
-          double w6 = -vn * qL[0] / (2 * cs) + qL[qn] / (2 * cs) + qL[4] / (2 * t);
-          double q[5];
+          oreal w5 = vn * qR[0] / (2 * cs) - qR[qn] / (2 * cs) + qR[4] / (2 * t);
+          oreal w6 = -vn * qL[0] / (2 * cs) + qL[qn] / (2 * cs) + qL[4] / (2 * t);
+          oreal q[5];
           q[0] = w1 + w5 + w6;
           q[qn] = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
           q[qa] = w2 + va * w5 + va * w6;
           q[qb] = w3 + vb * w5 + vb * w6;
           q[4] = t * w5 + t * w6;
-          double F[5];
+          oreal F[5];
           F[0] = q[qn];
           F[qn] = q[qn] * q[qn] / q[0] + C0 * OPOW(q[4], GAMMA);
           F[qa] = q[qn] * q[qa] / q[0];
@@ -526,8 +530,8 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++)
         for (int l = 0; l < NUMSTATE; l++) {
-          double fl = c->flux[fidx(c, l, k, j, i)];
-          double fr = dir == 0 ? c->flux[fidx(c, l, k, j, i + 1)]
+          oreal fl = c->flux[fidx(c, l, k, j, i)];
+          oreal fr = dir == 0 ? c->flux[fidx(c, l, k, j, i + 1)]
                     : (dir == 1 ? c->flux[fidx(c, l, k, j + 1, i)] : c->flux[fidx(c, l, k + 1, j, i)]);
           long ti = tidx(c, l, k, j, i);
           if (dir == 0) {
@@ -542,7 +546,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, double *st, double *tend, doub
 }
 
 /* Spatial:565-594 */
-void oracle_compute_tendencies(oracle_ctx *c, double *st, double *tend, double dt, int split) {
+void oracle_compute_tendencies(oracle_ctx *c, oreal *st, oreal *tend, oreal dt, int split) {
   int dir;
   if (c->dimswitch) dir = split == 0 ? 0 : (split == 1 ? 1 : 2);
   else dir = split == 0 ? 2 : (split == 1 ? 1 : 0);
@@ -556,7 +560,7 @@ void oracle_compute_tendencies(oracle_ctx *c, double *st, double *tend, double d
 }
 
 /* Temporal_ader.h:63-65 */
-void oracle_apply(const oracle_ctx *c, double *st, const double *tend, double dt) {
+void oracle_apply(const oracle_ctx *c, oreal *st, const oreal *tend, oreal dt) {
 #pragma omp parallel for collapse(3)
   for (int l = 0; l < NUMSTATE; l++)
     for (int k = 0; k < c->nz; k++)
@@ -566,9 +570,9 @@ void oracle_apply(const oracle_ctx *c, double *st, const double *tend, double dt
 }
 
 /* Temporal_ader.h:48-72 */
-void oracle_time_step(oracle_ctx *c, double *st, double dt) {
+void oracle_time_step(oracle_ctx *c, oreal *st, oreal dt) {
   long n = (long)NUMSTATE * c->nz * c->ny * c->nx;
-  double *tend = (double *)calloc((size_t)n, sizeof(double));
+  oreal *tend = (oreal *)calloc((size_t)n, sizeof(oreal));
   for (int spl = 0; spl < 3; spl++) {
     oracle_compute_tendencies(c, st, tend, dt, spl);
     oracle_apply(c, st, tend, dt);
@@ -581,23 +585,23 @@ void oracle_set_dimswitch(oracle_ctx *c, int v) { c->dimswitch = v != 0; }
 
 /* ---------------------------------------------------------------- CFL */
 /* Spatial:159-187 */
-double oracle_compute_dt(const oracle_ctx *c, const double *st, double cfl) {
-  double best = INFINITY;
+oreal oracle_compute_dt(const oracle_ctx *c, const oreal *st, oreal cfl) {
+  oreal best = INFINITY;
   int first = 1;
   for (int k = 0; k < c->nz; k++)
     for (int j = 0; j < c->ny; j++)
       for (int i = 0; i < c->nx; i++) {
-        double r = st[sidx(c, idR, HS + k, HS + j, HS + i)] + c->hyDensCells[HS + k];
-        double u = st[sidx(c, idU, HS + k, HS + j, HS + i)] / r;
-        double v = st[sidx(c, idV, HS + k, HS + j, HS + i)] / r;
-        double w = st[sidx(c, idW, HS + k, HS + j, HS + i)] / r;
-        double t = (st[sidx(c, idT, HS + k, HS + j, HS + i)] + c->hyDensThetaCells[HS + k]) / r;
-        double p = C0 * OPOW(r * t, GAMMA);
-        double cs = sqrt(GAMMA * p / r);
-        double udt = cfl * c->dx / dmax(fabs(u - cs), fabs(u + cs));
-        double vdt = cfl * c->dy / dmax(fabs(v - cs), fabs(v + cs));
-        double wdt = cfl * c->dz / dmax(fabs(w - cs), fabs(w + cs));
-        double d = dmin(dmin(udt, vdt), wdt);
+        oreal r = st[sidx(c, idR, HS + k, HS + j, HS + i)] + c->hyDensCells[HS + k];
+        oreal u = st[sidx(c, idU, HS + k, HS + j, HS + i)] / r;
+        oreal v = st[sidx(c, idV, HS + k, HS + j, HS + i)] / r;
+        oreal w = st[sidx(c, idW, HS + k, HS + j, HS + i)] / r;
+        oreal t = (st[sidx(c, idT, HS + k, HS + j, HS + i)] + c->hyDensThetaCells[HS + k]) / r;
+        oreal p = C0 * OPOW(r * t, GAMMA);
+        oreal cs = sqrt(GAMMA * p / r);
+        oreal udt = cfl * c->dx / dmax(fabs(u - cs), fabs(u + cs));
+        oreal vdt = cfl * c->dy / dmax(fabs(v - cs), fabs(v + cs));
+        oreal wdt = cfl * c->dz / dmax(fabs(w - cs), fabs(w + cs));
+        oreal d = dmin(dmin(udt, vdt), wdt);
         if (first || d < best) { best = d; first = 0; }
       }
   return best;
@@ -605,46 +609,46 @@ double oracle_compute_dt(const oracle_ctx *c, const double *st, double cfl) {
 
 /* ---------------------------------------------------------------- profiles */
 /* Profiles.h:8-46 */
-static double const_theta_density(double t0, double z) {
-  double exner = 1. - GRAV * z / (CP * t0);
-  double p = pow(exner, CP / RD) * P0;
-  double rt = pow(p / C0, 1. / GAMMA);
+static oreal const_theta_density(oreal t0, oreal z) {
+  oreal exner = 1. - GRAV * z / (CP * t0);
+  oreal p = pow(exner, CP / RD) * P0;
+  oreal rt = pow(p / C0, 1. / GAMMA);
   return rt / t0;
 }
-static double const_theta_pressure(double t0, double z) {
-  double r = const_theta_density(t0, z);
+static oreal const_theta_pressure(oreal t0, oreal z) {
+  oreal r = const_theta_density(t0, z);
   return C0 * pow(r * t0, GAMMA);
 }
-static double bvf_pot_temp(double t0, double bvf, double z) { return t0 * exp(bvf * bvf * z / GRAV); }
-static double bvf_density(double t0, double bvf, double z) {
-  double t = bvf_pot_temp(t0, bvf, z);
-  double exner = 1. - GRAV * GRAV / (CP * bvf * bvf) * (t - t0) / (t * t0);
-  double p = pow(exner, CP / RD) * P0;
-  double rt = pow(p / C0, 1. / GAMMA);
+static oreal bvf_pot_temp(oreal t0, oreal bvf, oreal z) { return t0 * exp(bvf * bvf * z / GRAV); }
+static oreal bvf_density(oreal t0, oreal bvf, oreal z) {
+  oreal t = bvf_pot_temp(t0, bvf, z);
+  oreal exner = 1. - GRAV * GRAV / (CP * bvf * bvf) * (t - t0) / (t * t0);
+  oreal p = pow(exner, CP / RD) * P0;
+  oreal rt = pow(p / C0, 1. / GAMMA);
   return rt / t;
 }
-static double bvf_pressure(double t0, double bvf, double z) {
-  double t = bvf_pot_temp(t0, bvf, z);
-  double r = bvf_density(t0, bvf, z);
+static oreal bvf_pressure(oreal t0, oreal bvf, oreal z) {
+  oreal t = bvf_pot_temp(t0, bvf, z);
+  oreal r = bvf_density(t0, bvf, z);
   return C0 * pow(r * t, GAMMA);
 }
 /* Profiles.h:49-81 */
-static double ellipsoid_linear(double x, double y, double z, double x0, double y0, double z0,
-                               double xrad, double yrad, double zrad, double amp) {
-  double xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
-  double dist = sqrt(xn * xn + yn * yn + zn * zn);
+static oreal ellipsoid_linear(oreal x, oreal y, oreal z, oreal x0, oreal y0, oreal z0,
+                               oreal xrad, oreal yrad, oreal zrad, oreal amp) {
+  oreal xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
+  oreal dist = sqrt(xn * xn + yn * yn + zn * zn);
   return amp * dmax(1. - dist, 0.);
 }
-static double ellipsoid_cosine(double x, double y, double z, double x0, double y0, double z0,
-                               double xrad, double yrad, double zrad, double amp, double pwr) {
-  double val = 0;
-  double xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
-  double dist = sqrt(xn * xn + yn * yn + zn * zn);
+static oreal ellipsoid_cosine(oreal x, oreal y, oreal z, oreal x0, oreal y0, oreal z0,
+                               oreal xrad, oreal yrad, oreal zrad, oreal amp, oreal pwr) {
+  oreal val = 0;
+  oreal xn = (x - x0) / xrad, yn = (y - y0) / yrad, zn = (z - z0) / zrad;
+  oreal dist = sqrt(xn * xn + yn * yn + zn * zn);
   if (dist <= 1.) val = amp * pow((cos(M_PI * dist) + 1) / 2, pwr);
   return val;
 }
-static double igw_prof(double x, double y, double z, double x0, double y0, double hr, double zlen, double amp) {
-  double xn = (x - x0) / hr, yn = (y - y0) / hr;
+static oreal igw_prof(oreal x, oreal y, oreal z, oreal x0, oreal y0, oreal hr, oreal zlen, oreal amp) {
+  oreal xn = (x - x0) / hr, yn = (y - y0) / hr;
   return amp * sin(M_PI * z / zlen) / sqrt(1 + xn * xn + yn * yn);
 }
 
@@ -654,15 +658,15 @@ static void init_background(oracle_ctx *c) {
   for (int k = 0; k < nz + 2 * HS; k++) {
     c->hyDensCells[k] = 0; c->hyPressureCells[k] = 0; c->hyThetaCells[k] = 0; c->hyDensThetaCells[k] = 0;
     for (int kk = 0; kk < ORD; kk++) {
-      double zloc = (k - HS + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
-      double th, rh, ph;
+      oreal zloc = (k - HS + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+      oreal th, rh, ph;
       if (c->data_spec == DATA_IGW) {
-        const double bvf = 0.01, t0 = 300;
+        const oreal bvf = 0.01, t0 = 300;
         th = bvf_pot_temp(t0, bvf, zloc); rh = bvf_density(t0, bvf, zloc); ph = bvf_pressure(t0, bvf, zloc);
       } else {
         th = 300; rh = const_theta_density(th, zloc); ph = const_theta_pressure(th, zloc);
       }
-      double wt = c->wts_ord[kk];
+      oreal wt = c->wts_ord[kk];
       c->hyDensCells[k] += rh * wt;
       c->hyThetaCells[k] += th * wt;
       c->hyDensThetaCells[k] += rh * th * wt;
@@ -671,10 +675,10 @@ static void init_background(oracle_ctx *c) {
   }
   for (int k = 0; k < nz; k++)
     for (int kk = 0; kk < NGLL; kk++) {
-      double zloc = (k + 0.5) * c->dz + c->pts_ngll[kk] * c->dz;
-      double th, rh, ph;
+      oreal zloc = (k + 0.5) * c->dz + c->pts_ngll[kk] * c->dz;
+      oreal th, rh, ph;
       if (c->data_spec == DATA_IGW) {
-        const double bvf = 0.01, t0 = 300;
+        const oreal bvf = 0.01, t0 = 300;
         th = bvf_pot_temp(t0, bvf, zloc); rh = bvf_density(t0, bvf, zloc); ph = bvf_pressure(t0, bvf, zloc);
       } else {
         th = 300; rh = const_theta_density(th, zloc); ph = const_theta_pressure(th, zloc);
@@ -687,7 +691,7 @@ static void init_background(oracle_ctx *c) {
 }
 
 /* Spatial:428-485 */
-void oracle_init_state(oracle_ctx *c, double *st) {
+void oracle_init_state(oracle_ctx *c, oreal *st) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
 #pragma omp parallel for collapse(3)
   for (int k = 0; k < nz; k++)
@@ -697,34 +701,34 @@ void oracle_init_state(oracle_ctx *c, double *st) {
         for (int kk = 0; kk < ORD; kk++)
           for (int jj = 0; jj < ORD; jj++)
             for (int ii = 0; ii < ORD; ii++) {
-              double zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
-              double yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
-              double xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
-              double wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
+              oreal zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+              oreal yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
+              oreal xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
+              oreal wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
               long it = sidx(c, idT, HS + k, HS + j, HS + i);
               if (c->data_spec == DATA_THERMAL) {
-                double th = 300, rh = const_theta_density(th, zloc);
-                double tp = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 2);
-                double t = th + tp;
+                oreal th = 300, rh = const_theta_density(th, zloc);
+                oreal tp = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 2);
+                oreal t = th + tp;
                 st[it] += (rh * t - rh * th) * wt;
               } else if (c->data_spec == DATA_COLLISION) {
-                double th = 300, rh = const_theta_density(th, zloc);
-                double tp = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 20);
+                oreal th = 300, rh = const_theta_density(th, zloc);
+                oreal tp = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 20);
                 tp += ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 8000, 2000, 2000, 2000, -20);
-                double t = th + tp;
+                oreal t = th + tp;
                 st[it] += (rh * t - rh * th) * wt;
               } else if (c->data_spec == DATA_STRAKA) {
-                double th = 300, rh = const_theta_density(th, zloc);
-                double tp = ellipsoid_cosine(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 3000, 4000, 2000, 2000, -15, 1);
-                double t = th + tp;
+                oreal th = 300, rh = const_theta_density(th, zloc);
+                oreal tp = ellipsoid_cosine(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 3000, 4000, 2000, 2000, -15, 1);
+                oreal t = th + tp;
                 st[it] += (rh * t - rh * th) * wt;
               } else if (c->data_spec == DATA_IGW) {
                 if (c->sim2d) yloc = c->ylen / 3;
-                const double t0 = 300, bvf = 0.01;
-                double rh = bvf_density(t0, bvf, zloc);
-                double th = bvf_pot_temp(t0, bvf, zloc);
-                double tp = igw_prof(xloc, yloc, zloc, c->xlen / 3, c->ylen / 3, 5000, c->zlen, 0.01);
-                double t = th + tp;
+                const oreal t0 = 300, bvf = 0.01;
+                oreal rh = bvf_density(t0, bvf, zloc);
+                oreal th = bvf_pot_temp(t0, bvf, zloc);
+                oreal tp = igw_prof(xloc, yloc, zloc, c->xlen / 3, c->ylen / 3, 5000, c->zlen, 0.01);
+                oreal t = th + tp;
                 st[it] += (rh * t - rh * th) * wt;
                 st[sidx(c, idU, HS + k, HS + j, HS + i)] += 20 * rh * wt;
                 if (!c->sim2d) st[sidx(c, idV, HS + k, HS + j, HS + i)] += 20 * rh * wt;
@@ -733,8 +737,8 @@ void oracle_init_state(oracle_ctx *c, double *st) {
       }
 }
 
-void oracle_set_bubble(oracle_ctx *c, double *st, int shape, double x0, double y0, double z0,
-                       double xrad, double yrad, double zrad, double amp, double pwr) {
+void oracle_set_bubble(oracle_ctx *c, oreal *st, int shape, oreal x0, oreal y0, oreal z0,
+                       oreal xrad, oreal yrad, oreal zrad, oreal amp, oreal pwr) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
 #pragma omp parallel for collapse(3)
   for (int k = 0; k < nz; k++)
@@ -744,14 +748,14 @@ void oracle_set_bubble(oracle_ctx *c, double *st, int shape, double x0, double y
         for (int kk = 0; kk < ORD; kk++)
           for (int jj = 0; jj < ORD; jj++)
             for (int ii = 0; ii < ORD; ii++) {
-              double zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
-              double yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
-              double xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
-              double wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
-              double th = 300, rh = const_theta_density(th, zloc);
-              double tp = shape == 0 ? ellipsoid_linear(xloc, yloc, zloc, x0, y0, z0, xrad, yrad, zrad, amp)
+              oreal zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+              oreal yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
+              oreal xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
+              oreal wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
+              oreal th = 300, rh = const_theta_density(th, zloc);
+              oreal tp = shape == 0 ? ellipsoid_linear(xloc, yloc, zloc, x0, y0, z0, xrad, yrad, zrad, amp)
                                      : ellipsoid_cosine(xloc, yloc, zloc, x0, y0, z0, xrad, yrad, zrad, amp, pwr);
-              double t = th + tp;
+              oreal t = th + tp;
               st[sidx(c, idT, HS + k, HS + j, HS + i)] += (rh * t - rh * th) * wt;
             }
       }
@@ -764,29 +768,33 @@ static inline uint64_t splitmix64(uint64_t x) {
   return x ^ (x >> 31);
 }
 
-void oracle_add_theta_noise(oracle_ctx *c, double *st, unsigned long long seed, double amp) {
+void oracle_add_theta_noise(oracle_ctx *c, oreal *st, unsigned long long seed, oreal amp) {
   for (int k = 0; k < c->nz; k++)
     for (int j = 0; j < c->ny; j++)
       for (int i = 0; i < c->nx; i++) {
         uint64_t idx = ((uint64_t)k * c->ny + j) * c->nx + i;
-        double u = (double)(splitmix64(seed * 0x100000001B3ULL + idx) >> 11) * (1.0 / 9007199254740992.0);
-        double n = (2.0 * u - 1.0) * amp;
+        oreal u = (oreal)(splitmix64(seed * 0x100000001B3ULL + idx) >> 11) * (1.0 / 9007199254740992.0);
+        oreal n = (2.0 * u - 1.0) * amp;
         st[sidx(c, idT, HS + k, HS + j, HS + i)] += c->hyDensCells[HS + k] * n;
       }
 }
 
 /* ---------------------------------------------------------------- setup */
+static void copy_tab(oreal *dst, const double *src, int n) {
+  for (int i = 0; i < n; i++) dst[i] = src[i];
+}
+
 /* matmul_cr: C(col,row) = sum_k A(k,row) * B(col,k), k ascending. */
-static void matmul_cr(const double *A, int K, int R, const double *B, int C, double *out) {
+static void matmul_cr(const oreal *A, int K, int R, const oreal *B, int C, oreal *out) {
   for (int cc = 0; cc < C; cc++)
     for (int r = 0; r < R; r++) {
-      double tmp = 0;
+      oreal tmp = 0;
       for (int k = 0; k < K; k++) tmp += A[k * R + r] * B[cc * K + k];
       out[cc * R + r] = tmp;
     }
 }
 
-oracle_ctx *oracle_create(int nx, int ny, int nz, double xlen, double ylen, double zlen,
+oracle_ctx *oracle_create(int nx, int ny, int nz, oreal xlen, oreal ylen, oreal zlen,
                           int bc_x, int bc_y, int bc_z, int weno_scalars, int weno_winds,
                           int data_spec) {
   oracle_ctx *c = (oracle_ctx *)calloc(1, sizeof(oracle_ctx));
@@ -798,37 +806,47 @@ oracle_ctx *oracle_create(int nx, int ny, int nz, double xlen, double ylen, doub
   c->data_spec = data_spec;
   c->dimswitch = 1;
   c->dx = xlen / nx; c->dy = ylen / ny; c->dz = zlen / nz;
-  /* Spatial:274-315 */
-  memcpy(c->recon, TBL(awfl_weno_recon), sizeof(c->recon));
-  memcpy(c->c2g, TBL(awfl_coefs_to_gll_lower), sizeof(c->c2g));
-  matmul_cr(TBL(awfl_coefs_to_gll_lower), ORD, NGLL, TBL(awfl_sten_to_coefs), ORD, &c->s2g[0][0]);
+  /* Spatial:274-315 (the generated tables are doubles; copied element by element so that
+   * the long-double variant holds the same values) */
+  copy_tab((oreal *)c->recon, TBL(awfl_weno_recon), ORD * ORD * ORD);
+  copy_tab((oreal *)c->c2g, TBL(awfl_coefs_to_gll_lower), ORD * NGLL);
   {
-    double tmp[NGLL * NGLL];
-#if ORD == 5
-    matmul_cr(awfl_coefs_to_deriv_n3_o5, NGLL, NGLL, awfl_gll_to_coefs_n3_o5, NGLL, tmp);
-    matmul_cr(awfl_coefs_to_gll_n3_o5, NGLL, NGLL, tmp, NGLL, &c->deriv[0][0]);
-#else
-    matmul_cr(awfl_coefs_to_deriv_n5_o9, NGLL, NGLL, awfl_gll_to_coefs_n5_o9, NGLL, tmp);
-    matmul_cr(awfl_coefs_to_gll_n5_o9, NGLL, NGLL, tmp, NGLL, &c->deriv[0][0]);
-#endif
+    oreal a[ORD * NGLL], b[ORD * ORD];
+    copy_tab(a, TBL(awfl_coefs_to_gll_lower), ORD * NGLL);
+    copy_tab(b, TBL(awfl_sten_to_coefs), ORD * ORD);
+    matmul_cr(a, ORD, NGLL, b, ORD, (oreal *)c->s2g);
   }
-  memcpy(c->pts_ord, TBL(awfl_gll_pts_ord), sizeof(c->pts_ord));
-  memcpy(c->wts_ord, TBL(awfl_gll_wts_ord), sizeof(c->wts_ord));
-  memcpy(c->pts_ngll, TBL(awfl_gll_pts_ngll), sizeof(c->pts_ngll));
-  memcpy(c->wts_ngll, TBL(awfl_gll_wts_ngll), sizeof(c->wts_ngll));
+  {
+    oreal tmp[NGLL * NGLL], d[NGLL * NGLL], g2c[NGLL * NGLL], c2g[NGLL * NGLL];
+#if ORD == 5
+    copy_tab(d, awfl_coefs_to_deriv_n3_o5, NGLL * NGLL);
+    copy_tab(g2c, awfl_gll_to_coefs_n3_o5, NGLL * NGLL);
+    copy_tab(c2g, awfl_coefs_to_gll_n3_o5, NGLL * NGLL);
+#else
+    copy_tab(d, awfl_coefs_to_deriv_n5_o9, NGLL * NGLL);
+    copy_tab(g2c, awfl_gll_to_coefs_n5_o9, NGLL * NGLL);
+    copy_tab(c2g, awfl_coefs_to_gll_n5_o9, NGLL * NGLL);
+#endif
+    matmul_cr(d, NGLL, NGLL, g2c, NGLL, tmp);
+    matmul_cr(c2g, NGLL, NGLL, tmp, NGLL, (oreal *)c->deriv);
+  }
+  copy_tab(c->pts_ord, TBL(awfl_gll_pts_ord), ORD);
+  copy_tab(c->wts_ord, TBL(awfl_gll_wts_ord), ORD);
+  copy_tab(c->pts_ngll, TBL(awfl_gll_pts_ngll), NGLL);
+  copy_tab(c->wts_ngll, TBL(awfl_gll_wts_ngll), NGLL);
   weno_set_ideal_sigma(c->idl, &c->sigma);
 
   int nzc = nz + 2 * HS;
-  c->hyDensCells = (double *)calloc(nzc, sizeof(double));
-  c->hyPressureCells = (double *)calloc(nzc, sizeof(double));
-  c->hyThetaCells = (double *)calloc(nzc, sizeof(double));
-  c->hyDensThetaCells = (double *)calloc(nzc, sizeof(double));
-  c->hyDensGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
-  c->hyPressureGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
-  c->hyThetaGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
-  c->hyDensThetaGLL = (double *)calloc((size_t)nz * NGLL, sizeof(double));
-  c->limits = (double *)calloc((size_t)5 * 2 * (nz + 1) * (ny + 1) * (nx + 1), sizeof(double));
-  c->flux = (double *)calloc((size_t)5 * (nz + 1) * (ny + 1) * (nx + 1), sizeof(double));
+  c->hyDensCells = (oreal *)calloc(nzc, sizeof(oreal));
+  c->hyPressureCells = (oreal *)calloc(nzc, sizeof(oreal));
+  c->hyThetaCells = (oreal *)calloc(nzc, sizeof(oreal));
+  c->hyDensThetaCells = (oreal *)calloc(nzc, sizeof(oreal));
+  c->hyDensGLL = (oreal *)calloc((size_t)nz * NGLL, sizeof(oreal));
+  c->hyPressureGLL = (oreal *)calloc((size_t)nz * NGLL, sizeof(oreal));
+  c->hyThetaGLL = (oreal *)calloc((size_t)nz * NGLL, sizeof(oreal));
+  c->hyDensThetaGLL = (oreal *)calloc((size_t)nz * NGLL, sizeof(oreal));
+  c->limits = (oreal *)calloc((size_t)5 * 2 * (nz + 1) * (ny + 1) * (nx + 1), sizeof(oreal));
+  c->flux = (oreal *)calloc((size_t)5 * (nz + 1) * (ny + 1) * (nx + 1), sizeof(oreal));
   init_background(c);
   return c;
 }
@@ -848,32 +866,32 @@ long oracle_state_size(const oracle_ctx *c) {
   return (long)NUMSTATE * (c->nz + 2 * HS) * (c->ny + 2 * HS) * (c->nx + 2 * HS);
 }
 
-void oracle_get_tables(const oracle_ctx *c, double *s2g, double *deriv, double *idl, double *sigma) {
+void oracle_get_tables(const oracle_ctx *c, oreal *s2g, oreal *deriv, oreal *idl, oreal *sigma) {
   memcpy(s2g, c->s2g, sizeof(c->s2g));
   memcpy(deriv, c->deriv, sizeof(c->deriv));
   memcpy(idl, c->idl, sizeof(c->idl));
   *sigma = c->sigma;
 }
 
-void oracle_get_background(const oracle_ctx *c, double *dens_c, double *pres_c, double *theta_c,
-                           double *denstheta_c, double *dens_g, double *pres_g, double *theta_g,
-                           double *denstheta_g) {
+void oracle_get_background(const oracle_ctx *c, oreal *dens_c, oreal *pres_c, oreal *theta_c,
+                           oreal *denstheta_c, oreal *dens_g, oreal *pres_g, oreal *theta_g,
+                           oreal *denstheta_g) {
   int nzc = c->nz + 2 * HS;
-  memcpy(dens_c, c->hyDensCells, nzc * sizeof(double));
-  memcpy(pres_c, c->hyPressureCells, nzc * sizeof(double));
-  memcpy(theta_c, c->hyThetaCells, nzc * sizeof(double));
-  memcpy(denstheta_c, c->hyDensThetaCells, nzc * sizeof(double));
-  memcpy(dens_g, c->hyDensGLL, (size_t)c->nz * NGLL * sizeof(double));
-  memcpy(pres_g, c->hyPressureGLL, (size_t)c->nz * NGLL * sizeof(double));
-  memcpy(theta_g, c->hyThetaGLL, (size_t)c->nz * NGLL * sizeof(double));
-  memcpy(denstheta_g, c->hyDensThetaGLL, (size_t)c->nz * NGLL * sizeof(double));
+  memcpy(dens_c, c->hyDensCells, nzc * sizeof(oreal));
+  memcpy(pres_c, c->hyPressureCells, nzc * sizeof(oreal));
+  memcpy(theta_c, c->hyThetaCells, nzc * sizeof(oreal));
+  memcpy(denstheta_c, c->hyDensThetaCells, nzc * sizeof(oreal));
+  memcpy(dens_g, c->hyDensGLL, (size_t)c->nz * NGLL * sizeof(oreal));
+  memcpy(pres_g, c->hyPressureGLL, (size_t)c->nz * NGLL * sizeof(oreal));
+  memcpy(theta_g, c->hyThetaGLL, (size_t)c->nz * NGLL * sizeof(oreal));
+  memcpy(denstheta_g, c->hyDensThetaGLL, (size_t)c->nz * NGLL * sizeof(oreal));
 }
 
-double oracle_coefs_to_tv(const double *a, int n) {
+oreal oracle_coefs_to_tv(const oreal *a, int n) {
   if (n == HS + 1) return tv_lo(a);
   return tv_hi(a);
 }
 
-void oracle_weno_coefs(const oracle_ctx *c, const double *stencil, double *coefs_out) {
+void oracle_weno_coefs(const oracle_ctx *c, const oreal *stencil, oreal *coefs_out) {
   weno_coefs(c, stencil, coefs_out);
 }

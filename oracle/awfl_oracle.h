@@ -8,7 +8,8 @@
  * the absent YAKL/yaml-cpp/netCDF dependencies) through the fixtures in tests/golden/.
  *
  * Compile-time order: ORACLE_ORD / ORACLE_NGLL (5/3 or 9/5), like the reference's
- * ORD/NGLL macros (const.h:21-27). FP64, compiled without FMA contraction.
+ * ORD/NGLL macros (const.h:21-27). FP64, compiled without FMA contraction (or the
+ * long-double variant, see oreal below).
  */
 #ifndef AWFL_ORACLE_H
 #define AWFL_ORACLE_H
@@ -17,11 +18,20 @@
 extern "C" {
 #endif
 
+/* The arithmetic type: oreal (the parity oracle), or long oreal (x87 80-bit) when built
+ * with ORACLE_LONG_DOUBLE -- the same restatement evaluated with 11 more bits, used only as
+ * a finite-difference reference for the discrete adjoint. */
+#ifdef ORACLE_LONG_DOUBLE
+typedef long double oreal;
+#else
+typedef double oreal;
+#endif
+
 typedef struct oracle_ctx oracle_ctx;
 
 /* bc: 0 periodic, 1 wall. data_spec: 1 thermal, 2 collision, 3 straka, 4 igw
  * (Spatial_euler3d_cons_expl_cart_fv_Agrid.h:75-78). */
-oracle_ctx *oracle_create(int nx, int ny, int nz, double xlen, double ylen, double zlen,
+oracle_ctx *oracle_create(int nx, int ny, int nz, oreal xlen, oreal ylen, oreal zlen,
                           int bc_x, int bc_y, int bc_z, int weno_scalars, int weno_winds,
                           int data_spec);
 void oracle_destroy(oracle_ctx *c);
@@ -31,35 +41,35 @@ int oracle_hs(void);
 long oracle_state_size(const oracle_ctx *c);
 
 /* Hydrostatic background + reference initial data (Spatial...h:345-485). */
-void oracle_init_state(oracle_ctx *c, double *state);
+void oracle_init_state(oracle_ctx *c, oreal *state);
 /* Bubble replacing the theta perturbation (shape 0 linear, 1 cosine) and seeded noise. */
-void oracle_set_bubble(oracle_ctx *c, double *state, int shape, double x0, double y0,
-                       double z0, double xrad, double yrad, double zrad, double amp, double pwr);
-void oracle_add_theta_noise(oracle_ctx *c, double *state, unsigned long long seed, double amp);
+void oracle_set_bubble(oracle_ctx *c, oreal *state, int shape, oreal x0, oreal y0,
+                       oreal z0, oreal xrad, oreal yrad, oreal zrad, oreal amp, oreal pwr);
+void oracle_add_theta_noise(oracle_ctx *c, oreal *state, unsigned long long seed, oreal amp);
 
 /* CFL time step (Spatial...h:159-187), NOT cached here. */
-double oracle_compute_dt(const oracle_ctx *c, const double *state, double cfl);
+oreal oracle_compute_dt(const oracle_ctx *c, const oreal *state, oreal cfl);
 
 /* One directional split: halo fill (in place on state) + tendencies (5,nz,ny,nx).
  * dir: 0 = x, 1 = y, 2 = z. */
-void oracle_compute_tendencies_dir(oracle_ctx *c, double *state, double *tend, double dt, int dir);
+void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *state, oreal *tend, oreal dt, int dir);
 /* computeTendencies(split) with the reference's dimSwitch alternation (Spatial...h:565-594). */
-void oracle_compute_tendencies(oracle_ctx *c, double *state, double *tend, double dt, int split);
+void oracle_compute_tendencies(oracle_ctx *c, oreal *state, oreal *tend, oreal dt, int split);
 /* state(l,hs+k,hs+j,hs+i) += dt * tend(l,k,j,i)  (Temporal_ader.h:63-65). */
-void oracle_apply(const oracle_ctx *c, double *state, const double *tend, double dt);
+void oracle_apply(const oracle_ctx *c, oreal *state, const oreal *tend, oreal dt);
 /* One full time step: 3 splits (Temporal_ader.h:48-72). */
-void oracle_time_step(oracle_ctx *c, double *state, double dt);
+void oracle_time_step(oracle_ctx *c, oreal *state, oreal dt);
 int oracle_get_dimswitch(const oracle_ctx *c);
 void oracle_set_dimswitch(oracle_ctx *c, int v);
 
 /* Derived tables and background, for pinning against the reference. */
-void oracle_get_tables(const oracle_ctx *c, double *s2g, double *deriv, double *idl, double *sigma);
-void oracle_get_background(const oracle_ctx *c, double *dens_c, double *pres_c, double *theta_c,
-                           double *denstheta_c, double *dens_g, double *pres_g, double *theta_g,
-                           double *denstheta_g);
+void oracle_get_tables(const oracle_ctx *c, oreal *s2g, oreal *deriv, oreal *idl, oreal *sigma);
+void oracle_get_background(const oracle_ctx *c, oreal *dens_c, oreal *pres_c, oreal *theta_c,
+                           oreal *denstheta_c, oreal *dens_g, oreal *pres_g, oreal *theta_g,
+                           oreal *denstheta_g);
 /* Single-function probes. */
-double oracle_coefs_to_tv(const double *a, int n);
-void oracle_weno_coefs(const oracle_ctx *c, const double *stencil, double *coefs_out);
+oreal oracle_coefs_to_tv(const oreal *a, int n);
+void oracle_weno_coefs(const oracle_ctx *c, const oreal *stencil, oreal *coefs_out);
 
 #ifdef __cplusplus
 }

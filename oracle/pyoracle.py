@@ -1,6 +1,8 @@
 """ctypes wrappers for the CPU test oracles (TEST INFRASTRUCTURE ONLY).
 
 * :class:`Oracle` -- the project's C restatement (``oracle/liboracle_o{ord}.so``).
+* :class:`OracleLD` -- the same restatement in x87 long double
+  (``oracle/liboracle_o5_ld.so``): a finite-difference reference for the adjoint.
 * :class:`RefHarness` -- the reference's own code built on project-written stand-ins
   (``oracle/_ref/libawflref_o{ord}.so``, only where it has been built).
 
@@ -177,6 +179,62 @@ class Oracle(_Grid):
         out = np.zeros(self.ord)
         self.L.oracle_weno_coefs(self.h, _ptr(s), _ptr(out))
         return out
+
+
+class OracleLD(_Grid):
+    """The C restatement compiled with ``oreal = long double`` (ord 5): states are numpy
+    ``longdouble`` arrays (80-bit x87 values in 16-byte slots, the C ``long double``)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            path = os.path.join(HERE, "liboracle_o5_ld.so")
+            if not os.path.exists(path):
+                build()
+            L = ctypes.CDLL(path)
+            LD = ctypes.c_longdouble
+            L.oracle_create.restype = _VP
+            L.oracle_create.argtypes = [_I] * 3 + [LD] * 3 + [_I] * 6
+            L.oracle_destroy.argtypes = [_VP]
+            L.oracle_compute_dt.restype = LD
+            L.oracle_compute_dt.argtypes = [_VP, _VP, LD]
+            L.oracle_time_step.argtypes = [_VP, _VP, LD]
+            L.oracle_set_dimswitch.argtypes = [_VP, _I]
+            cls._lib = L
+        return cls._lib
+
+    def __init__(self, nx, ny, nz, xlen=20000.0, ylen=20000.0, zlen=10000.0, bc=(0, 0, 1),
+                 weno_scalars=True, weno_winds=True, data="thermal"):
+        super().__init__(5, nx, ny, nz)
+        self.L = self.lib()
+        self.h = self.L.oracle_create(nx, ny, nz, xlen, ylen, zlen, bc[0], bc[1], bc[2],
+                                      int(weno_scalars), int(weno_winds), DATA_SPECS[data])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.oracle_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def _p(a):
+        assert a.dtype == np.longdouble and a.flags.c_contiguous
+        return a.ctypes.data_as(_VP)
+
+    def new_state(self):
+        return np.zeros(self.state_shape, dtype=np.longdouble)
+
+    def time_step(self, st, dt):
+        self.L.oracle_time_step(self.h, self._p(st), dt)
+
+    @property
+    def dimswitch(self):
+        raise AttributeError("write-only")
+
+    @dimswitch.setter
+    def dimswitch(self, v):
+        self.L.oracle_set_dimswitch(self.h, int(v))
 
 
 class RefHarness(_Grid):

@@ -196,6 +196,52 @@ def test_gradient_matches_central_finite_differences():
     assert err <= 3e-6, (err, gv, fd)
 
 
+def test_gradient_matches_extended_precision_finite_differences():
+    """The same gradient against central differences of the same J evaluated by the
+    oracle's restatement in x87 long double (oracle/liboracle_o5_ld.so, 11 more bits):
+    with the FD's rounding error out of the way, the fourth-order difference at eps = 1e-6
+    and the second-order one at eps = 1e-7 both agree with the adjoint to ~1e-8 (the
+    second-order difference at eps = 1e-6 carries ~1e-6 of truncation error)."""
+    from oracle.pyoracle import OracleLD
+    c = capi.Context(*N)
+    s0 = base_state(c)
+    dt = c.cfl(s0, 0.8)
+    target = interior(c, run(c, base_state(c, noise_sigma=0.1), STEPS, dt)[4])
+    x = s0.clone().requires_grad_(True)
+    c.dimswitch = 1
+    sN = euler_steps(x, c, STEPS, dt, ckpt_every=10)
+    (0.5 * torch.sum((interior(c, sN[4]) - target) ** 2)).backward()
+    grad = x.grad
+    O = OracleLD(*N)
+    tgt = target.cpu().numpy().astype(np.longdouble)
+    base = s0.cpu().numpy().astype(np.longdouble)
+    h = c.hs
+
+    def J(s):
+        s = s.copy()
+        O.dimswitch = 1
+        for _ in range(STEPS):
+            O.time_step(s, dt)
+        d = s[4, h:h + c.nz, h:h + c.ny, h:h + c.nx] - tgt
+        return 0.5 * np.sum(d * d)
+
+    g = torch.Generator().manual_seed(20261203)
+    gv, fd4, fd2 = [], [], []
+    for _ in range(16):
+        v = unit_direction(c, g)
+        gv.append(torch.sum(grad * v).item())
+        vl = v.cpu().numpy().astype(np.longdouble)
+        e = np.longdouble(1e-6)
+        fd4.append(float((8 * (J(base + e * vl) - J(base - e * vl)) - (J(base + 2 * e * vl) - J(base - 2 * e * vl)))
+                         / (12 * e)))
+        e = np.longdouble(1e-7)
+        fd2.append(float((J(base + e * vl) - J(base - e * vl)) / (2 * e)))
+    gv, fd4, fd2 = np.array(gv), np.array(fd4), np.array(fd2)
+    err4 = np.linalg.norm(gv - fd4) / np.linalg.norm(fd4)
+    err2 = np.linalg.norm(gv - fd2) / np.linalg.norm(fd2)
+    assert err4 <= 1e-7 and err2 <= 1e-7, (err4, err2)
+
+
 def test_adjoint_rejects_bad_arguments():
     c = capi.Context(*N)
     s = c.new_state()
