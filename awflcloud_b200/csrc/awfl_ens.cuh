@@ -9,8 +9,8 @@
 // equal up to where the compiler contracts multiply-adds).
 //
 // Tile shapes (C cells per chunk, W lines per CTA) are candidates for the autotuner
-// (awfl_ensemble_tune): per order and direction, EnsShapes lists them, entry 0 being the
-// single-grid default.
+// (awfl_ensemble_tune): per order and direction, EnsShapes lists them; entry 0 is used
+// until the ensemble is tuned.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -451,6 +451,11 @@ struct P32 {
   static __device__ __forceinline__ void store_tend(const Args &A, long g, float x) { A.tend[g] = x; }
 };
 
+// Single-grid sweep shapes of the FP32 form, ord 5 (chunk C x lines W; measured at
+// 256x256x128 against the other candidates of awfl_ens.cuh): x 16 x 8, y 8 x 16, z 4 x 32.
+template <> struct PolicyShape<P32, 5, 0> { static constexpr int C = 16, W = 8; };
+template <> struct PolicyShape<P32, 5, 1> { static constexpr int C = 8, W = 16; };
+
 // Uploads the FP32 tables into this translation unit's constant memory.
 static inline cudaError_t upload_tables32_here(int ord, const double *recon, const double *c2g, const double *s2g,
                                                const double *deriv, const double *idl, double sigma,

@@ -53,4 +53,10 @@ struct P64 {
   static __device__ __forceinline__ void store_tend(const Args &A, long g, double x) { A.tend[g] = x; }
 };
 
+// Single-grid sweep shapes of the FP64 path, ord 5 (measured at 256x256x128):
+// x 16 x 8, y and z 8 x 16.
+template <> struct PolicyShape<P64, 5, 0> { static constexpr int C = 16, W = 8; };
+template <> struct PolicyShape<P64, 5, 1> { static constexpr int C = 8, W = 16; };
+template <> struct PolicyShape<P64, 5, 2> { static constexpr int C = 8, W = 16; };
+
 }  // namespace awfl

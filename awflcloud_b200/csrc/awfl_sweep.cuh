@@ -286,10 +286,14 @@ template <> struct SweepShape<9, 0> { static constexpr int C = 32, W = 2; };
 template <> struct SweepShape<9, 1> { static constexpr int C = 8, W = 16; };
 template <> struct SweepShape<9, 2> { static constexpr int C = 8, W = 16; };
 
+// Shape of a policy's single-grid sweep: SweepShape unless the policy specialises it
+// (measured per form at 256x256x128).
+template <class P, int ORD, int DIR> struct PolicyShape : SweepShape<ORD, DIR> {};
+
 // Policies with wider elements (P::kWdiv > 1) use fewer lines per CTA to stay within the
 // 48 KB of static shared memory.
-template <class P, int ORD, int DIR, int C = SweepShape<ORD, DIR>::C,
-          int W = (SweepShape<ORD, DIR>::W / P::kWdiv > 0 ? SweepShape<ORD, DIR>::W / P::kWdiv : 1)>
+template <class P, int ORD, int DIR, int C = PolicyShape<P, ORD, DIR>::C,
+          int W = (PolicyShape<P, ORD, DIR>::W / P::kWdiv > 0 ? PolicyShape<P, ORD, DIR>::W / P::kWdiv : 1)>
 cudaError_t launch_sweep_t(const typename P::Args &A, cudaStream_t st) {
   dim3 block(DIR == 0 ? C : W, DIR == 0 ? W : C);
   dim3 grid;
