@@ -1,12 +1,12 @@
 // Differentiation form of the FP64 step: the tangent-linear sweep (forward mode, Dual
-// scalars through the same templated FP64 code) and the hand-written discrete adjoint.
-// Compiled with --fmad=false like the FP64 path.
+// scalars through the same templated FP64 code) and the recording forward sweep of the
+// discrete adjoint (its reverse sweeps are in awfl_adjrev.cu). Compiled with --fmad=false
+// like the FP64 path.
 #include <cuda_runtime.h>
 
-#include "awfl_device.cuh"
 #include "awfl_dual.cuh"
 #include "awfl_internal.h"
-#include "awfl_sweep.cuh"
+#include "awfl_p64.cuh"
 
 namespace awfl {
 
@@ -26,7 +26,7 @@ struct PTLM {
 
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, Dual (&eL)[5], Dual (&eR)[5],
-                                               Dual &src) {
+                                               Dual &src, long) {
     cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
   }
   template <int DIR, int NG>
@@ -55,6 +55,44 @@ struct PTLM {
 
 cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
   return launch_sweep_any<PTLM>(ord, dir, A, st);
+}
+
+// ------------------------------------------------------------------------------------
+// Recording FP64 policy for the adjoint's forward recomputation: the P64 arithmetic (so
+// the recomputed trajectory is bit-identical to awfl_step's) that also keeps, per cell,
+// the level-0 GLL values and the time-averaged edge states the reverse sweep starts from.
+// A.tend points at the split's record: q0 (5*NGLL planes of ncell), then eL, eR (10).
+// ------------------------------------------------------------------------------------
+struct P64Rec : P64 {
+  template <int ORD> struct Rec {
+    double *q0;
+    long n, cell;
+    __device__ __forceinline__ void level0(int v, int ii, const double &x) const {
+      q0[(v * OrdTraits<ORD>::NGLL + ii) * n + cell] = x;
+    }
+  };
+  template <int ORD, int DIR, class S>
+  static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],
+                                               double (&eR)[5], double &src, long cell) {
+    if (cell < 0) {  // the periodic prologue's repeat of cell L-1: recorded in its chunk
+      cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
+      return;
+    }
+    constexpr int NG = OrdTraits<ORD>::NGLL;
+    const long n = (long)A.nx * A.ny * A.nz;
+    cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell});
+    double *e = A.tend + 5L * NG * n;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      e[v * n + cell] = eL[v];
+      e[(5 + v) * n + cell] = eR[v];
+    }
+  }
+};
+template <int ORD, int DIR> struct PolicyShape<P64Rec, ORD, DIR> : PolicyShape<P64, ORD, DIR> {};
+
+cudaError_t launch_sweep_rec(int ord, int dir, const SweepArgs &A, cudaStream_t st) {
+  return launch_sweep_any<P64Rec>(ord, dir, A, st);
 }
 
 cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes) {

@@ -651,8 +651,9 @@ int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
   const long nspl = (c->sim2d ? 2L : 3L) * nsteps;
   const long ncell = (long)c->cfg.nx * c->cfg.ny * c->cfg.nz;
   const long nface = (long)(c->cfg.nx + 1) * (c->cfg.ny + 1) * (c->cfg.nz + 1);
-  *bytes = (long)sizeof(double) *
-           (nspl * state_plane(c) + 10L * ncell + 10L * nface + 5L * (c->cfg.ord + 2L * c->ngll) * ncell);
+  const long rec = (5L * c->ngll + 10L) * ncell;  // per split: level-0 values + edges
+  *bytes = (long)sizeof(double) * (nspl > 0 ? (nspl + 1) * state_plane(c) + nspl * rec : 0) +
+           (long)sizeof(double) * (10L * nface + 5L * (c->cfg.ord + c->ngll) * ncell);
   return AWFL_OK;
 }
 
@@ -683,33 +684,37 @@ int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int
     ds = !ds;
   }
   const long nspl = (long)dirs.size();
+  const long rec = (5L * c->ngll + 10L) * ncell;  // per split: level-0 values + edges
   if (nspl > 0) {
-    rc = ensure_buffer(c, &c->d_tape, &c->tape_bytes, sizeof(double) * (size_t)(nspl * plane), "adjoint tape");
+    rc = ensure_buffer(c, &c->d_tape, &c->tape_bytes, sizeof(double) * (size_t)((nspl + 1) * plane + nspl * rec),
+                       "adjoint tape");
     if (rc) return rc;
-    rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes,
-                       sizeof(double) * (size_t)(10 * ncell + 10 * nface + 5L * (ord + 2L * c->ngll) * ncell),
+    rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes, sizeof(double) * (size_t)(10 * nface + 5L * (ord + c->ngll) * ncell),
                        "adjoint scratch");
     if (rc) return rc;
   }
-  // forward recomputation: tape[s] = state at the start of split s
+  // forward recomputation: state s = state at the start of split s (s = 0..nspl), and the
+  // record of split s (its level-0 values and edges) taken by the recording sweep
+  double *states = c->d_tape, *recs = c->d_tape + (nspl + 1) * plane;
   cudaError_t e = cudaSuccess;
+  if (nspl > 0) e = cudaMemcpyAsync(states, d_state_ckpt, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
   for (long s = 0; s < nspl && e == cudaSuccess; s++) {
-    double *dst = c->d_tape + s * plane;
-    const double *src = s == 0 ? (const double *)d_state_ckpt : dst - plane;
-    e = cudaMemcpyAsync(dst, src, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess && s > 0) e = launch_sweep_fp64(ord, dirs[s - 1], sweep_args(c, dst, nullptr, dt, dirs[s - 1], MODE_APPLY), st);
+    double *dst = states + (s + 1) * plane;
+    e = cudaMemcpyAsync(dst, states + s * plane, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess)
+      e = launch_sweep_rec(ord, dirs[s], sweep_args(c, dst, recs + s * rec, dt, dirs[s], MODE_APPLY), st);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "adjoint forward recomputation");
   // reverse sweeps, last split first
   for (long s = nspl - 1; s >= 0 && e == cudaSuccess; s--) {
     const int dir = dirs[s];
     adj::SplitArgs A{};
-    A.state = c->d_tape + s * plane;
-    A.edges = c->d_adj;
-    A.lq = c->d_adj + 10 * ncell;
-    A.ls = c->d_adj + 10 * ncell + 10 * nface;
-    A.q0 = A.ls + 5L * ord * ncell;
-    A.lq0 = A.q0 + 5L * c->ngll * ncell;
+    A.state = states + s * plane;
+    A.q0 = recs + s * rec;
+    A.edges = A.q0 + 5L * c->ngll * ncell;
+    A.lq = c->d_adj;
+    A.ls = c->d_adj + 10 * nface;
+    A.lq0 = A.ls + 5L * ord * ncell;
     A.lam = (double *)d_lambda;
     A.nx = nx; A.ny = ny; A.nz = nz; A.hs = c->hs;
     A.sim2d = c->sim2d;
@@ -720,7 +725,7 @@ int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int
     A.ca.dt = dt;
     A.ca.dens_c = c->d_dens_c; A.ca.denstheta_c = c->d_denstheta_c;
     A.ca.dens_g = c->d_dens_g; A.ca.denstheta_g = c->d_denstheta_g; A.ca.pres_g = c->d_pres_g;
-    e = launch_adjoint_split(ord, dir, A, 1, c->nsm, st);
+    e = launch_adjoint_split(ord, dir, A, 0, c->nsm, st);
   }
   if (e == cudaSuccess) e = launch_zero_halo((double *)d_lambda, nx, ny, nz, c->hs, c->nsm, st);
   if (e != cudaSuccess) return cuda_fail(c, e, "adjoint reverse sweep");

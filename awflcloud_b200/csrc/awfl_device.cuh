@@ -135,9 +135,15 @@ __device__ __forceinline__ void reconstruct_gll(const Sc (&sten)[ORD], Sc (&out)
 // sten(v, s) returns stencil value s of variable v. kb is the k index of the cell (z) or of
 // the line (x, y). Outputs: the time-averaged left/right edge states and, for z, the
 // time-averaged, GLL-weighted gravity source.
-template <int ORD, int DIR, class Sten, class Sc>
+// A recorder that keeps nothing (the default): rec.level0(v, ii, x) sees every level-0
+// value (after hydrostasis and the wall), for the adjoint's tape.
+struct NoRecord {
+  template <class Sc> __device__ __forceinline__ void level0(int, int, const Sc &) const {}
+};
+
+template <int ORD, int DIR, class Sten, class Sc, class Rec = NoRecord>
 __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const SweepArgs &A, Sc (&eL)[5], Sc (&eR)[5],
-                                           Sc &src_avg) {
+                                           Sc &src_avg, const Rec &rec = Rec()) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
   constexpr int NA = NG;  // nAder = ngll (Temporal_ader.h:8)
@@ -168,6 +174,10 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
     if (kb == A.nz - 1) q[idW][0][NG - 1] = 0;
     if (kb == 0) q[idW][0][0] = 0;
   }
+#pragma unroll
+  for (int v = 0; v < 5; v++)
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) rec.level0(v, ii, q[v][0][ii]);
   // level-0 flux products (Spatial:704-715 and y/z equivalents)
   Sc f[4][NA][NG];
   Sc g[NA][NG];

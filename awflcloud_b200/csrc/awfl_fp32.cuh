@@ -424,7 +424,7 @@ struct P32 {
 
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, float (&eL)[5], float (&eR)[5],
-                                               float &src) {
+                                               float &src, long) {
     cell_recon32<ORD, DIR>(sten, kb, A, eL, eR, src);
   }
   template <int DIR, int NG>

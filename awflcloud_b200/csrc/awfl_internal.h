@@ -95,6 +95,8 @@ cudaError_t upload_tables_fp64(int ord, const void *tab, size_t bytes);
 cudaError_t launch_sweep_fp64(int ord, int dir, const SweepArgs &A, cudaStream_t st);
 // Differentiation TU (awfl_adjoint.cu)
 cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t st);
+// FP64 sweep that also records level-0 values and edges of every cell into A.tend
+cudaError_t launch_sweep_rec(int ord, int dir, const SweepArgs &A, cudaStream_t st);
 cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes);
 // Adjoint reverse sweeps (awfl_adjrev.cu)
 cudaError_t launch_adjoint_split(int ord, int dir, const adj::SplitArgs &A, int need_edges, int nsm, cudaStream_t st);

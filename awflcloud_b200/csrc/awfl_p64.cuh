@@ -25,7 +25,7 @@ struct P64 {
 
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],
-                                               double (&eR)[5], double &src) {
+                                               double (&eR)[5], double &src, long) {
     cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
   }
 

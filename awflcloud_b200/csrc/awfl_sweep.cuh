@@ -24,7 +24,9 @@
 // The physics policy P supplies the element type, the per-cell reconstruction (+ADER +
 // time average), the face flux, the tendency and the in-place update:
 //   using Real; using Args;                         Args has state/tend/nx/ny/nz/bc/mode/sim2d
-//   template <int ORD, int DIR, class S> recon(sten, kb, A, eL[5], eR[5], src)
+//   template <int ORD, int DIR, class S> recon(sten, kb, A, eL[5], eR[5], src, cell)
+//                                          (cell: the cell's (k,j,i) index, -1 for the
+//                                          periodic prologue's repeat of cell L-1)
 //   template <int DIR, int NG>            flux(qL[5], qR[5], kf, A, F[5])
 //                                          (kf: the face's k for z, the line's k for x, y)
 //   template <int DIR>                    tendency(v, Fl, Fr, src, A) -> Real
@@ -169,7 +171,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       return G(v, p);
     };
     Real eL[5], eR[5], sa;
-    P::template recon<ORD, DIR>(wrapSten, DIR == 2 ? L - 1 : kline, A, eL, eR, sa);
+    P::template recon<ORD, DIR>(wrapSten, DIR == 2 ? L - 1 : kline, A, eL, eR, sa, -1L);
 #pragma unroll
     for (int v = 0; v < 5; v++) sER[v][E(0)] = eR[v];
   }
@@ -205,7 +207,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       const int p = base + c;
       auto sten = [&](int v, int m) -> Real { return ringAt(v, p - HS + m); };
       Real eL[5], eR[5], sa;
-      P::template recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa);
+      P::template recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa, tb + p * tsd);
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         sEL[v][E(c)] = eL[v];
