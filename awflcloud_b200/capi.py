@@ -18,6 +18,7 @@ BC = {"periodic": 0, "wall": 1}
 DATA = {"thermal": 1, "collision": 2, "straka": 3, "igw": 4}
 FP64, FP32 = 0, 1
 INIT_REFERENCE, INIT_BUBBLE = 0, 1
+NOISE_UNIFORM, NOISE_NORMAL = 0, 1
 
 
 class AwflConfig(ctypes.Structure):
@@ -33,7 +34,8 @@ class AwflInitSpec(ctypes.Structure):
                 ("x0", ctypes.c_double), ("y0", ctypes.c_double), ("z0", ctypes.c_double),
                 ("xrad", ctypes.c_double), ("yrad", ctypes.c_double), ("zrad", ctypes.c_double),
                 ("amp", ctypes.c_double), ("pwr", ctypes.c_double),
-                ("noise_amp", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong)]
+                ("noise_amp", ctypes.c_double), ("noise_seed", ctypes.c_ulonglong),
+                ("noise_kind", ctypes.c_int)]
 
 
 class AwflError(RuntimeError):
@@ -52,6 +54,8 @@ _SIGS = {
     "awfl_sizes": (_I, [_VP, ctypes.POINTER(_L), ctypes.POINTER(_L), ctypes.POINTER(_I)]),
     "awfl_init_state": (_I, [_VP, _VP, ctypes.POINTER(AwflInitSpec), _VP]),
     "awfl_cfl": (_I, [_VP, _VP, _D, _DP, _VP]),
+    "awfl_state_sums": (_I, [_VP, _VP, _DP, _VP]),
+    "awfl_check_state": (_I, [_VP, _VP, ctypes.POINTER(_L), _VP]),
     "awfl_compute_tendencies": (_I, [_VP, _VP, _VP, _D, _I, _VP]),
     "awfl_apply_tendencies": (_I, [_VP, _VP, _VP, _D, _VP]),
     "awfl_split": (_I, [_VP, _VP, _D, _I, _VP]),
@@ -231,14 +235,30 @@ class Context:
     # ---- entry points
     def init_state(self, state, kind=INIT_REFERENCE, shape=1, x0=10000.0, y0=10000.0, z0=2000.0,
                    xrad=2000.0, yrad=2000.0, zrad=2000.0, amp=3.0, pwr=1.0, noise_amp=0.0,
-                   noise_seed=20261203, stream=None):
-        spec = AwflInitSpec(kind, shape, x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp, noise_seed)
+                   noise_seed=20261203, noise_kind=NOISE_UNIFORM, stream=None):
+        spec = AwflInitSpec(kind, shape, x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp, noise_seed, noise_kind)
         self._check(self.L.awfl_init_state(self.h, self._st(state), ctypes.byref(spec), _stream(stream)))
 
     def cfl(self, state, cfl=0.8, stream=None):
         out = ctypes.c_double()
         self._check(self.L.awfl_cfl(self.h, self._st(state), cfl, ctypes.byref(out), _stream(stream)))
         return out.value
+
+    def state_sums(self, state, stream=None):
+        """FP64 sums x dV of the five conserved variables over the interior."""
+        import numpy as np
+        out = np.zeros(5)
+        self._check(self.L.awfl_state_sums(self.h, self._st(state), out.ctypes.data_as(_DP), _stream(stream)))
+        return out
+
+    def check_state(self, state, stream=None):
+        """Number of interior cells with a non-finite value or a non-positive density (0 when
+        healthy; the C call returns AWFL_ERR_STATE otherwise)."""
+        n = _L()
+        rc = self.L.awfl_check_state(self.h, self._st(state), ctypes.byref(n), _stream(stream))
+        if rc not in (AWFL_OK, -4):
+            self._check(rc)
+        return n.value
 
     def compute_tendencies(self, state, tend, dt, d, stream=None):
         self._check(self.L.awfl_compute_tendencies(self.h, self._st(state), self._td(tend), dt, d, _stream(stream)))

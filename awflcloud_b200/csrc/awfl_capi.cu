@@ -45,6 +45,9 @@ struct awfl_ctx {
   size_t tape_bytes = 0;
   double *d_adj = nullptr;
   size_t adj_bytes = 0;
+  // diagnostics: 5 sums, a counter, then the block partials of the sums
+  double *d_diag = nullptr;
+  size_t diag_bytes = 0;
   std::string err;
 };
 
@@ -347,6 +350,32 @@ long state_plane(const awfl_ctx *c) {
 
 }  // namespace
 
+namespace {
+
+// Grows a device buffer owned by the context (contents are not kept).
+int ensure_buffer(awfl_ctx *c, double **buf, size_t *have, size_t need, const char *what) {
+  if (*have >= need) return AWFL_OK;
+  if (*buf) {
+    cudaFree(*buf);
+    *buf = nullptr;
+    *have = 0;
+  }
+  cudaError_t e = cudaMalloc(buf, need);
+  if (e != cudaSuccess) {
+    *buf = nullptr;
+    cudaGetLastError();
+    return fail(c, AWFL_ERR_NOMEM, "cudaMalloc %s (%zu bytes): %s", what, need, cudaGetErrorString(e));
+  }
+  *have = need;
+  return AWFL_OK;
+}
+
+int ensure_diag(awfl_ctx *c, int nblk) {
+  return ensure_buffer(c, &c->d_diag, &c->diag_bytes, sizeof(double) * (size_t)(8 + 5 * nblk), "diagnostics scratch");
+}
+
+}  // namespace
+
 // Accessors for the library's other host translation unit (awfl_ensemble.cu).
 namespace awfl {
 namespace host {
@@ -458,6 +487,7 @@ int awfl_destroy(awfl_ctx *c) {
     if (c->d_bg32) cudaFree(c->d_bg32);
     if (c->d_tape) cudaFree(c->d_tape);
     if (c->d_adj) cudaFree(c->d_adj);
+    if (c->d_diag) cudaFree(c->d_diag);
   }
   delete c;
   return AWFL_OK;
@@ -508,11 +538,51 @@ int awfl_init_state(awfl_ctx *c, void *d_state, const awfl_init_spec *spec, void
     L.kind = spec->kind; L.shape = spec->shape;
     L.x0 = spec->x0; L.y0 = spec->y0; L.z0 = spec->z0; L.xrad = spec->xrad; L.yrad = spec->yrad; L.zrad = spec->zrad;
     L.amp = spec->amp; L.pwr = spec->pwr; L.noise_amp = spec->noise_amp; L.seed = spec->noise_seed;
+    L.noise_kind = spec->noise_kind;
   }
   L.dens_c = c->d_dens_c;
   for (int m = 0; m < c->cfg.ord; m++) { L.pts[m] = c->pts_ord[m]; L.wts[m] = c->wts_ord[m]; }
   cudaError_t e = launch_init_state_fp64(L, (cudaStream_t)stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "init_state kernel");
+  return AWFL_OK;
+}
+
+int awfl_state_sums(awfl_ctx *c, const void *d_state, double *sums, void *stream) {
+  if (!c || !sums) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_state_sums: state pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int nblk = c->nsm * 2;
+  rc = ensure_diag(c, nblk);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = launch_state_sums(d_state, fp32(c), state_plane(c), c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs,
+                                    c->dx * c->dy * c->dz, c->d_diag + 8, nblk, c->d_diag, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sums, c->d_diag, 5 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_state_sums");
+  return AWFL_OK;
+}
+
+int awfl_check_state(awfl_ctx *c, const void *d_state, long *bad_cells, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_check_state: state pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  rc = ensure_diag(c, c->nsm * 2);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long *cnt = reinterpret_cast<unsigned long long *>(c->d_diag + 5);
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof *cnt, st);
+  if (e == cudaSuccess)
+    e = launch_check_state(d_state, fp32(c), state_plane(c), c->d_dens_c, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs,
+                           c->nsm, cnt, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, cnt, sizeof h, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_check_state");
+  if (bad_cells) *bad_cells = (long)h;
+  if (h) return fail(c, AWFL_ERR_STATE, "%llu cells with a non-finite value or a non-positive density", h);
   return AWFL_OK;
 }
 
@@ -624,27 +694,7 @@ int awfl_step_tlm(awfl_ctx *c, void *d_state_tangent, double dt, void *stream) {
   return AWFL_OK;
 }
 
-namespace {
 
-// Grows a device buffer owned by the context (contents are not kept).
-int ensure_buffer(awfl_ctx *c, double **buf, size_t *have, size_t need, const char *what) {
-  if (*have >= need) return AWFL_OK;
-  if (*buf) {
-    cudaFree(*buf);
-    *buf = nullptr;
-    *have = 0;
-  }
-  cudaError_t e = cudaMalloc(buf, need);
-  if (e != cudaSuccess) {
-    *buf = nullptr;
-    cudaGetLastError();
-    return fail(c, AWFL_ERR_NOMEM, "cudaMalloc %s (%zu bytes): %s", what, need, cudaGetErrorString(e));
-  }
-  *have = need;
-  return AWFL_OK;
-}
-
-}  // namespace
 
 int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
   if (!c || nsteps < 0 || !bytes) return AWFL_ERR_ARG;

@@ -119,6 +119,7 @@ struct InitArgs {
   double x0, y0, z0, xrad, yrad, zrad, amp, pwr;
   double noise_amp;
   unsigned long long seed;
+  int noise_kind;
   const double *dens_c;
   double pts[9], wts[9];
 };
@@ -217,8 +218,16 @@ __global__ void init_state_kernel(InitArgs a) {
       }
   if (a.noise_amp > 0) {
     const unsigned long long cell = ((unsigned long long)k * a.ny + j) * a.nx + i;
-    const double u = (double)(d_splitmix64(a.seed * 0x100000001B3ULL + cell) >> 11) * (1.0 / 9007199254740992.0);
-    const double nz_ = (2.0 * u - 1.0) * a.noise_amp;
+    const unsigned long long base = a.seed * 0x100000001B3ULL;
+    double nz_;
+    if (a.noise_kind == 1) {  // Box-Muller: u1 in (0, 1], u2 in [0, 1)
+      const double u1 = (double)((d_splitmix64(base + 2 * cell) >> 11) + 1) * (1.0 / 9007199254740992.0);
+      const double u2 = (double)(d_splitmix64(base + 2 * cell + 1) >> 11) * (1.0 / 9007199254740992.0);
+      nz_ = a.noise_amp * sqrt(-2.0 * log(u1)) * cos(6.283185307179586476925 * u2);
+    } else {
+      const double u = (double)(d_splitmix64(base + cell) >> 11) * (1.0 / 9007199254740992.0);
+      nz_ = (2.0 * u - 1.0) * a.noise_amp;
+    }
     acc[4] += a.dens_c[hs + k] * nz_;
   }
   if (a.state32) {  // FP32 context: value plane and a zeroed Kahan plane
@@ -243,9 +252,92 @@ cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st) {
   a.data_spec = L.data_spec; a.sim2d = L.sim2d; a.kind = L.kind; a.shape = L.shape;
   a.x0 = L.x0; a.y0 = L.y0; a.z0 = L.z0; a.xrad = L.xrad; a.yrad = L.yrad; a.zrad = L.zrad;
   a.amp = L.amp; a.pwr = L.pwr; a.noise_amp = L.noise_amp; a.seed = L.seed; a.dens_c = L.dens_c;
+  a.noise_kind = L.noise_kind;
   for (int m = 0; m < 9; m++) { a.pts[m] = m < L.ord ? L.pts[m] : 0; a.wts[m] = m < L.ord ? L.wts[m] : 0; }
   const long n = (long)L.nz * L.ny * L.nx;
   init_state_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
+// Diagnostics: FP64 interior sums x dV with a fixed reduction order (each block sums a
+// fixed stride of cells, then one block adds the block partials in order), and a count
+// of cells with a non-finite value or a non-positive total density.
+// ------------------------------------------------------------------------------------
+constexpr int kSumThreads = 256;
+
+__device__ __forceinline__ double state_at(const void *state, int fp32, long plane, long g) {
+  if (fp32) {
+    const float *s = (const float *)state;
+    return (double)s[g] - (double)s[g + plane];  // value minus Kahan compensation
+  }
+  return ((const double *)state)[g];
+}
+
+__global__ void __launch_bounds__(kSumThreads) state_sums_kernel(const void *state, int fp32, long plane, int nx,
+                                                                  int ny, int nz, int hs, double *partials) {
+  __shared__ double red[5][kSumThreads];
+  const long n = (long)nz * ny * nx;
+  const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
+  double acc[5] = {0., 0., 0., 0., 0.};
+  for (long c = blockIdx.x * (long)kSumThreads + threadIdx.x; c < n; c += (long)gridDim.x * kSumThreads) {
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long)nx * ny));
+    const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
+#pragma unroll
+    for (int v = 0; v < 5; v++) acc[v] += state_at(state, fp32, plane, g + v * sv);
+  }
+#pragma unroll
+  for (int v = 0; v < 5; v++) red[v][threadIdx.x] = acc[v];
+  __syncthreads();
+  for (int s = kSumThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) red[v][threadIdx.x] += red[v][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) partials[blockIdx.x * 5 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void state_sums_final_kernel(const double *partials, int nblk, double dv, double *out) {
+  if (threadIdx.x < 5) {
+    double s = 0.;
+    for (int b = 0; b < nblk; b++) s += partials[b * 5 + threadIdx.x];
+    out[threadIdx.x] = s * dv;
+  }
+}
+
+cudaError_t launch_state_sums(const void *state, int fp32, long plane, int nx, int ny, int nz, int hs, double dv,
+                              double *partials, int nblk, double *out, cudaStream_t st) {
+  state_sums_kernel<<<nblk, kSumThreads, 0, st>>>(state, fp32, plane, nx, ny, nz, hs, partials);
+  state_sums_final_kernel<<<1, 32, 0, st>>>(partials, nblk, dv, out);
+  return cudaGetLastError();
+}
+
+__global__ void check_state_kernel(const void *state, int fp32, long plane, const double *dens_c, int nx, int ny,
+                                   int nz, int hs, unsigned long long *count) {
+  const long n = (long)nz * ny * nx;
+  const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
+  unsigned long long bad = 0;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long)nx * ny));
+    const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
+    bool ok = true;
+#pragma unroll
+    for (int v = 0; v < 5; v++) ok = ok && isfinite(state_at(state, fp32, plane, g + v * sv));
+    ok = ok && (dens_c[hs + k] + state_at(state, fp32, plane, g)) > 0.0;
+    bad += ok ? 0 : 1;
+  }
+  if (bad) atomicAdd(count, bad);
+}
+
+cudaError_t launch_check_state(const void *state, int fp32, long plane, const double *dens_c, int nx, int ny,
+                               int nz, int hs, int nsm, unsigned long long *count, cudaStream_t st) {
+  const long n = (long)nz * ny * nx;
+  long blocks = (n + 255) / 256;
+  if (blocks > (long)nsm * 8) blocks = (long)nsm * 8;
+  if (blocks < 1) blocks = 1;
+  check_state_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, nx, ny, nz, hs, count);
   return cudaGetLastError();
 }
 

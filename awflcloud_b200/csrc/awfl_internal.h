@@ -62,6 +62,7 @@ struct InitLaunch {
   int data_spec, sim2d, kind, shape;
   double x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp;
   unsigned long long seed;
+  int noise_kind;
   const double *dens_c;
   double pts[9], wts[9];
 };
@@ -108,6 +109,11 @@ cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const dou
                             double dx, double dy, double dz, int nx, int ny, int nz, int hs, int nsm,
                             unsigned long long *d_out, cudaStream_t st);
 cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st);
+// interior sums x dV (partials[nblk*5] -> out[5], fixed order) and the bad-cell count
+cudaError_t launch_state_sums(const void *state, int fp32, long plane, int nx, int ny, int nz, int hs, double dv,
+                              double *partials, int nblk, double *out, cudaStream_t st);
+cudaError_t launch_check_state(const void *state, int fp32, long plane, const double *dens_c, int nx, int ny,
+                               int nz, int hs, int nsm, unsigned long long *count, cudaStream_t st);
 cudaError_t run_fma_peak(int fp32, int nsm, double *tflops);
 cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st);
 

@@ -17,7 +17,8 @@
 //    reference adds an uninitialised tendency array to them, Temporal_ader.h:67-69).
 //  * Optional extra YAML keys (absent = reference behaviour): precision (fp64 | fp32),
 //    device, bubble (cosine | linear) with bubble_x0/y0/z0, bubble_radius (or
-//    bubble_xrad/yrad/zrad), bubble_amp, bubble_pwr; noise_amp, noise_seed.
+//    bubble_xrad/yrad/zrad), bubble_amp, bubble_pwr; noise_amp, noise_seed, noise_dist
+//    (uniform | normal; noise_amp is then the standard deviation).
 #pragma once
 
 #include <cstring>
@@ -261,6 +262,11 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
     }
     if (config["noise_amp"]) initSpec.noise_amp = config["noise_amp"].as<double>();
     initSpec.noise_seed = config["noise_seed"] ? (unsigned long long)config["noise_seed"].as<double>() : 20261203ULL;
+    if (config["noise_dist"]) {
+      const std::string d = config["noise_dist"].as<std::string>();
+      if (d != "uniform" && d != "normal") endrun("ERROR: noise_dist must be uniform or normal");
+      initSpec.noise_kind = d == "normal" ? AWFL_NOISE_NORMAL : AWFL_NOISE_UNIFORM;
+    }
 
     numTracers = (int)tracerName.size();
 

@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble (batching) leg")
     ap.add_argument("--ens-members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=50)
-    ap.add_argument("--only", choices=["adjoint", "ensemble"],
+    ap.add_argument("--no-precision", action="store_true", help="skip the 512x512x128 precision leg")
+    ap.add_argument("--only", choices=["adjoint", "ensemble", "precision"],
                     help="run only that leg and print its JSON object (profiling aid)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison arm and the 100-step accuracy check")
@@ -359,6 +360,42 @@ def adjoint_leg(a, local):
             "note": "backward = recomputation of every segment from its checkpoint + reverse sweeps"}
 
 
+def precision_leg(a, local):
+    """The precision configuration: 512x512x128, ord 5, bubble amp 2 K radius 1.5 km +
+    N(0, 0.05 K) theta noise (Box-Muller on splitmix64), 100 steps of the FP32 form and of
+    the FP64 path from the same initial data: relative L2 per variable, and each form's
+    change of the total perturbation mass (FP64 sums, awfl_state_sums)."""
+    import numpy as np
+    import torch
+    from awflcloud_b200 import capi
+    n, steps = (512, 512, 128), 100
+    spec = dict(kind=1, shape=1, x0=10000.0, y0=10000.0, z0=2000.0, xrad=1500.0, yrad=1500.0, zrad=1500.0,
+                amp=2.0, pwr=1.0, noise_amp=0.05, noise_seed=20261203, noise_kind=capi.NOISE_NORMAL)
+    c64 = capi.Context(*n, precision=capi.FP64, device=local)
+    c32 = capi.Context(*n, precision=capi.FP32, device=local)
+    s64, s32 = c64.new_state(), c32.new_state()
+    c64.init_state(s64, **spec)
+    c32.init_state(s32, **spec)
+    dt = c64.cfl(s64, 0.8)
+    m64, m32 = c64.state_sums(s64)[0], c32.state_sums(s32)[0]
+    for _ in range(steps):
+        c64.step(s64, dt)
+        c32.step(s32, dt)
+    h = c64.hs
+    errs = {}
+    for v, name in enumerate(("rho", "rho_u", "rho_v", "rho_w", "rho_theta")):
+        x = s32[v, h:-h, h:-h, h:-h].double()
+        y = s64[v, h:-h, h:-h, h:-h]
+        errs[name] = (torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)).item()
+    dv = (20000.0 / n[0]) * (20000.0 / n[1]) * (10000.0 / n[2])
+    total = float(np.sum(c64.background()["hyDensCells"][h:-h])) * n[0] * n[1] * dv
+    return {"workload": "512x512x128, ord 5, bubble 2 K / 1.5 km + N(0, 0.05 K) theta noise, %d steps" % steps,
+            "rel_l2_fp32_vs_fp64": errs,
+            "mass_drift_rel": {"fp64": (c64.state_sums(s64)[0] - m64) / total,
+                               "fp32": (c32.state_sums(s32)[0] - m32) / total},
+            "bad_cells": {"fp64": c64.check_state(s64), "fp32": c32.check_state(s32)}}
+
+
 ENS_SIZES = ((32, 32, 32), (64, 64, 32), (96, 96, 48), (128, 128, 64))
 
 
@@ -462,6 +499,8 @@ def run_ours(a):
             line["adjoint"] = adjoint_leg(a, local)
         if not a.no_ensemble:
             line["ensemble"] = ensemble_leg(a, local)
+        if not a.no_precision:
+            line["precision"] = precision_leg(a, local)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a)
         print(json.dumps(line))
@@ -531,7 +570,7 @@ def main():
         import torch
         local = int(os.environ.get("LOCAL_RANK", "0"))
         torch.cuda.set_device(local)
-        leg = adjoint_leg(a, local) if a.only == "adjoint" else ensemble_leg(a, local)
+        leg = {"adjoint": adjoint_leg, "ensemble": ensemble_leg, "precision": precision_leg}[a.only](a, local)
         print(json.dumps({"leg": a.only, **leg}))
         return 0
     return run_ours(a)

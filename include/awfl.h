@@ -63,16 +63,21 @@ typedef struct {
  * Spatial::initState for the context's data_spec (Spatial:428-485); AWFL_INIT_BUBBLE
  * replaces the theta perturbation by an ellipsoid (shape 0 linear / 1 cosine, Profiles.h
  * 49-72) integrated with the same ord^3 GLL quadrature. noise_amp > 0 then adds seeded
- * uniform theta noise n in [-amp, amp) as state(rho*theta) += hyDensCells(k) * n, where
- * n = 2*u-1 times amp, u = top 53 bits of splitmix64(seed*0x100000001B3 + cell)/2^53,
- * cell = (k*ny + j)*nx + i. */
+ * theta noise n as state(rho*theta) += hyDensCells(k) * n, cell = (k*ny + j)*nx + i:
+ *   noise_kind AWFL_NOISE_UNIFORM: n = (2u-1)*amp, u = top 53 bits of
+ *     splitmix64(seed*0x100000001B3 + cell)/2^53;
+ *   noise_kind AWFL_NOISE_NORMAL: n = amp*sqrt(-2 ln u1)*cos(2 pi u2) (Box-Muller), u1 =
+ *     (top 53 bits of splitmix64(seed*0x100000001B3 + 2 cell) + 1)/2^53, u2 likewise from
+ *     2 cell + 1: normal noise of standard deviation amp. */
 enum { AWFL_INIT_REFERENCE = 0, AWFL_INIT_BUBBLE = 1 };
+enum { AWFL_NOISE_UNIFORM = 0, AWFL_NOISE_NORMAL = 1 };
 typedef struct {
   int kind;
   int shape;
   double x0, y0, z0, xrad, yrad, zrad, amp, pwr;
   double noise_amp;
   unsigned long long noise_seed;
+  int noise_kind;
 } awfl_init_spec;
 
 typedef struct awfl_ctx awfl_ctx;
@@ -93,6 +98,18 @@ int awfl_sizes(const awfl_ctx *ctx, long *state_elems, long *tend_elems, int *hs
 
 /* Spatial::initState (Spatial:345-500) on the device; writes the interior of d_state. */
 int awfl_init_state(awfl_ctx *ctx, void *d_state, const awfl_init_spec *spec, void *stream);
+
+/* Sums over the interior of the five conserved variables times the cell volume, in FP64
+ * (FP32 contexts: the value plane minus the Kahan compensation): sums[0] = sum rho' dV
+ * (the perturbation mass), sums[1..3] the momenta, sums[4] = sum (rho theta)' dV. Fixed
+ * reduction order, so the result is reproducible bit for bit. Synchronises the stream.
+ * (The reference has no such diagnostic; its run only prints dt and etime.) */
+int awfl_state_sums(awfl_ctx *ctx, const void *d_state, double *sums, void *stream);
+
+/* Device-side state check: counts interior cells with a non-finite value or a
+ * non-positive total density; AWFL_ERR_STATE if any (count in *bad_cells, may be NULL).
+ * Synchronises the stream. */
+int awfl_check_state(awfl_ctx *ctx, const void *d_state, long *bad_cells, void *stream);
 
 /* Spatial::computeTimeStep without the caching (Spatial:159-187): the acoustic CFL time
  * step, min over all cells, returned in *h_dt (synchronises the stream). */
