@@ -89,101 +89,137 @@ template <> __device__ __forceinline__ float tv_evalf<3>(const float *a) { retur
 template <> __device__ __forceinline__ float tv_evalf<5>(const float *a) { return awfl_tv_n5<float>(a); }
 template <> __device__ __forceinline__ float tv_evalf<9>(const float *a) { return awfl_tv_n9<float>(a); }
 
+// Two independent FP32 lanes evaluated with the paired sm_100 instructions (FFMA2, FMUL2,
+// FADD2: one instruction, two results, each rounded like the scalar operation), so that
+// two variables' reconstructions issue half the instructions. Divisions stay per lane.
+struct F2 {
+  float2 v;
+  __device__ __forceinline__ F2() {}
+  __device__ __forceinline__ F2(float2 x) : v(x) {}
+  __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
+  __device__ __forceinline__ explicit F2(double c) : v(make_float2((float)c, (float)c)) {}
+  __device__ __forceinline__ explicit F2(float c) : v(make_float2(c, c)) {}
+};
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd2_rn(a.v, b.v)); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y))); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(__fmul2_rn(a.v, b.v)); }
+__device__ __forceinline__ F2 operator*(float c, F2 b) { return F2(__fmul2_rn(make_float2(c, c), b.v)); }
+__device__ __forceinline__ F2 operator*(F2 a, float c) { return F2(__fmul2_rn(a.v, make_float2(c, c))); }
+__device__ __forceinline__ F2 operator+(F2 a, float c) { return F2(__fadd2_rn(a.v, make_float2(c, c))); }
+__device__ __forceinline__ F2 operator+(float c, F2 a) { return F2(__fadd2_rn(make_float2(c, c), a.v)); }
+__device__ __forceinline__ F2 &operator+=(F2 &a, F2 b) { return a = a + b; }
+
+// fma / reciprocal / quotient on either scalar type
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ F2 fmaT(float a, F2 b, F2 c) { return F2(__ffma2_rn(make_float2(a, a), b.v, c.v)); }
+__device__ __forceinline__ F2 fmaT(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
+__device__ __forceinline__ F2 fmaT(F2 a, float b, F2 c) { return F2(__ffma2_rn(a.v, make_float2(b, b), c.v)); }
+__device__ __forceinline__ float rcpT(float x) { return frcp(x); }
+__device__ __forceinline__ F2 rcpT(F2 x) { return F2(frcp(x.v.x), frcp(x.v.y)); }
+__device__ __forceinline__ float divT(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ F2 divT(float a, F2 b) { return F2(__fdividef(a, b.v.x), __fdividef(a, b.v.y)); }
+__device__ __forceinline__ F2 divT(F2 a, F2 b) { return F2(__fdividef(a.v.x, b.v.x), __fdividef(a.v.y, b.v.y)); }
+
+template <int N> __device__ __forceinline__ F2 tv_evalf2(const F2 *a) {
+  if constexpr (N == 3) return awfl_tv_n3<F2>(a);
+  else if constexpr (N == 5) return awfl_tv_n5<F2>(a);
+  else return awfl_tv_n9<F2>(a);
+}
+template <int N> __device__ __forceinline__ float tv_evalT(const float *a) { return tv_evalf<N>(a); }
+template <int N> __device__ __forceinline__ F2 tv_evalT(const F2 *a) { return tv_evalf2<N>(a); }
+
 // WenoLimiter.h:93-172 in FP32.
-template <int ORD>
-__device__ __forceinline__ void weno_coefs32(const float (&u)[ORD], float (&aw)[ORD]) {
+template <int ORD, class T>
+__device__ __forceinline__ void weno_coefs32(const T (&u)[ORD], T (&aw)[ORD]) {
   constexpr int HS = (ORD - 1) / 2;
-  const Tables32<ORD> &T = tab32<ORD>();
+  const Tables32<ORD> &Tb = tab32<ORD>();
   const float eps = 1.0e-20f;
-  float a[HS + 2][ORD];
+  T a[HS + 2][ORD];
 #pragma unroll
   for (int i = 0; i < HS + 1; i++)
 #pragma unroll
     for (int ii = 0; ii < HS + 1; ii++) {
-      float acc = 0.f;
+      T acc = T(0.f);
 #pragma unroll
-      for (int s = 0; s < HS + 1; s++) acc = fmaf(T.recon[(i * ORD + s) * ORD + ii], u[i + s], acc);
+      for (int s = 0; s < HS + 1; s++) acc = fmaT(Tb.recon[(i * ORD + s) * ORD + ii], u[i + s], acc);
       a[i][ii] = acc;
     }
 #pragma unroll
   for (int ii = 0; ii < ORD; ii++) {
-    float acc = 0.f;
+    T acc = T(0.f);
 #pragma unroll
-    for (int s = 0; s < ORD; s++) acc = fmaf(T.recon[((HS + 1) * ORD + s) * ORD + ii], u[s], acc);
+    for (int s = 0; s < ORD; s++) acc = fmaT(Tb.recon[((HS + 1) * ORD + s) * ORD + ii], u[s], acc);
     if (ii < HS + 1) {
 #pragma unroll
-      for (int i = 0; i < HS + 1; i++) acc = fmaf(-T.idl[i], a[i][ii], acc);
+      for (int i = 0; i < HS + 1; i++) acc = fmaT(-Tb.idl[i], a[i][ii], acc);
     }
-    a[HS + 1][ii] = acc * T.inv_idl_last;
+    a[HS + 1][ii] = acc * Tb.inv_idl_last;
   }
-  float tv[HS + 2];
+  T tv[HS + 2];
 #pragma unroll
-  for (int i = 0; i < HS + 1; i++) tv[i] = tv_evalf<HS + 1>(a[i]);
-  tv[HS + 1] = tv_evalf<ORD>(a[HS + 1]);
-  float lo_avg = 0.f;
+  for (int i = 0; i < HS + 1; i++) tv[i] = tv_evalT<HS + 1>(a[i]);
+  tv[HS + 1] = tv_evalT<ORD>(a[HS + 1]);
+  T lo_avg = T(0.f);
 #pragma unroll
   for (int i = 0; i < HS + 1; i++) lo_avg += tv[i];
-  lo_avg *= 1.0f / (HS + 1);
-  tv[HS + 1] = fmaf(tv[HS + 1] - lo_avg, T.sigma, lo_avg);
-  float wts[HS + 2];
-  float sum = 0.f;
+  lo_avg = lo_avg * (1.0f / (HS + 1));
+  tv[HS + 1] = fmaT(tv[HS + 1] - lo_avg, Tb.sigma, lo_avg);
+  T wts[HS + 2];
+  T sum = T(0.f);
 #pragma unroll
   for (int i = 0; i < HS + 2; i++) {
-    wts[i] = __fdividef(T.idl[i], fmaf(tv[i], tv[i], eps));
+    wts[i] = divT(Tb.idl[i], fmaT(tv[i], tv[i], T(eps)));
     sum += wts[i];
   }
-  float inv = frcp(sum + eps);
-  sum = 0.f;
+  T inv = rcpT(sum + eps);
+  sum = T(0.f);
 #pragma unroll
   for (int i = 0; i < HS + 2; i++) {
-    const float w = wts[i] * inv;
-    const float d = T.idl[i];
-    const float num = w * (d + d * d - 3.f * d * w + w * w);
-    const float den = d * d + w * (1.f - 2.f * d);
-    wts[i] = __fdividef(num, den);
+    const T w = wts[i] * inv;
+    const float d = Tb.idl[i];
+    const T num = w * ((d + d * d) + (w * w - (3.f * d) * w));
+    const T den = (d * d) + w * (1.f - 2.f * d);
+    wts[i] = divT(num, den);
     sum += wts[i];
   }
-  inv = frcp(sum + eps);
+  inv = rcpT(sum + eps);
 #pragma unroll
-  for (int ii = 0; ii < ORD; ii++) aw[ii] = 0.f;
+  for (int ii = 0; ii < ORD; ii++) aw[ii] = T(0.f);
 #pragma unroll
   for (int i = 0; i < HS + 2; i++) {
-    const float w = wts[i] * inv;
+    const T w = wts[i] * inv;
 #pragma unroll
     for (int ii = 0; ii < ORD; ii++) {
       if (i < HS + 1 && ii > HS) continue;  // zero coefficients of the low-order candidates
-      aw[ii] = fmaf(w, a[i][ii], aw[ii]);
+      aw[ii] = fmaT(w, a[i][ii], aw[ii]);
     }
   }
 }
-
-template <int ORD>
-__device__ __forceinline__ void reconstruct_gll32(const float (&sten)[ORD], float (&out)[OrdTraits<ORD>::NGLL],
-                                                  bool doweno) {
+template <int ORD, class T>
+__device__ __forceinline__ void reconstruct_gll32(const T (&sten)[ORD], T (&out)[OrdTraits<ORD>::NGLL], bool doweno) {
   constexpr int NG = OrdTraits<ORD>::NGLL;
-  const Tables32<ORD> &T = tab32<ORD>();
+  const Tables32<ORD> &Tb = tab32<ORD>();
   if (doweno) {
-    float wc[ORD];
+    T wc[ORD];
     weno_coefs32<ORD>(sten, wc);
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      float tmp = 0.f;
+      T tmp = T(0.f);
 #pragma unroll
-      for (int s = 0; s < ORD; s++) tmp = fmaf(T.c2g[s * NG + ii], wc[s], tmp);
+      for (int s = 0; s < ORD; s++) tmp = fmaT(Tb.c2g[s * NG + ii], wc[s], tmp);
       out[ii] = tmp;
     }
   } else {
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      float tmp = 0.f;
+      T tmp = T(0.f);
 #pragma unroll
-      for (int s = 0; s < ORD; s++) tmp = fmaf(T.s2g[s * NG + ii], sten[s], tmp);
+      for (int s = 0; s < ORD; s++) tmp = fmaT(Tb.s2g[s * NG + ii], sten[s], tmp);
       out[ii] = tmp;
     }
   }
 }
 
-// Reconstruction + ADER + edge time average of one cell in FP32 (perturbation form).
 template <int ORD, int DIR, class Sten>
 __device__ __forceinline__ void cell_recon32(const Sten &sten, int kb, const SweepArgs32 &A, float (&eL)[5],
                                              float (&eR)[5], float &src_avg) {
@@ -194,13 +230,25 @@ __device__ __forceinline__ void cell_recon32(const Sten &sten, int kb, const Swe
   const Tables32<ORD> &T = tab32<ORD>();
 
   float q[5][NA][NG];  // level 0: rho' (perturbation), rho*u/v/w, (rho*theta)' (perturbation)
+  // (rho', (rho theta)') and (rho u, rho v) in pairs on the paired FP32 instructions
 #pragma unroll
-  for (int v = 0; v < 5; v++) {
+  for (int pr = 0; pr < 2; pr++) {
+    const int va = pr == 0 ? idR : idU, vb = pr == 0 ? idT : idV;
+    F2 s2[ORD], o2[NG];
+#pragma unroll
+    for (int m = 0; m < ORD; m++) s2[m] = F2(sten(va, m), sten(vb, m));
+    reconstruct_gll32<ORD>(s2, o2, pr == 0 ? A.weno_s : A.weno_w);
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      q[va][0][ii] = o2[ii].v.x;
+      q[vb][0][ii] = o2[ii].v.y;
+    }
+  }
+  {
     float s[ORD];
 #pragma unroll
-    for (int m = 0; m < ORD; m++) s[m] = sten(v, m);
-    const bool doweno = (v == idR || v == idT) ? A.weno_s : A.weno_w;
-    reconstruct_gll32<ORD>(s, q[v][0], doweno);
+    for (int m = 0; m < ORD; m++) s[m] = sten(idW, m);
+    reconstruct_gll32<ORD>(s, q[idW][0], A.weno_w);
   }
   if (DIR == 2 && A.bc == BC_WALL) {  // Spatial:1413-1416
     if (kb == A.nz - 1) q[idW][0][NG - 1] = 0.f;
