@@ -277,9 +277,9 @@ def time_form(a, prec, local, world, clocks=None):
             "finite": bool(torch.isfinite(st).all().item())}
 
 
-# DRAM bytes per sweep launch (read + write), from ncu on the 256x256x128 workload
-# (profiles/sweep_kernel_256x256x128.md).
-TRAFFIC = {(0, 5): 633_800_000, (1, 5): 632_500_000}
+# DRAM bytes per sweep launch (read + write, mean over x/y/z), from ncu on the 256x256x128
+# workload (profiles/sweep_kernel_256x256x128.md).
+TRAFFIC = {(0, 5): 644_900_000, (1, 5): 630_000_000}
 
 
 def rel_l2_after(a, steps, local):
