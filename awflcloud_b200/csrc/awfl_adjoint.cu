@@ -19,6 +19,7 @@ struct PTLM {
   using Real = Dual;
   static constexpr int kWdiv = 2;
   static constexpr bool kAsyncRing = false;
+  static constexpr bool kTmaRing = false;
   static constexpr int min_blocks(int) { return 1; }
   using Args = SweepArgs;
   struct Aux {};

@@ -37,6 +37,7 @@ struct awfl_ctx {
   double *d_dens_c = nullptr, *d_denstheta_c = nullptr, *d_dens_g = nullptr, *d_denstheta_g = nullptr,
          *d_pres_g = nullptr;
   unsigned long long *d_cfl = nullptr;  // CFL reduction result (8 bytes)
+  unsigned int *d_err = nullptr;        // a sweep's bounded wait gave up (the next 8 bytes)
   // FP32 form: FP32 copies of FP64 background constants (awfl_fp32_args.h)
   float *d_bg32 = nullptr;
   Bg32 bg32{};
@@ -299,7 +300,7 @@ int build_bg32(awfl_ctx *c) {
 }
 
 SweepArgs32 sweep_args32(awfl_ctx *c, void *state, void *tend, double dt, int dir, int mode) {
-  SweepArgs32 A;
+  SweepArgs32 A{};
   const long n = 5L * (c->cfg.nz + 2 * c->hs) * (c->cfg.ny + 2 * c->hs) * (c->cfg.nx + 2 * c->hs);
   A.state = (float *)state;
   A.comp = (float *)state + n;
@@ -310,6 +311,8 @@ SweepArgs32 sweep_args32(awfl_ctx *c, void *state, void *tend, double dt, int di
   A.inv_dxd = (float)(1.0 / (dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz)));
   A.dt = (float)dt;
   A.bg = c->bg32;
+  A.tma = 0;  // a single-grid sweep launch encodes its own tensor map (awfl_sweep.cuh)
+  A.err = c->d_err;
   return A;
 }
 
@@ -462,6 +465,7 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   c->d_denstheta_g = c->d_dens_g + nz * g;
   c->d_pres_g = c->d_denstheta_g + nz * g;
   c->d_cfl = reinterpret_cast<unsigned long long *>(c->d_pres_g + nz * g);
+  c->d_err = reinterpret_cast<unsigned int *>(c->d_cfl + 1);
   std::vector<double> h;
   h.reserve(nbg);
   h.insert(h.end(), c->dens_c.begin(), c->dens_c.end());
@@ -470,9 +474,11 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   h.insert(h.end(), c->denstheta_g.begin(), c->denstheta_g.end());
   h.insert(h.end(), c->pres_g.begin(), c->pres_g.end());
   e = cudaMemcpy(c->d_bg, h.data(), nbg * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(unsigned int));
   if (e != cudaSuccess) { cuda_fail(nullptr, e, "upload background"); g_create_error = "upload background: " + std::string(cudaGetErrorString(e)); cudaFree(c->d_bg); delete c; return AWFL_ERR_CUDA; }
   if (cfg->precision == AWFL_FP32) {
     rc = build_bg32(c);
+    warm_tma_encoder();
     if (rc) { g_create_error = c->err; cudaFree(c->d_bg); if (c->d_bg32) cudaFree(c->d_bg32); delete c; return rc; }
   }
   *out = c;
@@ -583,6 +589,10 @@ int awfl_check_state(awfl_ctx *c, const void *d_state, long *bad_cells, void *st
   if (e != cudaSuccess) return cuda_fail(c, e, "awfl_check_state");
   if (bad_cells) *bad_cells = (long)h;
   if (h) return fail(c, AWFL_ERR_STATE, "%llu cells with a non-finite value or a non-positive density", h);
+  unsigned int werr = 0;  // a sweep whose bounded wait for its staged rows gave up
+  e = cudaMemcpy(&werr, c->d_err, sizeof werr, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_check_state");
+  if (werr) return fail(c, AWFL_ERR_TIMEOUT, "a sweep gave up waiting for its staged stencil rows");
   return AWFL_OK;
 }
 

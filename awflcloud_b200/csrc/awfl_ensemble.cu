@@ -114,9 +114,10 @@ int build_lists(awfl_ensemble *e, const std::vector<void *> &states, void **d_ou
                 EnsList<SweepArgs32> (&l32)[3]) {
   const int n = (int)e->mem.size();
   const size_t asz = e->prec == AWFL_FP32 ? sizeof(SweepArgs32) : sizeof(SweepArgs);
-  // layout per direction: args[n] | prefix[n+1] | nbx[n], 16-byte aligned pieces
-  auto up16 = [](size_t x) { return (x + 15) & ~size_t(15); };
-  const size_t per = up16(asz * n) + up16(sizeof(long) * (n + 1)) + up16(sizeof(int) * n);
+  // layout per direction: args[n] | prefix[n+1] | nbx[n], 64-byte aligned pieces (the
+  // FP32 arguments hold a 64-byte-aligned tensor map field)
+  auto up64 = [](size_t x) { return (x + 63) & ~size_t(63); };
+  const size_t per = up64(asz * n) + up64(sizeof(long) * (n + 1)) + up64(sizeof(int) * n);
   std::vector<unsigned char> host(per * 3, 0);
   for (int dir = 0; dir < 3; dir++) {
     int C, W;
@@ -129,8 +130,8 @@ int build_lists(awfl_ensemble *e, const std::vector<void *> &states, void **d_ou
     });
     unsigned char *base = host.data() + per * dir;
     unsigned char *pa = base;
-    long *pp = (long *)(base + up16(asz * n));
-    int *pn = (int *)(base + up16(asz * n) + up16(sizeof(long) * (n + 1)));
+    long *pp = (long *)(base + up64(asz * n));
+    int *pn = (int *)(base + up64(asz * n) + up64(sizeof(long) * (n + 1)));
     long total = 0;
     for (size_t q = 0; q < order.size(); q++) {
       const int m = order[q];
@@ -164,8 +165,8 @@ int build_lists(awfl_ensemble *e, const std::vector<void *> &states, void **d_ou
     unsigned char *base = (unsigned char *)d + per * dir;
     l64[dir].args = (const SweepArgs *)base;
     l32[dir].args = (const SweepArgs32 *)base;
-    l64[dir].prefix = l32[dir].prefix = (const long *)(base + up16(asz * n));
-    l64[dir].nbx = l32[dir].nbx = (const int *)(base + up16(asz * n) + up16(sizeof(long) * (n + 1)));
+    l64[dir].prefix = l32[dir].prefix = (const long *)(base + up64(asz * n));
+    l64[dir].nbx = l32[dir].nbx = (const int *)(base + up64(asz * n) + up64(sizeof(long) * (n + 1)));
   }
   *d_out = d;
   return AWFL_OK;

@@ -1,11 +1,58 @@
 // FP32 precision form of the AWFL Euler-3D ADER/WENO step, sm_100a: sweep, apply, CFL
 // and conversion kernels. The scheme's FP32 arithmetic and the sweep policy P32 are in
 // awfl_fp32.cuh.
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
 
 #include "awfl_fp32.cuh"
 
 namespace awfl {
+
+static_assert(sizeof(TmaMap) == sizeof(CUtensorMap) && alignof(TmaMap) >= 64, "TmaMap holds a CUtensorMap");
+
+namespace {
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+// The driver's tensor-map encoder, looked up once through the runtime (no libcuda link).
+EncodeTiledFn encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+}  // namespace
+
+void warm_tma_encoder() { (void)encoder(); }
+
+bool encode_state_map32(TmaMap *m, const float *state, int xe, int ye, int ze, const unsigned (&box)[3]) {
+  if (reinterpret_cast<uintptr_t>(state) % 16 != 0 || ((long)xe * 4) % 16 != 0) return false;
+  for (int d = 0; d < 3; d++)
+    if (box[d] < 1 || box[d] > 256) return false;
+  if ((box[0] * 4u) % 16 != 0) return false;
+  EncodeTiledFn fn = encoder();
+  if (!fn) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)xe, (cuuint64_t)ye, (cuuint64_t)5 * ze};
+  const cuuint64_t strides[2] = {(cuuint64_t)xe * 4, (cuuint64_t)xe * ye * 4};
+  const cuuint32_t bx[3] = {box[0], box[1], box[2]}, es[3] = {1, 1, 1};
+  CUtensorMap t;
+  const CUresult r = fn(&t, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(state), dims, strides, bx, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return false;
+  static_assert(sizeof t == sizeof *m, "tensor map size");
+  __builtin_memcpy(m, &t, sizeof t);
+  return true;
+}
 
 cudaError_t launch_sweep_fp32(int ord, int dir, const SweepArgs32 &A, cudaStream_t st) {
   return launch_sweep_any<P32>(ord, dir, A, st);

@@ -459,6 +459,21 @@ struct P32 {
   using Real = float;
   static constexpr int kWdiv = 1;
   static constexpr bool kAsyncRing = true;
+  // single-grid sweeps stage interior chunks by tiled TMA (the ensemble's persistent
+  // sweeps, whose arguments sit in shared memory, keep cp.async)
+  static constexpr bool kTmaRing = true;
+  template <int ORD, int DIR, int C, int W, int RW>
+  static bool prepare_tma(SweepArgs32 &A) {
+    const int hs = (ORD - 1) / 2;
+    const unsigned box[3] = {DIR == 0 ? (unsigned)C : (unsigned)RW, DIR == 0 ? (unsigned)W : (DIR == 1 ? (unsigned)C : 1u),
+                             DIR == 2 ? (unsigned)C : 1u};
+    A.tma = encode_state_map32(&A.tmap, A.state, A.nx + 2 * hs, A.ny + 2 * hs, A.nz + 2 * hs, box) ? 1 : 0;
+    return A.tma != 0;
+  }
+  static __device__ __forceinline__ const void *tma_map(const SweepArgs32 &A) { return &A.tmap; }
+  static __device__ __forceinline__ void flag_timeout(const SweepArgs32 &A) {
+    if (A.err) atomicOr(A.err, 1u);
+  }
   static constexpr int min_blocks(int) { return 1; }  // forcing more CTAs per SM measured slower
   using Args = SweepArgs32;
   // the Kahan compensations of the cell's five variables, loaded before the reconstruction

@@ -10,7 +10,15 @@ struct Bg32 {
   const float *rho_f, *rt_f, *irt_f, *p_f;  // z faces 0..nz: bottom point of cell k, top of cell nz-1 for face nz
 };
 
+// A TMA tensor map (the 128-byte CUtensorMap of the CUDA driver API, opaque here),
+// 64-byte aligned as TMA requires.
+struct alignas(64) TmaMap {
+  unsigned long long w[16];
+};
+
 struct SweepArgs32 {
+  TmaMap tmap;   // single-grid sweeps with tma != 0: the state as a 3-D tensor
+                 // {nx+2hs, ny+2hs, 5*(nz+2hs)} floats, box = one chunk of one variable
   float *state;  // plane 0 of the FP32 state
   float *comp;   // plane 1: Kahan compensation
   float *tend;
@@ -19,6 +27,16 @@ struct SweepArgs32 {
   float inv_dxd;
   float dt;
   Bg32 bg;
+  int tma;             // interior chunks' stencil rows arrive by TMA through tmap
+  unsigned int *err;   // set to nonzero if a bounded wait of the sweep gave up
 };
+
+// Encodes *m as the tiled tensor map of an FP32 state with halo-inclusive extents
+// xe x ye x ze per variable (dims {xe, ye, 5*ze}) and the given box (x, y, z extents).
+// Returns false (m untouched) where TMA cannot address the layout: a state base not
+// 16-byte aligned, a row pitch not a multiple of 16 bytes, or an encoder error.
+bool encode_state_map32(TmaMap *m, const float *state, int xe, int ye, int ze, const unsigned (&box)[3]);
+// Looks the encoder up now (context creation), not inside a caller's stream capture.
+void warm_tma_encoder();
 
 }  // namespace awfl

@@ -34,6 +34,10 @@
 //                                          g0 + v*sv), loaded a reconstruction ahead
 //   apply(A, gidx, orig, tnd, aux, v)      state[gidx] = orig "+" dt*tnd (MODE_APPLY)
 //   kAsyncRing                             next-chunk rows by cp.async into a 4C ring
+//   kTmaRing, prepare_tma<ORD,DIR,C,W,RW>(A) (host), tma_map(A), flag_timeout(A)
+//                                          next-chunk rows of interior chunks by tiled TMA
+//                                          copies through a tensor map in the kernel
+//                                          parameter (single-grid sweeps only)
 //   min_blocks(ORD)                        CTAs per SM the register budget must allow
 //   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
 //   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
@@ -51,9 +55,63 @@ template <class T> __device__ __forceinline__ void cp_async_row(T *dst_smem, con
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Tiled TMA loads (cp.async.bulk.tensor) completing on a shared-memory mbarrier. The
+// destination is the CTA's own shared memory (128-byte aligned boxes), the source this
+// GPU's global memory through a tensor map held in the kernel parameter; no multicast.
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *mb, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(mb)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned long long *mb) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_addr(mb)) : "memory");
+}
+__device__ __forceinline__ void mbar_arm(unsigned long long *mb, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(mb)), "r"(bytes) : "memory");
+}
+// Waits for the phase of the given parity, giving up after a bounded number of polls
+// (each poll may suspend the thread for a while); returns false then.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *mb, unsigned parity) {
+  const unsigned a = smem_addr(mb);
+  for (int i = 0; i < (1 << 20); i++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// One 3-D box of the tensor map at element coordinates (x, y, z) into shared memory.
+__device__ __forceinline__ void tma_load_3d(void *dst_smem, const void *tmap, int x, int y, int z,
+                                            unsigned long long *mb) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smem_addr(dst_smem)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_addr(mb))
+      : "memory");
+}
+// orders this thread's generic-proxy shared-memory accesses before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// Row pitch (elements) of the ring of a y/z sweep fed by TMA: the box starts at the
+// 16-byte-aligned x = bx*W of the halo-inclusive row (the tile's first line sits at
+// column HS), spans at least W + HS columns in a multiple of 4, and a chunk's C rows
+// (one box) are a multiple of 128 bytes so that every box lands 128-byte aligned.
+template <int ORD, int C, int W, int ESZ> __host__ __device__ constexpr int tma_ring_pitch() {
+  int rw = (W + (ORD - 1) / 2 + 3) / 4 * 4;
+  while ((C * rw * ESZ) % 128 != 0) rw += 4;
+  return rw;
+}
+
 // One CTA's tile: lines bx*W .. bx*W+W-1 of plane `by` (x, y sweeps: by = k; z: by = j).
-template <class P, int ORD, int DIR, int C, int W>
-__device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int bx, const int by) {
+// tmap: the tensor map of the TMA path (a kernel-parameter address), or nullptr; only
+// instantiations with TMA = true (single-grid sweeps of a kTmaRing policy) read it.
+template <class P, int ORD, int DIR, int C, int W, bool TMA = false>
+__device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int bx, const int by,
+                                           const void *tmap = nullptr) {
   using Real = typename P::Real;
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
@@ -63,6 +121,19 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   // otherwise they are loaded into registers and stored at the next chunk's start.
   constexpr bool ASYNC = P::kAsyncRing;
   constexpr int R = ASYNC ? 4 * C : 2 * C;  // ring length (power of two, >= C + 2*HS)
+  // TMA path (TMA, with the async ring): a chunk whose rows are all interior arrives as
+  // five tiled TMA boxes, one per variable, issued by one thread and completing on an
+  // mbarrier -- x sweep: box {C positions, W lines}, landing as one page [W][C] of the
+  // ring; y/z sweeps: box {RW columns from x = bx*W, C positions}, landing as C ring rows
+  // of pitch RW with line w at column HS + w. Other chunks (and a tile whose wait gave
+  // up) use cp.async. Out-of-range box elements (the last tile's missing lines) read as
+  // zero and are never used.
+  static_assert(!TMA || ASYNC, "the TMA path feeds the async ring");
+  constexpr int RW = (TMA && DIR != 0) ? tma_ring_pitch<ORD, C, W, (int)sizeof(Real)>() : W;
+  static_assert(!TMA || DIR != 0 || ((C * W * (int)sizeof(Real)) % 128 == 0 && (2 * HS * (int)sizeof(Real)) % 16 == 0 &&
+                                     (C * (int)sizeof(Real)) % 16 == 0),
+                "x-sweep TMA pages must be 128-byte multiples starting at 16-byte-aligned x");
+  static_assert(!TMA || DIR == 0 || (W * (int)sizeof(Real)) % 16 == 0, "y/z-sweep TMA boxes start at x = bx*W");
   constexpr int NM = 1 + DIR;
   static_assert((C & (C - 1)) == 0 && C >= 2 * HS, "chunk must be a power of two >= 2*HS");
   // Register path: load the next chunk's rows before the reconstruction (latency hidden
@@ -70,7 +141,9 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   // whole planes; after the updates for x and y, where occupancy matters more (measured).
   constexpr bool EARLY_PREFETCH = !ASYNC && DIR == 2;
 
-  __shared__ Real ring[5][R * W];
+  __shared__ __align__(128) Real ring[5][R * RW];
+  __shared__ __align__(8) unsigned long long mbar;  // TMA path only
+  __shared__ int sAbort;                            // TMA path: a wait of this tile gave up
   __shared__ Real sEL[5][(C + 1) * W];
   __shared__ Real sER[5][(C + 1) * W];
   __shared__ Real sF[5][(C + 1) * W];
@@ -111,9 +184,19 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   const bool periodic = A.bc == BC_PERIODIC;
 
   auto G = [&](int v, int p) -> Real { return P::load(A, lb + v * sv + p * sd); };
+  // ring slot of position p: the async ring counts from p = HS so that a chunk's rows
+  // (positions base+HS .. base+C+HS-1) fill one aligned run of C slots. The x sweep's
+  // async ring is paged: page s/C holds [line][slot % C], so the two lines of a warp
+  // read 32 consecutive words (no bank conflict) and a chunk is one TMA box.
   auto ringAt = [&](int v, int p) -> Real & {
-    const int s = p & (R - 1);
-    return DIR == 0 ? ring[v][w * R + s] : ring[v][s * W + w];
+    if constexpr (ASYNC) {
+      const int s = (p - HS) & (R - 1);
+      if constexpr (DIR == 0) return ring[v][(s / C) * (W * C) + w * C + (s & (C - 1))];
+      else return ring[v][s * RW + (TMA ? HS : 0) + w];
+    } else {
+      const int s = p & (R - 1);
+      return DIR == 0 ? ring[v][w * R + s] : ring[v][s * W + w];
+    }
   };
   auto topval = [&](int v, int p, bool first) -> Real {  // p >= L
     const int q = p - L;
@@ -136,8 +219,29 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       else ringAt(v, p) = topval(v, p, first);
     }
   };
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  // the chunk whose rows start at position p0 comes by TMA (uniform in the CTA)
+  auto chunk_tma = [&](int p0) { return TMA && p0 + C <= L; };
+  constexpr unsigned kTmaBytes = 5u * C * (DIR == 0 ? W : RW) * (unsigned)sizeof(Real);
+  auto issue_tma = [&](int p0) {  // thread 0 only
+    if constexpr (TMA) {
+      const int s0 = (p0 - HS) & (R - 1);  // a multiple of C
+      const int zp = nz + 2 * HS;          // the map's z extent per variable
+      mbar_arm(&mbar, kTmaBytes);
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        if (DIR == 0) tma_load_3d(&ring[v][(s0 / C) * (W * C)], tmap, HS + p0, HS + bx * W, v * zp + HS + by, &mbar);
+        else if (DIR == 1) tma_load_3d(&ring[v][s0 * RW], tmap, bx * W, HS + p0, v * zp + HS + by, &mbar);
+        else tma_load_3d(&ring[v][s0 * RW], tmap, bx * W, HS + by, v * zp + HS + p0, &mbar);
+      }
+    }
+  };
 
   // ---- prologue: bottom halo, saved wrap rows, top halo; chunk-0 prefetch
+  if (TMA && tid == 0) {
+    mbar_init(&mbar, 1);
+    sAbort = 0;
+  }
   if (valid && c < HS) {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
@@ -152,7 +256,16 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
     }
   }
   Real pre[ASYNC ? 1 : 5];
-  if (valid) {
+  bool cur_tma = false;  // this chunk's rows come by TMA (uniform in the CTA)
+  unsigned phase = 0;    // TMA phases of the mbarrier issued so far
+  if constexpr (TMA) {
+    cur_tma = chunk_tma(HS);
+    fence_proxy_async();  // the prologue's generic writes to ring slots before any TMA write
+    __syncthreads();      // the mbarrier is initialised before its first use
+    if (cur_tma && tid == 0) issue_tma(HS);
+    if (cur_tma) phase++;
+  }
+  if (valid && !cur_tma) {
     const int p = HS + c;
     if constexpr (ASYNC) {
 #pragma unroll
@@ -180,6 +293,17 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   for (int t = 0; t < nchunk; t++) {
     const int base = t * C;
     const int nvalid = min(C, L - base);
+    if constexpr (TMA) {
+      // the chunk's boxes have landed; a wait that gives up flags the error and ends the
+      // tile's use of TMA (the rest of the tile's chunks come by cp.async)
+      if (cur_tma && !mbar_wait(&mbar, (phase - 1) & 1u)) {
+        P::flag_timeout(A);
+        sAbort = 1;
+      }
+      // (generic reads of a slot, then a TMA write into it after barrier (A): ordered by
+      // the barrier. Generic writes into slots a TMA box later fills happen only in the
+      // prologue -- fenced there -- or in the last chunks, after the tile's last box.)
+    }
     if constexpr (ASYNC) {
       cp_async_wait_all();  // this thread's rows of the chunk have landed
     } else if (valid) {
@@ -188,10 +312,17 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
     }
     __syncthreads();  // (A)
     if constexpr (ASYNC) {  // the next chunk's rows, a chunk ahead
-      if (valid && t + 1 < nchunk) {
+      bool next_tma = false;
+      if constexpr (TMA) {
+        next_tma = t + 1 < nchunk && chunk_tma(base + C + HS) && !*(volatile int *)&sAbort;
+        if (next_tma && tid == 0) issue_tma(base + C + HS);
+        if (next_tma) phase++;
+      }
+      if (!next_tma && valid && t + 1 < nchunk) {
 #pragma unroll
         for (int v = 0; v < 5; v++) stage(v, base + C + HS + c, false);
       }
+      cur_tma = next_tma;
     }
     // the compensation (or other per-cell input) of the cell this thread updates below
     typename P::Aux aux;
@@ -273,11 +404,23 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
     if (A.mode == MODE_APPLY) P::load_aux(A, lb + (L - 1) * sd, sv, aux);
     finish(L - 1, Fl, F, DIR == 2 ? sSrc[E(0)] : Real(0), aux);
   }
+  if constexpr (TMA) {  // every issued phase has completed (or been given up on, flagged)
+    __syncthreads();
+    if (tid == 0) {
+      // after a give-up, a last bounded wait so that no box is still landing in this
+      // CTA's shared memory when the tile ends
+      if (sAbort && phase > 0) (void)mbar_wait(&mbar, (phase - 1) & 1u);
+      mbar_inval(&mbar);
+    }
+  }
 }
 
-template <class P, int ORD, int DIR, int C, int W>
-__global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) sweep_kernel(typename P::Args A) {
-  sweep_tile<P, ORD, DIR, C, W>(A, blockIdx.x, blockIdx.y);
+// TMA: the policy's single-grid TMA path; its tensor map lives in the (grid-constant)
+// kernel parameter, the only place besides global memory a TMA copy may read it from.
+template <class P, int ORD, int DIR, int C, int W, bool TMA>
+__global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) sweep_kernel(const __grid_constant__ typename P::Args A) {
+  if constexpr (TMA) sweep_tile<P, ORD, DIR, C, W, true>(A, blockIdx.x, blockIdx.y, P::tma_map(A));
+  else sweep_tile<P, ORD, DIR, C, W, false>(A, blockIdx.x, blockIdx.y);
 }
 
 template <int ORD, int DIR> struct SweepShape;
@@ -302,7 +445,16 @@ cudaError_t launch_sweep_t(const typename P::Args &A, cudaStream_t st) {
   if (DIR == 0) grid = dim3((A.ny + W - 1) / W, A.nz);
   else if (DIR == 1) grid = dim3((A.nx + W - 1) / W, A.nz);
   else grid = dim3((A.nx + W - 1) / W, A.ny);
-  sweep_kernel<P, ORD, DIR, C, W><<<grid, block, 0, st>>>(A);
+  if constexpr (P::kTmaRing) {
+    // the policy encodes this launch's tensor map (box = one chunk of one variable); a
+    // layout TMA cannot address (alignment) leaves tma off and the cp.async path runs
+    typename P::Args a = A;
+    if (P::template prepare_tma<ORD, DIR, C, W, tma_ring_pitch<ORD, C, W, (int)sizeof(typename P::Real)>()>(a)) {
+      sweep_kernel<P, ORD, DIR, C, W, true><<<grid, block, 0, st>>>(a);
+      return cudaGetLastError();
+    }
+  }
+  sweep_kernel<P, ORD, DIR, C, W, false><<<grid, block, 0, st>>>(A);
   return cudaGetLastError();
 }
 

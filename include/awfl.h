@@ -108,7 +108,8 @@ int awfl_state_sums(awfl_ctx *ctx, const void *d_state, double *sums, void *stre
 
 /* Device-side state check: counts interior cells with a non-finite value or a
  * non-positive total density; AWFL_ERR_STATE if any (count in *bad_cells, may be NULL).
- * Synchronises the stream. */
+ * AWFL_ERR_TIMEOUT if a sweep of this context ever gave up its bounded wait for staged
+ * stencil rows (the state is then not to be trusted). Synchronises the stream. */
 int awfl_check_state(awfl_ctx *ctx, const void *d_state, long *bad_cells, void *stream);
 
 /* Spatial::computeTimeStep without the caching (Spatial:159-187): the acoustic CFL time
