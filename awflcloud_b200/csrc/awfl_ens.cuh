@@ -41,7 +41,15 @@ __global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) ens_sweep_kernel(Ens
     const int nbx = E.nbx[lo];
     if (threadIdx.x == 0 && threadIdx.y == 0) sA = E.args[lo];
     __syncthreads();
-    sweep_tile<P, ORD, DIR, C, W>(sA, (int)(local % nbx), (int)(local / nbx));
+    if constexpr (P::kTmaRing) {
+      // the member's tensor map, in the list in global memory (nullptr: cp.async only)
+      const void *tm = P::tma_map_global(sA, E.args + lo);
+      if (tm && threadIdx.x == 0 && threadIdx.y == 0)  // the issuing thread sees the host-written map
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(tm) : "memory");
+      sweep_tile<P, ORD, DIR, C, W, true>(sA, (int)(local % nbx), (int)(local / nbx), tm);
+    } else {
+      sweep_tile<P, ORD, DIR, C, W>(sA, (int)(local % nbx), (int)(local / nbx));
+    }
     __syncthreads();  // the next tile reuses sA and the shared-memory ring
   }
 }
@@ -49,7 +57,7 @@ __global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) ens_sweep_kernel(Ens
 template <int ORD, int DIR> struct EnsShapes;
 template <> struct EnsShapes<5, 0> {
   static constexpr int n = 4;
-  static constexpr int C[4] = {32, 32, 64, 16}, W[4] = {4, 2, 2, 8};
+  static constexpr int C[4] = {32, 32, 8, 16}, W[4] = {4, 2, 16, 8};
 };
 template <> struct EnsShapes<5, 1> {
   static constexpr int n = 4;

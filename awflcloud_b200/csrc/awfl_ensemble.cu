@@ -138,6 +138,7 @@ int build_lists(awfl_ensemble *e, const std::vector<void *> &states, void **d_ou
       awfl_ctx *c = e->mem[m];
       if (e->prec == AWFL_FP32) {
         SweepArgs32 A = ctx_sweep_args32(c, states[m], e->dt[m], dir);
+        prepare_sweep_map32(A, e->ord, dir, C, W);  // the member's tensor map for this shape
         std::memcpy(pa + q * asz, &A, asz);
       } else {
         SweepArgs A = ctx_sweep_args64(c, states[m], e->dt[m], dir);

@@ -34,6 +34,15 @@ EncodeTiledFn encoder() {
 
 void warm_tma_encoder() { (void)encoder(); }
 
+bool prepare_sweep_map32(SweepArgs32 &A, int ord, int dir, int C, int W) {
+  const int hs = (ord - 1) / 2;
+  const unsigned rw = (unsigned)tma_ring_pitch_of(ord, C, W, 4);
+  const unsigned box[3] = {dir == 0 ? (unsigned)C : rw, dir == 0 ? (unsigned)W : (dir == 1 ? (unsigned)C : 1u),
+                           dir == 2 ? (unsigned)C : 1u};
+  A.tma = encode_state_map32(&A.tmap, A.state, A.nx + 2 * hs, A.ny + 2 * hs, A.nz + 2 * hs, box) ? 1 : 0;
+  return A.tma != 0;
+}
+
 bool encode_state_map32(TmaMap *m, const float *state, int xe, int ye, int ze, const unsigned (&box)[3]) {
   if (reinterpret_cast<uintptr_t>(state) % 16 != 0 || ((long)xe * 4) % 16 != 0) return false;
   for (int d = 0; d < 3; d++)

@@ -459,18 +459,18 @@ struct P32 {
   using Real = float;
   static constexpr int kWdiv = 1;
   static constexpr bool kAsyncRing = true;
-  // single-grid sweeps stage interior chunks by tiled TMA (the ensemble's persistent
-  // sweeps, whose arguments sit in shared memory, keep cp.async)
+  // interior chunks are staged by tiled TMA: the single-grid sweep reads the tensor map
+  // from its kernel parameter, the ensemble's persistent sweep from the work list in
+  // global memory (its shared-memory copy of the arguments is no place for one)
   static constexpr bool kTmaRing = true;
-  template <int ORD, int DIR, int C, int W, int RW>
-  static bool prepare_tma(SweepArgs32 &A) {
-    const int hs = (ORD - 1) / 2;
-    const unsigned box[3] = {DIR == 0 ? (unsigned)C : (unsigned)RW, DIR == 0 ? (unsigned)W : (DIR == 1 ? (unsigned)C : 1u),
-                             DIR == 2 ? (unsigned)C : 1u};
-    A.tma = encode_state_map32(&A.tmap, A.state, A.nx + 2 * hs, A.ny + 2 * hs, A.nz + 2 * hs, box) ? 1 : 0;
-    return A.tma != 0;
+  static bool prepare_tma(SweepArgs32 &A, int ord, int dir, int C, int W) {
+    return prepare_sweep_map32(A, ord, dir, C, W);
   }
   static __device__ __forceinline__ const void *tma_map(const SweepArgs32 &A) { return &A.tmap; }
+  static __device__ __forceinline__ const void *tma_map_global(const SweepArgs32 &shared_copy,
+                                                               const SweepArgs32 *in_global) {
+    return shared_copy.tma ? (const void *)&in_global->tmap : nullptr;
+  }
   static __device__ __forceinline__ void flag_timeout(const SweepArgs32 &A) {
     if (A.err) atomicOr(A.err, 1u);
   }
@@ -515,8 +515,10 @@ struct P32 {
 };
 
 // Single-grid sweep shapes of the FP32 form, ord 5 (chunk C x lines W; measured at
-// 256x256x128 against the other candidates of awfl_ens.cuh): x 16 x 8, y 8 x 16, z 4 x 32.
-template <> struct PolicyShape<P32, 5, 0> { static constexpr int C = 16, W = 8; };
+// 256x256x128 with TMA staging against x {16,8} {32,4} {4,32} {8,32} {16,16}, y {4,32}
+// {16,8} {16,16} {8,32} {4,16}, z {8,16} {16,8} {8,32} {4,64} {4,16}): x 8 x 16, y 8 x 16,
+// z 4 x 32.
+template <> struct PolicyShape<P32, 5, 0> { static constexpr int C = 8, W = 16; };
 template <> struct PolicyShape<P32, 5, 1> { static constexpr int C = 8, W = 16; };
 
 // Uploads the FP32 tables into this translation unit's constant memory.

@@ -36,6 +36,9 @@ struct SweepArgs32 {
 // Returns false (m untouched) where TMA cannot address the layout: a state base not
 // 16-byte aligned, a row pitch not a multiple of 16 bytes, or an encoder error.
 bool encode_state_map32(TmaMap *m, const float *state, int xe, int ye, int ze, const unsigned (&box)[3]);
+// Sets A.tmap/A.tma for a sweep of direction dir with chunk C and W lines per CTA (the box
+// of awfl_sweep.cuh's TMA path); A.tma = 0 where TMA cannot address the layout.
+bool prepare_sweep_map32(SweepArgs32 &A, int ord, int dir, int C, int W);
 // Looks the encoder up now (context creation), not inside a caller's stream capture.
 void warm_tma_encoder();
 

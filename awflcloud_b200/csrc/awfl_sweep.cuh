@@ -100,15 +100,18 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 // 16-byte-aligned x = bx*W of the halo-inclusive row (the tile's first line sits at
 // column HS), spans at least W + HS columns in a multiple of 4, and a chunk's C rows
 // (one box) are a multiple of 128 bytes so that every box lands 128-byte aligned.
-template <int ORD, int C, int W, int ESZ> __host__ __device__ constexpr int tma_ring_pitch() {
-  int rw = (W + (ORD - 1) / 2 + 3) / 4 * 4;
-  while ((C * rw * ESZ) % 128 != 0) rw += 4;
+__host__ __device__ constexpr int tma_ring_pitch_of(int ord, int C, int W, int esz) {
+  int rw = (W + (ord - 1) / 2 + 3) / 4 * 4;
+  while ((C * rw * esz) % 128 != 0) rw += 4;
   return rw;
+}
+template <int ORD, int C, int W, int ESZ> __host__ __device__ constexpr int tma_ring_pitch() {
+  return tma_ring_pitch_of(ORD, C, W, ESZ);
 }
 
 // One CTA's tile: lines bx*W .. bx*W+W-1 of plane `by` (x, y sweeps: by = k; z: by = j).
-// tmap: the tensor map of the TMA path (a kernel-parameter address), or nullptr; only
-// instantiations with TMA = true (single-grid sweeps of a kTmaRing policy) read it.
+// tmap: the tensor map of the TMA path (a kernel-parameter or global address), or nullptr
+// (the instantiation with TMA = true then stages every chunk by cp.async).
 template <class P, int ORD, int DIR, int C, int W, bool TMA = false>
 __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int bx, const int by,
                                            const void *tmap = nullptr) {
@@ -221,7 +224,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   };
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   // the chunk whose rows start at position p0 comes by TMA (uniform in the CTA)
-  auto chunk_tma = [&](int p0) { return TMA && p0 + C <= L; };
+  auto chunk_tma = [&](int p0) { return TMA && tmap != nullptr && p0 + C <= L; };
   constexpr unsigned kTmaBytes = 5u * C * (DIR == 0 ? W : RW) * (unsigned)sizeof(Real);
   auto issue_tma = [&](int p0) {  // thread 0 only
     if constexpr (TMA) {
@@ -449,7 +452,7 @@ cudaError_t launch_sweep_t(const typename P::Args &A, cudaStream_t st) {
     // the policy encodes this launch's tensor map (box = one chunk of one variable); a
     // layout TMA cannot address (alignment) leaves tma off and the cp.async path runs
     typename P::Args a = A;
-    if (P::template prepare_tma<ORD, DIR, C, W, tma_ring_pitch<ORD, C, W, (int)sizeof(typename P::Real)>()>(a)) {
+    if (P::prepare_tma(a, ORD, DIR, C, W)) {
       sweep_kernel<P, ORD, DIR, C, W, true><<<grid, block, 0, st>>>(a);
       return cudaGetLastError();
     }
