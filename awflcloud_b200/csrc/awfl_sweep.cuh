@@ -93,6 +93,20 @@ __device__ __forceinline__ void tma_load_3d(void *dst_smem, const void *tmap, in
       "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_addr(mb))
       : "memory");
 }
+// Warp shuffle up by `delta` lanes within segments of `width` lanes, for a value of any
+// type made of 4-byte words (float, double, a dual number); every lane of the warp calls it.
+template <class T> __device__ __forceinline__ T shfl_up_any(const T &x, int delta, int width) {
+  static_assert(sizeof(T) % 4 == 0, "shuffled types are made of 4-byte words");
+  constexpr int N = (int)(sizeof(T) / 4);
+  unsigned u[N];
+  __builtin_memcpy(u, &x, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < N; i++) u[i] = __shfl_up_sync(0xffffffffu, u[i], delta, width);
+  T y;
+  __builtin_memcpy(&y, u, sizeof(T));
+  return y;
+}
+
 // orders this thread's generic-proxy shared-memory accesses before later async-proxy ones
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
@@ -143,6 +157,13 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   // behind it, at the cost of 5 live registers) for the z sweep, whose loads stride over
   // whole planes; after the updates for x and y, where occupancy matters more (measured).
   constexpr bool EARLY_PREFETCH = !ASYNC && DIR == 2;
+  // x sweep: the C cells of a chunk of one line are C consecutive lanes of one warp, so the
+  // interface states and fluxes pass between neighbouring cells by warp shuffles (the
+  // first cell's left neighbour is the previous chunk's last cell, carried per line in
+  // shared memory); the chunk needs no CTA barrier besides the ring's (A). In the y/z
+  // sweeps a warp runs across lines (coalesced along x), so neighbouring cells of a line
+  // sit in different warps and trade through shared memory between barriers.
+  constexpr bool SHFL = DIR == 0 && C <= 32 && (C * W) % 32 == 0;
 
   __shared__ __align__(128) Real ring[5][R * RW];
   __shared__ __align__(8) unsigned long long mbar;  // TMA path only
@@ -189,8 +210,8 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   auto G = [&](int v, int p) -> Real { return P::load(A, lb + v * sv + p * sd); };
   // ring slot of position p: the async ring counts from p = HS so that a chunk's rows
   // (positions base+HS .. base+C+HS-1) fill one aligned run of C slots. The x sweep's
-  // async ring is paged: page s/C holds [line][slot % C], so the two lines of a warp
-  // read 32 consecutive words (no bank conflict) and a chunk is one TMA box.
+  // async ring is paged: page s/C holds [line][slot % C], so the lines of a warp read
+  // 32 consecutive words (no bank conflict) and a chunk is one TMA box.
   auto ringAt = [&](int v, int p) -> Real & {
     if constexpr (ASYNC) {
       const int s = (p - HS) & (R - 1);
@@ -337,21 +358,72 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 #pragma unroll
       for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
     }
+    Real eL[5], eR[5];
+    if constexpr (SHFL) {  // defined values on the lanes that reconstruct nothing
+#pragma unroll
+      for (int v = 0; v < 5; v++) eL[v] = eR[v] = Real(0);
+    }
     if (valid && c < nvalid) {
       const int p = base + c;
       auto sten = [&](int v, int m) -> Real { return ringAt(v, p - HS + m); };
-      Real eL[5], eR[5], sa;
+      Real sa;
       P::template recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa, tb + p * tsd);
+      if constexpr (!SHFL) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) {
-        sEL[v][E(c)] = eL[v];
-        sER[v][E(c + 1)] = eR[v];
+        for (int v = 0; v < 5; v++) {
+          sEL[v][E(c)] = eL[v];
+          sER[v][E(c + 1)] = eR[v];
+        }
+        if (DIR == 2) sSrc[E(c + 1)] = sa;
       }
-      if (DIR == 2) sSrc[E(c + 1)] = sa;
       if (p == 0) {
 #pragma unroll
         for (int v = 0; v < 5; v++) sEL0[v][w] = eL[v];
       }
+    }
+    if constexpr (SHFL) {
+      const bool act = valid && c < nvalid;
+      // face base+c: left state = right edge of cell base+c-1 (the lane below, or the carry)
+      Real qL[5], F[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        const Real up = shfl_up_any(eR[v], 1, C);
+        qL[v] = c == 0 ? sER[v][E(0)] : up;
+      }
+      if (act) {
+        if (base + c == 0 && !periodic) {
+#pragma unroll
+          for (int v = 0; v < 5; v++) qL[v] = eL[v];
+        }
+        P::template flux<DIR, NG>(qL, eL, kline, A, F);
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; v++) F[v] = Real(0);
+      }
+      // cell base+c-1: its left face's flux from the lane below (or the carry), its right
+      // face's from this lane
+      Real Fl[5];
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        const Real up = shfl_up_any(F[v], 1, C);
+        Fl[v] = c == 0 ? sF[v][E(0)] : up;
+      }
+      if (act && base + c >= 1) finish(base + c - 1, Fl, F, Real(0), aux);
+      if (!ASYNC && valid && t + 1 < nchunk) {
+        const int p = base + C + HS + c;
+#pragma unroll
+        for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
+      }
+      __syncwarp();  // the line's reads of its ring rows and carry are done
+      if (valid && c == nvalid - 1) {  // the carry: last cell's right edge and right-face flux
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          sER[v][E(0)] = eR[v];
+          sF[v][E(0)] = F[v];
+        }
+      }
+      __syncwarp();
+      continue;
     }
     __syncthreads();  // (B)
     if (valid && c < nvalid) {
