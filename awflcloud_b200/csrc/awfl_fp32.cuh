@@ -515,11 +515,11 @@ struct P32 {
 };
 
 // Single-grid sweep shapes of the FP32 form, ord 5 (chunk C x lines W; measured at
-// 256x256x128 with TMA staging against x {16,8} {32,4} {4,32} {8,32} {16,16}, y {4,32}
-// {16,8} {16,16} {8,32} {4,16}, z {8,16} {16,8} {8,32} {4,64} {4,16}): x 8 x 16, y 8 x 16,
-// z 4 x 32.
+// 256x256x128 with TMA staging against x {16,8} {32,4} {4,32} {8,32} {16,16}, y {8,16}
+// {16,8} {16,16} {8,32} {4,16}, z {8,16} {16,8} {8,32} {4,64} {4,16}): x 8 x 16, y 4 x 32,
+// z 4 x 32 (y/z: a warp = 8 lines x 4 positions, 32-byte row segments).
 template <> struct PolicyShape<P32, 5, 0> { static constexpr int C = 8, W = 16; };
-template <> struct PolicyShape<P32, 5, 1> { static constexpr int C = 8, W = 16; };
+template <> struct PolicyShape<P32, 5, 1> { static constexpr int C = 4, W = 32; };
 
 // Uploads the FP32 tables into this translation unit's constant memory.
 static inline cudaError_t upload_tables32_here(int ord, const double *recon, const double *c2g, const double *s2g,

@@ -157,13 +157,17 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   // behind it, at the cost of 5 live registers) for the z sweep, whose loads stride over
   // whole planes; after the updates for x and y, where occupancy matters more (measured).
   constexpr bool EARLY_PREFETCH = !ASYNC && DIR == 2;
-  // x sweep: the C cells of a chunk of one line are C consecutive lanes of one warp, so the
-  // interface states and fluxes pass between neighbouring cells by warp shuffles (the
+  // The C cells of a chunk of one line are C consecutive lanes of one warp (x sweep: a
+  // warp holds 32/C lines along x; y/z sweeps: 32/C neighbouring lines, so that a warp's
+  // global accesses are 32/C consecutive x cells in each of C rows), so the interface
+  // states, fluxes and z sources pass between neighbouring cells by warp shuffles (the
   // first cell's left neighbour is the previous chunk's last cell, carried per line in
-  // shared memory); the chunk needs no CTA barrier besides the ring's (A). In the y/z
-  // sweeps a warp runs across lines (coalesced along x), so neighbouring cells of a line
-  // sit in different warps and trade through shared memory between barriers.
-  constexpr bool SHFL = DIR == 0 && C <= 32 && (C * W) % 32 == 0;
+  // shared memory); the chunk needs no CTA barrier besides the ring's (A). The y/z sweeps
+  // of the register-staged path keep a warp along x across lines (32/W positions) and
+  // trade through shared memory between barriers: a warp's next-chunk loads from global
+  // memory would otherwise touch C rows instead of 32/W (FP64 z split measured 3.61 ->
+  // 3.71 ms with the shuffles).
+  constexpr bool SHFL = C <= 32 && (C * W) % 32 == 0 && (DIR == 0 || ASYNC);
 
   __shared__ __align__(128) Real ring[5][R * RW];
   __shared__ __align__(8) unsigned long long mbar;  // TMA path only
@@ -175,8 +179,10 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   __shared__ Real sWrap[5][HS * W];
   __shared__ Real sEL0[5][W];
 
-  const int c = DIR == 0 ? threadIdx.x : threadIdx.y;  // position in chunk
-  const int w = DIR == 0 ? threadIdx.y : threadIdx.x;  // line within CTA
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  // position in chunk, line within CTA
+  const int c = DIR == 0 ? (int)threadIdx.x : (SHFL ? (tid & (C - 1)) : (int)threadIdx.y);
+  const int w = DIR == 0 ? (int)threadIdx.y : (SHFL ? tid / C : (int)threadIdx.x);
   // edge/flux slot (0..C) of this line: consecutive threads of a warp hit consecutive words
   auto E = [&](int slot) { return DIR == 0 ? w * (C + 1) + slot : slot * W + w; };
 
@@ -243,7 +249,6 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       else ringAt(v, p) = topval(v, p, first);
     }
   };
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   // the chunk whose rows start at position p0 comes by TMA (uniform in the CTA)
   auto chunk_tma = [&](int p0) { return TMA && tmap != nullptr && p0 + C <= L; };
   constexpr unsigned kTmaBytes = 5u * C * (DIR == 0 ? W : RW) * (unsigned)sizeof(Real);
@@ -358,15 +363,15 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 #pragma unroll
       for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
     }
-    Real eL[5], eR[5];
+    Real eL[5], eR[5], sa;
     if constexpr (SHFL) {  // defined values on the lanes that reconstruct nothing
 #pragma unroll
       for (int v = 0; v < 5; v++) eL[v] = eR[v] = Real(0);
+      sa = Real(0);
     }
     if (valid && c < nvalid) {
       const int p = base + c;
       auto sten = [&](int v, int m) -> Real { return ringAt(v, p - HS + m); };
-      Real sa;
       P::template recon<ORD, DIR>(sten, DIR == 2 ? p : kline, A, eL, eR, sa, tb + p * tsd);
       if constexpr (!SHFL) {
 #pragma unroll
@@ -395,7 +400,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 #pragma unroll
           for (int v = 0; v < 5; v++) qL[v] = eL[v];
         }
-        P::template flux<DIR, NG>(qL, eL, kline, A, F);
+        P::template flux<DIR, NG>(qL, eL, DIR == 2 ? base + c : kline, A, F);
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) F[v] = Real(0);
@@ -408,19 +413,25 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
         const Real up = shfl_up_any(F[v], 1, C);
         Fl[v] = c == 0 ? sF[v][E(0)] : up;
       }
-      if (act && base + c >= 1) finish(base + c - 1, Fl, F, Real(0), aux);
+      Real sl = Real(0);  // z: the source term of cell base+c-1
+      if constexpr (DIR == 2) {
+        const Real up = shfl_up_any(sa, 1, C);
+        sl = c == 0 ? sSrc[E(0)] : up;
+      }
+      if (act && base + c >= 1) finish(base + c - 1, Fl, F, sl, aux);
       if (!ASYNC && valid && t + 1 < nchunk) {
         const int p = base + C + HS + c;
 #pragma unroll
         for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, false);
       }
       __syncwarp();  // the line's reads of its ring rows and carry are done
-      if (valid && c == nvalid - 1) {  // the carry: last cell's right edge and right-face flux
+      if (valid && c == nvalid - 1) {  // the carry: last cell's right edge, right-face flux, source
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           sER[v][E(0)] = eR[v];
           sF[v][E(0)] = F[v];
         }
+        if (DIR == 2) sSrc[E(0)] = sa;
       }
       __syncwarp();
       continue;
