@@ -15,7 +15,9 @@ FP64 path (`fp64`), each with CUDA events on the launching stream after W warm-u
 barrier + synchronize on both sides, max over ranks, and reports the FP32-vs-FP64 relative
 L2 after 100 steps, the cost of the discrete adjoint against the forward step
 (`adjoint`, FP64 at 128x128x64, 200 steps, checkpoint every 20), and the batching form
-(`ensemble`: 64 FP32 members of uneven sizes, 50 steps, persistent kernels in a CUDA graph). The state (357 MB in FP64) is larger
+(`ensemble`: 64 FP32 members of uneven sizes, 50 steps, persistent kernels in a CUDA graph),
+the 512x512x128 precision configuration (`precision`) and the same grid at ord 9 / ngll 5
+(`ord9`: both forms' throughput and their relative L2 after 100 steps). The state (357 MB in FP64) is larger
 than the 126 MB L2, so no flush is needed between steps. N > 1 runs N independent
 replicas (one grid per GPU, no collective): the single-domain path has no exchange step.
 
@@ -64,7 +66,8 @@ def parse():
     ap.add_argument("--ens-members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=50)
     ap.add_argument("--no-precision", action="store_true", help="skip the 512x512x128 precision leg")
-    ap.add_argument("--only", choices=["adjoint", "ensemble", "precision"],
+    ap.add_argument("--no-ord9", action="store_true", help="skip the ord-9 leg (256x256x128, ngll 5)")
+    ap.add_argument("--only", choices=["adjoint", "ensemble", "precision", "ord9"],
                     help="run only that leg and print its JSON object (profiling aid)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison arm and the 100-step accuracy check")
@@ -305,6 +308,27 @@ def rel_l2_after(a, steps, local):
     return out
 
 
+def ord9_leg(a, local):
+    """The same grid and bubble at WENO ord 9 / ngll 5 (CFL 0.4): FP32 form and FP64 path
+    throughput (K steps after W warm-up steps each) and their relative L2 after 100 steps."""
+    import copy
+    from awflcloud_b200 import capi
+    b = copy.copy(a)
+    b.ord = 9
+    b.steps = min(a.steps, 10)
+    r32 = time_form(b, capi.FP32, local, 1)
+    r64 = time_form(b, capi.FP64, local, 1)
+    errs = rel_l2_after(b, 100, local)
+    pick = lambda r: {"value": round(r["value"], 3), "ms_per_step": round(r["ms_per_step"], 4),
+                      "roofline_frac": r["roofline"]["frac"], "roofline_bound": r["roofline"]["bound"],
+                      "finite": r["finite"]}
+    return {"workload": "rising thermal bubble %dx%dx%d, ord 9 / ngll 5, CFL 0.4" % (b.nx, b.ny, b.nz),
+            "steps": b.steps, "warmup": b.warmup, "fp32": pick(r32), "fp64": pick(r64),
+            "fp32_over_fp64": round(r32["value"] / r64["value"], 3),
+            "flops_per_cell_step": r32["flops"]["flops"],
+            "rel_l2_fp32_vs_fp64_after_100_steps": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_theta"], errs))}
+
+
 def adjoint_leg(a, local):
     """Cost of the discrete adjoint against the forward step (FP64, ord 5, 128x128x64,
     same bubble): the forward pass of a gradient computation (adj_steps steps, a state
@@ -501,6 +525,8 @@ def run_ours(a):
             line["ensemble"] = ensemble_leg(a, local)
         if not a.no_precision:
             line["precision"] = precision_leg(a, local)
+        if not a.no_ord9 and a.ord == 5:
+            line["ord9"] = ord9_leg(a, local)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a)
         print(json.dumps(line))
@@ -570,7 +596,8 @@ def main():
         import torch
         local = int(os.environ.get("LOCAL_RANK", "0"))
         torch.cuda.set_device(local)
-        leg = {"adjoint": adjoint_leg, "ensemble": ensemble_leg, "precision": precision_leg}[a.only](a, local)
+        leg = {"adjoint": adjoint_leg, "ensemble": ensemble_leg, "precision": precision_leg,
+               "ord9": ord9_leg}[a.only](a, local)
         print(json.dumps({"leg": a.only, **leg}))
         return 0
     return run_ours(a)
