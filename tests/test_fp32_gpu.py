@@ -126,3 +126,39 @@ def test_fp32_full_size_rhotheta_bar():
     e = rel_l2(interior(s32, hs)[4].double(), interior(s64, hs)[4])
     print("256x256x128 x 100 steps: FP32 vs FP64 rel L2 (rho*theta) = %.3e" % e)
     assert e <= 1e-5
+
+
+@pytest.mark.parametrize("ord_", [5, 9])
+@pytest.mark.parametrize("bc", [("periodic", "periodic", "wall"), ("wall", "wall", "wall")])
+def test_tma_staging_matches_cp_async_staging(ord_, bc):
+    """Interior chunks of the FP32 sweeps arrive by tiled TMA when the state is 16-byte
+    aligned with a row pitch that is a multiple of 16 bytes; the same state two floats
+    further on (8-byte aligned, as the C ABI requires) takes the per-thread cp.async path
+    in every chunk. Both stage the same values into the ring; the two kernels (separate
+    instantiations, compiled with multiply-add contraction) may still round a few
+    operations differently, so the bound is FP32 rounding: relative L2 <= 1e-6 per
+    variable after 4 steps (a staging fault would show as O(1) differences). The grid
+    leaves partial tiles (missing lines inside a box) and a partial last chunk in every
+    direction, and no bounded TMA wait may have given up
+    (awfl_check_state would report AWFL_ERR_TIMEOUT). Each state has its own context: a
+    context alternates the split order from one step to the next."""
+    n = (60, 44, 36)  # nx + 2hs = 64 (ord 5) / 68 (ord 9): a multiple of 4 floats
+    ca = capi.Context(*n, ord_=ord_, bc=bc, precision=capi.FP32)
+    cb = capi.Context(*n, ord_=ord_, bc=bc, precision=capi.FP32)
+    s = ca.new_state()
+    ca.init_state(s, **BUBBLE)
+    dt = ca.cfl(s, 0.8 if ord_ == 5 else 0.4)
+    buf = torch.empty(s.numel() + 2, dtype=torch.float32, device=s.device)
+    u = buf[2:].view(s.shape)
+    u.copy_(s)
+    assert s.data_ptr() % 16 == 0 and u.data_ptr() % 16 == 8
+    for _ in range(4):
+        ca.step(s, dt)
+        cb.step(u, dt)
+    torch.cuda.synchronize()
+    assert torch.isfinite(s).all()
+    for v in range(5):
+        x, y = interior(s, ca.hs, 10)[v].double(), interior(u, cb.hs, 10)[v].double()
+        err = (torch.linalg.vector_norm(x - y) / torch.linalg.vector_norm(y)).item()
+        assert err <= 1e-6, (v, err)
+    assert ca.check_state(s) == 0 and cb.check_state(u) == 0
