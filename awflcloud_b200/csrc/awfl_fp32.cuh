@@ -325,22 +325,29 @@ __device__ __forceinline__ void cell_recon32(const Sten &sten, int kb, const Swe
           if (l == 0) return m == idR ? rtot[ii] : (m == idT ? rttot[ii] : q[m][0][ii]);
           return q[m][l][ii];
         };
-        auto Fx = [&](int x, int l) -> float { return l == kt + 1 ? 0.f : f[x][l][ii]; };
+        // Cauchy products of the series; the not-yet-known level kt+1 of f and g enters
+        // with a zero coefficient and is left out (an IEEE multiply by zero is not
+        // removed by the compiler)
 #pragma unroll
         for (int x = 0; x < 4; x++) {
           float tot = 0.f;
 #pragma unroll
-          for (int ir = 0; ir <= kt + 1; ir++)
-            tot += Q(NM, ir) * Q(x + 1, kt + 1 - ir) - Q(idR, ir) * Fx(x, kt + 1 - ir);
+          for (int ir = 0; ir <= kt + 1; ir++) {
+            tot = fmaf(Q(NM, ir), Q(x + 1, kt + 1 - ir), tot);
+            if (ir != 0) tot = fmaf(-Q(idR, ir), f[x][kt + 1 - ir][ii], tot);
+          }
           f[x][kt + 1][ii] = tot * ir0;
         }
         // scaled (rho theta)^gamma: g~(0) = 1 + B
-        auto Gs = [&](int l) -> float { return l == 0 ? 1.f + g[0][ii] : (l == kt + 1 ? 0.f : g[l][ii]); };
+        auto Gs = [&](int l) -> float { return l == 0 ? 1.f + g[0][ii] : g[l][ii]; };
         float tg = 0.f;
 #pragma unroll
-        for (int ir = 0; ir <= kt; ir++)
-          tg += (kt + 1.f - ir) * (GAMMAF * Gs(ir) * Q(idT, kt + 1 - ir) - Q(idT, ir) * Gs(kt + 1 - ir));
-        g[kt + 1][ii] = (GAMMAF * Gs(0) * q[idT][kt + 1][ii] + tg * (1.0f / (kt + 1))) * frcp(rttot[ii]);
+        for (int ir = 0; ir <= kt; ir++) {
+          float term = GAMMAF * Gs(ir) * Q(idT, kt + 1 - ir);
+          if (ir != 0) term = fmaf(-Q(idT, ir), Gs(kt + 1 - ir), term);
+          tg = fmaf(kt + 1.f - ir, term, tg);
+        }
+        g[kt + 1][ii] = fmaf(tg, 1.0f / (kt + 1), GAMMAF * Gs(0) * q[idT][kt + 1][ii]) * frcp(rttot[ii]);
       }
     }
   }
