@@ -12,6 +12,7 @@ Translation units and their numerics flags:
   awfl_ens32.cu    ensemble persistent sweeps, FP32 form: the awfl_fp32.cu flags
   awfl_ens64.cu    ensemble persistent sweeps, FP64 path: --fmad=false
   awfl_ensemble.cu ensemble host side: work lists, CUDA graph, autotuner (host code only)
+  awfl_netcdf.cu   netCDF output file writer (host code only)
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
 source tree. ``python -m awflcloud_b200.build [--force]``.
@@ -43,6 +44,7 @@ UNITS = {
     "awfl_ens32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "awfl_ens64.cu": ["--fmad=false"],
     "awfl_ensemble.cu": [],
+    "awfl_netcdf.cu": [],
 }
 
 

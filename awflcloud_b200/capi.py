@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "lib", "libawfl.so")
 
 AWFL_OK = 0
 STATUS = {0: "AWFL_OK", -1: "AWFL_ERR_ARG", -2: "AWFL_ERR_CUDA", -3: "AWFL_ERR_NOMEM",
-          -4: "AWFL_ERR_STATE", -5: "AWFL_ERR_TIMEOUT", -6: "AWFL_ERR_NOT_BUILT"}
+          -4: "AWFL_ERR_STATE", -5: "AWFL_ERR_TIMEOUT", -6: "AWFL_ERR_NOT_BUILT",
+          -7: "AWFL_ERR_IO"}
 BC = {"periodic": 0, "wall": 1}
 DATA = {"thermal": 1, "collision": 2, "straka": 3, "igw": 4}
 FP64, FP32 = 0, 1
@@ -56,6 +57,9 @@ _SIGS = {
     "awfl_cfl": (_I, [_VP, _VP, _D, _DP, _VP]),
     "awfl_state_sums": (_I, [_VP, _VP, _DP, _VP]),
     "awfl_check_state": (_I, [_VP, _VP, ctypes.POINTER(_L), _VP]),
+    "awfl_output_fields": (_I, [_VP, _VP, _VP, _VP]),
+    "awfl_write_netcdf": (_I, [_VP, ctypes.c_char_p, _VP, _D, _VP]),
+    "awfl_write_netcdf_fields": (_I, [_VP, ctypes.c_char_p, _DP, _D]),
     "awfl_compute_tendencies": (_I, [_VP, _VP, _VP, _D, _I, _VP]),
     "awfl_apply_tendencies": (_I, [_VP, _VP, _VP, _D, _VP]),
     "awfl_split": (_I, [_VP, _VP, _D, _I, _VP]),
@@ -250,6 +254,33 @@ class Context:
         out = np.zeros(5)
         self._check(self.L.awfl_state_sums(self.h, self._st(state), out.ctypes.data_as(_DP), _stream(stream)))
         return out
+
+    def output_fields(self, state, fields=None, stream=None):
+        """Spatial::output's diagnostics (dens_pert, u, v, w, pot_temp_pert, pressure_pert)
+        as a (6, nz, ny, nx) FP64 CUDA tensor (allocated when `fields` is None)."""
+        import torch
+        shape = (6, self.nz, self.ny, self.nx)
+        if fields is None:
+            fields = torch.empty(shape, dtype=torch.float64, device="cuda:%d" % max(self.device, 0))
+        elif (not isinstance(fields, int) and (fields.numel() < 6 * self.nz * self.ny * self.nx
+                                               or not fields.is_contiguous() or fields.dtype != torch.float64
+                                               or not fields.is_cuda)):
+            raise ValueError("fields must be a contiguous CUDA float64 tensor with >= %d elements" % (6 * self.nz * self.ny * self.nx))
+        self._check(self.L.awfl_output_fields(self.h, self._st(state), _ptr(fields), _stream(stream)))
+        return fields
+
+    def write_netcdf(self, path, state, etime, stream=None):
+        """Spatial::output: create (etime == 0) or append to the netCDF output file."""
+        self._check(self.L.awfl_write_netcdf(self.h, os.fsencode(path), self._st(state), float(etime),
+                                             _stream(stream)))
+
+    def write_netcdf_fields(self, path, fields, etime):
+        """The same file from host fields, an array of shape (6, nz, ny, nx) (no device needed)."""
+        import numpy as np
+        a = np.ascontiguousarray(fields, dtype=np.float64)
+        if a.size != 6 * self.nz * self.ny * self.nx:
+            raise ValueError("fields must have 6*nz*ny*nx = %d elements" % (6 * self.nz * self.ny * self.nx))
+        self._check(self.L.awfl_write_netcdf_fields(self.h, os.fsencode(path), a.ctypes.data_as(_DP), float(etime)))
 
     def check_state(self, state, stream=None):
         """Number of interior cells with a non-finite value or a non-positive density (0 when

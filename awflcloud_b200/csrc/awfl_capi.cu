@@ -17,6 +17,7 @@
 #include "awfl_fp32_args.h"
 #include "awfl_adj_split.h"
 #include "awfl_internal.h"
+#include "awfl_netcdf.h"
 #include "awfl_tables.h"
 
 using namespace awfl;
@@ -33,9 +34,10 @@ struct awfl_ctx {
   double sigma = 0;
   // hydrostatic background (Spatial:371-425)
   std::vector<double> dens_c, pres_c, theta_c, denstheta_c, dens_g, pres_g, theta_g, denstheta_g;
-  double *d_bg = nullptr;  // device: dens_c | denstheta_c | dens_g | denstheta_g | pres_g
+  double *d_bg = nullptr;  // device: dens_c | denstheta_c | dens_g | denstheta_g | pres_g | pres_c
   double *d_dens_c = nullptr, *d_denstheta_c = nullptr, *d_dens_g = nullptr, *d_denstheta_g = nullptr,
          *d_pres_g = nullptr;
+  double *d_pres_c = nullptr;           // hydrostatic pressure cell averages (output)
   unsigned long long *d_cfl = nullptr;  // CFL reduction result (8 bytes)
   unsigned int *d_err = nullptr;        // a sweep's bounded wait gave up (the next 8 bytes)
   // FP32 form: FP32 copies of FP64 background constants (awfl_fp32_args.h)
@@ -48,6 +50,8 @@ struct awfl_ctx {
   size_t adj_bytes = 0;
   // diagnostics: 5 sums, a counter, then the block partials of the sums
   double *d_diag = nullptr;
+  double *d_out = nullptr;  // output diagnostics (awfl_write_netcdf)
+  size_t out_bytes = 0;
   size_t diag_bytes = 0;
   std::string err;
 };
@@ -456,7 +460,7 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   rc = ensure_tables(c);
   if (rc) { g_create_error = c->err; delete c; return rc; }
   const int nz = cfg->nz, g = c->ngll;
-  const size_t nbg = (size_t)2 * (nz + 2 * hs) + (size_t)3 * nz * g;
+  const size_t nbg = (size_t)3 * (nz + 2 * hs) + (size_t)3 * nz * g;
   cudaError_t e = cudaMalloc(&c->d_bg, nbg * sizeof(double) + 64);
   if (e != cudaSuccess) { fail(nullptr, AWFL_ERR_NOMEM, "cudaMalloc background: %s", cudaGetErrorString(e)); delete c; return AWFL_ERR_NOMEM; }
   c->d_dens_c = c->d_bg;
@@ -464,7 +468,8 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   c->d_dens_g = c->d_denstheta_c + (nz + 2 * hs);
   c->d_denstheta_g = c->d_dens_g + nz * g;
   c->d_pres_g = c->d_denstheta_g + nz * g;
-  c->d_cfl = reinterpret_cast<unsigned long long *>(c->d_pres_g + nz * g);
+  c->d_pres_c = c->d_pres_g + nz * g;
+  c->d_cfl = reinterpret_cast<unsigned long long *>(c->d_pres_c + (nz + 2 * hs));
   c->d_err = reinterpret_cast<unsigned int *>(c->d_cfl + 1);
   std::vector<double> h;
   h.reserve(nbg);
@@ -473,6 +478,7 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
   h.insert(h.end(), c->dens_g.begin(), c->dens_g.end());
   h.insert(h.end(), c->denstheta_g.begin(), c->denstheta_g.end());
   h.insert(h.end(), c->pres_g.begin(), c->pres_g.end());
+  h.insert(h.end(), c->pres_c.begin(), c->pres_c.end());
   e = cudaMemcpy(c->d_bg, h.data(), nbg * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(unsigned int));
   if (e != cudaSuccess) { cuda_fail(nullptr, e, "upload background"); g_create_error = "upload background: " + std::string(cudaGetErrorString(e)); cudaFree(c->d_bg); delete c; return AWFL_ERR_CUDA; }
@@ -494,6 +500,7 @@ int awfl_destroy(awfl_ctx *c) {
     if (c->d_tape) cudaFree(c->d_tape);
     if (c->d_adj) cudaFree(c->d_adj);
     if (c->d_diag) cudaFree(c->d_diag);
+    if (c->d_out) cudaFree(c->d_out);
   }
   delete c;
   return AWFL_OK;
@@ -568,6 +575,48 @@ int awfl_state_sums(awfl_ctx *c, const void *d_state, double *sums, void *stream
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(c, e, "awfl_state_sums");
   return AWFL_OK;
+}
+
+int awfl_output_fields(awfl_ctx *c, const void *d_state, double *d_fields, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_output_fields: state pointer is NULL or misaligned");
+  if (bad_ptr(d_fields)) return fail(c, AWFL_ERR_ARG, "awfl_output_fields: fields pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaError_t e = launch_output_fields(d_state, fp32(c), state_plane(c), c->d_dens_c, c->d_denstheta_c, c->d_pres_c,
+                                       c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs, c->nsm, d_fields,
+                                       (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_output_fields");
+  return AWFL_OK;
+}
+
+int awfl_write_netcdf_fields(awfl_ctx *c, const char *path, const double *h_fields, double etime) {
+  if (!c) return AWFL_ERR_ARG;
+  if (!path || !h_fields) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf_fields: path or fields is NULL");
+  std::string err;
+  if (nc::write(path, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->dx, c->dy, c->dz, c->hs, c->dens_c.data(),
+                c->pres_c.data(), c->theta_c.data(), h_fields, etime, &err) != 0)
+    return fail(c, AWFL_ERR_IO, "awfl_write_netcdf: %s", err.c_str());
+  return AWFL_OK;
+}
+
+int awfl_write_netcdf(awfl_ctx *c, const char *path, const void *d_state, double etime, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (!path) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: path is NULL");
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: state pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const size_t n = (size_t)6 * c->cfg.nx * c->cfg.ny * c->cfg.nz;
+  rc = ensure_buffer(c, &c->d_out, &c->out_bytes, n * sizeof(double), "output fields");
+  if (rc) return rc;
+  rc = awfl_output_fields(c, d_state, c->d_out, stream);
+  if (rc) return rc;
+  std::vector<double> h(n);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(h.data(), c->d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_write_netcdf");
+  return awfl_write_netcdf_fields(c, path, h.data(), etime);
 }
 
 int awfl_check_state(awfl_ctx *c, const void *d_state, long *bad_cells, void *stream) {

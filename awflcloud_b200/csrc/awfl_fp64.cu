@@ -341,6 +341,43 @@ cudaError_t launch_check_state(const void *state, int fp32, long plane, const do
   return cudaGetLastError();
 }
 
+// Output diagnostics of Spatial::output (Spatial:1744-1778), FP64 from either state form:
+// out[f][k][j][i], f = dens_pert, u, v, w, pot_temp_pert, pressure_pert. Same operations
+// and order as the reference (IEEE division, no contraction in this translation unit,
+// the correctly rounded pow for C0*(r*t)^gamma).
+__global__ void output_fields_kernel(const void *state, int fp32, long plane, const double *dens_c,
+                                     const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
+                                     double *out) {
+  const long n = (long)nz * ny * nx;
+  const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long)nx * ny));
+    const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
+    const double rp = state_at(state, fp32, plane, g);
+    const double r = rp + dens_c[hs + k];
+    out[c] = rp;
+    out[n + c] = state_at(state, fp32, plane, g + 1 * sv) / r;
+    out[2 * n + c] = state_at(state, fp32, plane, g + 2 * sv) / r;
+    out[3 * n + c] = state_at(state, fp32, plane, g + 3 * sv) / r;
+    const double t = (state_at(state, fp32, plane, g + 4 * sv) + denstheta_c[hs + k]) / r;
+    out[4 * n + c] = t - denstheta_c[hs + k] / dens_c[hs + k];
+    const double p = C0 * pow_cr(r * t, GAMMA);
+    out[5 * n + c] = p - pres_c[hs + k];
+  }
+}
+
+cudaError_t launch_output_fields(const void *state, int fp32, long plane, const double *dens_c,
+                                 const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
+                                 int nsm, double *out, cudaStream_t st) {
+  const long n = (long)nz * ny * nx;
+  long blocks = (n + 255) / 256;
+  if (blocks > (long)nsm * 8) blocks = (long)nsm * 8;
+  if (blocks < 1) blocks = 1;
+  output_fields_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, denstheta_c, pres_c, nx, ny, nz,
+                                                         hs, out);
+  return cudaGetLastError();
+}
+
 // Device math self-test: out[i] = pow(x[i], y) by the library's pow_cr (mode 0) or by
 // the CUDA math library (mode 1); exp_cr(x[i]) (mode 2).
 __global__ void selftest_pow_kernel(const double *x, double y, double *out, long n, int mode) {

@@ -115,6 +115,9 @@ cudaError_t launch_state_sums(const void *state, int fp32, long plane, int nx, i
 cudaError_t launch_check_state(const void *state, int fp32, long plane, const double *dens_c, int nx, int ny,
                                int nz, int hs, int nsm, unsigned long long *count, cudaStream_t st);
 cudaError_t run_fma_peak(int fp32, int nsm, double *tflops);
+cudaError_t launch_output_fields(const void *state, int fp32, long plane, const double *dens_c,
+                                 const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
+                                 int nsm, double *out, cudaStream_t st);
 cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st);
 
 }  // namespace awfl

@@ -9,9 +9,11 @@
 // call is a C-ABI call on the legacy default stream.
 //
 // Differences from the reference, each deliberate:
-//  * output(): netCDF output (Spatial:1705-1791) is not part of this build. If outFile ends
-//    in ".bin", the state (5 variables, halos included, FP64) is written there raw at every
-//    output time, overwriting the previous one; otherwise output() does nothing.
+//  * output(): an outFile ending in ".nc" gets the reference's netCDF file (Spatial:1705-1791)
+//    from awfl_write_netcdf, the library's own writer of the netCDF classic data model
+//    (64-bit offset format; no netCDF library). An outFile ending in ".bin" gets the state
+//    (5 variables, halos included, FP64) raw at every output time, overwriting the previous
+//    one; any other name: output() does nothing.
 //  * Tracers (compiled out in the reference by NO_TRACERS, Spatial:10): the arrays exist,
 //    initTracers() zero-fills them and their tendencies are zero, so they stay constant (the
 //    reference adds an uninitialised tendency array to them, Temporal_ader.h:67-69).
@@ -347,7 +349,10 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
 
   void output(StateArr const &state, TracerArr const &tracers, real etime) {
     (void)tracers;
-    (void)etime;
+    if (outFile.size() >= 3 && outFile.compare(outFile.size() - 3, 3, ".nc") == 0) {
+      awfl_dropin::check(awfl_write_netcdf(ctx, outFile.c_str(), state.data(), etime, nullptr), ctx, "output");
+      return;
+    }
     if (outFile.size() < 4 || outFile.compare(outFile.size() - 4, 4, ".bin") != 0) return;
     std::vector<double> h = state.createHostCopy();
     const size_t n = (size_t)numState * (nz + 2 * hs) * (ny + 2 * hs) * (nx + 2 * hs);

@@ -37,7 +37,8 @@ typedef enum {
   AWFL_ERR_NOMEM = -3,     /* device allocation failed */
   AWFL_ERR_STATE = -4,     /* device-side check failed (NaN / non-positive density) */
   AWFL_ERR_TIMEOUT = -5,   /* a bounded device wait gave up */
-  AWFL_ERR_NOT_BUILT = -6  /* the requested variant is not compiled into this library */
+  AWFL_ERR_NOT_BUILT = -6, /* the requested variant is not compiled into this library */
+  AWFL_ERR_IO = -7         /* an output file could not be written, or is not this grid's */
 } awfl_status;
 
 enum { AWFL_BC_PERIODIC = 0, AWFL_BC_WALL = 1 };           /* Spatial:80-81 */
@@ -111,6 +112,24 @@ int awfl_state_sums(awfl_ctx *ctx, const void *d_state, double *sums, void *stre
  * AWFL_ERR_TIMEOUT if a sweep of this context ever gave up its bounded wait for staged
  * stencil rows (the state is then not to be trusted). Synchronises the stream. */
 int awfl_check_state(awfl_ctx *ctx, const void *d_state, long *bad_cells, void *stream);
+
+/* The diagnostics of Spatial::output (Spatial:1744-1778) on the device, FP64, from either
+ * state form: d_fields = [6][nz][ny][nx] doubles, in the order dens_pert, u, v, w,
+ * pot_temp_pert, pressure_pert (rho', rho*u/rho, ..., theta - theta_h, C0*(rho*theta)^gamma
+ * - p_h), with the reference's operations. Asynchronous on the stream. */
+int awfl_output_fields(awfl_ctx *ctx, const void *d_state, double *d_fields, void *stream);
+
+/* Spatial::output (Spatial:1705-1791) without the netCDF library: writes the reference's
+ * output file with a project-written writer of the netCDF classic data model (64-bit
+ * offset format, readable by any netCDF reader). etime == 0 creates the file (coordinates
+ * x, y, z; hyDens, hyPressure, hyTheta; record 0 of t and the six fields); any other etime
+ * appends a record to a file this grid created. Synchronises the stream; allocates (once
+ * per context) a device buffer for the fields. AWFL_ERR_IO on a file error. */
+int awfl_write_netcdf(awfl_ctx *ctx, const char *path, const void *d_state, double etime, void *stream);
+
+/* The same file from host-side fields ([6][nz][ny][nx] doubles, as awfl_output_fields
+ * gives them); needs no device (host-only contexts too). */
+int awfl_write_netcdf_fields(awfl_ctx *ctx, const char *path, const double *h_fields, double etime);
 
 /* Spatial::computeTimeStep without the caching (Spatial:159-187): the acoustic CFL time
  * step, min over all cells, returned in *h_dt (synchronises the stream). */

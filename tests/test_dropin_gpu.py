@@ -20,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "awflcloud_b200", "dropin", "bin", "driver_o5")
 
 
-def _yaml(path, out, sim_time, extra=""):
+def _yaml(path, out, sim_time, extra="", out_freq=None):
     with open(path, "w") as f:
         f.write("""---
 simTime  : %r
@@ -39,7 +39,7 @@ initData : thermal
 outFile  : %s
 outFreq  : %r
 perturb: false
-%s""" % (sim_time, out, sim_time, extra))
+%s""" % (sim_time, out, sim_time if out_freq is None else out_freq, extra))
 
 
 def _oracle_run(sim_time):
@@ -102,3 +102,37 @@ def test_reference_driver_fp32(tmp_path):
             assert np.abs(a).max() < 1e-6
         else:
             assert _rel(a, b) <= 1e-5, (v, _rel(a, b))
+
+
+def test_reference_driver_netcdf_output(tmp_path):
+    """outFile *.nc: the driver's output calls (driver.cpp:41, 55-59) write the reference's
+    netCDF file (Spatial:1705-1791) -- records at etime 0, at the first step past outFreq
+    and at the end -- whose last record holds the diagnostics of the oracle's final state."""
+    from scipy.io import netcdf_file
+    from awflcloud_b200 import capi
+    O = Oracle(32, 24, 16, bc=(0, 1, 1), crpow=True)
+    st = O.new_state()
+    O.init_state(st)
+    dt0 = O.compute_dt(st, 0.8)
+    sim_time = 3.5 * dt0
+    inp, out = str(tmp_path / "in.yaml"), str(tmp_path / "out.nc")
+    _yaml(inp, out, sim_time, out_freq=sim_time / 2)
+    p = subprocess.run([BIN, inp], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    ref, _, _ = _oracle_run(sim_time)
+    c = capi.Context(32, 24, 16, bc=("periodic", "wall", "wall"), device=-1)
+    bg = c.background()
+    h = c.hs
+    s = ref[:, h:-h, h:-h, h:-h]
+    d = bg["hyDensCells"][h:-h, None, None]
+    dt = bg["hyDensThetaCells"][h:-h, None, None]
+    r = s[0] + d
+    t = (s[4] + dt) / r
+    want = [s[0], s[1] / r, s[2] / r, s[3] / r, t - dt / d]
+    with netcdf_file(out, "r", mmap=False) as nc:
+        tt = nc.variables["t"][:].copy()
+        assert len(tt) == 3 and tt[0] == 0.0
+        assert abs(tt[1] - 2 * dt0) <= 1e-12 * dt0 and abs(tt[2] - sim_time) <= 1e-12 * sim_time
+        for i, name in enumerate(["dens_pert", "u", "v", "w", "pot_temp_pert"]):
+            got = nc.variables[name][2]
+            assert _rel(got, want[i]) <= 5e-12, name

@@ -1,0 +1,74 @@
+"""Output file of Spatial::output (Spatial:1705-1791) from the library's own netCDF writer
+(classic data model, 64-bit offset format), checked with an independent reader
+(scipy.io.netcdf_file) on a host-only context: dimensions, the fixed variables (coordinates
+and the background profiles, Spatial:1716-1734), records appended one per output time
+(Spatial:1738-1741), and the refusal to append to another grid's file."""
+import numpy as np
+import pytest
+
+from awflcloud_b200 import capi
+
+netcdf = pytest.importorskip("scipy.io").netcdf_file
+
+
+def _ctx(nx=12, ny=10, nz=8):
+    return capi.Context(nx, ny, nz, 20000.0, 16000.0, 10000.0, device=-1)
+
+
+def _fields(c, seed):
+    return np.random.default_rng(seed).standard_normal((6, c.nz, c.ny, c.nx))
+
+
+def test_file_layout_and_records(tmp_path):
+    c = _ctx()
+    path = str(tmp_path / "out.nc")
+    f0, f1, f2 = _fields(c, 1), _fields(c, 2), _fields(c, 3)
+    c.write_netcdf_fields(path, f0, 0.0)
+    c.write_netcdf_fields(path, f1, 2.5)
+    c.write_netcdf_fields(path, f2, 7.25)
+    bg = c.background()
+    h = c.hs
+    with netcdf(path, "r", mmap=False) as nc:
+        assert nc.version_byte == 2
+        assert nc.dimensions == {"x": 12, "y": 10, "z": 8, "t": None}
+        assert list(nc.variables) == ["x", "y", "z", "hyDens", "hyPressure", "hyTheta", "t", "dens_pert", "u",
+                                      "v", "w", "pot_temp_pert", "pressure_pert"]
+        np.testing.assert_array_equal(nc.variables["x"][:], (np.arange(12) + 0.5) * (20000.0 / 12))
+        np.testing.assert_array_equal(nc.variables["y"][:], (np.arange(10) + 0.5) * (16000.0 / 10))
+        np.testing.assert_array_equal(nc.variables["z"][:], (np.arange(8) + 0.5) * (10000.0 / 8))
+        np.testing.assert_array_equal(nc.variables["hyDens"][:], bg["hyDensCells"][h:h + 8])
+        np.testing.assert_array_equal(nc.variables["hyPressure"][:], bg["hyPressureCells"][h:h + 8])
+        np.testing.assert_array_equal(nc.variables["hyTheta"][:], bg["hyThetaCells"][h:h + 8])
+        np.testing.assert_array_equal(nc.variables["t"][:], [0.0, 2.5, 7.25])
+        for i, name in enumerate(["dens_pert", "u", "v", "w", "pot_temp_pert", "pressure_pert"]):
+            v = nc.variables[name]
+            assert v.dimensions == ("t", "z", "y", "x")
+            for r, f in enumerate((f0, f1, f2)):
+                np.testing.assert_array_equal(v[r], f[i])
+
+
+def test_etime_zero_starts_a_new_file(tmp_path):
+    c = _ctx()
+    path = str(tmp_path / "out.nc")
+    c.write_netcdf_fields(path, _fields(c, 1), 0.0)
+    c.write_netcdf_fields(path, _fields(c, 2), 1.0)
+    f = _fields(c, 3)
+    c.write_netcdf_fields(path, f, 0.0)
+    with netcdf(path, "r", mmap=False) as nc:
+        np.testing.assert_array_equal(nc.variables["t"][:], [0.0])
+        np.testing.assert_array_equal(nc.variables["u"][0], f[1])
+
+
+def test_append_refuses_missing_or_foreign_files(tmp_path):
+    c = _ctx()
+    with pytest.raises(capi.AwflError) as e:
+        c.write_netcdf_fields(str(tmp_path / "absent.nc"), _fields(c, 1), 1.0)
+    assert e.value.code == -7
+    other = _ctx(14, 10, 8)
+    path = str(tmp_path / "other.nc")
+    other.write_netcdf_fields(path, _fields(other, 1), 0.0)
+    with pytest.raises(capi.AwflError) as e:
+        c.write_netcdf_fields(path, _fields(c, 2), 1.0)
+    assert e.value.code == -7
+    with pytest.raises(ValueError):
+        c.write_netcdf_fields(path, np.zeros(5), 1.0)
