@@ -308,6 +308,42 @@ def rel_l2_after(a, steps, local):
     return out
 
 
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), GB/s."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (copy, read+write)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def output_leg(ctx, st, reps=20):
+    """The output diagnostics kernel (Spatial::output's six fields, one launch) on the timed
+    state: HBM-bound, so reported as algorithmic GB/s against the measured copy bandwidth.
+    Algorithmic bytes per cell: the state read (5 FP64 values, or 5 FP32 values + 5 FP32
+    compensations: 40 B) + 6 FP64 fields written (48 B)."""
+    import torch
+    cells = ctx.nx * ctx.ny * ctx.nz
+    out = torch.empty((6, ctx.nz, ctx.ny, ctx.nx), dtype=torch.float64, device=st.device)
+    for _ in range(3):
+        ctx.output_fields(st, out)
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        ctx.output_fields(st, out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nbytes = cells * (40 + 48)
+    peak, src = hbm_peak()
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"kernel": "output_fields_kernel", "ms_per_launch": round(ms, 4), "bytes_algorithmic": nbytes,
+            "achieved_gbs": round(gbs, 1), "peak_gbs": peak, "frac": round(gbs / peak, 4), "peak_source": src,
+            "l2": "357 MB state + 403 MB fields > 126 MB L2"}
+
+
 def ord9_leg(a, local):
     """The same grid and bubble at WENO ord 9 / ngll 5 (CFL 0.4): FP32 form and FP64 path
     throughput (K steps after W warm-up steps each) and their relative L2 after 100 steps."""
@@ -519,6 +555,7 @@ def run_ours(a):
                                                       "rho_w": errs[3], "rho_theta": errs[4]}
         if e2e is not None:
             line["e2e"] = e2e
+        line["output"] = output_leg(main["ctx"], main["state"])
         if not a.no_adjoint:
             line["adjoint"] = adjoint_leg(a, local)
         if not a.no_ensemble:
