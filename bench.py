@@ -282,7 +282,7 @@ def time_form(a, prec, local, world, clocks=None):
 
 # DRAM bytes per sweep launch (read + write, mean over x/y/z), from ncu on the 256x256x128
 # workload (profiles/sweep_kernel_256x256x128.md).
-TRAFFIC = {(0, 5): 652_100_000, (1, 5): 634_800_000}
+TRAFFIC = {(0, 5): 650_500_000, (1, 5): 635_700_000}
 
 
 def rel_l2_after(a, steps, local):
