@@ -74,6 +74,25 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x, world):
+    """The largest of every rank's value (the slowest replica's time): an all-reduce on the
+    process group's device (CUDA tensor for NCCL, host tensor for gloo); x itself at N = 1."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def job_throughput(world, cells, steps, max_ms):
+    """Whole-job Mcell-steps/s of N replicas of one grid (weak scaling): every rank advances
+    its own grid `steps` times; the job takes the slowest rank's time."""
+    return world * cells * steps / (max_ms * 1e-3) / 1e6
+
+
 def cfl_for(ord_):
     # The driver's CFL 0.8 (driver.cpp:46). At ord 9 the reference's own scheme diverges
     # at 0.8 (NaN within 8 steps, reproduced with its code), so ord 9 runs at 0.4.
@@ -197,8 +216,8 @@ def run_reference(a):
     R.set_bubble(1, 10000.0, 10000.0, 2000.0, 2000.0, 2000.0, 2000.0, 3.0, 1.0)
     R.add_theta_noise(20261203, 0.01)
     dt = R.compute_dt(cfl_for(a.ord))
-    # bound the run: each step is one full time step of the workload unless that would
-    # take more than ~3 minutes in total, then each step is a fraction of the grid's lines
+    # each step is one full time step of the workload (about 1 s on 16 host threads at
+    # 256x256x128), so the default --steps 20 --warmup 3 ends in well under a minute
     t0 = time.perf_counter()
     R.time_step(dt)
     one = time.perf_counter() - t0
@@ -260,10 +279,7 @@ def time_form(a, prec, local, world, clocks=None):
     clk = clocks.stop() if clocks is not None else None
     total_ms = ev[0].elapsed_time(ev[-1])
     launch_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(3 * a.steps)]
-    t = torch.tensor([total_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = t.item()
+    max_ms = max_over_ranks(total_ms, world)
     fl = flops.flops_per_cell_step(a.ord)
     flops_launch = fl["flops"] / 3.0 * cells  # per split launch, averaged over directions
     avg_launch_s = statistics.mean(launch_ms) * 1e-3
@@ -275,7 +291,7 @@ def time_form(a, prec, local, world, clocks=None):
                 "peak_source": "measured in this run: awfl_measure_fma_peak (FMA chains, 2 flops/FMA)",
                 "flops_per_launch": flops_launch, "launch_ms_avg": round(avg_launch_s * 1e3, 4),
                 "bytes_algorithmic_per_launch": cells * 10 * esz * (1 if prec == capi.FP64 else 2)}
-    return {"ctx": ctx, "state": st, "dt": dt, "value": world * cells * a.steps / (max_ms * 1e-3) / 1e6,
+    return {"ctx": ctx, "state": st, "dt": dt, "value": job_throughput(world, cells, a.steps, max_ms),
             "ms_per_step": max_ms / a.steps, "roofline": roofline, "clocks": clk, "flops": fl,
             "finite": bool(torch.isfinite(st).all().item())}
 
@@ -616,12 +632,9 @@ def e2e_leg(a, ctx, st, dt, stream, world):
         stream.wait_stream(s_)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = max_over_ranks(e0.elapsed_time(e1), world)
     cells = a.nx * a.ny * a.nz
-    return {"value": round(world * cells * a.steps / (t.item() * 1e-3) / 1e6, 3), "unit": UNIT,
+    return {"value": round(job_throughput(world, cells, a.steps, max_ms), 3), "unit": UNIT,
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
             "path": "per step: awfl_copy_h2d + awfl_step + awfl_copy_d2h from/to pinned host buffers, "
                     "three device buffers on three streams (copies overlap compute and each other)"}
