@@ -68,11 +68,13 @@ template <int ORD> struct Tables32 {
   static constexpr int HS = (ORD - 1) / 2;
   static constexpr int NG = OrdTraits<ORD>::NGLL;
   float recon[ORD * ORD * ORD];
+  // the high-order candidate's coefficients straight from the stencil: (its full-stencil
+  // map minus the idl-weighted low-order candidates' maps) / idl[hs+1], formed in FP64
+  float hi[ORD * ORD];
   float c2g[ORD * NG];
   float s2g[ORD * NG];
   float deriv[NG * NG];
   float idl[HS + 2];
-  float inv_idl_last;  // 1 / idl[hs+1]
   float sigma;
   float wts[NG];
 };
@@ -148,12 +150,8 @@ __device__ __forceinline__ void weno_coefs32(const T (&u)[ORD], T (&aw)[ORD]) {
   for (int ii = 0; ii < ORD; ii++) {
     T acc = T(0.f);
 #pragma unroll
-    for (int s = 0; s < ORD; s++) acc = fmaT(Tb.recon[((HS + 1) * ORD + s) * ORD + ii], u[s], acc);
-    if (ii < HS + 1) {
-#pragma unroll
-      for (int i = 0; i < HS + 1; i++) acc = fmaT(-Tb.idl[i], a[i][ii], acc);
-    }
-    a[HS + 1][ii] = acc * Tb.inv_idl_last;
+    for (int s = 0; s < ORD; s++) acc = fmaT(Tb.hi[s * ORD + ii], u[s], acc);
+    a[HS + 1][ii] = acc;
   }
   T tv[HS + 2];
 #pragma unroll
@@ -535,10 +533,17 @@ static inline cudaError_t upload_tables32_here(int ord, const double *recon, con
   auto fill = [&](auto &t, int o, int g) {
     const int hs = (o - 1) / 2;
     for (int i = 0; i < o * o * o; i++) t.recon[i] = (float)recon[i];
+    for (int sidx = 0; sidx < o; sidx++)
+      for (int ii = 0; ii < o; ii++) {
+        double m = recon[((hs + 1) * o + sidx) * o + ii];
+        if (ii <= hs)
+          for (int i = 0; i <= hs; i++)
+            if (sidx - i >= 0 && sidx - i <= hs) m -= idl[i] * recon[(i * o + (sidx - i)) * o + ii];
+        t.hi[sidx * o + ii] = (float)(m / idl[hs + 1]);
+      }
     for (int i = 0; i < o * g; i++) { t.c2g[i] = (float)c2g[i]; t.s2g[i] = (float)s2g[i]; }
     for (int i = 0; i < g * g; i++) t.deriv[i] = (float)deriv[i];
     for (int i = 0; i < hs + 2; i++) t.idl[i] = (float)idl[i];
-    t.inv_idl_last = (float)(1.0 / idl[hs + 1]);
     t.sigma = (float)sigma;
     for (int i = 0; i < g; i++) t.wts[i] = (float)wts[i];
   };
