@@ -28,6 +28,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "awfl_internal.h"
 #include "awfl_fp32_args.h"
 #include "awfl_pow.cuh"
@@ -136,6 +138,9 @@ __device__ __forceinline__ void weno_coefs32(const T (&u)[ORD], T (&aw)[ORD]) {
   constexpr int HS = (ORD - 1) / 2;
   const Tables32<ORD> &Tb = tab32<ORD>();
   const float eps = 1.0e-20f;
+  // Structural zeros (symmetric stencils; checked when the tables are uploaded) are left
+  // out: the centred low-order candidate's odd coefficients and the high-order map's odd
+  // coefficients take nothing from the stencil's centre value.
   T a[HS + 2][ORD];
 #pragma unroll
   for (int i = 0; i < HS + 1; i++)
@@ -143,14 +148,20 @@ __device__ __forceinline__ void weno_coefs32(const T (&u)[ORD], T (&aw)[ORD]) {
     for (int ii = 0; ii < HS + 1; ii++) {
       T acc = T(0.f);
 #pragma unroll
-      for (int s = 0; s < HS + 1; s++) acc = fmaT(Tb.recon[(i * ORD + s) * ORD + ii], u[i + s], acc);
+      for (int s = 0; s < HS + 1; s++) {
+        if (HS % 2 == 0 && i == HS / 2 && s == HS / 2 && ii % 2 == 1) continue;
+        acc = fmaT(Tb.recon[(i * ORD + s) * ORD + ii], u[i + s], acc);
+      }
       a[i][ii] = acc;
     }
 #pragma unroll
   for (int ii = 0; ii < ORD; ii++) {
     T acc = T(0.f);
 #pragma unroll
-    for (int s = 0; s < ORD; s++) acc = fmaT(Tb.hi[s * ORD + ii], u[s], acc);
+    for (int s = 0; s < ORD; s++) {
+      if (s == HS && ii % 2 == 1) continue;
+      acc = fmaT(Tb.hi[s * ORD + ii], u[s], acc);
+    }
     a[HS + 1][ii] = acc;
   }
   T tv[HS + 2];
@@ -200,12 +211,21 @@ __device__ __forceinline__ void reconstruct_gll32(const T (&sten)[ORD], T (&out)
   if (doweno) {
     T wc[ORD];
     weno_coefs32<ORD>(sten, wc);
+    // polynomial coefficients -> values at the GLL points, which sit symmetrically about
+    // the cell centre (x = 0): the centre takes the constant coefficient alone, the mirror
+    // points x and -x the even part plus and minus the odd part
+    static_assert(NG % 2 == 1, "an odd number of GLL points, one at the centre");
+    out[NG / 2] = wc[0];
 #pragma unroll
-    for (int ii = 0; ii < NG; ii++) {
-      T tmp = T(0.f);
+    for (int ii = 0; ii < NG / 2; ii++) {
+      const int jr = NG - 1 - ii;
+      T ev = T(0.f), od = T(0.f);
 #pragma unroll
-      for (int s = 0; s < ORD; s++) tmp = fmaT(Tb.c2g[s * NG + ii], wc[s], tmp);
-      out[ii] = tmp;
+      for (int s = 0; s < ORD; s += 2) ev = fmaT(Tb.c2g[s * NG + jr], wc[s], ev);
+#pragma unroll
+      for (int s = 1; s < ORD; s += 2) od = fmaT(Tb.c2g[s * NG + jr], wc[s], od);
+      out[jr] = ev + od;
+      out[ii] = ev - od;
     }
   } else {
 #pragma unroll
@@ -293,6 +313,7 @@ __device__ __forceinline__ void cell_recon32(const Sten &sten, int kb, const Swe
       float dq[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int s = 0; s < NG; s++) {
+        if (ii == NG / 2 && s == NG / 2) continue;  // d/dx at the centre: no centre weight
         const float D = T.deriv[s * NG + ii];
         dq[idR] = fmaf(D, q[NM][kt][s], dq[idR]);
 #pragma unroll
@@ -547,13 +568,35 @@ static inline cudaError_t upload_tables32_here(int ord, const double *recon, con
     t.sigma = (float)sigma;
     for (int i = 0; i < g; i++) t.wts[i] = (float)wts[i];
   };
+  // the structural zeros and symmetries the FP32 reconstruction leaves out of its sums
+  auto structure_ok = [&](const auto &t, int o, int g) {
+    const int hs = (o - 1) / 2;
+    double dmax = 0, rmax = 0;
+    for (int x = 0; x < g * g; x++) dmax = fmax(dmax, fabs((double)t.deriv[x]));
+    for (int x = 0; x < o * o * o; x++) rmax = fmax(rmax, fabs((double)t.recon[x]));
+    bool ok = g % 2 == 1 && hs % 2 == 0 && t.c2g[0 * g + g / 2] == 1.f &&
+              fabs((double)t.deriv[(g / 2) * g + g / 2]) <= 1e-6 * dmax;
+    for (int sidx = 1; sidx < o; sidx++) ok = ok && t.c2g[sidx * g + g / 2] == 0.f;
+    for (int sidx = 0; sidx < o; sidx++)
+      for (int ii = 0; ii < g; ii++)
+        ok = ok && t.c2g[sidx * g + ii] == ((sidx % 2) ? -1.f : 1.f) * t.c2g[sidx * g + (g - 1 - ii)];
+    double hmax = 0;
+    for (int x = 0; x < o * o; x++) hmax = fmax(hmax, fabs((double)t.hi[x]));
+    for (int ii = 1; ii < o; ii += 2) {
+      ok = ok && fabs((double)t.hi[hs * o + ii]) <= 1e-6 * hmax;
+      if (ii <= hs) ok = ok && fabs((double)t.recon[((hs / 2) * o + hs / 2) * o + ii]) <= 1e-6 * rmax;
+    }
+    return ok;
+  };
   if (ord == 5) {
     Tables32<5> t;
     fill(t, 5, 3);
+    if (!structure_ok(t, 5, 3)) return cudaErrorInvalidValue;
     return cudaMemcpyToSymbol(c32_tab5, &t, sizeof t);
   }
   Tables32<9> t;
   fill(t, 9, 5);
+  if (!structure_ok(t, 9, 5)) return cudaErrorInvalidValue;
   return cudaMemcpyToSymbol(c32_tab9, &t, sizeof t);
 }
 
