@@ -8,12 +8,15 @@
 // (needed again by the periodic wrap at the end of the line) are saved before they are
 // overwritten.
 //
-// Per chunk: (A) store the prefetched ring rows; (B) reconstruct cells base..base+C-1
-// -> left/right edge states; (C) Riemann flux at their left faces (the left state of
-// the first face is carried from the previous chunk); (D) divergence and update of
-// cells base-1..base+C-2 (the last cell's right face is computed in the next chunk).
-// The next chunk's rows are loaded into registers at the start of each chunk. The last cell of the line
-// is finished after the loop.
+// Per chunk: (A) the chunk's ring rows are in place (landed by TMA or cp.async, or stored
+// from registers); the next chunk's rows are requested; reconstruct cells base..base+C-1
+// -> left/right edge states; Riemann flux at their left faces (the left state of the
+// first face is carried from the previous chunk); divergence and update of cells
+// base-1..base+C-2 (the last cell's right face is computed in the next chunk). Where a
+// line's C cells are consecutive lanes of one warp (SHFL) the edge states and fluxes move
+// between neighbouring cells by warp shuffles and (A) is the chunk's only CTA barrier;
+// otherwise they go through shared memory with barriers (B), (C), (D) between the steps.
+// The last cell of the line is finished after the loop.
 //
 // Boundary handling reproduces the reference's halo fill (Spatial_euler3d_cons_expl_
 // cart_fv_Agrid.h:631-662, 994-1025, 1351-1382) and edge-value BCs (:816-837, 1176-1197,
@@ -34,10 +37,11 @@
 //                                          g0 + v*sv), loaded a reconstruction ahead
 //   apply(A, gidx, orig, tnd, aux, v)      state[gidx] = orig "+" dt*tnd (MODE_APPLY)
 //   kAsyncRing                             next-chunk rows by cp.async into a 4C ring
-//   kTmaRing, prepare_tma<ORD,DIR,C,W,RW>(A) (host), tma_map(A), flag_timeout(A)
-//                                          next-chunk rows of interior chunks by tiled TMA
-//                                          copies through a tensor map in the kernel
-//                                          parameter (single-grid sweeps only)
+//   kTmaRing, prepare_tma(A, ord, dir, C, W) (host), tma_map(A), tma_map_global(a, g),
+//   flag_timeout(A)                        next-chunk rows of interior chunks by tiled TMA
+//                                          boxes through a tensor map (kernel parameter
+//                                          for single-grid sweeps, the work list in
+//                                          global memory for ensembles)
 //   min_blocks(ORD)                        CTAs per SM the register budget must allow
 //   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
 //   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
