@@ -60,6 +60,10 @@ _SIGS = {
     "awfl_output_fields": (_I, [_VP, _VP, _VP, _VP]),
     "awfl_write_netcdf": (_I, [_VP, ctypes.c_char_p, _VP, _D, _VP]),
     "awfl_write_netcdf_fields": (_I, [_VP, ctypes.c_char_p, _DP, _D]),
+    "awfl_init_tracers": (_I, [_VP, _VP, _I, _VP]),
+    "awfl_output_tracer_fields": (_I, [_VP, _VP, _VP, _I, _VP, _VP]),
+    "awfl_write_netcdf_tracers": (_I, [_VP, ctypes.c_char_p, _VP, _VP, _I, ctypes.POINTER(ctypes.c_char_p), _D, _VP]),
+    "awfl_write_netcdf_fields_tracers": (_I, [_VP, ctypes.c_char_p, _DP, _I, ctypes.POINTER(ctypes.c_char_p), _D]),
     "awfl_compute_tendencies": (_I, [_VP, _VP, _VP, _D, _I, _VP]),
     "awfl_apply_tendencies": (_I, [_VP, _VP, _VP, _D, _VP]),
     "awfl_split": (_I, [_VP, _VP, _D, _I, _VP]),
@@ -281,6 +285,57 @@ class Context:
         if a.size != 6 * self.nz * self.ny * self.nx:
             raise ValueError("fields must have 6*nz*ny*nx = %d elements" % (6 * self.nz * self.ny * self.nx))
         self._check(self.L.awfl_write_netcdf_fields(self.h, os.fsencode(path), a.ctypes.data_as(_DP), float(etime)))
+
+    # ---- tracers (FP64 arrays of shape (ntracers, nz+2hs, ny+2hs, nx+2hs) for every precision)
+    def tracer_shape(self, ntracers):
+        h = 2 * self.hs
+        return (ntracers, self.nz + h, self.ny + h, self.nx + h)
+
+    def new_tracers(self, ntracers):
+        import torch
+        return torch.zeros(self.tracer_shape(ntracers), dtype=torch.float64, device="cuda:%d" % max(self.device, 0))
+
+    def _tr(self, x, ntracers):
+        import math
+        import torch
+        if isinstance(x, int) or x is None:
+            return _ptr(x)
+        need = math.prod(self.tracer_shape(ntracers))
+        if x.numel() < need or not x.is_contiguous() or x.dtype != torch.float64 or not x.is_cuda:
+            raise ValueError("tracers must be a contiguous CUDA float64 tensor with >= %d elements" % need)
+        return _ptr(x)
+
+    def init_tracers(self, tracers, ntracers=None, stream=None):
+        """Spatial::initTracers: the driver's tracers (uniform, theta, block; any further zero)."""
+        n = tracers.shape[0] if ntracers is None else ntracers
+        self._check(self.L.awfl_init_tracers(self.h, self._tr(tracers, n), n, _stream(stream)))
+
+    def output_tracer_fields(self, state, tracers, ntracers=None, stream=None):
+        """tracer / (rho' + rho_h) per tracer, as a (ntracers, nz, ny, nx) FP64 CUDA tensor."""
+        import torch
+        n = tracers.shape[0] if ntracers is None else ntracers
+        out = torch.empty((n, self.nz, self.ny, self.nx), dtype=torch.float64, device="cuda:%d" % max(self.device, 0))
+        self._check(self.L.awfl_output_tracer_fields(self.h, self._st(state), self._tr(tracers, n), n, _ptr(out),
+                                                     _stream(stream)))
+        return out
+
+    def write_netcdf_tracers(self, path, state, tracers, names, etime, stream=None):
+        """write_netcdf with the tracer_<name> record variables."""
+        arr = (ctypes.c_char_p * max(len(names), 1))(*[n.encode() for n in names])
+        self._check(self.L.awfl_write_netcdf_tracers(self.h, os.fsencode(path), self._st(state),
+                                                     self._tr(tracers, len(names)) if names else None, len(names),
+                                                     arr, float(etime), _stream(stream)))
+
+    def write_netcdf_fields_tracers(self, path, fields, names, etime):
+        """The same file from host fields of shape (6 + len(names), nz, ny, nx)."""
+        import numpy as np
+        a = np.ascontiguousarray(fields, dtype=np.float64)
+        need = (6 + len(names)) * self.nz * self.ny * self.nx
+        if a.size != need:
+            raise ValueError("fields must have (6+ntracers)*nz*ny*nx = %d elements" % need)
+        arr = (ctypes.c_char_p * max(len(names), 1))(*[n.encode() for n in names])
+        self._check(self.L.awfl_write_netcdf_fields_tracers(self.h, os.fsencode(path), a.ctypes.data_as(_DP),
+                                                            len(names), arr, float(etime)))
 
     def check_state(self, state, stream=None):
         """Number of interior cells with a non-finite value or a non-positive density (0 when

@@ -590,33 +590,89 @@ int awfl_output_fields(awfl_ctx *c, const void *d_state, double *d_fields, void 
   return AWFL_OK;
 }
 
-int awfl_write_netcdf_fields(awfl_ctx *c, const char *path, const double *h_fields, double etime) {
+int awfl_output_tracer_fields(awfl_ctx *c, const void *d_state, const double *d_tracers, int ntracers,
+                              double *d_fields, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (ntracers < 0) return fail(c, AWFL_ERR_ARG, "awfl_output_tracer_fields: ntracers < 0");
+  if (ntracers == 0) return AWFL_OK;
+  if (bad_ptr(d_state) || bad_ptr(d_tracers) || bad_ptr(d_fields))
+    return fail(c, AWFL_ERR_ARG, "awfl_output_tracer_fields: a pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaError_t e = launch_tracer_fields(d_state, fp32(c), state_plane(c), c->d_dens_c, d_tracers, ntracers, c->cfg.nx,
+                                       c->cfg.ny, c->cfg.nz, c->hs, c->nsm, d_fields, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "awfl_output_tracer_fields");
+  return AWFL_OK;
+}
+
+int awfl_write_netcdf_fields_tracers(awfl_ctx *c, const char *path, const double *h_fields, int ntracers,
+                                     const char *const *names, double etime) {
   if (!c) return AWFL_ERR_ARG;
   if (!path || !h_fields) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf_fields: path or fields is NULL");
+  if (ntracers < 0 || (ntracers > 0 && !names))
+    return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: ntracers < 0, or tracer names missing");
+  std::vector<std::string> tn;
+  for (int t = 0; t < ntracers; t++) {
+    if (!names[t] || !names[t][0]) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: tracer %d has no name", t);
+    tn.emplace_back(names[t]);
+  }
   std::string err;
   if (nc::write(path, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->dx, c->dy, c->dz, c->hs, c->dens_c.data(),
-                c->pres_c.data(), c->theta_c.data(), h_fields, etime, &err) != 0)
+                c->pres_c.data(), c->theta_c.data(), h_fields, etime, &err, tn) != 0)
     return fail(c, AWFL_ERR_IO, "awfl_write_netcdf: %s", err.c_str());
   return AWFL_OK;
 }
 
-int awfl_write_netcdf(awfl_ctx *c, const char *path, const void *d_state, double etime, void *stream) {
+int awfl_write_netcdf_fields(awfl_ctx *c, const char *path, const double *h_fields, double etime) {
+  return awfl_write_netcdf_fields_tracers(c, path, h_fields, 0, nullptr, etime);
+}
+
+int awfl_write_netcdf_tracers(awfl_ctx *c, const char *path, const void *d_state, const double *d_tracers,
+                              int ntracers, const char *const *names, double etime, void *stream) {
   if (!c) return AWFL_ERR_ARG;
   if (!path) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: path is NULL");
   if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: state pointer is NULL or misaligned");
+  if (ntracers < 0 || (ntracers > 0 && (!names || bad_ptr(d_tracers))))
+    return fail(c, AWFL_ERR_ARG, "awfl_write_netcdf: ntracers < 0, or tracers / names missing");
   int rc = set_device(c);
   if (rc) return rc;
-  const size_t n = (size_t)6 * c->cfg.nx * c->cfg.ny * c->cfg.nz;
+  const size_t cells = (size_t)c->cfg.nx * c->cfg.ny * c->cfg.nz;
+  const size_t n = (6 + (size_t)ntracers) * cells;
   rc = ensure_buffer(c, &c->d_out, &c->out_bytes, n * sizeof(double), "output fields");
   if (rc) return rc;
   rc = awfl_output_fields(c, d_state, c->d_out, stream);
+  if (rc) return rc;
+  rc = awfl_output_tracer_fields(c, d_state, d_tracers, ntracers, c->d_out + 6 * cells, stream);
   if (rc) return rc;
   std::vector<double> h(n);
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMemcpyAsync(h.data(), c->d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(c, e, "awfl_write_netcdf");
-  return awfl_write_netcdf_fields(c, path, h.data(), etime);
+  return awfl_write_netcdf_fields_tracers(c, path, h.data(), ntracers, names, etime);
+}
+
+int awfl_write_netcdf(awfl_ctx *c, const char *path, const void *d_state, double etime, void *stream) {
+  return awfl_write_netcdf_tracers(c, path, d_state, nullptr, 0, nullptr, etime, stream);
+}
+
+int awfl_init_tracers(awfl_ctx *c, double *d_tracers, int ntracers, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (ntracers < 0) return fail(c, AWFL_ERR_ARG, "awfl_init_tracers: ntracers < 0");
+  if (ntracers == 0) return AWFL_OK;
+  if (bad_ptr(d_tracers)) return fail(c, AWFL_ERR_ARG, "awfl_init_tracers: tracer pointer is NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  InitLaunch L;
+  std::memset(&L, 0, sizeof L);
+  L.state = d_tracers;
+  L.nx = c->cfg.nx; L.ny = c->cfg.ny; L.nz = c->cfg.nz; L.hs = c->hs; L.ord = c->cfg.ord;
+  L.dx = c->dx; L.dy = c->dy; L.dz = c->dz; L.xlen = c->cfg.xlen; L.ylen = c->cfg.ylen; L.zlen = c->cfg.zlen;
+  L.sim2d = c->sim2d;
+  for (int m = 0; m < c->cfg.ord; m++) { L.pts[m] = c->pts_ord[m]; L.wts[m] = c->wts_ord[m]; }
+  cudaError_t e = launch_init_tracers_fp64(L, ntracers, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "init_tracers kernel");
+  return AWFL_OK;
 }
 
 int awfl_check_state(awfl_ctx *c, const void *d_state, long *bad_cells, void *stream) {

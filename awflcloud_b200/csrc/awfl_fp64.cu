@@ -10,6 +10,8 @@
 //   init_state_kernel      K9 initial data quadrature (Spatial:428-485)
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "awfl_internal.h"
 #include "awfl_p64.cuh"
 
@@ -260,6 +262,59 @@ cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st) {
 }
 
 // ------------------------------------------------------------------------------------
+// Spatial::initTracers (Spatial:505-560): per cell and tracer, the ord^3 GLL quadrature of
+// rho_h * tval with the reference's three profiles (uniform 1; the 2 K linear ellipsoid of
+// radius 2 km at (xlen/2, ylen/2, 2 km); the block indicator, integer-divided bounds);
+// tracers beyond the third are zero. One thread per cell; tracers (ntr, nz+2hs, ny+2hs,
+// nx+2hs) FP64, interior written.
+// ------------------------------------------------------------------------------------
+__global__ void init_tracers_kernel(InitArgs a, int ntr) {
+  const long n = (long)a.nz * a.ny * a.nx;
+  const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const int i = idx % a.nx, j = (idx / a.nx) % a.ny, k = idx / ((long)a.nx * a.ny);
+  const int hs = a.hs;
+  const long sy = a.nx + 2 * hs, sz = (long)(a.ny + 2 * hs) * sy, sv = (long)(a.nz + 2 * hs) * sz;
+  const long s = (hs + k) * sz + (hs + j) * sy + hs + i;
+  bool inside = k >= 1 * a.nz / 10 && k < 3 * a.nz / 10 && i >= 4 * a.nx / 10 && i < 6 * a.nx / 10;
+  if (!a.sim2d) inside = inside && j >= 4 * a.ny / 10 && j < 6 * a.ny / 10;
+  for (int l = 0; l < ntr; l++) {
+    double acc = 0;
+    if (l < 3) {
+      for (int kk = 0; kk < a.ord; kk++)
+        for (int jj = 0; jj < a.ord; jj++)
+          for (int ii = 0; ii < a.ord; ii++) {
+            const double zloc = (k + 0.5) * a.dz + a.pts[kk] * a.dz;
+            const double yloc = a.sim2d ? a.ylen / 2 : (j + 0.5) * a.dy + a.pts[jj] * a.dy;
+            const double xloc = (i + 0.5) * a.dx + a.pts[ii] * a.dx;
+            const double wt = a.wts[kk] * a.wts[jj] * a.wts[ii];
+            const double rh = d_const_theta_density(300, zloc);
+            double tval;
+            if (l == 0) tval = 1;
+            else if (l == 1) tval = d_ellipsoid_linear(xloc, yloc, zloc, a.xlen / 2, a.ylen / 2, 2000, 2000, 2000, 2000, 2);
+            else tval = inside ? 1 : 0;
+            acc += rh * tval * wt;
+          }
+    }
+    a.state[s + l * sv] = acc;
+  }
+}
+
+cudaError_t launch_init_tracers_fp64(const InitLaunch &L, int ntr, cudaStream_t st) {
+  InitArgs a;
+  memset(&a, 0, sizeof a);
+  a.state = (double *)L.state;
+  a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.hs = L.hs; a.ord = L.ord;
+  a.dx = L.dx; a.dy = L.dy; a.dz = L.dz; a.xlen = L.xlen; a.ylen = L.ylen; a.zlen = L.zlen;
+  a.sim2d = L.sim2d;
+  for (int m = 0; m < 9; m++) { a.pts[m] = m < L.ord ? L.pts[m] : 0; a.wts[m] = m < L.ord ? L.wts[m] : 0; }
+  const long n = (long)L.nz * L.ny * L.nx;
+  if (n == 0 || ntr == 0) return cudaSuccess;
+  init_tracers_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a, ntr);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------
 // Diagnostics: FP64 interior sums x dV with a fixed reduction order (each block sums a
 // fixed stride of cells, then one block adds the block partials in order), and a count
 // of cells with a non-finite value or a non-positive total density.
@@ -375,6 +430,32 @@ cudaError_t launch_output_fields(const void *state, int fp32, long plane, const 
   if (blocks < 1) blocks = 1;
   output_fields_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, denstheta_c, pres_c, nx, ny, nz,
                                                          hs, out);
+  return cudaGetLastError();
+}
+
+// Tracer fields of Spatial::output (Spatial:1778-1783): out[tr][k][j][i] =
+// tracers(tr, hs+k, hs+j, hs+i) / (rho'(k,j,i) + hyDensCells(hs+k)).
+__global__ void tracer_fields_kernel(const void *state, int fp32, long plane, const double *dens_c,
+                                     const double *tracers, int ntr, int nx, int ny, int nz, int hs, double *out) {
+  const long n = (long)nz * ny * nx;
+  const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
+  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long)nx * ny));
+    const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
+    const double r = state_at(state, fp32, plane, g) + dens_c[hs + k];
+    for (int t = 0; t < ntr; t++) out[t * n + c] = tracers[t * sv + g] / r;
+  }
+}
+
+cudaError_t launch_tracer_fields(const void *state, int fp32, long plane, const double *dens_c,
+                                 const double *tracers, int ntr, int nx, int ny, int nz, int hs, int nsm, double *out,
+                                 cudaStream_t st) {
+  const long n = (long)nz * ny * nx;
+  if (n == 0 || ntr == 0) return cudaSuccess;
+  long blocks = (n + 255) / 256;
+  if (blocks > (long)nsm * 8) blocks = (long)nsm * 8;
+  tracer_fields_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, tracers, ntr, nx, ny, nz, hs,
+                                                         out);
   return cudaGetLastError();
 }
 

@@ -109,6 +109,10 @@ cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const dou
                             double dx, double dy, double dz, int nx, int ny, int nz, int hs, int nsm,
                             unsigned long long *d_out, cudaStream_t st);
 cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st);
+cudaError_t launch_init_tracers_fp64(const InitLaunch &L, int ntr, cudaStream_t st);
+cudaError_t launch_tracer_fields(const void *state, int fp32, long plane, const double *dens_c,
+                                 const double *tracers, int ntr, int nx, int ny, int nz, int hs, int nsm, double *out,
+                                 cudaStream_t st);
 // interior sums x dV (partials[nblk*5] -> out[5], fixed order) and the bad-cell count
 cudaError_t launch_state_sums(const void *state, int fp32, long plane, int nx, int ny, int nz, int hs, double dv,
                               double *partials, int nblk, double *out, cudaStream_t st);

@@ -7,7 +7,7 @@
 // The file holds what the reference's SimpleNetCDF calls write (Spatial:1715-1778):
 // dimensions x, y, z and the unlimited t; fixed variables x(x), y(y), z(z), hyDens(z),
 // hyPressure(z), hyTheta(z); record variables t(t) and dens_pert, u, v, w, pot_temp_pert,
-// pressure_pert (t, z, y, x), all double. etime == 0 creates the file with record 0;
+// pressure_pert and one tracer_<name> per tracer (t, z, y, x), all double. etime == 0 creates the file with record 0;
 // any other etime appends a record (the reference reads the current length of t).
 // Host code only.
 #include <cstdint>
@@ -52,7 +52,8 @@ void put_doubles(std::vector<unsigned char> &b, const double *x, size_t n) {
 
 }  // namespace
 
-Layout layout(int nx, int ny, int nz) {
+Layout layout(int nx, int ny, int nz, const std::vector<std::string> &tracers) {
+  const int nrec = 6 + (int)tracers.size();  // record fields after t
   Layout L;
   std::vector<unsigned char> &h = L.header;
   const char magic[4] = {'C', 'D', 'F', 2};
@@ -69,7 +70,7 @@ Layout layout(int nx, int ny, int nz) {
   }
   put64(h, 0);  // no global attributes (ABSENT: two zero words)
   put32(h, kVarTag);
-  put32(h, 13);
+  put32(h, (uint32_t)(7 + nrec));
   std::vector<size_t> begin_at;
   auto var = [&](const char *name, std::initializer_list<uint32_t> dims, uint64_t vsize) {
     put_name(h, name);
@@ -87,6 +88,7 @@ Layout layout(int nx, int ny, int nz) {
   for (int f = 2; f < 6; f++) var(kFixed[f], {2}, 8ull * nz);
   var(kRecord[0], {3}, 8);
   for (int f = 1; f < 7; f++) var(kRecord[f], {3, 2, 1, 0}, 8 * cells);
+  for (const std::string &t : tracers) var(("tracer_" + t).c_str(), {3, 2, 1, 0}, 8 * cells);
   // file offsets: fixed variables back to back after the header, then the records
   uint64_t off = h.size();
   const uint64_t fixed_len[6] = {8ull * nx, 8ull * ny, 8ull * nz, 8ull * nz, 8ull * nz, 8ull * nz};
@@ -98,19 +100,20 @@ Layout layout(int nx, int ny, int nz) {
   L.rec_begin = off;
   set64(h, begin_at[6], off);
   off += 8;
-  for (int f = 1; f < 7; f++) {
+  for (int f = 1; f <= nrec; f++) {
     set64(h, begin_at[6 + f], off);
     off += 8 * cells;
   }
-  L.rec_size = 8 + 6 * 8 * cells;
+  L.rec_size = 8 + (uint64_t)nrec * 8 * cells;
+  L.nrec = nrec;
   L.cells = cells;
   return L;
 }
 
 int write(const char *path, int nx, int ny, int nz, double dx, double dy, double dz, int hs,
           const double *hy_dens, const double *hy_pres, const double *hy_theta, const double *fields, double etime,
-          std::string *err) {
-  const Layout L = layout(nx, ny, nz);
+          std::string *err, const std::vector<std::string> &tracers) {
+  const Layout L = layout(nx, ny, nz, tracers);
   FILE *f = nullptr;
   uint32_t rec = 0;
   if (etime == 0.) {
@@ -149,7 +152,7 @@ int write(const char *path, int nx, int ny, int nz, double dx, double dy, double
   std::vector<unsigned char> b;
   b.reserve((size_t)L.rec_size);
   put_doubles(b, &etime, 1);
-  put_doubles(b, fields, 6 * (size_t)L.cells);
+  put_doubles(b, fields, (size_t)L.nrec * L.cells);
   const uint64_t at = L.rec_begin + (uint64_t)rec * L.rec_size;
   bool ok = std::fseek(f, (long)at, SEEK_SET) == 0 && std::fwrite(b.data(), 1, b.size(), f) == b.size();
   std::vector<unsigned char> nr;

@@ -14,9 +14,12 @@
 //    (64-bit offset format; no netCDF library). An outFile ending in ".bin" gets the state
 //    (5 variables, halos included, FP64) raw at every output time, overwriting the previous
 //    one; any other name: output() does nothing.
-//  * Tracers (compiled out in the reference by NO_TRACERS, Spatial:10): the arrays exist,
-//    initTracers() zero-fills them and their tendencies are zero, so they stay constant (the
-//    reference adds an uninitialised tendency array to them, Temporal_ader.h:67-69).
+//  * Tracers: the reference compiles their transport out (NO_TRACERS, Spatial:10) but still
+//    runs initTracers (Spatial:505-560) and writes tracer_<name> fields in output
+//    (Spatial:1778-1783); both are here on the device (awfl_init_tracers,
+//    awfl_write_netcdf_tracers; tracers are FP64 for either precision, halos zero). Their
+//    tendencies are zero, so they stay constant (the reference adds an uninitialised
+//    tendency array to them, Temporal_ader.h:67-69).
 //  * Optional extra YAML keys (absent = reference behaviour): precision (fp64 | fp32),
 //    device, bubble (cosine | linear) with bubble_x0/y0/z0, bubble_radius (or
 //    bubble_xrad/yrad/zrad), bubble_amp, bubble_pwr; noise_amp, noise_seed, noise_dist
@@ -301,8 +304,11 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
   }
 
   void initTracers(TracerArr &tracers) {
+    if (!tracers.initialized() || tracers.totElems() == 0) return;
     awfl_dropin::check(awfl_memset_device(tracers.data(), 0, (long)(tracers.totElems() * tracers.elemBytes()), nullptr),
                        ctx, "initTracers");
+    awfl_dropin::check(awfl_init_tracers(ctx, static_cast<double *>(tracers.data()), numTracers, nullptr), ctx,
+                       "initTracers");
   }
 
   // Spatial:565-594: X,Y,Z then Z,Y,X; the dir-halos of the state are filled in place.
@@ -348,9 +354,14 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
   const char *getName() { return "1-D Uniform Transport with upwind FV on A-grid"; }
 
   void output(StateArr const &state, TracerArr const &tracers, real etime) {
-    (void)tracers;
     if (outFile.size() >= 3 && outFile.compare(outFile.size() - 3, 3, ".nc") == 0) {
-      awfl_dropin::check(awfl_write_netcdf(ctx, outFile.c_str(), state.data(), etime, nullptr), ctx, "output");
+      const bool tr = numTracers > 0 && tracers.initialized() && tracers.totElems() > 0;
+      std::vector<const char *> names;
+      for (int t = 0; tr && t < numTracers; t++) names.push_back(tracerName[t].c_str());
+      awfl_dropin::check(awfl_write_netcdf_tracers(ctx, outFile.c_str(), state.data(),
+                                                   tr ? static_cast<const double *>(tracers.data()) : nullptr,
+                                                   tr ? numTracers : 0, names.data(), etime, nullptr),
+                         ctx, "output");
       return;
     }
     if (outFile.size() < 4 || outFile.compare(outFile.size() - 4, 4, ".bin") != 0) return;

@@ -131,6 +131,28 @@ int awfl_write_netcdf(awfl_ctx *ctx, const char *path, const void *d_state, doub
  * gives them); needs no device (host-only contexts too). */
 int awfl_write_netcdf_fields(awfl_ctx *ctx, const char *path, const double *h_fields, double etime);
 
+/* Spatial::initTracers (Spatial:505-560; the reference runs it although its tracer
+ * transport is compiled out by NO_TRACERS, Spatial:10): d_tracers = double
+ * (ntracers, nz+2hs, ny+2hs, nx+2hs), interior written, for either context precision.
+ * Tracer 0 = rho_h (uniform 1), 1 = rho_h x the 2 K linear ellipsoid of radius 2 km at
+ * (xlen/2, ylen/2, 2 km), 2 = rho_h x the block indicator, as ord^3 GLL cell averages;
+ * tracers beyond the third are zero (the reference's loop leaves them so). Asynchronous. */
+int awfl_init_tracers(awfl_ctx *ctx, double *d_tracers, int ntracers, void *stream);
+
+/* The tracer fields of Spatial::output (Spatial:1778-1783): d_fields = [ntracers][nz][ny][nx]
+ * doubles, tracers(t, hs+k, hs+j, hs+i) / (rho' + hyDensCells(hs+k)). Asynchronous. */
+int awfl_output_tracer_fields(awfl_ctx *ctx, const void *d_state, const double *d_tracers, int ntracers,
+                              double *d_fields, void *stream);
+
+/* awfl_write_netcdf with the reference's tracer record variables "tracer_<name>"
+ * (Spatial:1778-1783) after the six diagnostics; names holds ntracers non-empty C strings.
+ * Appending needs the same tracer names as the call that created the file. */
+int awfl_write_netcdf_tracers(awfl_ctx *ctx, const char *path, const void *d_state, const double *d_tracers,
+                              int ntracers, const char *const *names, double etime, void *stream);
+/* The same from host-side fields ([6 + ntracers][nz][ny][nx] doubles). */
+int awfl_write_netcdf_fields_tracers(awfl_ctx *ctx, const char *path, const double *h_fields, int ntracers,
+                                     const char *const *names, double etime);
+
 /* Spatial::computeTimeStep without the caching (Spatial:159-187): the acoustic CFL time
  * step, min over all cells, returned in *h_dt (synchronises the stream). */
 int awfl_cfl(awfl_ctx *ctx, const void *d_state, double cfl, double *h_dt, void *stream);

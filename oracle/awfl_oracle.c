@@ -737,6 +737,44 @@ void oracle_init_state(oracle_ctx *c, oreal *st) {
       }
 }
 
+/* Spatial:505-560 (initTracers; not under NO_TRACERS, so the reference runs it): ord^3 GLL
+ * quadrature of rho_h * tval per tracer, with tval = 1 (tracer 0), the 2 K linear ellipsoid
+ * of radius 2 km at (xlen/2, ylen/2, 2 km) (tracer 1) or the block indicator of
+ * k in [nz/10, 3nz/10), i in [4nx/10, 6nx/10), j in [4ny/10, 6ny/10) unless sim2d (tracer 2)
+ * (integer division); any further tracer is zero. tr: (ntr, nz+2hs, ny+2hs, nx+2hs), only
+ * the interior is written. */
+void oracle_init_tracers(oracle_ctx *c, oreal *tr, int ntr) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        for (int l = 0; l < ntr; l++) {
+          long it = sidx(c, l, HS + k, HS + j, HS + i);
+          tr[it] = 0;
+          for (int kk = 0; kk < ORD; kk++)
+            for (int jj = 0; jj < ORD; jj++)
+              for (int ii = 0; ii < ORD; ii++) {
+                oreal zloc = (k + 0.5) * c->dz + c->pts_ord[kk] * c->dz;
+                oreal yloc = c->sim2d ? c->ylen / 2 : (j + 0.5) * c->dy + c->pts_ord[jj] * c->dy;
+                oreal xloc = (i + 0.5) * c->dx + c->pts_ord[ii] * c->dx;
+                oreal wt = c->wts_ord[kk] * c->wts_ord[jj] * c->wts_ord[ii];
+                oreal th = 300, rh = const_theta_density(th, zloc);
+                if (l == 0) {
+                  tr[it] += rh * 1 * wt;
+                } else if (l == 1) {
+                  oreal tval = ellipsoid_linear(xloc, yloc, zloc, c->xlen / 2, c->ylen / 2, 2000, 2000, 2000, 2000, 2);
+                  tr[it] += rh * tval * wt;
+                } else if (l == 2) {
+                  int inside = k >= 1 * nz / 10 && k < 3 * nz / 10 && i >= 4 * nx / 10 && i < 6 * nx / 10;
+                  if (!c->sim2d) inside = inside && j >= 4 * ny / 10 && j < 6 * ny / 10;
+                  oreal tval = inside ? 1 : 0;
+                  tr[it] += rh * tval * wt;
+                }
+              }
+        }
+}
+
 void oracle_set_bubble(oracle_ctx *c, oreal *st, int shape, oreal x0, oreal y0, oreal z0,
                        oreal xrad, oreal yrad, oreal zrad, oreal amp, oreal pwr) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;

@@ -46,6 +46,10 @@ void oracle_init_state(oracle_ctx *c, oreal *state);
 void oracle_set_bubble(oracle_ctx *c, oreal *state, int shape, oreal x0, oreal y0,
                        oreal z0, oreal xrad, oreal yrad, oreal zrad, oreal amp, oreal pwr);
 void oracle_add_theta_noise(oracle_ctx *c, oreal *state, unsigned long long seed, oreal amp);
+/* Spatial::initTracers (Spatial...h:505-560): the driver's three tracers (uniform, theta
+ * replica, block) as rho_h-weighted GLL cell averages; tracers beyond the third are zero.
+ * tracers: (ntr, nz+2hs, ny+2hs, nx+2hs), interior written. */
+void oracle_init_tracers(oracle_ctx *c, oreal *tracers, int ntr);
 
 /* CFL time step (Spatial...h:159-187), NOT cached here. */
 oreal oracle_compute_dt(const oracle_ctx *c, const oreal *state, oreal cfl);

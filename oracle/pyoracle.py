@@ -94,6 +94,7 @@ class Oracle(_Grid):
             L.oracle_init_state.argtypes = [_VP, _DP]
             L.oracle_set_bubble.argtypes = [_VP, _DP, _I] + [_D] * 8
             L.oracle_add_theta_noise.argtypes = [_VP, _DP, ctypes.c_ulonglong, _D]
+            L.oracle_init_tracers.argtypes = [_VP, _DP, _I]
             L.oracle_compute_dt.restype = _D
             L.oracle_compute_dt.argtypes = [_VP, _DP, _D]
             L.oracle_compute_tendencies_dir.argtypes = [_VP, _DP, _DP, _D, _I]
@@ -132,6 +133,14 @@ class Oracle(_Grid):
 
     def add_theta_noise(self, st, seed, amp):
         self.L.oracle_add_theta_noise(self.h, _ptr(st), seed, amp)
+
+    def new_tracers(self, ntr):
+        hs = self.hs
+        return np.zeros((ntr, self.nz + 2 * hs, self.ny + 2 * hs, self.nx + 2 * hs))
+
+    def init_tracers(self, tr):
+        """Spatial::initTracers on tr (ntr, nz+2hs, ny+2hs, nx+2hs)."""
+        self.L.oracle_init_tracers(self.h, _ptr(tr), tr.shape[0])
 
     def compute_dt(self, st, cfl=0.8):
         return self.L.oracle_compute_dt(self.h, _ptr(st), cfl)
@@ -260,6 +269,11 @@ class RefHarness(_Grid):
             L.awflref_set_state.argtypes = [_VP, _DP]
             L.awflref_set_bubble.argtypes = [_VP, _I] + [_D] * 8
             L.awflref_add_theta_noise.argtypes = [_VP, ctypes.c_ulonglong, _D]
+            L.awflref_set_num_tracers.argtypes = [_I]
+            L.awflref_init_tracers.argtypes = [_VP]
+            L.awflref_tracer_size.restype = ctypes.c_long
+            L.awflref_tracer_size.argtypes = [_VP]
+            L.awflref_get_tracers.argtypes = [_VP, _DP]
             L.awflref_compute_dt.restype = _D
             L.awflref_compute_dt.argtypes = [_VP, _D]
             L.awflref_time_step.argtypes = [_VP, _D]
@@ -276,11 +290,14 @@ class RefHarness(_Grid):
         return cls._libs[key]
 
     def __init__(self, nx, ny, nz, xlen=20000.0, ylen=20000.0, zlen=10000.0, bc=(0, 0, 1),
-                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5, crpow=False):
+                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5, crpow=False, ntracers=0):
         """crpow: the reference's code with its pow/exp calls bound to a correctly rounded
-        implementation instead of glibc's."""
+        implementation instead of glibc's. ntracers: tracers registered with addTracer
+        before init (the driver's names: uniform, theta, block)."""
         super().__init__(ord_, nx, ny, nz)
         self.L = self.lib(ord_, crpow)
+        self.L.awflref_set_num_tracers(ntracers)
+        self.ntracers = ntracers
         self.h = self.L.awflref_create(nx, ny, nz, xlen, ylen, zlen, bc[0], bc[1], bc[2],
                                        int(weno_scalars), int(weno_winds), data.encode())
         if not self.h:
@@ -293,6 +310,16 @@ class RefHarness(_Grid):
 
     def init_state(self):
         self.L.awflref_init_state(self.h)
+
+    def init_tracers(self):
+        self.L.awflref_init_tracers(self.h)
+
+    def get_tracers(self):
+        hs = self.hs
+        tr = np.zeros((self.ntracers, self.nz + 2 * hs, self.ny + 2 * hs, self.nx + 2 * hs))
+        assert tr.size == self.L.awflref_tracer_size(self.h)
+        self.L.awflref_get_tracers(self.h, _ptr(tr))
+        return tr
 
     def get_state(self):
         st = self.new_state()

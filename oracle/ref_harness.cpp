@@ -59,7 +59,13 @@ inline double unit_uniform(uint64_t seed, uint64_t i) {
 
 }  // namespace
 
+// Number of tracers the next awflref_create registers with addTracer before init, named
+// like the reference driver's three (driver.cpp:27-29); 0 by default.
+int g_pending_tracers = 0;
+
 extern "C" {
+
+void awflref_set_num_tracers(int n) { g_pending_tracers = n < 0 ? 0 : n; }
 
 int awflref_ord() { return ord; }
 int awflref_ngll() { return ngll; }
@@ -86,6 +92,9 @@ void *awflref_create(int nx, int ny, int nz, double xlen, double ylen, double zl
     f << "initData : " << initData << "\noutFile : none.nc\nperturb : false\n";
   }
   RefHandle *h = new RefHandle();
+  static const char *const names[3] = {"uniform", "theta", "block"};
+  for (int t = 0; t < g_pending_tracers; t++)
+    h->model.spaceOp.addTracer(t < 3 ? names[t] : "tracer" + std::to_string(t), true, "");
   try {
     h->model.init(path);
   } catch (...) {
@@ -105,6 +114,20 @@ void awflref_destroy(void *p) { delete static_cast<RefHandle *>(p); }
 void awflref_init_state(void *p) {
   RefHandle *h = static_cast<RefHandle *>(p);
   h->model.spaceOp.initState(h->state);
+}
+
+// Reference initTracers (Spatial...h:505-560), run on the tracers awflref_create registered.
+void awflref_init_tracers(void *p) {
+  RefHandle *h = static_cast<RefHandle *>(p);
+  h->model.spaceOp.initTracers(h->tracers);
+}
+
+long awflref_tracer_size(void *p) { return (long)static_cast<RefHandle *>(p)->tracers.totElems(); }
+
+void awflref_get_tracers(void *p, double *out) {
+  RefHandle *h = static_cast<RefHandle *>(p);
+  size_t n = h->tracers.totElems();
+  for (size_t i = 0; i < n; i++) out[i] = h->tracers.data()[i];
 }
 
 long awflref_state_size(void *p) {

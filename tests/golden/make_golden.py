@@ -10,7 +10,8 @@ drives that build through ``oracle.pyoracle.RefHarness`` and stores:
 * ``probes_o{5,9}.npz``  -- coefs_to_tv and compute_weno_coefs on seeded inputs;
 * ``case_<name>.npz``    -- per configuration: background, initial state, CFL dt,
                             tendencies of every split of steps 1-2, the state after
-                            each split of step 1 and after every step.
+                            each split of step 1 and after every step;
+* ``tracers_init.npz``   -- initTracers of the driver's tracers on three grids.
 
 Needs the reference sources (REF, default /root/reference) and g++ with OpenMP.
 Run from the repository root:  python tests/golden/make_golden.py
@@ -109,8 +110,32 @@ def make_probes(ord_):
                         tv_lo=tv_lo, tv_hi_in=tv_hi_in, tv_hi=tv_hi, weno_in=sten, weno=weno)
 
 
+# initTracers (Spatial_euler3d_cons_expl_cart_fv_Agrid.h:505-560) with the driver's three
+# tracers plus one more: (ord, nx, ny, nz, bc, data)
+TRACER_CASES = {
+    "o5_3d": (5, 20, 20, 10, (0, 0, 1), "thermal"),
+    "o5_sim2d": (5, 30, 1, 20, (0, 0, 1), "thermal"),
+    "o9_walls": (9, 20, 10, 10, (1, 1, 1), "collision"),
+}
+
+
+def make_tracers():
+    out = {}
+    for name, (ord_, nx, ny, nz, bc, data) in TRACER_CASES.items():
+        R = RefHarness(nx, ny, nz, bc=bc, data=data, ord_=ord_, ntracers=4)
+        R.init_state()
+        R.init_tracers()
+        out[name + "_config"] = np.array([ord_, nx, ny, nz, bc[0], bc[1], bc[2]])
+        out[name + "_data"] = np.array(data)
+        out[name + "_tracers"] = R.get_tracers()
+    path = os.path.join(OUT, "tracers_init.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
 def main():
     pyoracle.build(ref=True)
+    print("wrote", make_tracers())
     for o in (5, 9):
         make_tables(o)
         make_probes(o)

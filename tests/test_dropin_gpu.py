@@ -136,3 +136,17 @@ def test_reference_driver_netcdf_output(tmp_path):
         for i, name in enumerate(["dens_pert", "u", "v", "w", "pot_temp_pert"]):
             got = nc.variables[name][2]
             assert _rel(got, want[i]) <= 5e-12, name
+        # the driver's three tracers (driver.cpp:27-29): initTracers (Spatial:505-560) on the
+        # device, written as tracer / rho (Spatial:1778-1783); transport is compiled out in
+        # the reference, so they keep their initial values
+        tr = O.new_tracers(3)
+        O.init_tracers(tr)
+        tr = tr[:, h:-h, h:-h, h:-h]
+        r0 = st[0, h:-h, h:-h, h:-h] + d
+        for i, name in enumerate(["uniform", "theta", "block"]):
+            v = nc.variables["tracer_" + name]
+            assert v.dimensions == ("t", "z", "y", "x")
+            # the device's profile pow is correctly rounded, glibc's (the oracle's) is not
+            # always: last-bit differences in a few cells
+            np.testing.assert_allclose(v[0], tr[i] / r0, rtol=1e-15, atol=0)
+            assert _rel(v[2], tr[i] / r) <= 5e-12, name

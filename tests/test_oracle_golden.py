@@ -148,3 +148,20 @@ def test_glibc_pow_rounding_spread():
     spread = [np.linalg.norm(res[0][v] - res[1][v]) / np.linalg.norm(res[1][v]) for v in range(5)]
     assert max(spread) > 0          # glibc's pow is not correctly rounded everywhere
     assert max(spread) < 5e-12      # ... but only in the last bit
+
+
+def test_init_tracers_bit_exact():
+    """initTracers (Spatial:505-560) of the driver's three tracers plus a fourth (zero)."""
+    g = np.load(os.path.join(GOLDEN, "tracers_init.npz"))
+    names = sorted({k.rsplit("_", 1)[0] for k in g.files})
+    assert len(names) == 3
+    for name in names:
+        ord_, nx, ny, nz, bx, by, bz = [int(v) for v in g[name + "_config"]]
+        O = Oracle(nx, ny, nz, bc=(bx, by, bz), data=str(g[name + "_data"]), ord_=ord_)
+        tr = O.new_tracers(4)
+        O.init_tracers(tr)
+        ref = g[name + "_tracers"]
+        assert np.array_equal(tr, ref), name
+        h = O.hs
+        assert np.all(ref[3] == 0)
+        assert np.all(ref[0, h:h + nz, h:h + ny, h:h + nx] > 0)  # rho_h-weighted uniform tracer

@@ -72,3 +72,29 @@ def test_append_refuses_missing_or_foreign_files(tmp_path):
     assert e.value.code == -7
     with pytest.raises(ValueError):
         c.write_netcdf_fields(path, np.zeros(5), 1.0)
+
+
+def test_tracer_record_variables(tmp_path):
+    """Spatial:1778-1783: one tracer_<name> record variable per tracer after the six fields."""
+    c = _ctx()
+    names = ["uniform", "theta", "block"]
+    path = str(tmp_path / "tr.nc")
+    rng = np.random.default_rng(7)
+    f0 = rng.standard_normal((9, c.nz, c.ny, c.nx))
+    f1 = rng.standard_normal((9, c.nz, c.ny, c.nx))
+    c.write_netcdf_fields_tracers(path, f0, names, 0.0)
+    c.write_netcdf_fields_tracers(path, f1, names, 1.5)
+    with netcdf(path, "r", mmap=False) as nc:
+        assert list(nc.variables)[-3:] == ["tracer_uniform", "tracer_theta", "tracer_block"]
+        np.testing.assert_array_equal(nc.variables["t"][:], [0.0, 1.5])
+        for i, name in enumerate(["dens_pert", "u", "v", "w", "pot_temp_pert", "pressure_pert"]
+                                 + ["tracer_" + n for n in names]):
+            assert nc.variables[name].dimensions == ("t", "z", "y", "x")
+            np.testing.assert_array_equal(nc.variables[name][0], f0[i])
+            np.testing.assert_array_equal(nc.variables[name][1], f1[i])
+    # a file made without these tracers is another layout: appending is refused
+    with pytest.raises(capi.AwflError) as e:
+        c.write_netcdf_fields(path, f1[:6], 3.0)
+    assert e.value.code == -7
+    with pytest.raises(ValueError):
+        c.write_netcdf_fields_tracers(path, f1[:8], names, 3.0)
