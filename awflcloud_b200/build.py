@@ -13,6 +13,7 @@ Translation units and their numerics flags:
   awfl_ens64.cu    ensemble persistent sweeps, FP64 path: --fmad=false
   awfl_ensemble.cu ensemble host side: work lists, CUDA graph, autotuner (host code only)
   awfl_netcdf.cu   netCDF output file writer (host code only)
+  awfl_tracers.cu  tracer transport of the FP64 path: --fmad=false
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
 source tree. ``python -m awflcloud_b200.build [--force]``.
@@ -45,6 +46,7 @@ UNITS = {
     "awfl_ens64.cu": ["--fmad=false"],
     "awfl_ensemble.cu": [],
     "awfl_netcdf.cu": [],
+    "awfl_tracers.cu": ["--fmad=false"],
 }
 
 

@@ -61,6 +61,8 @@ _SIGS = {
     "awfl_write_netcdf": (_I, [_VP, ctypes.c_char_p, _VP, _D, _VP]),
     "awfl_write_netcdf_fields": (_I, [_VP, ctypes.c_char_p, _DP, _D]),
     "awfl_init_tracers": (_I, [_VP, _VP, _I, _VP]),
+    "awfl_tracer_split": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_I), _D, _I, _VP]),
+    "awfl_step_tracers": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_I), _D, _VP]),
     "awfl_output_tracer_fields": (_I, [_VP, _VP, _VP, _I, _VP, _VP]),
     "awfl_write_netcdf_tracers": (_I, [_VP, ctypes.c_char_p, _VP, _VP, _I, ctypes.POINTER(ctypes.c_char_p), _D, _VP]),
     "awfl_write_netcdf_fields_tracers": (_I, [_VP, ctypes.c_char_p, _DP, _I, ctypes.POINTER(ctypes.c_char_p), _D]),
@@ -309,6 +311,25 @@ class Context:
         """Spatial::initTracers: the driver's tracers (uniform, theta, block; any further zero)."""
         n = tracers.shape[0] if ntracers is None else ntracers
         self._check(self.L.awfl_init_tracers(self.h, self._tr(tracers, n), n, _stream(stream)))
+
+    def _pos(self, pos, n):
+        if pos is None:
+            pos = [1] * n
+        if len(pos) != n:
+            raise ValueError("pos needs one flag per tracer")
+        return (_I * max(n, 1))(*[int(bool(p)) for p in pos])
+
+    def tracer_split(self, state, tracers, dt, d, pos=None, stream=None):
+        """One split's tracer transport (before that split's state sweep)."""
+        n = tracers.shape[0]
+        self._check(self.L.awfl_tracer_split(self.h, self._st(state), self._tr(tracers, n), n, self._pos(pos, n),
+                                             dt, d, _stream(stream)))
+
+    def step_tracers(self, state, tracers, dt, pos=None, stream=None):
+        """One time step of state and tracers (pos: positive-definite flags, default all)."""
+        n = tracers.shape[0]
+        self._check(self.L.awfl_step_tracers(self.h, self._st(state), self._tr(tracers, n), n, self._pos(pos, n),
+                                             dt, _stream(stream)))
 
     def output_tracer_fields(self, state, tracers, ntracers=None, stream=None):
         """tracer / (rho' + rho_h) per tracer, as a (ntracers, nz, ny, nx) FP64 CUDA tensor."""

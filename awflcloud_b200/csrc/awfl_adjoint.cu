@@ -71,6 +71,7 @@ struct P64Rec : P64 {
     __device__ __forceinline__ void level0(int v, int ii, const double &x) const {
       q0[(v * OrdTraits<ORD>::NGLL + ii) * n + cell] = x;
     }
+    template <class Q> __device__ __forceinline__ void series(const Q &) const {}
   };
   template <int ORD, int DIR, class S>
   static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],

@@ -52,6 +52,8 @@ struct awfl_ctx {
   double *d_diag = nullptr;
   double *d_out = nullptr;  // output diagnostics (awfl_write_netcdf)
   size_t out_bytes = 0;
+  double *d_trc = nullptr;  // tracer transport scratch (awfl_tracer_split)
+  size_t trc_bytes = 0;
   size_t diag_bytes = 0;
   std::string err;
 };
@@ -228,6 +230,7 @@ int ensure_tables(awfl_ctx *c) {
     std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
     e = upload_tables_fp64(5, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adj(5, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_tracers(5, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adjrev(5, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_ens64(5, &t, sizeof t);
   } else {
@@ -241,6 +244,7 @@ int ensure_tables(awfl_ctx *c) {
     std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
     e = upload_tables_fp64(9, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adj(9, &t, sizeof t);
+    if (e == cudaSuccess) e = upload_tables_tracers(9, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adjrev(9, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_ens64(9, &t, sizeof t);
   }
@@ -501,6 +505,7 @@ int awfl_destroy(awfl_ctx *c) {
     if (c->d_adj) cudaFree(c->d_adj);
     if (c->d_diag) cudaFree(c->d_diag);
     if (c->d_out) cudaFree(c->d_out);
+    if (c->d_trc) cudaFree(c->d_trc);
   }
   delete c;
   return AWFL_OK;
@@ -785,6 +790,44 @@ int awfl_step(awfl_ctx *c, void *d_state, double dt, void *stream) {
   for (int spl = 0; spl < 3; spl++) {
     const int dir = c->dimswitch ? spl : 2 - spl;
     int rc = awfl_split(c, d_state, dt, dir, stream);
+    if (rc) return rc;
+  }
+  c->dimswitch = !c->dimswitch;
+  return AWFL_OK;
+}
+
+int awfl_tracer_split(awfl_ctx *c, const void *d_state, double *d_tracers, int ntracers, const int *pos,
+                      double dt, int dir, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (fp32(c)) return fail(c, AWFL_ERR_ARG, "tracer transport needs an FP64 context");
+  if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
+  if (ntracers < 0 || ntracers > 64) return fail(c, AWFL_ERR_ARG, "ntracers must be in [0, 64]");
+  if (ntracers == 0) return AWFL_OK;
+  if (bad_ptr(d_state) || bad_ptr(d_tracers)) return fail(c, AWFL_ERR_ARG, "state or tracer pointer is NULL or misaligned");
+  if (!pos) return fail(c, AWFL_ERR_ARG, "pos (positive-definite flags) is NULL");
+  int rc = set_device(c);
+  if (rc) return rc;
+  if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendency (Spatial:572-575)
+  unsigned long long mask = 0;
+  for (int l = 0; l < ntracers; l++)
+    if (pos[l]) mask |= 1ull << l;
+  const size_t need = sizeof(double) * (size_t)tracer_scratch_doubles(c->cfg.nx, c->cfg.ny, c->cfg.nz, ntracers);
+  rc = ensure_buffer(c, &c->d_trc, &c->trc_bytes, need, "tracer scratch");
+  if (rc) return rc;
+  SweepArgs A = sweep_args(c, const_cast<void *>(d_state), nullptr, dt, dir, MODE_TEND);
+  cudaError_t e = launch_tracer_split(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "tracer_split");
+  return AWFL_OK;
+}
+
+int awfl_step_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
+                      void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  for (int spl = 0; spl < 3; spl++) {
+    const int dir = c->dimswitch ? spl : 2 - spl;
+    int rc = awfl_tracer_split(c, d_state, d_tracers, ntracers, pos, dt, dir, stream);
+    if (rc) return rc;
+    rc = awfl_split(c, d_state, dt, dir, stream);
     if (rc) return rc;
   }
   c->dimswitch = !c->dimswitch;

@@ -136,9 +136,11 @@ __device__ __forceinline__ void reconstruct_gll(const Sc (&sten)[ORD], Sc (&out)
 // the line (x, y). Outputs: the time-averaged left/right edge states and, for z, the
 // time-averaged, GLL-weighted gravity source.
 // A recorder that keeps nothing (the default): rec.level0(v, ii, x) sees every level-0
-// value (after hydrostasis and the wall), for the adjoint's tape.
+// value (after hydrostasis and the wall), for the adjoint's tape; rec.series(q) sees the
+// whole ADER series q[v][kt][ii] before the edge time average, for the tracer transport.
 struct NoRecord {
   template <class Sc> __device__ __forceinline__ void level0(int, int, const Sc &) const {}
+  template <class Q> __device__ __forceinline__ void series(const Q &) const {}
 };
 
 template <int ORD, int DIR, class Sten, class Sc, class Rec = NoRecord>
@@ -267,6 +269,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
       g[kt + 1][ii] = (GAMMA * g[0][ii] * q[idT][kt + 1][ii] + tg / (kt + 1.)) / q[idT][0][ii];
     }
   }
+  rec.series(q);
   // compute_timeAvg_edges (Spatial:2153-2177)
 #pragma unroll
   for (int v = 0; v < 5; v++) {

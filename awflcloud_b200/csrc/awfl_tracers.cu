@@ -1,0 +1,375 @@
+// Tracer transport of the FP64 path: the reference's tracer code, which it compiles out
+// with NO_TRACERS (Spatial:10), built in. Per directional split, four launches run BEFORE
+// that split's state sweep (they read the pre-split state):
+//
+//   tracer_cell_kernel    per cell: the state's reconstruction + ADER (cell_recon, the same
+//                         device function and arithmetic as the state sweep) recording the
+//                         density and normal-momentum series, then per tracer the
+//                         reconstruction of tracer/density, the rho*tracer ADER series
+//                         (diffTransformTracer, Spatial:2095-2125) and its edge time
+//                         average (Spatial:760-809, 1123-1170, 1500-1548)
+//   tracer_face_kernel    per face: edge BCs (Spatial:826-835), the state's Riemann flux
+//                         (riemann) and the upwind tracer fluxes (Spatial:891-901,
+//                         1249-1259, 1633-1643)
+//   tracer_limit_kernel   per face: the positivity limiter (Spatial:904-935, 1262-1293,
+//                         1646-1677) from the unscaled fluxes
+//   tracer_update_kernel  per cell: tendency, density multiplied back, apply
+//                         (Spatial:948-955; Temporal_ader.h:67-69), and the halo cells of
+//                         this direction left holding tracer/density, as the reference's
+//                         in-place halo fill leaves them
+//
+// Decisions where the reference's code is not well defined: the limiter reads unscaled
+// fluxes (the reference scales tracerFlux in place while other iterations read it); the
+// y branch for v < 0 reads the faces along y (the reference indexes tracerFlux(tr,k,j,ind_j),
+// Spatial:1285-1286); a periodic z wraps like x and y (the reference reads outside the
+// array there). Stencil halos are computed from the boundary conditions (periodic wrap;
+// wall: the edge cell, the state's normal momentum zero), as the reference's halo fill
+// writes them. Compiled with --fmad=false like the FP64 path.
+#include <cuda_runtime.h>
+
+#include "awfl_internal.h"
+#include "awfl_p64.cuh"
+
+namespace awfl {
+
+namespace {
+
+struct TracerArgs {
+  SweepArgs A;               // the state (pre-split), background, grid, bc, dt of this split
+  double *tr;                // (ntr, nz+2hs, ny+2hs, nx+2hs), rho*tracer
+  int ntr;
+  unsigned long long pos;    // bit l: tracer l is positive definite (limited)
+  double *E;                 // (10, ncell): the state's time-averaged edges eL[5], eR[5]
+  double *TE;                // (ntr, 2, ncell): the tracers' edges (left, right)
+  double *TF, *TF2, *UN;     // (ntr, nface) unscaled / limited fluxes, (nface) limiter velocity
+};
+
+__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }
+
+// Along-direction geometry of one split: cells (k, j, i); p = the index along DIR.
+template <int DIR> struct Geo {
+  int nx, ny, nz, hs;
+  long sy, sz, sv;  // state strides (halo-inclusive)
+  __device__ Geo(const SweepArgs &A, int hs_) : nx(A.nx), ny(A.ny), nz(A.nz), hs(hs_) {
+    sy = nx + 2 * hs;
+    sz = (long)(ny + 2 * hs) * sy;
+    sv = (long)(nz + 2 * hs) * sz;
+  }
+  __device__ int n() const { return DIR == 0 ? nx : (DIR == 1 ? ny : nz); }
+  __device__ long cell(int k, int j, int i) const { return ((long)k * ny + j) * nx + i; }
+  // state offset of interior cell (k, j, i)
+  __device__ long g(int k, int j, int i) const { return (long)(hs + k) * sz + (long)(hs + j) * sy + hs + i; }
+  // face index (faces along DIR: n+1 per line)
+  __device__ long face(int k, int j, int i) const {
+    if (DIR == 0) return ((long)k * ny + j) * (nx + 1) + i;
+    if (DIR == 1) return ((long)k * (ny + 1) + j) * nx + i;
+    return ((long)k * ny + j) * nx + i;
+  }
+  __device__ long nface() const {
+    return (long)(nz + (DIR == 2)) * (ny + (DIR == 1)) * (nx + (DIR == 0));
+  }
+  // cell (k, j, i) moved to index p along DIR
+  __device__ void at(int k, int j, int i, int p, int &kk, int &jj, int &ii) const {
+    kk = DIR == 2 ? p : k;
+    jj = DIR == 1 ? p : j;
+    ii = DIR == 0 ? p : i;
+  }
+};
+
+// Index p (possibly in the halo) -> the interior index whose value the halo holds, and
+// whether it is a wall halo (normal momentum zero).
+__device__ __forceinline__ int halo_src(int p, int n, int bc, bool &wall) {
+  wall = false;
+  if (p >= 0 && p < n) return p;
+  if (bc == BC_PERIODIC) return p < 0 ? p + n : p - n;
+  wall = true;
+  return p < 0 ? 0 : n - 1;
+}
+
+template <int ORD> struct SeriesRec {
+  double (*r)[OrdTraits<ORD>::NGLL];
+  double (*ru)[OrdTraits<ORD>::NGLL];
+  int nm;
+  __device__ __forceinline__ void level0(int, int, const double &) const {}
+  template <class Q> __device__ __forceinline__ void series(const Q &q) const {
+    constexpr int NG = OrdTraits<ORD>::NGLL;
+#pragma unroll
+    for (int kt = 0; kt < NG; kt++)
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) {
+        r[kt][ii] = q[idR][kt][ii];
+        ru[kt][ii] = q[nm][kt][ii];
+      }
+  }
+};
+
+template <int ORD, int DIR>
+__global__ void __launch_bounds__(128) tracer_cell_kernel(TracerArgs T) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int NM = 1 + DIR;
+  const SweepArgs &A = T.A;
+  const Geo<DIR> G(A, HS);
+  const long ncell = (long)G.nz * G.ny * G.nx;
+  const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int i = (int)(c % G.nx), j = (int)((c / G.nx) % G.ny), k = (int)(c / ((long)G.nx * G.ny));
+  const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  // state stencil with the halo rules of Spatial:631-662 (x), 994-1025 (y), 1351-1382 (z)
+  auto sten = [&](int v, int m) -> double {
+    bool wall;
+    const int p = halo_src(p0 - HS + m, n, A.bc, wall);
+    if (wall && v == NM) return 0.0;
+    int kk, jj, ii;
+    G.at(k, j, i, p, kk, jj, ii);
+    return A.state[v * G.sv + G.g(kk, jj, ii)];
+  };
+  double rser[NG][NG], ruser[NG][NG];
+  double eL[5], eR[5], src;
+  cell_recon<ORD, DIR>(sten, k, A, eL, eR, src, SeriesRec<ORD>{rser, ruser, NM});
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    T.E[v * ncell + c] = eL[v];
+    T.E[(5 + v) * ncell + c] = eR[v];
+  }
+  const Tables<ORD> &TB = tab<ORD>();
+  for (int l = 0; l < T.ntr; l++) {
+    const bool posdef = (T.pos >> l) & 1ull;
+    double s[ORD];
+#pragma unroll
+    for (int m = 0; m < ORD; m++) {
+      bool wall;
+      const int p = halo_src(p0 - HS + m, n, A.bc, wall);
+      int kk, jj, ii;
+      G.at(k, j, i, p, kk, jj, ii);
+      const long gg = G.g(kk, jj, ii);
+      // tracers /= (rho' + rho_h) (Spatial:624-627), then the halo copy
+      s[m] = T.tr[l * G.sv + gg] / (A.state[gg] + A.dens_c[HS + kk]);
+    }
+    double rt[NG][NG], rut[NG][NG];
+    reconstruct_gll<ORD>(s, rt[0], A.weno_s != 0);
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      rt[0][ii] *= rser[0][ii];
+      if (posdef) rt[0][ii] = dmax(0., rt[0][ii]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) rut[0][ii] = rt[0][ii] * ruser[0][ii] / rser[0][ii];
+    // diffTransformTracer (Spatial:2095-2125)
+#pragma unroll
+    for (int kt = 1; kt < NG; kt++)
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) rut[kt][ii] = 0;
+#pragma unroll
+    for (int kt = 0; kt < NG - 1; kt++) {
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) {
+        double df = 0;
+#pragma unroll
+        for (int q = 0; q < NG; q++) df += TB.deriv[q * NG + ii] * rut[kt][q];
+        rt[kt + 1][ii] = -df / A.dxd / (kt + 1.);
+      }
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) {
+        double tot = 0;
+#pragma unroll
+        for (int ir = 0; ir <= kt + 1; ir++) tot += ruser[ir][ii] * rt[kt + 1 - ir][ii] - rser[ir][ii] * rut[kt + 1 - ir][ii];
+        rut[kt + 1][ii] = tot / rser[0][ii];
+      }
+    }
+    // compute_timeAvg_edges (Spatial:2153-2177), then the positivity clamp of the edges
+    double tl = rt[0][0], trr = rt[0][NG - 1];
+    double dtmult = A.dt;
+#pragma unroll
+    for (int kt = 1; kt < NG; kt++) {
+      tl += rt[kt][0] * dtmult / (kt + 1.);
+      trr += rt[kt][NG - 1] * dtmult / (kt + 1.);
+      dtmult *= A.dt;
+    }
+    if (posdef) {
+      tl = dmax(0., tl);
+      trr = dmax(0., trr);
+    }
+    T.TE[(2L * l) * ncell + c] = tl;
+    T.TE[(2L * l + 1) * ncell + c] = trr;
+  }
+}
+
+// The left (side 0) and right (side 1) values at face f along a line, with the edge BCs:
+// periodic faces 0 and n both see (right edge of cell n-1, left edge of cell 0); at a wall
+// the outside value copies the inside one (Spatial:816-837).
+template <int DIR, int NG>
+__global__ void __launch_bounds__(128) tracer_face_kernel(TracerArgs T, int hs) {
+  const SweepArgs &A = T.A;
+  const Geo<DIR> G(A, hs);
+  const long nf = G.nface();
+  const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const int fx = G.nx + (DIR == 0), fy = G.ny + (DIR == 1);
+  const int i = (int)(f % fx), j = (int)((f / fx) % fy), k = (int)(f / ((long)fx * fy));
+  const int pf = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  const long ncell = (long)G.nz * G.ny * G.nx;
+  int pl = pf - 1, pr = pf;  // cells whose right / left edges meet at the face
+  bool lside_from_right = false, rside_from_left = false;  // wall copies
+  if (pf == 0) {
+    if (A.bc == BC_PERIODIC) pl = n - 1;
+    else { pl = 0; lside_from_right = true; }
+  }
+  if (pf == n) {
+    if (A.bc == BC_PERIODIC) pr = 0;
+    else { pr = n - 1; rside_from_left = true; }
+  }
+  int kl, jl, il, kr, jr, ir;
+  G.at(k, j, i, pl, kl, jl, il);
+  G.at(k, j, i, pr, kr, jr, ir);
+  const long cl = G.cell(kl, jl, il), cr = G.cell(kr, jr, ir);
+  double qL[5], qR[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    qL[v] = lside_from_right ? T.E[v * ncell + cl] : T.E[(5 + v) * ncell + cl];
+    qR[v] = rside_from_left ? T.E[(5 + v) * ncell + cr] : T.E[v * ncell + cr];
+  }
+  double F[5];
+  riemann<DIR, NG>(qL, qR, k, A, F);  // k: the face's k (z) or the line's k
+  constexpr int NM = 1 + DIR;
+  const double vn = DIR == 1 ? 0.5 * (qL[NM] + qR[NM]) : 0.5 * (qL[NM] / qL[0] + qR[NM] / qR[0]);
+  T.UN[f] = 0.5 * (qL[NM] + qR[NM]);
+  for (int l = 0; l < T.ntr; l++) {
+    const double tL = lside_from_right ? T.TE[(2L * l) * ncell + cl] : T.TE[(2L * l + 1) * ncell + cl];
+    const double tR = rside_from_left ? T.TE[(2L * l + 1) * ncell + cr] : T.TE[(2L * l) * ncell + cr];
+    T.TF[l * nf + f] = vn > 0 ? F[0] * tL / qL[0] : F[0] * tR / qR[0];
+  }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(128) tracer_limit_kernel(TracerArgs T, int hs) {
+  const SweepArgs &A = T.A;
+  const Geo<DIR> G(A, hs);
+  const long nf = G.nface();
+  const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const int fx = G.nx + (DIR == 0), fy = G.ny + (DIR == 1);
+  const int i = (int)(f % fx), j = (int)((f / fx) % fy), k = (int)(f / ((long)fx * fy));
+  const int pf = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  const double un = T.UN[f];
+  int ind = -1;
+  if (un > 0) { ind = pf - 1; if (ind == -1) ind = n - 1; }
+  else if (un < 0) { ind = pf; if (ind == n) ind = 0; }
+  int ck, cj, ci, fk, fj, fi;
+  if (ind >= 0) {
+    G.at(k, j, i, ind, ck, cj, ci);
+    G.at(k, j, i, ind + 1, fk, fj, fi);
+  }
+  const double eps = 1.e-10;
+  for (int l = 0; l < T.ntr; l++) {
+    const double F = T.TF[l * nf + f];
+    double out = F;
+    if (ind >= 0 && ((T.pos >> l) & 1ull)) {
+      const double f1 = dmin(T.TF[l * nf + G.face(ck, cj, ci)], 0.);
+      const double f2 = dmax(T.TF[l * nf + G.face(fk, fj, fi)], 0.);
+      const double fluxOut = A.dt * (f2 - f1) / A.dxd;
+      const long gg = G.g(ck, cj, ci);
+      const double dens = A.state[gg] + A.dens_c[hs + ck];
+      const double q = T.tr[l * G.sv + gg] / dens;  // the divided tracer (Spatial:624-627)
+      out = F * dmin(1., q * dens / (fluxOut + eps));
+    }
+    T.TF2[l * nf + f] = out;
+  }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(128) tracer_update_kernel(TracerArgs T, int hs) {
+  const SweepArgs &A = T.A;
+  const Geo<DIR> G(A, hs);
+  const long ncell = (long)G.nz * G.ny * G.nx;
+  const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int i = (int)(c % G.nx), j = (int)((c / G.nx) % G.ny), k = (int)(c / ((long)G.nx * G.ny));
+  const int p = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  const long nf = G.nface();
+  int rk, rj, ri;
+  G.at(k, j, i, p + 1, rk, rj, ri);
+  const long fl = G.face(k, j, i), fr = G.face(rk, rj, ri);
+  const long gg = G.g(k, j, i);
+  const double dens = A.state[gg] + A.dens_c[hs + k];
+  // halo cell of index h along DIR (state offset)
+  auto halo = [&](int h) -> long {
+    int kk, jj, ii;
+    G.at(k, j, i, h, kk, jj, ii);
+    return G.g(kk, jj, ii);
+  };
+  for (int l = 0; l < T.ntr; l++) {
+    double *t = T.tr + l * G.sv;
+    const double q = t[gg] / dens;  // Spatial:624-627
+    const double tend = -(T.TF2[l * nf + fr] - T.TF2[l * nf + fl]) / A.dxd;
+    t[gg] = q * dens + A.dt * tend;  // Spatial:952-953, then Temporal_ader.h:67-69
+    if (A.bc == BC_PERIODIC) {
+      if (p >= n - hs) t[halo(p - n)] = q;   // low halo (index p - n in [-hs, 0))
+      if (p < hs) t[halo(n + p)] = q;        // high halo
+    } else {
+      if (p == 0)
+        for (int h = 1; h <= hs; h++) t[halo(-h)] = q;
+      if (p == n - 1)
+        for (int h = 0; h < hs; h++) t[halo(n + h)] = q;
+    }
+  }
+}
+
+template <int ORD, int DIR>
+cudaError_t run(const TracerArgs &T, cudaStream_t st) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  const SweepArgs &A = T.A;
+  const long ncell = (long)A.nz * A.ny * A.nx;
+  const long nf = (long)(A.nz + (DIR == 2)) * (A.ny + (DIR == 1)) * (A.nx + (DIR == 0));
+  const unsigned gc = (unsigned)((ncell + 127) / 128), gf = (unsigned)((nf + 127) / 128);
+  tracer_cell_kernel<ORD, DIR><<<gc, 128, 0, st>>>(T);
+  tracer_face_kernel<DIR, NG><<<gf, 128, 0, st>>>(T, HS);
+  tracer_limit_kernel<DIR><<<gf, 128, 0, st>>>(T, HS);
+  tracer_update_kernel<DIR><<<gc, 128, 0, st>>>(T, HS);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_tracer_split(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
+                                unsigned long long pos, double *scratch, cudaStream_t st) {
+  TracerArgs T;
+  T.A = A;
+  T.tr = tracers;
+  T.ntr = ntr;
+  T.pos = pos;
+  const long ncell = (long)A.nz * A.ny * A.nx;
+  const long nfmax = (long)(A.nz + 1) * (A.ny + 1) * (A.nx + 1);
+  T.E = scratch;
+  T.TE = T.E + 10 * ncell;
+  T.TF = T.TE + 2L * ntr * ncell;
+  T.TF2 = T.TF + (long)ntr * nfmax;
+  T.UN = T.TF2 + (long)ntr * nfmax;
+  if (ord == 5) {
+    if (dir == 0) return run<5, 0>(T, st);
+    if (dir == 1) return run<5, 1>(T, st);
+    return run<5, 2>(T, st);
+  }
+  if (dir == 0) return run<9, 0>(T, st);
+  if (dir == 1) return run<9, 1>(T, st);
+  return run<9, 2>(T, st);
+}
+
+long tracer_scratch_doubles(int nx, int ny, int nz, int ntr) {
+  const long ncell = (long)nz * ny * nx;
+  const long nfmax = (long)(nz + 1) * (ny + 1) * (nx + 1);
+  return 10 * ncell + 2L * ntr * ncell + 2L * ntr * nfmax + nfmax;
+}
+
+cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes) {
+  if (ord == 5) return cudaMemcpyToSymbol(c_tab5, tab, bytes);
+  return cudaMemcpyToSymbol(c_tab9, tab, bytes);
+}
+
+}  // namespace awfl

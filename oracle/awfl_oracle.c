@@ -93,6 +93,12 @@ struct oracle_ctx {
   /* scratch (Spatial:327-330) */
   oreal *limits; /* (5,2,nz+1,ny+1,nx+1) */
   oreal *flux;   /* (5,nz+1,ny+1,nx+1) */
+  /* tracer transport (Spatial:624-627, 760-809, 826-835, 891-935, 948-955 and the y/z
+   * equivalents): set by oracle_tracer_step for the duration of one call */
+  int ntr;
+  const int *trpos;
+  oreal *tr, *ttend;        /* (ntr,nz+2hs,ny+2hs,nx+2hs), (ntr,nz,ny,nx) */
+  oreal *tlimits, *tflux, *tflux_lim;  /* (ntr,2,...), (ntr,...), (ntr,...) */
 };
 
 /* ---------------------------------------------------------------- indexing */
@@ -281,6 +287,26 @@ static void diff_transform(const oracle_ctx *c, ader_t *A, int dir, oreal dxd, i
     for (int ii = 0; ii < NGLL; ii++) A->g[kt][ii] /= 2;
 }
 
+/* diffTransformTracer (Spatial:2095-2125): rho*tracer time derivatives from the density
+ * and normal-momentum series r, ru; rut is the normal tracer flux series. */
+static void diff_transform_tracer(const oracle_ctx *c, oreal r[NADER][NGLL], oreal ru[NADER][NGLL],
+                                  oreal rt[NADER][NGLL], oreal rut[NADER][NGLL], oreal dxd) {
+  for (int kt = 1; kt < NADER; kt++)
+    for (int ii = 0; ii < NGLL; ii++) rut[kt][ii] = 0;
+  for (int kt = 0; kt < NADER - 1; kt++) {
+    for (int ii = 0; ii < NGLL; ii++) {
+      oreal df_dx = 0;
+      for (int s = 0; s < NGLL; s++) df_dx += c->deriv[s][ii] * rut[kt][s];
+      rt[kt + 1][ii] = -df_dx / dxd / (kt + 1.);
+    }
+    for (int ii = 0; ii < NGLL; ii++) {
+      oreal tot = 0;
+      for (int ir = 0; ir <= kt + 1; ir++) tot += ru[ir][ii] * rt[kt + 1 - ir][ii] - r[ir][ii] * rut[kt + 1 - ir][ii];
+      rut[kt + 1][ii] = tot / r[0][ii];
+    }
+  }
+}
+
 /* compute_timeAvg_edges (Spatial:2153-2177): edge points only. */
 static void time_avg_edges(oreal dts[NADER][NGLL], oreal dt) {
   oreal dtmult = dt;
@@ -365,8 +391,38 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
   const int nm = 1 + dir;
   const oreal dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
   const int bc = c->bc[dir];
+  const int ntr = c->ntr;
+  oreal *tr = c->tr;
+
+  /* tracers /= (rho' + rho_h) inside the domain (Spatial:624-627, 985-990, 1342-1347) */
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        for (int l = 0; l < ntr; l++)
+          tr[sidx(c, l, HS + k, HS + j, HS + i)] /= (st[sidx(c, idR, HS + k, HS + j, HS + i)] + c->hyDensCells[HS + k]);
 
   fill_halos(c, st, dir);
+  /* tracer halos: periodic copy, or the edge cell at a wall (Spatial:637-642, 655-660 and
+   * the y/z equivalents) */
+  if (ntr > 0) {
+    const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    const int na = dir == 2 ? ny : nz, nb = dir == 0 ? ny : nx;
+    for (int a = 0; a < na; a++)
+      for (int b2 = 0; b2 < nb; b2++)
+        for (int h = 0; h < HS; h++)
+          for (int l = 0; l < ntr; l++) {
+#define TIDX(p) (dir == 0 ? sidx(c, l, HS + a, HS + b2, (p)) : (dir == 1 ? sidx(c, l, HS + a, (p), HS + b2) : sidx(c, l, (p), HS + a, HS + b2)))
+            if (bc == BC_PERIODIC) {
+              tr[TIDX(h)] = tr[TIDX(n + h)];
+              tr[TIDX(HS + n + h)] = tr[TIDX(HS + h)];
+            } else {
+              tr[TIDX(h)] = tr[TIDX(HS)];
+              tr[TIDX(HS + n + h)] = tr[TIDX(HS + n - 1)];
+            }
+#undef TIDX
+          }
+  }
 
   /* Reconstruct + ADER + time average; store cell-edge states (K2). */
 #pragma omp parallel for collapse(3)
@@ -417,11 +473,36 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
             for (int ii = 0; ii < NGLL; ii++) A.src[kt][ii] = srcfill;
         }
         if (NADER > 1) diff_transform(c, &A, dir, dxd, k);
+        oreal rser[NADER][NGLL], ruser[NADER][NGLL]; /* "still exist and are computed" (Spatial:762) */
+        memcpy(rser, A.q[idR], sizeof rser);
+        memcpy(ruser, A.q[nm], sizeof ruser);
         for (int v = 0; v < NUMSTATE; v++) time_avg_edges(A.q[v], dt);
         int kl = k, jl = j, il = i, kr = k, jr = j, ir = i;
         if (dir == 0) ir = i + 1;
         else if (dir == 1) jr = j + 1;
         else kr = k + 1;
+        /* tracers (Spatial:760-809, 1123-1170, 1500-1548) */
+        for (int l = 0; l < ntr; l++) {
+          oreal rt[NADER][NGLL], rut[NADER][NGLL], sten[ORD];
+          for (int s2 = 0; s2 < ORD; s2++) {
+            if (dir == 0) sten[s2] = tr[sidx(c, l, HS + k, HS + j, i + s2)];
+            else if (dir == 1) sten[s2] = tr[sidx(c, l, HS + k, j + s2, HS + i)];
+            else sten[s2] = tr[sidx(c, l, k + s2, HS + j, HS + i)];
+          }
+          reconstruct_gll(c, sten, rt[0], c->weno_scalars);
+          for (int ii = 0; ii < NGLL; ii++) rt[0][ii] *= rser[0][ii];
+          if (c->trpos[l])
+            for (int ii = 0; ii < NGLL; ii++) rt[0][ii] = dmax(0., rt[0][ii]);
+          for (int ii = 0; ii < NGLL; ii++) rut[0][ii] = rt[0][ii] * ruser[0][ii] / rser[0][ii];
+          if (NADER > 1) diff_transform_tracer(c, rser, ruser, rt, rut, dxd);
+          time_avg_edges(rt, dt);
+          if (c->trpos[l]) {
+            rt[0][0] = dmax(0., rt[0][0]);
+            rt[0][NGLL - 1] = dmax(0., rt[0][NGLL - 1]);
+          }
+          c->tlimits[lidx(c, l, 1, kl, jl, il)] = rt[0][0];
+          c->tlimits[lidx(c, l, 0, kr, jr, ir)] = rt[0][NGLL - 1];
+        }
         for (int v = 0; v < NUMSTATE; v++) {
           c->limits[lidx(c, v, 1, kl, jl, il)] = A.q[v][0][0];
           c->limits[lidx(c, v, 0, kr, jr, ir)] = A.q[v][0][NGLL - 1];
@@ -456,6 +537,20 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
           } else {
             c->limits[i0] = c->limits[i0s1];
             c->limits[in] = c->limits[ins0];
+          }
+        }
+    for (int a = 0; a < na; a++) /* tracers (Spatial:826-835, 1186-1195, 1567-1576) */
+      for (int b = 0; b < nb; b++)
+        for (int l = 0; l < ntr; l++) {
+#define LIM(side, f) (dir == 0 ? lidx(c, l, side, a, b, f) : (dir == 1 ? lidx(c, l, side, a, f, b) : lidx(c, l, side, f, a, b)))
+          long i0 = LIM(0, 0), in = LIM(1, n), i0s1 = LIM(1, 0), ins0 = LIM(0, n);
+#undef LIM
+          if (bc == BC_PERIODIC) {
+            c->tlimits[i0] = c->tlimits[ins0];
+            c->tlimits[in] = c->tlimits[i0s1];
+          } else {
+            c->tlimits[i0] = c->tlimits[i0s1];
+            c->tlimits[in] = c->tlimits[ins0];
           }
         }
   }
@@ -521,7 +616,48 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
             if (k == nz) F[idW] -= c->hyPressureGLL[(nz - 1) * NGLL + NGLL - 1];
           }
           for (int l = 0; l < 5; l++) c->flux[fidx(c, l, k, j, i)] = F[l];
+          /* upwind tracer fluxes (Spatial:891-901, 1249-1259, 1633-1643) */
+          for (int l = 0; l < ntr; l++) {
+            if (vn > 0) c->tflux[fidx(c, l, k, j, i)] = F[0] * c->tlimits[lidx(c, l, 0, k, j, i)] / qL[0];
+            else c->tflux[fidx(c, l, k, j, i)] = F[0] * c->tlimits[lidx(c, l, 1, k, j, i)] / qR[0];
+          }
         }
+  }
+
+  /* Positivity limiter of the tracer fluxes (Spatial:904-935, 1262-1293, 1646-1677). Each
+   * face's flux is scaled by the factor of its upwind cell, computed from that cell's
+   * UNSCALED face fluxes: the reference scales tracerFlux in place while other iterations
+   * read it (a data race under its parallel_for), so the read-before-any-scaling order is
+   * taken. The y branch for v < 0 reads the faces along y (the reference indexes
+   * tracerFlux(tr,k,j,ind_j) there, Spatial:1285-1286, with j and i swapped), and a
+   * periodic z wraps like x and y (the reference reads outside the array there). */
+  if (ntr > 0) {
+    const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
+    const oreal eps = 1.e-10;
+    int ek = nz + (dir == 2), ej = ny + (dir == 1), ei = nx + (dir == 0);
+#pragma omp parallel for collapse(3)
+    for (int k = 0; k < ek; k++)
+      for (int j = 0; j < ej; j++)
+        for (int i = 0; i < ei; i++)
+          for (int l = 0; l < ntr; l++) {
+            long fi = fidx(c, l, k, j, i);
+            oreal F = c->tflux[fi];
+            c->tflux_lim[fi] = F;
+            if (!c->trpos[l]) continue;
+            oreal un = 0.5 * (c->limits[lidx(c, nm, 0, k, j, i)] + c->limits[lidx(c, nm, 1, k, j, i)]);
+            int f = dir == 0 ? i : (dir == 1 ? j : k);
+            int ind;
+            if (un > 0) { ind = f - 1; if (ind == -1) ind = n - 1; }
+            else if (un < 0) { ind = f; if (ind == n) ind = 0; }
+            else continue;
+            int ck = dir == 2 ? ind : k, cj = dir == 1 ? ind : j, ci = dir == 0 ? ind : i;
+            int fk1 = dir == 2 ? ind + 1 : k, fj1 = dir == 1 ? ind + 1 : j, fi1 = dir == 0 ? ind + 1 : i;
+            oreal f1 = dmin(c->tflux[fidx(c, l, ck, cj, ci)], 0.);
+            oreal f2 = dmax(c->tflux[fidx(c, l, fk1, fj1, fi1)], 0.);
+            oreal fluxOut = dt * (f2 - f1) / dxd;
+            oreal dens = st[sidx(c, idR, HS + ck, HS + cj, HS + ci)] + c->hyDensCells[HS + ck];
+            c->tflux_lim[fi] = F * dmin(1., tr[sidx(c, l, HS + ck, HS + cj, HS + ci)] * dens / (fluxOut + eps));
+          }
   }
 
   /* Flux divergence (K5: Spatial:940-956, 1298-1310, 1680-1696). */
@@ -543,6 +679,56 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
             else tend[ti] += -(fr - fl) / dxd;
           }
         }
+  /* tracer tendencies, and density multiplied back onto the tracers (Spatial:948-955,
+   * 1302-1309, 1688-1695) */
+#pragma omp parallel for collapse(3)
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        for (int l = 0; l < ntr; l++) {
+          oreal fl = c->tflux_lim[fidx(c, l, k, j, i)];
+          oreal fr = dir == 0 ? c->tflux_lim[fidx(c, l, k, j, i + 1)]
+                    : (dir == 1 ? c->tflux_lim[fidx(c, l, k, j + 1, i)] : c->tflux_lim[fidx(c, l, k + 1, j, i)]);
+          c->ttend[tidx(c, l, k, j, i)] = -(fr - fl) / dxd;
+          tr[sidx(c, l, HS + k, HS + j, HS + i)] *= (st[sidx(c, idR, HS + k, HS + j, HS + i)] + c->hyDensCells[HS + k]);
+        }
+}
+
+/* Temporal_ader::timeStep (Temporal_ader.h:48-72) with the tracer transport compiled in:
+ * per split, computeTendencies on state and tracers, then state += dt*tend and
+ * tracers += dt*tracerTend. sim2d's y split zeroes both tendencies (Spatial:572-575). */
+void oracle_time_step_tracers(oracle_ctx *c, oreal *st, oreal *tr, int ntr, const int *pos, oreal dt) {
+  const long nf = (long)(c->nz + 1) * (c->ny + 1) * (c->nx + 1);
+  const long ncell = (long)c->nz * c->ny * c->nx;
+  oreal *tend = (oreal *)calloc((size_t)NUMSTATE * ncell, sizeof(oreal));
+  c->ntr = ntr;
+  c->trpos = pos;
+  c->tr = tr;
+  c->ttend = (oreal *)calloc((size_t)ntr * ncell + 1, sizeof(oreal));
+  c->tlimits = (oreal *)calloc((size_t)ntr * 2 * nf + 1, sizeof(oreal));
+  c->tflux = (oreal *)calloc((size_t)ntr * nf + 1, sizeof(oreal));
+  c->tflux_lim = (oreal *)calloc((size_t)ntr * nf + 1, sizeof(oreal));
+  for (int split = 0; split < 3; split++) {
+    int dir;
+    if (c->dimswitch) dir = split;
+    else dir = 2 - split;
+    if (dir == 1 && c->sim2d) {
+      memset(tend, 0, sizeof(oreal) * NUMSTATE * ncell);
+      memset(c->ttend, 0, sizeof(oreal) * ntr * ncell);
+    } else {
+      oracle_compute_tendencies_dir(c, st, tend, dt, dir);
+    }
+    oracle_apply(c, st, tend, dt);
+    for (int k = 0; k < c->nz; k++)
+      for (int j = 0; j < c->ny; j++)
+        for (int i = 0; i < c->nx; i++)
+          for (int l = 0; l < ntr; l++)
+            tr[sidx(c, l, HS + k, HS + j, HS + i)] += dt * c->ttend[tidx(c, l, k, j, i)];
+  }
+  c->dimswitch = !c->dimswitch;
+  free(tend); free(c->ttend); free(c->tlimits); free(c->tflux); free(c->tflux_lim);
+  c->ntr = 0; c->trpos = NULL; c->tr = NULL; c->ttend = NULL;
+  c->tlimits = c->tflux = c->tflux_lim = NULL;
 }
 
 /* Spatial:565-594 */

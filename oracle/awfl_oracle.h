@@ -63,6 +63,12 @@ void oracle_compute_tendencies(oracle_ctx *c, oreal *state, oreal *tend, oreal d
 void oracle_apply(const oracle_ctx *c, oreal *state, const oreal *tend, oreal dt);
 /* One full time step: 3 splits (Temporal_ader.h:48-72). */
 void oracle_time_step(oracle_ctx *c, oreal *state, oreal dt);
+/* The same step with the reference's tracer transport compiled in (its code under
+ * #ifndef NO_TRACERS, Spatial...h:624-955 and the y/z equivalents; the reference itself
+ * defines NO_TRACERS, Spatial...h:10). tracers: (ntr, nz+2hs, ny+2hs, nx+2hs) rho*q;
+ * pos[l] != 0 marks a positive-definite tracer (limited). Decisions where the reference's
+ * code is not well defined are stated at the limiter. */
+void oracle_time_step_tracers(oracle_ctx *c, oreal *state, oreal *tracers, int ntr, const int *pos, oreal dt);
 int oracle_get_dimswitch(const oracle_ctx *c);
 void oracle_set_dimswitch(oracle_ctx *c, int v);
 

@@ -95,6 +95,7 @@ class Oracle(_Grid):
             L.oracle_set_bubble.argtypes = [_VP, _DP, _I] + [_D] * 8
             L.oracle_add_theta_noise.argtypes = [_VP, _DP, ctypes.c_ulonglong, _D]
             L.oracle_init_tracers.argtypes = [_VP, _DP, _I]
+            L.oracle_time_step_tracers.argtypes = [_VP, _DP, _DP, _I, ctypes.POINTER(_I), _D]
             L.oracle_compute_dt.restype = _D
             L.oracle_compute_dt.argtypes = [_VP, _DP, _D]
             L.oracle_compute_tendencies_dir.argtypes = [_VP, _DP, _DP, _D, _I]
@@ -141,6 +142,13 @@ class Oracle(_Grid):
     def init_tracers(self, tr):
         """Spatial::initTracers on tr (ntr, nz+2hs, ny+2hs, nx+2hs)."""
         self.L.oracle_init_tracers(self.h, _ptr(tr), tr.shape[0])
+
+    def time_step_tracers(self, st, tr, dt, pos=None):
+        """One step of state and tracers with the reference's tracer code compiled in."""
+        n = tr.shape[0]
+        pos = [1] * n if pos is None else pos
+        flags = (_I * max(n, 1))(*[int(bool(p)) for p in pos])
+        self.L.oracle_time_step_tracers(self.h, _ptr(st), _ptr(tr), n, flags, dt)
 
     def compute_dt(self, st, cfl=0.8):
         return self.L.oracle_compute_dt(self.h, _ptr(st), cfl)
