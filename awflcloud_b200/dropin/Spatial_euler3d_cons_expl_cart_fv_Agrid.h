@@ -19,8 +19,12 @@
 //    (Spatial:1778-1783); both are here on the device (awfl_init_tracers,
 //    awfl_write_netcdf_tracers; tracers are FP64 for either precision, halos zero). Their
 //    tendencies are zero, so they stay constant (the reference adds an uninitialised
-//    tendency array to them, Temporal_ader.h:67-69).
-//  * Optional extra YAML keys (absent = reference behaviour): precision (fp64 | fp32),
+//    tendency array to them, Temporal_ader.h:67-69) -- unless the extra YAML key
+//    tracer_transport is true (FP64 only): the reference's compiled-out tracer code then
+//    runs (awfl_tracer_split before each split's state sweep; addTracer's posDef flags
+//    select the limited tracers).
+//  * Optional extra YAML keys (absent = reference behaviour): tracer_transport (bool),
+//    precision (fp64 | fp32),
 //    device, bubble (cosine | linear) with bubble_x0/y0/z0, bubble_radius (or
 //    bubble_xrad/yrad/zrad), bubble_amp, bubble_pwr; noise_amp, noise_seed, noise_dist
 //    (uniform | normal; noise_amp is then the standard deviation).
@@ -161,6 +165,7 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
   // B200 library context and the optional extensions read from the YAML file
   awfl_ctx *ctx = nullptr;
   int precision = AWFL_FP64;
+  bool tracerTransport = false;  // YAML tracer_transport: run the tracer code
   int device = 0;
   awfl_init_spec initSpec{};
 
@@ -248,6 +253,7 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
       else endrun("ERROR: precision must be fp64 or fp32");
     }
     if (config["device"]) device = config["device"].as<int>();
+    if (config["tracer_transport"]) tracerTransport = config["tracer_transport"].as<bool>();
     initSpec = awfl_init_spec{};
     initSpec.kind = AWFL_INIT_REFERENCE;
     if (config["bubble"]) {
@@ -329,6 +335,21 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
   // kernel; the same results, without a tendency array.
   void computeAndApplyTendencies(StateArr &state, real dt, int splitIndex) {
     const int dir = dirOf(splitIndex);
+    awfl_dropin::check(awfl_split(ctx, state.data(), dt, dir, nullptr), ctx, "computeAndApplyTendencies");
+    if (splitIndex == numSplit() - 1) dimSwitch = !dimSwitch;
+  }
+
+  // The same split with the tracers advanced first (tracer_transport: true), from the
+  // pre-split state: awfl_tracer_split then the fused state split.
+  void computeAndApplyTendencies(StateArr &state, TracerArr &tracers, real dt, int splitIndex) {
+    const int dir = dirOf(splitIndex);
+    if (tracerTransport && numTracers > 0 && tracers.initialized() && tracers.totElems() > 0) {
+      std::vector<int> pos(numTracers);
+      for (int t = 0; t < numTracers; t++) pos[t] = tracerPosVect[t] ? 1 : 0;
+      awfl_dropin::check(awfl_tracer_split(ctx, state.data(), static_cast<double *>(tracers.data()), numTracers,
+                                           pos.data(), dt, dir, nullptr),
+                         ctx, "tracer transport");
+    }
     awfl_dropin::check(awfl_split(ctx, state.data(), dt, dir, nullptr), ctx, "computeAndApplyTendencies");
     if (splitIndex == numSplit() - 1) dimSwitch = !dimSwitch;
   }

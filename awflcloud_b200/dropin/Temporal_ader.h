@@ -4,8 +4,8 @@
 // timeStep() runs the three directional splits (Temporal_ader.h:48-72); each split is the
 // spatial operator's computeTendencies followed by the apply, executed as one fused kernel
 // (Spatial::computeAndApplyTendencies), which gives the same results as the two calls.
-// Tracer tendencies are zero (tracer transport is not part of this build), so tracers
-// are left unchanged.
+// Tracers are left unchanged, as the reference's are (it compiles their transport out),
+// unless the YAML key tracer_transport is true: then each split advances them first.
 #pragma once
 
 #include "const.h"
@@ -36,9 +36,8 @@ template <class Spatial> class Temporal_ader {
   }
 
   void timeStep(StateArr &stateArr, TracerArr &tracerArr, real dt) {
-    (void)tracerArr;
     for (int spl = 0; spl < spaceOp.numSplit(); spl++) {
-      spaceOp.computeAndApplyTendencies(stateArr, dt, spl);
+      spaceOp.computeAndApplyTendencies(stateArr, tracerArr, dt, spl);
     }
   }
 

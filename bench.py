@@ -21,7 +21,8 @@ the 512x512x128 precision configuration (`precision`) and the same grid at ord 9
 than the 126 MB L2, so no flush is needed between steps. N > 1 runs N independent
 replicas (one grid per GPU, no collective): the single-domain path has no exchange step.
 
-Printed on rank 0: one JSON line (see DESIGN.md for every key).
+Printed on rank 0: one JSON line; `tracers` adds the cost of the tracer transport (FP64,
+three tracers) on the same grid.
 """
 from __future__ import annotations
 
@@ -67,7 +68,8 @@ def parse():
     ap.add_argument("--ens-steps", type=int, default=50)
     ap.add_argument("--no-precision", action="store_true", help="skip the 512x512x128 precision leg")
     ap.add_argument("--no-ord9", action="store_true", help="skip the ord-9 leg (256x256x128, ngll 5)")
-    ap.add_argument("--only", choices=["adjoint", "ensemble", "precision", "ord9"],
+    ap.add_argument("--no-tracers", action="store_true", help="skip the tracer-transport leg")
+    ap.add_argument("--only", choices=["adjoint", "ensemble", "precision", "ord9", "tracers"],
                     help="run only that leg and print its JSON object (profiling aid)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 comparison arm and the 100-step accuracy check")
@@ -381,6 +383,44 @@ def ord9_leg(a, local):
             "rel_l2_fp32_vs_fp64_after_100_steps": dict(zip(["rho", "rho_u", "rho_v", "rho_w", "rho_theta"], errs))}
 
 
+def tracers_leg(a, local, ntr=3, steps=5, warmup=2):
+    """Tracer transport (the reference's compiled-out tracer code, built in): the FP64 path on
+    the main grid with the driver's three positive-definite tracers, awfl_step_tracers vs
+    awfl_step, CUDA events on the launching stream."""
+    import torch
+    from awflcloud_b200 import capi
+    c = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=capi.FP64, device=local)
+    st = c.new_state()
+    c.init_state(st, kind=capi.INIT_BUBBLE, noise_amp=0.01)
+    tr = c.new_tracers(ntr)
+    c.init_tracers(tr)
+    dt = c.cfl(st, cfl_for(a.ord))
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_tr = timed(lambda: c.step_tracers(st, tr, dt))
+    ms_plain = timed(lambda: c.step(st, dt))
+    cells = a.nx * a.ny * a.nz
+    return {"workload": "%s, FP64, %d positive-definite tracers (uniform, theta, block)" % (workload_name(a), ntr),
+            "steps": steps, "warmup": warmup, "ms_per_step_with_tracers": round(ms_tr, 4),
+            "ms_per_step_without": round(ms_plain, 4), "tracer_ms_per_step": round(ms_tr - ms_plain, 4),
+            "value": round(cells / (ms_tr * 1e-3) / 1e6, 3), "unit": "Mcell-steps/s",
+            "finite": bool(torch.isfinite(tr).all().item()),
+            "note": "per split, four tracer launches before the state sweep; the cell launch "
+                    "recomputes the state's reconstruction + ADER for the density and momentum series"}
+
+
 def adjoint_leg(a, local):
     """Cost of the discrete adjoint against the forward step (FP64, ord 5, 128x128x64,
     same bubble): the forward pass of a gradient computation (adj_steps steps, a state
@@ -580,6 +620,8 @@ def run_ours(a):
             line["precision"] = precision_leg(a, local)
         if not a.no_ord9 and a.ord == 5:
             line["ord9"] = ord9_leg(a, local)
+        if not a.no_tracers:
+            line["tracers"] = tracers_leg(a, local)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(a)
         print(json.dumps(line))
@@ -649,7 +691,7 @@ def main():
         local = int(os.environ.get("LOCAL_RANK", "0"))
         torch.cuda.set_device(local)
         leg = {"adjoint": adjoint_leg, "ensemble": ensemble_leg, "precision": precision_leg,
-               "ord9": ord9_leg}[a.only](a, local)
+               "ord9": ord9_leg, "tracers": tracers_leg}[a.only](a, local)
         print(json.dumps({"leg": a.only, **leg}))
         return 0
     return run_ours(a)

@@ -7,7 +7,7 @@
 // Compiled by oracle/Makefile into oracle/_ref/libawflref_o{ORD}.so. Nothing in the
 // shipped library links it.
 //
-// The only arithmetic written here (not in the reference) is the BASELINE initial-data
+// The only arithmetic written here (not in the reference) is the benchmark initial-data
 // extension: a cosine-squared bubble and seeded white theta noise, both integrated with
 // the same ord^3 GLL quadrature as Spatial...h:428-485.
 #ifdef AWFL_REF_CR_POW

@@ -1,6 +1,6 @@
 """FP32 precision form (perturbation form + Kahan-compensated stage updates).
 
-Bar (north star): relative L2 <= 1e-5 in rho*theta after 100 steps at 256x256x128 against
+Bar: relative L2 <= 1e-5 in rho*theta after 100 steps at 256x256x128 against
 the FP64 path (itself bit-identical to the reference arithmetic, test_parity_gpu.py).
 Smaller grids and every variable are checked as well, with the measured accuracy of
 single precision as the bound.
@@ -116,7 +116,7 @@ def test_fp32_mass_conservation():
 
 
 def test_fp32_full_size_rhotheta_bar():
-    """The north-star bar: 256x256x128, ord 5, 100 steps, rel L2 <= 1e-5 in rho*theta."""
+    """The accuracy bar: 256x256x128, ord 5, 100 steps, rel L2 <= 1e-5 in rho*theta."""
     c64, c32, s64, s32 = pair((256, 256, 128))
     dt = c64.cfl(s64, 0.8)
     for _ in range(100):
