@@ -61,7 +61,7 @@ _SIGS = {
     "awfl_write_netcdf": (_I, [_VP, ctypes.c_char_p, _VP, _D, _VP]),
     "awfl_write_netcdf_fields": (_I, [_VP, ctypes.c_char_p, _DP, _D]),
     "awfl_init_tracers": (_I, [_VP, _VP, _I, _VP]),
-    "awfl_tracer_split": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_I), _D, _I, _VP]),
+    "awfl_split_tracers": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_I), _D, _I, _VP]),
     "awfl_step_tracers": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_I), _D, _VP]),
     "awfl_output_tracer_fields": (_I, [_VP, _VP, _VP, _I, _VP, _VP]),
     "awfl_write_netcdf_tracers": (_I, [_VP, ctypes.c_char_p, _VP, _VP, _I, ctypes.POINTER(ctypes.c_char_p), _D, _VP]),
@@ -319,11 +319,11 @@ class Context:
             raise ValueError("pos needs one flag per tracer")
         return (_I * max(n, 1))(*[int(bool(p)) for p in pos])
 
-    def tracer_split(self, state, tracers, dt, d, pos=None, stream=None):
-        """One split's tracer transport (before that split's state sweep)."""
+    def split_tracers(self, state, tracers, dt, d, pos=None, stream=None):
+        """One split of state and tracers."""
         n = tracers.shape[0]
-        self._check(self.L.awfl_tracer_split(self.h, self._st(state), self._tr(tracers, n), n, self._pos(pos, n),
-                                             dt, d, _stream(stream)))
+        self._check(self.L.awfl_split_tracers(self.h, self._st(state), self._tr(tracers, n), n, self._pos(pos, n),
+                                              dt, d, _stream(stream)))
 
     def step_tracers(self, state, tracers, dt, pos=None, stream=None):
         """One time step of state and tracers (pos: positive-definite flags, default all)."""

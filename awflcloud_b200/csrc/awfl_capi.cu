@@ -52,7 +52,7 @@ struct awfl_ctx {
   double *d_diag = nullptr;
   double *d_out = nullptr;  // output diagnostics (awfl_write_netcdf)
   size_t out_bytes = 0;
-  double *d_trc = nullptr;  // tracer transport scratch (awfl_tracer_split)
+  double *d_trc = nullptr;  // tracer transport scratch (awfl_split_tracers)
   size_t trc_bytes = 0;
   size_t diag_bytes = 0;
   std::string err;
@@ -796,27 +796,28 @@ int awfl_step(awfl_ctx *c, void *d_state, double dt, void *stream) {
   return AWFL_OK;
 }
 
-int awfl_tracer_split(awfl_ctx *c, const void *d_state, double *d_tracers, int ntracers, const int *pos,
-                      double dt, int dir, void *stream) {
+int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
+                       int dir, void *stream) {
   if (!c) return AWFL_ERR_ARG;
   if (fp32(c)) return fail(c, AWFL_ERR_ARG, "tracer transport needs an FP64 context");
   if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
   if (ntracers < 0 || ntracers > 64) return fail(c, AWFL_ERR_ARG, "ntracers must be in [0, 64]");
-  if (ntracers == 0) return AWFL_OK;
+  if (ntracers == 0) return awfl_split(c, d_state, dt, dir, stream);
   if (bad_ptr(d_state) || bad_ptr(d_tracers)) return fail(c, AWFL_ERR_ARG, "state or tracer pointer is NULL or misaligned");
   if (!pos) return fail(c, AWFL_ERR_ARG, "pos (positive-definite flags) is NULL");
   int rc = set_device(c);
   if (rc) return rc;
-  if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendency (Spatial:572-575)
+  if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendencies (Spatial:572-575)
   unsigned long long mask = 0;
   for (int l = 0; l < ntracers; l++)
     if (pos[l]) mask |= 1ull << l;
-  const size_t need = sizeof(double) * (size_t)tracer_scratch_doubles(c->cfg.nx, c->cfg.ny, c->cfg.nz, ntracers);
+  const size_t need =
+      sizeof(double) * (size_t)tracer_scratch_doubles(c->cfg.ord, c->cfg.nx, c->cfg.ny, c->cfg.nz, ntracers);
   rc = ensure_buffer(c, &c->d_trc, &c->trc_bytes, need, "tracer scratch");
   if (rc) return rc;
-  SweepArgs A = sweep_args(c, const_cast<void *>(d_state), nullptr, dt, dir, MODE_TEND);
-  cudaError_t e = launch_tracer_split(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, (cudaStream_t)stream);
-  if (e != cudaSuccess) return cuda_fail(c, e, "tracer_split");
+  SweepArgs A = sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY);
+  cudaError_t e = launch_split_tracers(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "split_tracers");
   return AWFL_OK;
 }
 
@@ -825,9 +826,7 @@ int awfl_step_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracer
   if (!c) return AWFL_ERR_ARG;
   for (int spl = 0; spl < 3; spl++) {
     const int dir = c->dimswitch ? spl : 2 - spl;
-    int rc = awfl_tracer_split(c, d_state, d_tracers, ntracers, pos, dt, dir, stream);
-    if (rc) return rc;
-    rc = awfl_split(c, d_state, dt, dir, stream);
+    int rc = awfl_split_tracers(c, d_state, d_tracers, ntracers, pos, dt, dir, stream);
     if (rc) return rc;
   }
   c->dimswitch = !c->dimswitch;

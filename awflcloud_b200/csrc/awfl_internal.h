@@ -99,11 +99,11 @@ cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t 
 // FP64 sweep that also records level-0 values and edges of every cell into A.tend
 cudaError_t launch_sweep_rec(int ord, int dir, const SweepArgs &A, cudaStream_t st);
 cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes);
-// Tracer transport of the FP64 path (awfl_tracers.cu): one split's tracer update, run
-// before that split's state sweep; scratch holds tracer_scratch_doubles(...) doubles.
-cudaError_t launch_tracer_split(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
-                                unsigned long long pos, double *scratch, cudaStream_t st);
-long tracer_scratch_doubles(int nx, int ny, int nz, int ntr);
+// Tracer transport of the FP64 path (awfl_tracers.cu): one split of state (fused, MODE_APPLY
+// arithmetic of awfl_split) and tracers; scratch holds tracer_scratch_doubles(...) doubles.
+cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
+                                 unsigned long long pos, double *scratch, cudaStream_t st);
+long tracer_scratch_doubles(int ord, int nx, int ny, int nz, int ntr);
 cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes);
 // Adjoint reverse sweeps (awfl_adjrev.cu)
 cudaError_t launch_adjoint_split(int ord, int dir, const adj::SplitArgs &A, int need_edges, int nsm, cudaStream_t st);

@@ -1,13 +1,14 @@
 // Tracer transport of the FP64 path: the reference's tracer code, which it compiles out
-// with NO_TRACERS (Spatial:10), built in. Per directional split, four launches run BEFORE
-// that split's state sweep (they read the pre-split state):
+// with NO_TRACERS (Spatial:10), built in. Per directional split:
 //
-//   tracer_cell_kernel    per cell: the state's reconstruction + ADER (cell_recon, the same
-//                         device function and arithmetic as the state sweep) recording the
-//                         density and normal-momentum series, then per tracer the
-//                         reconstruction of tracer/density, the rho*tracer ADER series
-//                         (diffTransformTracer, Spatial:2095-2125) and its edge time
-//                         average (Spatial:760-809, 1123-1170, 1500-1548)
+//   sweep_kernel<P64Trc>  the state's fused split (the P64 arithmetic, so the state is
+//                         bit-identical to awfl_split's) that also records, per cell, the
+//                         density and normal-momentum ADER series, the time-averaged edge
+//                         states and the pre-split density perturbation
+//   tracer_cell_kernel    per cell and tracer: the reconstruction of tracer/density, the
+//                         rho*tracer ADER series (diffTransformTracer, Spatial:2095-2125)
+//                         along the recorded series and its edge time average
+//                         (Spatial:760-809, 1123-1170, 1500-1548)
 //   tracer_face_kernel    per face: edge BCs (Spatial:826-835), the state's Riemann flux
 //                         (riemann) and the upwind tracer fluxes (Spatial:891-901,
 //                         1249-1259, 1633-1643)
@@ -32,13 +33,60 @@
 
 namespace awfl {
 
+// Recording FP64 policy: the P64 arithmetic plus, per interior cell, the records the
+// tracer kernels read. A.tend points at the record base: R (NG*NG planes of ncell), U
+// (NG*NG), E (10: eL, eR), D (1: the pre-split rho', the stencil centre).
+struct P64Trc : P64 {
+  // the record stores need registers: 3 CTAs per SM at ord 5 instead of the plain sweep's 4
+  static constexpr int min_blocks(int ord) { return ord == 5 ? 3 : 1; }
+  template <int ORD> struct Rec {
+    double *base;
+    long n, cell;
+    int nm;
+    __device__ __forceinline__ void level0(int, int, const double &) const {}
+    template <class Q> __device__ __forceinline__ void series(const Q &q) const {
+      constexpr int NG = OrdTraits<ORD>::NGLL;
+#pragma unroll
+      for (int kt = 0; kt < NG; kt++)
+#pragma unroll
+        for (int ii = 0; ii < NG; ii++) {
+          base[(kt * NG + ii) * n + cell] = q[idR][kt][ii];
+          base[(NG * NG + kt * NG + ii) * n + cell] = q[nm][kt][ii];
+        }
+    }
+  };
+  template <int ORD, int DIR, class S>
+  static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, double (&eL)[5],
+                                               double (&eR)[5], double &src, long cell) {
+    if (cell < 0) {  // the periodic prologue's repeat of cell L-1: recorded in its chunk
+      cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src);
+      return;
+    }
+    constexpr int NG = OrdTraits<ORD>::NGLL;
+    constexpr int HS = (ORD - 1) / 2;
+    const long n = (long)A.nx * A.ny * A.nz;
+    cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell, 1 + DIR});
+    double *e = A.tend + 2L * NG * NG * n;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      e[v * n + cell] = eL[v];
+      e[(5 + v) * n + cell] = eR[v];
+    }
+    e[10 * n + cell] = sten(idR, HS);
+  }
+};
+
+template <int ORD, int DIR> struct PolicyShape<P64Trc, ORD, DIR> : PolicyShape<P64, ORD, DIR> {};
+
 namespace {
 
 struct TracerArgs {
-  SweepArgs A;               // the state (pre-split), background, grid, bc, dt of this split
+  SweepArgs A;               // background, grid, bc, dt of this split (A.state unused)
   double *tr;                // (ntr, nz+2hs, ny+2hs, nx+2hs), rho*tracer
   int ntr;
   unsigned long long pos;    // bit l: tracer l is positive definite (limited)
+  const double *R, *U;       // (ngll*ngll, ncell): recorded density / normal-momentum series
+  const double *D;           // (ncell): recorded pre-split rho'
   double *E;                 // (10, ncell): the state's time-averaged edges eL[5], eR[5]
   double *TE;                // (ntr, 2, ncell): the tracers' edges (left, right)
   double *TF, *TF2, *UN;     // (ntr, nface) unscaled / limited fluxes, (nface) limiter velocity
@@ -87,28 +135,10 @@ __device__ __forceinline__ int halo_src(int p, int n, int bc, bool &wall) {
   return p < 0 ? 0 : n - 1;
 }
 
-template <int ORD> struct SeriesRec {
-  double (*r)[OrdTraits<ORD>::NGLL];
-  double (*ru)[OrdTraits<ORD>::NGLL];
-  int nm;
-  __device__ __forceinline__ void level0(int, int, const double &) const {}
-  template <class Q> __device__ __forceinline__ void series(const Q &q) const {
-    constexpr int NG = OrdTraits<ORD>::NGLL;
-#pragma unroll
-    for (int kt = 0; kt < NG; kt++)
-#pragma unroll
-      for (int ii = 0; ii < NG; ii++) {
-        r[kt][ii] = q[idR][kt][ii];
-        ru[kt][ii] = q[nm][kt][ii];
-      }
-  }
-};
-
 template <int ORD, int DIR>
 __global__ void __launch_bounds__(128) tracer_cell_kernel(TracerArgs T) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
-  constexpr int NM = 1 + DIR;
   const SweepArgs &A = T.A;
   const Geo<DIR> G(A, HS);
   const long ncell = (long)G.nz * G.ny * G.nx;
@@ -117,23 +147,14 @@ __global__ void __launch_bounds__(128) tracer_cell_kernel(TracerArgs T) {
   const int i = (int)(c % G.nx), j = (int)((c / G.nx) % G.ny), k = (int)(c / ((long)G.nx * G.ny));
   const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
   const int n = G.n();
-  // state stencil with the halo rules of Spatial:631-662 (x), 994-1025 (y), 1351-1382 (z)
-  auto sten = [&](int v, int m) -> double {
-    bool wall;
-    const int p = halo_src(p0 - HS + m, n, A.bc, wall);
-    if (wall && v == NM) return 0.0;
-    int kk, jj, ii;
-    G.at(k, j, i, p, kk, jj, ii);
-    return A.state[v * G.sv + G.g(kk, jj, ii)];
-  };
   double rser[NG][NG], ruser[NG][NG];
-  double eL[5], eR[5], src;
-  cell_recon<ORD, DIR>(sten, k, A, eL, eR, src, SeriesRec<ORD>{rser, ruser, NM});
 #pragma unroll
-  for (int v = 0; v < 5; v++) {
-    T.E[v * ncell + c] = eL[v];
-    T.E[(5 + v) * ncell + c] = eR[v];
-  }
+  for (int kt = 0; kt < NG; kt++)
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      rser[kt][ii] = T.R[(kt * NG + ii) * ncell + c];
+      ruser[kt][ii] = T.U[(kt * NG + ii) * ncell + c];
+    }
   const Tables<ORD> &TB = tab<ORD>();
   for (int l = 0; l < T.ntr; l++) {
     const bool posdef = (T.pos >> l) & 1ull;
@@ -144,9 +165,8 @@ __global__ void __launch_bounds__(128) tracer_cell_kernel(TracerArgs T) {
       const int p = halo_src(p0 - HS + m, n, A.bc, wall);
       int kk, jj, ii;
       G.at(k, j, i, p, kk, jj, ii);
-      const long gg = G.g(kk, jj, ii);
       // tracers /= (rho' + rho_h) (Spatial:624-627), then the halo copy
-      s[m] = T.tr[l * G.sv + gg] / (A.state[gg] + A.dens_c[HS + kk]);
+      s[m] = T.tr[l * G.sv + G.g(kk, jj, ii)] / (T.D[G.cell(kk, jj, ii)] + A.dens_c[HS + kk]);
     }
     double rt[NG][NG], rut[NG][NG];
     reconstruct_gll<ORD>(s, rt[0], A.weno_s != 0);
@@ -272,9 +292,8 @@ __global__ void __launch_bounds__(128) tracer_limit_kernel(TracerArgs T, int hs)
       const double f1 = dmin(T.TF[l * nf + G.face(ck, cj, ci)], 0.);
       const double f2 = dmax(T.TF[l * nf + G.face(fk, fj, fi)], 0.);
       const double fluxOut = A.dt * (f2 - f1) / A.dxd;
-      const long gg = G.g(ck, cj, ci);
-      const double dens = A.state[gg] + A.dens_c[hs + ck];
-      const double q = T.tr[l * G.sv + gg] / dens;  // the divided tracer (Spatial:624-627)
+      const double dens = T.D[G.cell(ck, cj, ci)] + A.dens_c[hs + ck];
+      const double q = T.tr[l * G.sv + G.g(ck, cj, ci)] / dens;  // the divided tracer (Spatial:624-627)
       out = F * dmin(1., q * dens / (fluxOut + eps));
     }
     T.TF2[l * nf + f] = out;
@@ -296,7 +315,7 @@ __global__ void __launch_bounds__(128) tracer_update_kernel(TracerArgs T, int hs
   G.at(k, j, i, p + 1, rk, rj, ri);
   const long fl = G.face(k, j, i), fr = G.face(rk, rj, ri);
   const long gg = G.g(k, j, i);
-  const double dens = A.state[gg] + A.dens_c[hs + k];
+  const double dens = T.D[c] + A.dens_c[hs + k];
   // halo cell of index h along DIR (state offset)
   auto halo = [&](int h) -> long {
     int kk, jj, ii;
@@ -328,6 +347,8 @@ cudaError_t run(const TracerArgs &T, cudaStream_t st) {
   const long ncell = (long)A.nz * A.ny * A.nx;
   const long nf = (long)(A.nz + (DIR == 2)) * (A.ny + (DIR == 1)) * (A.nx + (DIR == 0));
   const unsigned gc = (unsigned)((ncell + 127) / 128), gf = (unsigned)((nf + 127) / 128);
+  cudaError_t e = launch_sweep_t<P64Trc, ORD, DIR>(A, st);  // state split + records
+  if (e != cudaSuccess) return e;
   tracer_cell_kernel<ORD, DIR><<<gc, 128, 0, st>>>(T);
   tracer_face_kernel<DIR, NG><<<gf, 128, 0, st>>>(T, HS);
   tracer_limit_kernel<DIR><<<gf, 128, 0, st>>>(T, HS);
@@ -337,17 +358,23 @@ cudaError_t run(const TracerArgs &T, cudaStream_t st) {
 
 }  // namespace
 
-cudaError_t launch_tracer_split(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
-                                unsigned long long pos, double *scratch, cudaStream_t st) {
+cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &Ain, double *tracers, int ntr,
+                                 unsigned long long pos, double *scratch, cudaStream_t st) {
+  const int ng = ord == 5 ? 3 : 5;
+  const long ncell = (long)Ain.nz * Ain.ny * Ain.nx;
+  const long nfmax = (long)(Ain.nz + 1) * (Ain.ny + 1) * (Ain.nx + 1);
   TracerArgs T;
-  T.A = A;
+  T.A = Ain;
+  T.A.tend = scratch;  // the recording sweep's record base
+  T.A.mode = MODE_APPLY;
   T.tr = tracers;
   T.ntr = ntr;
   T.pos = pos;
-  const long ncell = (long)A.nz * A.ny * A.nx;
-  const long nfmax = (long)(A.nz + 1) * (A.ny + 1) * (A.nx + 1);
-  T.E = scratch;
-  T.TE = T.E + 10 * ncell;
+  T.R = scratch;
+  T.U = scratch + (long)ng * ng * ncell;
+  T.E = scratch + 2L * ng * ng * ncell;
+  T.D = T.E + 10 * ncell;
+  T.TE = T.E + 11 * ncell;
   T.TF = T.TE + 2L * ntr * ncell;
   T.TF2 = T.TF + (long)ntr * nfmax;
   T.UN = T.TF2 + (long)ntr * nfmax;
@@ -361,10 +388,11 @@ cudaError_t launch_tracer_split(int ord, int dir, const SweepArgs &A, double *tr
   return run<9, 2>(T, st);
 }
 
-long tracer_scratch_doubles(int nx, int ny, int nz, int ntr) {
+long tracer_scratch_doubles(int ord, int nx, int ny, int nz, int ntr) {
+  const int ng = ord == 5 ? 3 : 5;
   const long ncell = (long)nz * ny * nx;
   const long nfmax = (long)(nz + 1) * (ny + 1) * (nx + 1);
-  return 10 * ncell + 2L * ntr * ncell + 2L * ntr * nfmax + nfmax;
+  return (2L * ng * ng + 11) * ncell + 2L * ntr * ncell + 2L * ntr * nfmax + nfmax;
 }
 
 cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes) {

@@ -21,8 +21,8 @@
 //    tendencies are zero, so they stay constant (the reference adds an uninitialised
 //    tendency array to them, Temporal_ader.h:67-69) -- unless the extra YAML key
 //    tracer_transport is true (FP64 only): the reference's compiled-out tracer code then
-//    runs (awfl_tracer_split before each split's state sweep; addTracer's posDef flags
-//    select the limited tracers).
+//    runs (awfl_split_tracers per split; addTracer's posDef flags select the limited
+//    tracers).
 //  * Optional extra YAML keys (absent = reference behaviour): tracer_transport (bool),
 //    precision (fp64 | fp32),
 //    device, bubble (cosine | linear) with bubble_x0/y0/z0, bubble_radius (or
@@ -339,18 +339,19 @@ template <int nTimeDerivs, bool timeAvg, int nAder> class Spatial_euler3d_cons_e
     if (splitIndex == numSplit() - 1) dimSwitch = !dimSwitch;
   }
 
-  // The same split with the tracers advanced first (tracer_transport: true), from the
-  // pre-split state: awfl_tracer_split then the fused state split.
+  // The same split with the tracers advanced too (tracer_transport: true): one
+  // awfl_split_tracers call (the state as awfl_split advances it).
   void computeAndApplyTendencies(StateArr &state, TracerArr &tracers, real dt, int splitIndex) {
     const int dir = dirOf(splitIndex);
     if (tracerTransport && numTracers > 0 && tracers.initialized() && tracers.totElems() > 0) {
       std::vector<int> pos(numTracers);
       for (int t = 0; t < numTracers; t++) pos[t] = tracerPosVect[t] ? 1 : 0;
-      awfl_dropin::check(awfl_tracer_split(ctx, state.data(), static_cast<double *>(tracers.data()), numTracers,
-                                           pos.data(), dt, dir, nullptr),
+      awfl_dropin::check(awfl_split_tracers(ctx, state.data(), static_cast<double *>(tracers.data()), numTracers,
+                                            pos.data(), dt, dir, nullptr),
                          ctx, "tracer transport");
+    } else {
+      awfl_dropin::check(awfl_split(ctx, state.data(), dt, dir, nullptr), ctx, "computeAndApplyTendencies");
     }
-    awfl_dropin::check(awfl_split(ctx, state.data(), dt, dir, nullptr), ctx, "computeAndApplyTendencies");
     if (splitIndex == numSplit() - 1) dimSwitch = !dimSwitch;
   }
 

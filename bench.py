@@ -417,8 +417,9 @@ def tracers_leg(a, local, ntr=3, steps=5, warmup=2):
             "ms_per_step_without": round(ms_plain, 4), "tracer_ms_per_step": round(ms_tr - ms_plain, 4),
             "value": round(cells / (ms_tr * 1e-3) / 1e6, 3), "unit": "Mcell-steps/s",
             "finite": bool(torch.isfinite(tr).all().item()),
-            "note": "per split, four tracer launches before the state sweep; the cell launch "
-                    "recomputes the state's reconstruction + ADER for the density and momentum series"}
+            "note": "per split: the state's fused sweep recording the density / normal-momentum ADER "
+                    "series, edges and pre-split density, then four tracer launches (cell, face, "
+                    "limiter, update)"}
 
 
 def adjoint_leg(a, local):

@@ -155,21 +155,22 @@ int awfl_write_netcdf_fields_tracers(awfl_ctx *ctx, const char *path, const doub
 
 /* Tracer transport: the reference's tracer code (Spatial:624-955 and the y/z equivalents),
  * which the reference itself compiles out (NO_TRACERS, Spatial:10), built in. FP64
- * contexts only. One split's tracer update for dir = 0/1/2 -- tracers divided by the
- * density, reconstructed, advanced by their ADER series along the state's density and
- * normal momentum, upwind fluxes from the state's Riemann mass flux, the positivity limiter
- * for tracers with pos[l] != 0, then tracers = (tracers/rho)*rho + dt*tend in place. It
- * reads the PRE-split state, so it runs before that split's awfl_split. ntracers <= 64;
- * tracers as for awfl_init_tracers (rho*tracer). The halo cells along dir are left holding
- * tracer/rho, as the reference's in-place halo fill leaves them. Allocates (once per
- * context, grown when ntracers grows) a scratch buffer. Decisions where the reference's
- * code is not well defined: the limiter scales each face by its upwind cell's factor
- * computed from unscaled fluxes; the y limiter's v < 0 branch reads the y faces; a periodic
- * z wraps. */
-int awfl_tracer_split(awfl_ctx *ctx, const void *d_state, double *d_tracers, int ntracers, const int *pos,
-                      double dt, int dir, void *stream);
+ * contexts only. One split (dir = 0/1/2) of state AND tracers: the state exactly as
+ * awfl_split advances it, and the tracers -- divided by the pre-split density,
+ * reconstructed, advanced by their ADER series along the state's density and normal
+ * momentum, upwind fluxes from the state's Riemann mass flux, the positivity limiter for
+ * tracers with pos[l] != 0, then tracers = (tracers/rho)*rho + dt*tend in place.
+ * ntracers <= 64 (0: awfl_split); tracers as for awfl_init_tracers (rho*tracer). The halo
+ * cells along dir are left holding tracer/rho, as the reference's in-place halo fill leaves
+ * them. Allocates (once per context, grown when ntracers grows) a scratch buffer of
+ * (2*ngll^2 + 11 + 2*ntracers) doubles per cell and (2*ntracers + 1) per face. Decisions
+ * where the reference's code is not well defined: the limiter scales each face by its
+ * upwind cell's factor computed from unscaled fluxes; the y limiter's v < 0 branch reads
+ * the y faces; a periodic z wraps. */
+int awfl_split_tracers(awfl_ctx *ctx, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
+                       int dir, void *stream);
 /* One time step with tracers (Temporal_ader::timeStep with the tracer code compiled in):
- * per split in the dimSwitch order, awfl_tracer_split then awfl_split. */
+ * awfl_split_tracers for each split in the dimSwitch order. */
 int awfl_step_tracers(awfl_ctx *ctx, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
                       void *stream);
 

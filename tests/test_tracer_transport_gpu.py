@@ -1,4 +1,4 @@
-"""Tracer transport on the device (awfl_step_tracers / awfl_tracer_split; the reference's
+"""Tracer transport on the device (awfl_step_tracers / awfl_split_tracers; the reference's
 tracer code, compiled out there by NO_TRACERS, built in) against the oracle's restatement
 of the same code: bit for bit, tracers and their halos, for several configurations.
 
@@ -69,7 +69,7 @@ def test_step_tracers_bit_exact(case):
     assert np.abs(got_tr[2] - t0[2])[h:h + nz, h:h + ny, h:h + nx].max() > 1e-6
 
 
-def test_tracer_split_rejects_fp32_and_bad_args():
+def test_split_tracers_rejects_fp32_and_bad_args():
     c = capi.Context(16, 12, 10, precision=capi.FP32)
     st = c.new_state()
     tr = c.new_tracers(2)
