@@ -805,6 +805,9 @@ int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntrace
   if (ntracers == 0) return awfl_split(c, d_state, dt, dir, stream);
   if (bad_ptr(d_state) || bad_ptr(d_tracers)) return fail(c, AWFL_ERR_ARG, "state or tracer pointer is NULL or misaligned");
   if (!pos) return fail(c, AWFL_ERR_ARG, "pos (positive-definite flags) is NULL");
+  const int ext = dir == 0 ? c->cfg.nx : (dir == 1 ? c->cfg.ny : c->cfg.nz);
+  if (ext < c->hs && !(dir == 1 && c->sim2d))
+    return fail(c, AWFL_ERR_ARG, "tracer transport needs at least %d cells along direction %d", c->hs, dir);
   int rc = set_device(c);
   if (rc) return rc;
   if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendencies (Spatial:572-575)

@@ -75,3 +75,21 @@ def test_wrapper_rejects_wrong_buffers_before_any_device_call():
         c.step(torch.zeros((5,) + c.state_shape[1:], dtype=torch.float32), 0.1)  # one plane only, on the CPU
     with pytest.raises(ValueError):
         c.step(torch.zeros(c.state_shape, dtype=torch.float64), 0.1)  # wrong dtype
+
+
+def test_split_tracers_argument_checks_before_any_device_call():
+    """awfl_split_tracers refuses bad arguments on the host: FP32 contexts, more than 64
+    tracers, a NULL flag array, and a direction shorter than the stencil half-width."""
+    import ctypes
+    L = capi.lib()
+    pos = (ctypes.c_int * 2)(1, 1)
+    short = capi.Context(1, 8, 6, bc=("wall", "periodic", "wall"), device=-1)  # periodic is refused at create
+    assert L.awfl_split_tracers(short.h, 8, 8, 2, pos, 0.1, 0, None) == -1
+    assert b"at least 2 cells" in L.awfl_last_error(short.h)
+    c = capi.Context(10, 8, 6, device=-1)
+    assert L.awfl_split_tracers(c.h, 8, 8, 65, pos, 0.1, 0, None) == -1
+    assert L.awfl_split_tracers(c.h, 8, 8, 2, None, 0.1, 0, None) == -1
+    assert L.awfl_split_tracers(c.h, 8, 8, 2, pos, 0.1, 3, None) == -1
+    c32 = capi.Context(10, 8, 6, precision=capi.FP32, device=-1)
+    assert L.awfl_split_tracers(c32.h, 8, 8, 2, pos, 0.1, 0, None) == -1
+    assert b"FP64" in L.awfl_last_error(c32.h)
