@@ -73,8 +73,7 @@ def _stale(target: str, deps) -> bool:
 def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
-    objs = []
-    rebuilt = False
+    objs, cmds = [], []
     for unit, flags in UNITS.items():
         src = os.path.join(SRC, unit)
         if not os.path.exists(src):
@@ -85,10 +84,24 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
-            if verbose:
-                print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
-            rebuilt = True
+            cmds.append(cmd)
+    # the translation units are independent: compile them concurrently
+    from concurrent.futures import ThreadPoolExecutor
+    jobs = max(1, min(len(cmds), os.cpu_count() or 1))
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        results = list(ex.map(run, cmds))
+    for cmd, r in zip(cmds, results):
+        if r.stdout or r.stderr:
+            sys.stdout.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+    rebuilt = bool(cmds)
     if rebuilt or force or _stale(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
         if verbose:

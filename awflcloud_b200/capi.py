@@ -533,8 +533,12 @@ def header_symbols(path=None):
     return sorted(set(re.findall(r"^\s*(?:int|const char \*|void)\s*\*?\s*(awfl_\w+)\s*\(", src, re.M)))
 
 
+PEAK_FP32_PAIRED = 2
+
+
 def measure_fma_peak(precision=FP64, device=0):
-    """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 CUDA-core pipe."""
+    """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 CUDA-core pipe; precision
+    PEAK_FP32_PAIRED measures sm_100's paired FP32 FMA (two lanes per instruction)."""
     out = ctypes.c_double()
     rc = lib().awfl_measure_fma_peak(precision, device, ctypes.byref(out))
     if rc != AWFL_OK:

@@ -227,6 +227,7 @@ int ensure_tables(awfl_ctx *c) {
     std::memcpy(t.deriv, c->deriv.data(), sizeof t.deriv);
     std::memcpy(t.idl, c->idl.data(), sizeof t.idl);
     t.sigma = c->sigma;
+    t.ridl = 1.0 / t.idl[t.HS + 1];
     std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
     e = upload_tables_fp64(5, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adj(5, &t, sizeof t);
@@ -241,6 +242,7 @@ int ensure_tables(awfl_ctx *c) {
     std::memcpy(t.deriv, c->deriv.data(), sizeof t.deriv);
     std::memcpy(t.idl, c->idl.data(), sizeof t.idl);
     t.sigma = c->sigma;
+    t.ridl = 1.0 / t.idl[t.HS + 1];
     std::memcpy(t.wts, c->wts_ngll.data(), sizeof t.wts);
     e = upload_tables_fp64(9, &t, sizeof t);
     if (e == cudaSuccess) e = upload_tables_adj(9, &t, sizeof t);
@@ -344,6 +346,7 @@ SweepArgs sweep_args(awfl_ctx *c, void *state, void *tend, double dt, int dir, i
   A.bc = dir == 0 ? c->cfg.bc_x : (dir == 1 ? c->cfg.bc_y : c->cfg.bc_z);
   A.weno_s = c->cfg.weno_scalars; A.weno_w = c->cfg.weno_winds; A.sim2d = c->sim2d; A.mode = mode;
   A.dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+  A.rdxd = 1.0 / A.dxd;
   A.dt = dt;
   A.plane = 0;
   A.dens_c = c->d_dens_c; A.denstheta_c = c->d_denstheta_c;
@@ -968,19 +971,20 @@ int awfl_get_background(const awfl_ctx *c, double *dens_c, double *pres_c, doubl
 }
 
 int awfl_selftest_pow(const void *d_x, double y, void *d_out, long n, int mode, void *stream) {
-  if (n < 0 || mode < 0 || mode > 2 || (n > 0 && (bad_ptr(d_x) || bad_ptr(d_out)))) return AWFL_ERR_ARG;
+  if (n < 0 || mode < 0 || mode > 4 || (n > 0 && (bad_ptr(d_x) || bad_ptr(d_out)))) return AWFL_ERR_ARG;
   cudaError_t e = launch_selftest_pow((const double *)d_x, y, (double *)d_out, n, mode, (cudaStream_t)stream);
   return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
 }
 
 int awfl_measure_fma_peak(int precision, int device, double *tflops) {
-  if (!tflops || (precision != AWFL_FP64 && precision != AWFL_FP32)) return AWFL_ERR_ARG;
+  if (!tflops || (precision != AWFL_FP64 && precision != AWFL_FP32 && precision != AWFL_PEAK_FP32_PAIRED))
+    return AWFL_ERR_ARG;
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return AWFL_ERR_CUDA;
   int nsm = 148;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) nsm = prop.multiProcessorCount;
-  e = run_fma_peak(precision == AWFL_FP32, nsm, tflops);
+  e = run_fma_peak(precision == AWFL_FP64 ? 0 : (precision == AWFL_FP32 ? 1 : 2), nsm, tflops);
   return e == cudaSuccess ? AWFL_OK : AWFL_ERR_CUDA;
 }
 

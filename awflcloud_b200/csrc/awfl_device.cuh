@@ -11,6 +11,7 @@
 
 #include <cstdint>
 
+#include "awfl_div.cuh"
 #include "awfl_internal.h"
 #include "awfl_pow.cuh"
 #include "awfl_tv.h"
@@ -59,8 +60,9 @@ __device__ __forceinline__ void weno_coefs(const Sc (&u)[ORD], Sc (&aw)[ORD]) {
   for (int i = 0; i < HS + 1; i++)
 #pragma unroll
     for (int ii = 0; ii < HS + 1; ii++) a[HS + 1][ii] -= T.idl[i] * a[i][ii];
+  const Rcp<double> ridl = rcp_known(T.idl[HS + 1], T.ridl);
 #pragma unroll
-  for (int ii = 0; ii < ORD; ii++) a[HS + 1][ii] /= T.idl[HS + 1];
+  for (int ii = 0; ii < ORD; ii++) a[HS + 1][ii] = divd(a[HS + 1][ii], ridl);
   Sc tv[HS + 2];
 #pragma unroll
   for (int i = 0; i < HS + 1; i++) tv[i] = tv_eval<HS + 1>(a[i]);
@@ -68,7 +70,7 @@ __device__ __forceinline__ void weno_coefs(const Sc (&u)[ORD], Sc (&aw)[ORD]) {
   Sc lo_avg = 0.;
 #pragma unroll
   for (int i = 0; i < HS + 1; i++) lo_avg += tv[i];
-  lo_avg /= HS + 1;
+  lo_avg = divk(lo_avg, HS + 1);
   tv[HS + 1] = lo_avg + (tv[HS + 1] - lo_avg) * T.sigma;
   Sc wts[HS + 2];
 #pragma unroll
@@ -78,8 +80,9 @@ __device__ __forceinline__ void weno_coefs(const Sc (&u)[ORD], Sc (&aw)[ORD]) {
     Sc sum = 0.;
 #pragma unroll
     for (int i = 0; i < HS + 2; i++) sum += wts[i];
+    const Rcp<Sc> rs = make_rcp<Sc>(sum + eps);
 #pragma unroll
-    for (int i = 0; i < HS + 2; i++) wts[i] /= (sum + eps);
+    for (int i = 0; i < HS + 2; i++) wts[i] = divr(wts[i], rs);
   }
   // map_weights (Weno:12-17)
 #pragma unroll
@@ -91,8 +94,9 @@ __device__ __forceinline__ void weno_coefs(const Sc (&u)[ORD], Sc (&aw)[ORD]) {
     Sc sum = 0.;
 #pragma unroll
     for (int i = 0; i < HS + 2; i++) sum += wts[i];
+    const Rcp<Sc> rs = make_rcp<Sc>(sum + eps);
 #pragma unroll
-    for (int i = 0; i < HS + 2; i++) wts[i] /= (sum + eps);
+    for (int i = 0; i < HS + 2; i++) wts[i] = divr(wts[i], rs);
   }
 #pragma unroll
   for (int i = 0; i < ORD; i++) aw[i] = 0.;
@@ -184,13 +188,16 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
   Sc f[4][NA][NG];
   Sc g[NA][NG];
   Sc srcfill = 0;
+  Rcp<Sc> rr[NG];  // the density of each GLL point: divisor of its velocities and products
+  const Rcp<double> rdx = rcp_known(A.dxd, A.rdxd);
 #pragma unroll
   for (int ii = 0; ii < NG; ii++) {
     const Sc r = q[idR][0][ii];
-    const Sc u = q[idU][0][ii] / r;
-    const Sc v = q[idV][0][ii] / r;
-    const Sc w = q[idW][0][ii] / r;
-    const Sc t = q[idT][0][ii] / r;
+    rr[ii] = make_rcp<Sc>(r);
+    const Sc u = divr(q[idU][0][ii], rr[ii]);
+    const Sc v = divr(q[idV][0][ii], rr[ii]);
+    const Sc w = divr(q[idW][0][ii], rr[ii]);
+    const Sc t = divr(q[idT][0][ii], rr[ii]);
     const Sc vn = NM == 1 ? u : (NM == 2 ? v : w);
     f[0][0][ii] = r * vn * u;
     f[1][0][ii] = r * vn * v;
@@ -241,9 +248,9 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
         dq[idT] += D * (f[3][kt][s]);
       }
 #pragma unroll
-      for (int m = 0; m < 5; m++) q[m][kt + 1][ii] = -dq[m] / A.dxd / (kt + 1.);
+      for (int m = 0; m < 5; m++) q[m][kt + 1][ii] = divk(divd(-dq[m], rdx), kt + 1);
       if (DIR == 2) {
-        q[idW][kt + 1][ii] = -dq[idW] / A.dxd / (kt + 1.) + sr[kt][ii] / (kt + 1.);
+        q[idW][kt + 1][ii] = divk(divd(-dq[idW], rdx), kt + 1) + divk(sr[kt][ii], kt + 1);
         if (A.bc == BC_WALL) {
           if (kb == A.nz - 1) q[idW][kt + 1][NG - 1] = 0;
           if (kb == 0) q[idW][kt + 1][0] = 0;
@@ -261,12 +268,12 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
           tot[x] += q[NM][ir][ii] * q[x + 1][kt + 1 - ir][ii] - q[idR][ir][ii] * f[x][kt + 1 - ir][ii];
       }
 #pragma unroll
-      for (int x = 0; x < 4; x++) f[x][kt + 1][ii] = tot[x] / q[idR][0][ii];
+      for (int x = 0; x < 4; x++) f[x][kt + 1][ii] = divr(tot[x], rr[ii]);
       Sc tg = 0.;
 #pragma unroll
       for (int ir = 0; ir <= kt; ir++)
         tg += (kt + 1. - ir) * (GAMMA * g[ir][ii] * q[idT][kt + 1 - ir][ii] - q[idT][ir][ii] * g[kt + 1 - ir][ii]);
-      g[kt + 1][ii] = (GAMMA * g[0][ii] * q[idT][kt + 1][ii] + tg / (kt + 1.)) / q[idT][0][ii];
+      g[kt + 1][ii] = (GAMMA * g[0][ii] * q[idT][kt + 1][ii] + divk(tg, kt + 1)) / q[idT][0][ii];
     }
   }
   rec.series(q);
@@ -277,8 +284,8 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
     double dtmult = A.dt;
 #pragma unroll
     for (int kt = 1; kt < NA; kt++) {
-      l += q[v][kt][0] * dtmult / (kt + 1.);
-      r += q[v][kt][NG - 1] * dtmult / (kt + 1.);
+      l += divk(q[v][kt][0] * dtmult, kt + 1);
+      r += divk(q[v][kt][NG - 1] * dtmult, kt + 1);
       dtmult *= A.dt;
     }
     eL[v] = l;
@@ -290,7 +297,7 @@ __device__ __forceinline__ void cell_recon(const Sten &sten, int kb, const Sweep
 #pragma unroll
     for (int kt = 1; kt < NA; kt++) {
 #pragma unroll
-      for (int ii = 0; ii < NG; ii++) sr[0][ii] += sr[kt][ii] * dtmult / (kt + 1.);
+      for (int ii = 0; ii < NG; ii++) sr[0][ii] += divk(sr[kt][ii] * dtmult, kt + 1);
       dtmult *= A.dt;
     }
     Sc sa = 0.;
@@ -318,38 +325,41 @@ __device__ __forceinline__ void riemann(const Sc (&qL)[5], const Sc (&qR)[5], in
     vel[2] = 0.5 * (qL[3] + qR[3]);
     t = 0.5 * (qL[4] + qR[4]);
   } else {
-    vel[0] = 0.5 * (qL[1] / qL[0] + qR[1] / qR[0]);
-    vel[1] = 0.5 * (qL[2] / qL[0] + qR[2] / qR[0]);
-    vel[2] = 0.5 * (qL[3] / qL[0] + qR[3] / qR[0]);
-    t = 0.5 * (qL[4] / qL[0] + qR[4] / qR[0]);
+    const Rcp<Sc> rl = make_rcp<Sc>(qL[0]), rg = make_rcp<Sc>(qR[0]);
+    vel[0] = 0.5 * (divr(qL[1], rl) + divr(qR[1], rg));
+    vel[1] = 0.5 * (divr(qL[2], rl) + divr(qR[2], rg));
+    vel[2] = 0.5 * (divr(qL[3], rl) + divr(qR[3], rg));
+    t = 0.5 * (divr(qL[4], rl) + divr(qR[4], rg));
   }
   const Sc p = C0 * pow_cr(r * t, GAMMA);
   const Sc cs2 = GAMMA * p / r;
   const Sc cs = sqrt(cs2);
   const Sc vn = vel[DIR], va = vel[TA], vb = vel[TB];
+  const Rcp<Sc> rt = make_rcp<Sc>(t), rt2 = rcp_twice(rt), rc2 = make_rcp<Sc>(2. * cs);
   Sc w1, w2, w3;
   if (vn > 0) {
-    w1 = qL[0] - qL[4] / t;
-    w2 = qL[QA] - va * qL[4] / t;
-    w3 = qL[QB] - vb * qL[4] / t;
+    w1 = qL[0] - divr(qL[4], rt);
+    w2 = qL[QA] - divr(va * qL[4], rt);
+    w3 = qL[QB] - divr(vb * qL[4], rt);
   } else {
-    w1 = qR[0] - qR[4] / t;
-    w2 = qR[QA] - va * qR[4] / t;
-    w3 = qR[QB] - vb * qR[4] / t;
+    w1 = qR[0] - divr(qR[4], rt);
+    w2 = qR[QA] - divr(va * qR[4], rt);
+    w3 = qR[QB] - divr(vb * qR[4], rt);
   }
-  const Sc w5 = vn * qR[0] / (2. * cs) - qR[QN] / (2. * cs) + qR[4] / (2. * t);
-  const Sc w6 = -vn * qL[0] / (2. * cs) + qL[QN] / (2. * cs) + qL[4] / (2. * t);
+  const Sc w5 = divr(vn * qR[0], rc2) - divr(qR[QN], rc2) + divr(qR[4], rt2);
+  const Sc w6 = divr(-vn * qL[0], rc2) + divr(qL[QN], rc2) + divr(qL[4], rt2);
   Sc q[5];
   q[0] = w1 + w5 + w6;
   q[QN] = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
   q[QA] = w2 + va * w5 + va * w6;
   q[QB] = w3 + vb * w5 + vb * w6;
   q[4] = t * w5 + t * w6;
+  const Rcp<Sc> r0 = make_rcp<Sc>(q[0]);
   F[0] = q[QN];
-  F[QN] = q[QN] * q[QN] / q[0] + C0 * pow_cr(q[4], GAMMA);
-  F[QA] = q[QN] * q[QA] / q[0];
-  F[QB] = q[QN] * q[QB] / q[0];
-  F[4] = q[QN] * q[4] / q[0];
+  F[QN] = divr(q[QN] * q[QN], r0) + C0 * pow_cr(q[4], GAMMA);
+  F[QA] = divr(q[QN] * q[QA], r0);
+  F[QB] = divr(q[QN] * q[QB], r0);
+  F[4] = divr(q[QN] * q[4], r0);
   if (DIR == 2) {  // Spatial:1628-1629
     if (kf < A.nz) F[idW] -= A.pres_g[kf * NG + 0];
     if (kf == A.nz) F[idW] -= A.pres_g[(A.nz - 1) * NG + NG - 1];

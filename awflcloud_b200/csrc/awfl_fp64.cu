@@ -460,11 +460,14 @@ cudaError_t launch_tracer_fields(const void *state, int fp32, long plane, const 
 }
 
 // Device math self-test: out[i] = pow(x[i], y) by the library's pow_cr (mode 0) or by
-// the CUDA math library (mode 1); exp_cr(x[i]) (mode 2).
+// the CUDA math library (mode 1); exp_cr(x[i]) (mode 2); x[i] / x[n+i] through the shared
+// reciprocal (mode 3) or by IEEE division (mode 4).
 __global__ void selftest_pow_kernel(const double *x, double y, double *out, long n, int mode) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  out[i] = mode == 0 ? pow_cr(x[i], y) : (mode == 1 ? pow(x[i], y) : exp_cr(x[i]));
+  if (mode == 3) out[i] = divr(x[i], make_rcp<double>(x[n + i]));
+  else if (mode == 4) out[i] = x[i] / x[n + i];
+  else out[i] = mode == 0 ? pow_cr(x[i], y) : (mode == 1 ? pow(x[i], y) : exp_cr(x[i]));
 }
 
 cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st) {
@@ -490,7 +493,24 @@ __global__ void __launch_bounds__(256) fma_peak_kernel(T *sink, int iters, T a, 
   if (s == (T)123.456) sink[threadIdx.x] = s;
 }
 
-cudaError_t run_fma_peak(int fp32, int nsm, double *tflops) {
+// The same with sm_100's paired FP32 FMA (one instruction, two lanes): 4 flops each.
+__global__ void __launch_bounds__(256) fma2_peak_kernel(float *sink, int iters, float a, float b) {
+  float2 x[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) x[c] = make_float2((threadIdx.x + c) * 1e-3f, (threadIdx.x + c + 1) * 1e-3f);
+  const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) x[c] = __ffma2_rn(x[c], a2, b2);
+  }
+  float s = 0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) s += x[c].x + x[c].y;
+  if (s == 123.456f) sink[threadIdx.x] = s;
+}
+
+// kind 0: FP64 FMA, 1: FP32 FMA, 2: paired FP32 FMA.
+cudaError_t run_fma_peak(int kind, int nsm, double *tflops) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -498,10 +518,11 @@ cudaError_t run_fma_peak(int fp32, int nsm, double *tflops) {
   cudaError_t e = cudaMalloc(&sink, 256 * sizeof(double));
   if (e != cudaSuccess) return e;
   const int blocks = nsm * 8, threads = 256;
-  const int iters = fp32 ? 16384 : 8192;
+  const int iters = kind == 0 ? 8192 : (kind == 1 ? 16384 : 8192);
   for (int rep = 0; rep < 2; rep++) {  // first launch warms up
     cudaEventRecord(e0);
-    if (fp32) fma_peak_kernel<float><<<blocks, threads>>>((float *)sink, iters, 0.999999f, 1e-7f);
+    if (kind == 1) fma_peak_kernel<float><<<blocks, threads>>>((float *)sink, iters, 0.999999f, 1e-7f);
+    else if (kind == 2) fma2_peak_kernel<<<blocks, threads>>>((float *)sink, iters, 0.999999f, 1e-7f);
     else fma_peak_kernel<double><<<blocks, threads>>>((double *)sink, iters, 0.999999999, 1e-9);
     cudaEventRecord(e1);
   }
@@ -513,7 +534,8 @@ cudaError_t run_fma_peak(int fp32, int nsm, double *tflops) {
   cudaFree(sink);
   if (e != cudaSuccess) return e;
   e = cudaGetLastError();
-  *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e12;
+  const double flops_per_inst = kind == 2 ? 4.0 : 2.0;
+  *tflops = flops_per_inst * 8.0 * (double)iters * blocks * threads / (ms * 1e-3) / 1e12;
   return e;
 }
 

@@ -37,6 +37,7 @@ template <int ORD> struct Tables {
   double idl[HS + 2];
   double sigma;
   double wts[NG];                 // gllWts_ngll
+  double ridl;                    // RN(1/idl[HS+1]), the bridge polynomial's divisor
 };
 
 // Per-line constants of one sweep.
@@ -48,6 +49,7 @@ struct SweepArgs {
   int bc;          // BC along the sweep direction
   int weno_s, weno_w, sim2d, mode;
   double dxd;      // dx, dy or dz
+  double rdxd;     // RN(1/dxd)
   double dt;
   const double *dens_c, *denstheta_c;             // hyDensCells, hyDensThetaCells (nz+2hs)
   const double *dens_g, *denstheta_g, *pres_g;    // hyDensGLL, hyDensThetaGLL, hyPressureGLL (nz*ngll)
@@ -124,7 +126,7 @@ cudaError_t launch_state_sums(const void *state, int fp32, long plane, int nx, i
                               double *partials, int nblk, double *out, cudaStream_t st);
 cudaError_t launch_check_state(const void *state, int fp32, long plane, const double *dens_c, int nx, int ny,
                                int nz, int hs, int nsm, unsigned long long *count, cudaStream_t st);
-cudaError_t run_fma_peak(int fp32, int nsm, double *tflops);
+cudaError_t run_fma_peak(int kind, int nsm, double *tflops);  // 0 FP64, 1 FP32, 2 paired FP32
 cudaError_t launch_output_fields(const void *state, int fp32, long plane, const double *dens_c,
                                  const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
                                  int nsm, double *out, cudaStream_t st);

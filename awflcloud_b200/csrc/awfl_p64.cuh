@@ -39,7 +39,7 @@ struct P64 {
   // K5 divergence (Spatial:940-956, 1298-1310, 1680-1696): z adds onto the gravity source.
   template <int DIR>
   static __device__ __forceinline__ double tendency(int v, double Fl, double Fr, double sa, const Args &A) {
-    const double d = -(Fr - Fl) / A.dxd;
+    const double d = divd(-(Fr - Fl), rcp_known(A.dxd, A.rdxd));
     if (DIR == 0) return (A.sim2d && v == idV) ? 0.0 : d;
     if (DIR == 1) return d;
     return (A.sim2d && v == idV) ? 0.0 : (v == idW ? sa : 0.0) + d;

@@ -7,7 +7,11 @@
 // Evaluating pow to ~2^-75 relative and rounding once makes the GPU results agree with
 // the reference bit for bit except in the rare near-midpoint cases.
 //
-// Method (textbook table-driven log/exp in double-double arithmetic, own derivation):
+// Method: Tang's table-driven logarithm and exponential (P. T. P. Tang, "Table-driven
+// implementation of the exponential function in IEEE floating-point arithmetic", ACM TOMS
+// 15(2), 1989; "... of the logarithm function", ACM TOMS 16(4), 1990) carried out in
+// double-double arithmetic (Dekker's exact product by FMA, Knuth's two-sum); the tables
+// and the Taylor coefficients are this library's own:
 //   x = 2^e * m, m in [1,2); j = top 7 bits of m; r = m*inv_j - 1 exactly as a
 //   double-double (inv_j ~ 1/(1+(j+1/2)/128), |r| <= 2^-8);
 //   ln x = e*ln2 - ln(inv_j) + log1p(r), log1p by its Taylor series through r^9 with the

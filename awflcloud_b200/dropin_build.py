@@ -43,4 +43,8 @@ def build(ref_dir: str, orders=((5, 3), (9, 5))) -> list:
 
 
 if __name__ == "__main__":
-    print(build(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("AWFL_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: python -m awflcloud_b200.dropin_build <reference source tree> "
+                 "(or set AWFL_REFERENCE_DIR)")
+    print(build(ref))

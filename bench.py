@@ -101,6 +101,15 @@ def cfl_for(ord_):
     return 0.8 if ord_ == 5 else 0.4
 
 
+def bench_config(a):
+    """The workload, identical in both arms (the arithmetic type is the line's dtype)."""
+    h2 = a.ord - 1  # two halos of (ord-1)/2 cells
+    mb = 5 * (a.nx + h2) * (a.ny + h2) * (a.nz + h2) * 8 / 1e6
+    return {"workload": workload_name(a), "nx": a.nx, "ny": a.ny, "nz": a.nz, "ord": a.ord,
+            "l2": "inputs larger than L2: the state is %.0f MB (FP64, or FP32 values + compensations) "
+                  "> 126 MB, no flush" % mb}
+
+
 def workload_name(a):
     return "rising thermal bubble %dx%dx%d, ord %d / ngll %d, CFL %.1f" % (
         a.nx, a.ny, a.nz, a.ord, 3 if a.ord == 5 else 5, cfl_for(a.ord))
@@ -233,9 +242,9 @@ def run_reference(a):
     line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(el / a.steps * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
-            "config": {"workload": workload_name(a), "nx": a.nx, "ny": a.ny, "nz": a.nz, "ord": a.ord,
-                       "parallelism": "reference CPU build (OpenMP), rank 0 only"},
-            "impl": "reference",
+            "config": bench_config(a),
+            "impl": "reference", "impl_note": "the reference's own code (oracle/_ref) on the host cores "
+                                              "with OpenMP, rank 0 only",
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": "%d full time steps after %d warm-up, first step %.2f s" % (a.steps, a.warmup, one)},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -256,6 +265,13 @@ def time_form(a, prec, local, world, clocks=None):
     dt = ctx.cfl(st, cfl_for(a.ord))
     stream = torch.cuda.current_stream()
     peak = capi.measure_fma_peak(prec, local)
+    peaks = {"peak_scalar": round(peak, 3)}
+    if prec == capi.FP32:
+        # sm_100's paired FP32 FMA retires two lanes per instruction: the pipe's ceiling is
+        # the larger of the two measured rates
+        paired = capi.measure_fma_peak(capi.PEAK_FP32_PAIRED, local)
+        peaks["peak_paired"] = round(paired, 3)
+        peak = max(peak, paired)
     for _ in range(a.warmup):
         ctx.step(st, dt)
     torch.cuda.synchronize()
@@ -290,17 +306,29 @@ def time_form(a, prec, local, world, clocks=None):
     roofline = {"bound": "fp64" if prec == capi.FP64 else "fp32",
                 "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4), "traffic": TRAFFIC.get((prec, a.ord)),
-                "peak_source": "measured in this run: awfl_measure_fma_peak (FMA chains, 2 flops/FMA)",
-                "flops_per_launch": flops_launch, "launch_ms_avg": round(avg_launch_s * 1e3, 4),
+                "peak_source": "measured in this run: awfl_measure_fma_peak (FMA chains, 2 flops per "
+                               "FMA lane; FP32: the larger of scalar and paired FMA)",
+                **peaks,
+                "ops_algorithmic": flops_launch,
+                "ops_executed": EXECUTED_OPS.get((prec, a.ord), {}).get("ops_per_launch"),
+                "ops_executed_source": EXECUTED_OPS.get((prec, a.ord), {}).get("source"),
+                "launch_ms_avg": round(avg_launch_s * 1e3, 4),
                 "bytes_algorithmic_per_launch": cells * 10 * esz * (1 if prec == capi.FP64 else 2)}
     return {"ctx": ctx, "state": st, "dt": dt, "value": job_throughput(world, cells, a.steps, max_ms),
             "ms_per_step": max_ms / a.steps, "roofline": roofline, "clocks": clk, "flops": fl,
             "finite": bool(torch.isfinite(st).all().item())}
 
 
-# DRAM bytes per sweep launch (read + write, mean over x/y/z), from ncu on the 256x256x128
-# workload (profiles/sweep_kernel_256x256x128.md).
+# DRAM bytes per sweep launch (read + write, mean over x/y/z): ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum of the sweep kernels on this 256x256x128
+# workload (one capture of the same build; ncu cannot run inside the timed process).
 TRAFFIC = {(0, 5): 650_500_000, (1, 5): 635_700_000}
+# Floating-point operations the sweep kernels execute per launch (mean over x/y/z), from
+# ncu's per-opcode thread-instruction counters of the same capture: FP32 form: FADD + FMUL
+# + 2 x FFMA, paired instructions counted per lane; FP64: DADD + DMUL + 2 x DFMA (the
+# division and pow sequences included). The algorithmic count (flops.py) follows the
+# reference's loops instead.
+EXECUTED_OPS = {}
 
 
 def rel_l2_after(a, steps, local):
@@ -590,22 +618,25 @@ def run_ours(a):
     main = time_form(a, main_prec, local, world, clocks=ClockSampler(local))
     other = time_form(a, capi.FP64, local, world) if (main_prec == capi.FP32 and not a.no_compare) else None
     e2e = None if a.no_e2e else e2e_leg(a, main["ctx"], main["state"], main["dt"], torch.cuda.current_stream(), world)
+    # the precision-matched end-to-end figure: the FP64 path through the same C ABI calls
+    e2e64 = None
+    if other is not None and not a.no_e2e:
+        e2e64 = e2e_leg(a, other["ctx"], other["state"], other["dt"], torch.cuda.current_stream(), world)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(main["value"], 3), "unit": UNIT, "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(main["ms_per_step"], 4),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if main_prec == capi.FP64 else "f32", "data": DATA,
-                "config": {"workload": workload_name(a), "nx": a.nx, "ny": a.ny, "nz": a.nz, "ord": a.ord,
-                           "precision": a.precision,
-                           "l2": "state %.0f MB > 126 MB L2: no flush needed"
-                                 % (main["state"].numel() * main["state"].element_size() / 1e6),
-                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                "config": bench_config(a),
+                "parallelism": "replicas (one domain per GPU, no collective)" if world > 1 else "single GPU",
                 "roofline": main["roofline"], "gpu_launches": 3 * a.steps, "finite": main["finite"],
                 "clocks": main["clocks"], "flops_per_cell_step": main["flops"]}
         if other is not None:
             line["fp64"] = {"value": round(other["value"], 3), "ms_per_step": round(other["ms_per_step"], 4),
                             "roofline": other["roofline"], "finite": other["finite"]}
+            if e2e64 is not None:
+                line["fp64"]["e2e"] = e2e64
             line["fp32_over_fp64"] = round(main["value"] / other["value"], 3)
             errs = rel_l2_after(a, 100, local)
             line["rel_l2_vs_fp64_after_100_steps"] = {"rho": errs[0], "rho_u": errs[1], "rho_v": errs[2],

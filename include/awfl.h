@@ -248,7 +248,10 @@ int awfl_get_background(const awfl_ctx *ctx, double *dens_c, double *pres_c, dou
  * (512 KiB per GPU that loads it, held until exit). Result: the same value as awfl_cfl.
  * Limits: FP64 only; nx*ny*nz <= 16,777,216 cells, larger grids are rejected with
  * AWFL_ERR_ARG (use awfl_cfl). The first call on each device looks up the array's device
- * address; make that first call before any stream capture. Every call shares the one
+ * address and keeps it for the life of the process; make that first call before any stream
+ * capture, and do not call this entry point again on a device after cudaDeviceReset (the
+ * reset unloads the library's device code, so the kept address no longer names the
+ * array). Every call shares the one
  * array: calls that overlap on the GPU (other streams, other host threads) race.
  * Synchronises `stream`. Errors are reported by awfl_last_error(NULL). */
 int awfl_cfl_noalloc(const awfl_config *cfg, const void *d_state, const void *d_hy_dens_cells,
@@ -257,12 +260,17 @@ int awfl_cfl_noalloc(const awfl_config *cfg, const void *d_state, const void *d_
 /* Diagnostic: the FP64 path's device math on n doubles (device pointers). mode 0:
  * out = pow(x, y) by the library's correctly rounded pow (the one every FP64 kernel uses
  * in place of the reference's glibc pow); mode 1: the CUDA math library's pow, for
- * comparison; mode 2: the library's correctly rounded exp(x) (y ignored). */
+ * comparison; mode 2: the library's correctly rounded exp(x) (y ignored); mode 3:
+ * out[i] = x[i] / x[n+i] by the FP64 kernels' division through a shared reciprocal (d_x
+ * holds 2n doubles, y ignored); mode 4: the same quotients by the GPU's IEEE division. */
 int awfl_selftest_pow(const void *d_x, double y, void *d_out, long n, int mode, void *stream);
 
-/* Diagnostic: measured FMA throughput of the CUDA-core pipe the kernels run on (FP64 or
- * FP32), in TFLOP/s (2 flops per FMA), from a ~0.1 s FMA-chain kernel on `device`. The
- * roofline denominator of the ADER/WENO kernels, which are bound by these pipes. */
+/* Diagnostic: measured FMA throughput of the CUDA-core pipe the kernels run on, in TFLOP/s
+ * (2 flops per FMA lane), from a ~0.1 s FMA-chain kernel on `device`: precision AWFL_FP64,
+ * AWFL_FP32 (scalar FFMA) or AWFL_PEAK_FP32_PAIRED (sm_100's paired FP32 FMA, one
+ * instruction for two lanes). The roofline denominator of the ADER/WENO kernels, which
+ * are bound by these pipes. */
+enum { AWFL_PEAK_FP32_PAIRED = 2 };
 int awfl_measure_fma_peak(int precision, int device, double *tflops);
 
 /* Device memory helpers for hosts that do not link the CUDA runtime themselves. */

@@ -1,7 +1,8 @@
 /* Correctly rounded pow/exp for the CPU test oracles (TEST INFRASTRUCTURE ONLY).
  *
- * The same table-driven double-double algorithm as the library's device pow
- * (awflcloud_b200/csrc/awfl_pow.cuh), written in plain C with fma(): ln x through a
+ * The same algorithm as the library's device pow (awflcloud_b200/csrc/awfl_pow.cuh):
+ * Tang's table-driven logarithm and exponential (ACM TOMS 1989/1990) in double-double
+ * arithmetic, written in plain C with fma(): ln x through a
  * 128-entry table and a degree-9 log1p series, exp through 2^(j/64) and a degree-8
  * series, ~2^-75 relative before the single final rounding.
  *

@@ -31,10 +31,17 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(_DP)
 
 
-def build(ref: bool = False) -> None:
-    """Build the oracle libraries (and, with ``ref``, the reference harness) via make."""
+def build(ref: bool = False, ref_dir: str | None = None) -> None:
+    """Build the oracle libraries (and, with ``ref``, the reference harness from the
+    reference's source tree ``ref_dir``, default $AWFL_REFERENCE_DIR) via make."""
     targets = ["oracle"] + (["ref"] if ref else [])
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    extra = []
+    if ref:
+        ref_dir = ref_dir or os.environ.get("AWFL_REFERENCE_DIR")
+        if not ref_dir:
+            raise RuntimeError("the reference's source tree is needed: set AWFL_REFERENCE_DIR")
+        extra = ["REF=" + ref_dir]
+    subprocess.run(["make", "-s", "-C", HERE] + targets + extra, check=True)
 
 
 def oracle_path(ord_: int, crpow: bool = False) -> str:

@@ -13,8 +13,8 @@ drives that build through ``oracle.pyoracle.RefHarness`` and stores:
                             each split of step 1 and after every step;
 * ``tracers_init.npz``   -- initTracers of the driver's tracers on three grids.
 
-Needs the reference sources (REF, default /root/reference) and g++ with OpenMP.
-Run from the repository root:  python tests/golden/make_golden.py
+Needs the reference's source tree (``--ref DIR`` or $AWFL_REFERENCE_DIR) and g++ with OpenMP.
+Run from the repository root:  python tests/golden/make_golden.py --ref DIR
 """
 from __future__ import annotations
 
@@ -134,7 +134,14 @@ def make_tracers():
 
 
 def main():
-    pyoracle.build(ref=True)
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=os.environ.get("AWFL_REFERENCE_DIR"),
+                    help="the reference's source tree (mrnorman/awflCloud)")
+    a = ap.parse_args()
+    if not a.ref:
+        ap.error("--ref or AWFL_REFERENCE_DIR is required")
+    pyoracle.build(ref=True, ref_dir=a.ref)
     print("wrote", make_tracers())
     for o in (5, 9):
         make_tables(o)

@@ -74,3 +74,68 @@ def test_exp_correctly_rounded():
         assert mine[i] == float(mp.exp(mp.mpf(float(x[i])))), x[i]
     for i in rng.integers(0, x.size, 300):
         assert mine[i] == float(mp.exp(mp.mpf(float(x[i])))), x[i]
+
+
+def _hard_quotients(rng, n):
+    """Operand pairs whose quotient lies within ~2^-53 ulp of a rounding midpoint, where a
+    division that is not correctly rounded would show: with integer significands B (odd,
+    53 bits) and M (odd, 54 bits: the midpoint), B*M = A*2^53 +- 1 makes A/B = M/2^53
+    -+ 1/(B*2^53), so M = +-B^-1 mod 2^53 and A = (B*M -+ 1)/2^53 must fit 53 bits."""
+    a, b = [], []
+    P = 1 << 53
+    while len(a) < n:
+        B = int(rng.integers(1 << 52, 1 << 53)) | 1
+        s = 1 if len(a) % 2 else -1
+        M = (s * pow(B, -1, P)) % P
+        lo = (1 << 105) // B + 1
+        M += ((lo - M + P - 1) // P) * P  # smallest M >= lo in the class
+        if M >= (1 << 54) or B * M >= (1 << 106) or M % 2 == 0:
+            continue
+        A, r = divmod(B * M - s, P)
+        assert r == 0 and (1 << 52) <= A < (1 << 53)
+        ea, eb = int(rng.integers(-30, 30)), int(rng.integers(-30, 30))
+        a.append(math.ldexp(A, ea - 52))
+        b.append(math.ldexp(B, eb - 52))
+    return np.array(a), np.array(b)
+
+
+def test_shared_reciprocal_division_is_ieee():
+    """The FP64 kernels divide by a shared divisor through its correctly rounded reciprocal
+    plus two Markstein corrections (awfl_div.cuh); that must be the IEEE quotient bit for
+    bit, signed zeros included."""
+    rng = np.random.default_rng(11)
+    n = 400_000
+    a = np.exp(rng.uniform(-46.0, 46.0, n)) * rng.choice([-1.0, 1.0], n)
+    b = np.exp(rng.uniform(-46.0, 46.0, n)) * rng.choice([-1.0, 1.0], n)
+    # physical ranges of the path and edge cases: significands of all ones, b = 1, a = b,
+    # signed zeros, operands one ulp apart, the constant divisors 3 and 5
+    a[:4000] = rng.uniform(0.5, 2.0, 4000)
+    b[:4000] = rng.uniform(0.5, 2.0, 4000)
+    ones = np.nextafter(np.array([2.0, 4.0, 1.0, 0.5]), 0.0)
+    b[4000:4004] = ones
+    a[4004:4010] = [0.0, -0.0, 0.0, -0.0, 1.0, 3.0]
+    b[4004:4010] = [3.0, 3.0, -7.0, -7.0, 1.0, 3.0]
+    b[4010:4020] = 3.0
+    b[4020:4030] = 5.0
+    a[4030:4040] = np.nextafter(b[4030:4040], np.inf)
+    ha, hb = _hard_quotients(rng, 20_000)
+    a[4040:4040 + ha.size] = ha
+    b[4040:4040 + hb.size] = hb
+    x = np.concatenate([a, b])
+    mine = _device_pairs(x, 3)
+    ieee = _device_pairs(x, 4)
+    host = a / b
+    assert np.array_equal(ieee.view(np.int64), host.view(np.int64))
+    bad = np.nonzero(mine.view(np.int64) != ieee.view(np.int64))[0]
+    assert bad.size == 0, [(a[i], b[i], mine[i], ieee[i]) for i in bad[:5]]
+
+
+def _device_pairs(x, mode):
+    L = capi.lib()
+    n = x.size // 2
+    d_x = torch.from_numpy(x).cuda()
+    d_o = torch.empty(n, dtype=torch.float64, device="cuda")
+    rc = L.awfl_selftest_pow(d_x.data_ptr(), 0.0, d_o.data_ptr(), n, mode, torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return d_o.cpu().numpy()
