@@ -16,6 +16,7 @@ STATUS = {0: "AWFL_OK", -1: "AWFL_ERR_ARG", -2: "AWFL_ERR_CUDA", -3: "AWFL_ERR_N
           -4: "AWFL_ERR_STATE", -5: "AWFL_ERR_TIMEOUT", -6: "AWFL_ERR_NOT_BUILT",
           -7: "AWFL_ERR_IO"}
 BC = {"periodic": 0, "wall": 1}
+BC_PERIODIC, BC_WALL = 0, 1
 DATA = {"thermal": 1, "collision": 2, "straka": 3, "igw": 4}
 FP64, FP32 = 0, 1
 INIT_REFERENCE, INIT_BUBBLE = 0, 1
@@ -71,6 +72,10 @@ _SIGS = {
     "awfl_split": (_I, [_VP, _VP, _D, _I, _VP]),
     "awfl_step": (_I, [_VP, _VP, _D, _VP]),
     "awfl_step_tlm": (_I, [_VP, _VP, _D, _VP]),
+    "awfl_create_slab": (_I, [ctypes.POINTER(AwflConfig), _I, _I, _I, ctypes.POINTER(_VP)]),
+    "awfl_slab_info": (_I, [_VP] + [ctypes.POINTER(_I)] * 4 + [ctypes.POINTER(_L)]),
+    "awfl_slab_pack": (_I, [_VP, _VP, _VP, _VP]),
+    "awfl_split_slab": (_I, [_VP, _VP, _VP, _D, _VP]),
     "awfl_step_adjoint": (_I, [_VP, _VP, _VP, _I, _D, _VP]),
     "awfl_adjoint_tape_bytes": (_I, [_VP, _I, ctypes.POINTER(_L)]),
     "awfl_get_dimswitch": (_I, [_VP, ctypes.POINTER(_I)]),
@@ -168,6 +173,57 @@ class Context:
         self.device = device
 
     @classmethod
+    def slab(cls, nx, ny, nz, nslabs, slab, xlen=20000.0, ylen=20000.0, zlen=10000.0,
+             bc=("periodic", "periodic", "wall"), weno_scalars=True, weno_winds=True, data="thermal", ord_=5,
+             precision=FP64, device=0):
+        """Slab `slab` of `nslabs` of the nx x ny x nz grid decomposed in x
+        (awfl_create_slab); self.nx is the slab's own width, self.xoff its first cell."""
+        self = cls.__new__(cls)
+        self.L = lib()
+        bcv = [BC[b] if isinstance(b, str) else int(b) for b in bc]
+        self.cfg = AwflConfig(nx, ny, nz, xlen, ylen, zlen, bcv[0], bcv[1], bcv[2], int(weno_scalars),
+                              int(weno_winds), DATA[data] if isinstance(data, str) else int(data), ord_, precision)
+        h = _VP()
+        rc = self.L.awfl_create_slab(ctypes.byref(self.cfg), nslabs, slab, device, ctypes.byref(h))
+        if rc != AWFL_OK:
+            raise AwflError(rc, self.L.awfl_last_error(None).decode())
+        self.h = h
+        self.ord = ord_
+        self.ngll = 3 if ord_ == 5 else 5
+        self.hs = (ord_ - 1) // 2
+        self.precision = precision
+        self.device = device
+        info = self.slab_info()
+        self.nslabs, self.slab_index, self.xoff, self.nx_global = (info[k] for k in
+                                                                   ("nslabs", "slab", "xoff", "nx_global"))
+        self.halo_elems = info["halo_elems"]
+        self.nx = self._local_nx(nx, nslabs, slab)
+        self.ny, self.nz = ny, nz
+        return self
+
+    @staticmethod
+    def _local_nx(nx, nslabs, slab):
+        return nx // nslabs + (1 if slab < nx % nslabs else 0)
+
+    def slab_info(self):
+        v = [_I() for _ in range(4)]
+        n = _L()
+        self._check(self.L.awfl_slab_info(self.h, *[ctypes.byref(x) for x in v], ctypes.byref(n)))
+        return dict(nslabs=v[0].value, slab=v[1].value, xoff=v[2].value, nx_global=v[3].value,
+                    halo_elems=n.value)
+
+    def slab_pack(self, state, send, stream=None):
+        """The slab's first and last hs+1 interior x columns into send
+        ([2][5][nz][ny][hs+1], the state's element type)."""
+        self._check_buf(send, (self.slab_info()["halo_elems"],), "send", plane_dtype=True)
+        self._check(self.L.awfl_slab_pack(self.h, self._st(state), _ptr(send), _stream(stream)))
+
+    def split_slab(self, state, recv, dt, stream=None):
+        """The x split with the neighbouring slabs' columns (recv, the layout of send)."""
+        self._check_buf(recv, (self.slab_info()["halo_elems"],), "recv", plane_dtype=True)
+        self._check(self.L.awfl_split_slab(self.h, self._st(state), _ptr(recv), dt, _stream(stream)))
+
+    @classmethod
     def _borrow(cls, handle, cfg, device):
         """A Context view of a member context owned by an ensemble (not destroyed here)."""
         self = cls.__new__(cls)
@@ -225,7 +281,7 @@ class Context:
         import torch
         return torch.float64 if self.precision == FP64 else torch.float32
 
-    def _check_buf(self, x, shape, what):
+    def _check_buf(self, x, shape, what, plane_dtype=False):
         if isinstance(x, int) or x is None:
             return  # raw device address: the caller vouches for its size
         import math

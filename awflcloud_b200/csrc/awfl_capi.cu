@@ -55,6 +55,10 @@ struct awfl_ctx {
   double *d_trc = nullptr;  // tracer transport scratch (awfl_split_tracers)
   size_t trc_bytes = 0;
   size_t diag_bytes = 0;
+  // a slab of a grid decomposed in x (awfl_create_slab): nslabs, this slab, the global x
+  // index of its first cell, the grid's nx, and which ends border another slab
+  int nslabs = 1, slab = 0, xoff = 0, nx_global = 0;
+  bool xlo_ex = false, xhi_ex = false;
   std::string err;
 };
 
@@ -339,7 +343,7 @@ int set_device(awfl_ctx *c) {
 }
 
 SweepArgs sweep_args(awfl_ctx *c, void *state, void *tend, double dt, int dir, int mode) {
-  SweepArgs A;
+  SweepArgs A{};
   A.state = (double *)state;
   A.tend = (double *)tend;
   A.nx = c->cfg.nx; A.ny = c->cfg.ny; A.nz = c->cfg.nz;
@@ -545,7 +549,7 @@ int awfl_init_state(awfl_ctx *c, void *d_state, const awfl_init_spec *spec, void
     return fail(c, AWFL_ERR_ARG, "awfl_init_state: bubble initial data needs a constant-theta background");
   int rc = set_device(c);
   if (rc) return rc;
-  InitLaunch L;
+  InitLaunch L{};
   std::memset(&L, 0, sizeof L);
   L.state = d_state;
   if (fp32(c)) {
@@ -553,6 +557,7 @@ int awfl_init_state(awfl_ctx *c, void *d_state, const awfl_init_spec *spec, void
     L.comp32 = (float *)d_state + state_plane(c);
   }
   L.nx = c->cfg.nx; L.ny = c->cfg.ny; L.nz = c->cfg.nz; L.hs = c->hs; L.ord = c->cfg.ord;
+  L.xoff = c->xoff; L.nx_global = c->nx_global > 0 ? c->nx_global : c->cfg.nx;
   L.dx = c->dx; L.dy = c->dy; L.dz = c->dz; L.xlen = c->cfg.xlen; L.ylen = c->cfg.ylen; L.zlen = c->cfg.zlen;
   L.data_spec = c->cfg.data_spec; L.sim2d = c->sim2d;
   if (spec) {
@@ -671,10 +676,11 @@ int awfl_init_tracers(awfl_ctx *c, double *d_tracers, int ntracers, void *stream
   if (bad_ptr(d_tracers)) return fail(c, AWFL_ERR_ARG, "awfl_init_tracers: tracer pointer is NULL or misaligned");
   int rc = set_device(c);
   if (rc) return rc;
-  InitLaunch L;
+  InitLaunch L{};
   std::memset(&L, 0, sizeof L);
   L.state = d_tracers;
   L.nx = c->cfg.nx; L.ny = c->cfg.ny; L.nz = c->cfg.nz; L.hs = c->hs; L.ord = c->cfg.ord;
+  L.xoff = c->xoff; L.nx_global = c->nx_global > 0 ? c->nx_global : c->cfg.nx;
   L.dx = c->dx; L.dy = c->dy; L.dz = c->dz; L.xlen = c->cfg.xlen; L.ylen = c->cfg.ylen; L.zlen = c->cfg.zlen;
   L.sim2d = c->sim2d;
   for (int m = 0; m < c->cfg.ord; m++) { L.pts[m] = c->pts_ord[m]; L.wts[m] = c->wts_ord[m]; }
@@ -740,6 +746,8 @@ int awfl_cfl(awfl_ctx *c, const void *d_state, double cfl, double *h_dt, void *s
 int awfl_compute_tendencies(awfl_ctx *c, void *d_state, void *d_tend, double dt, int dir, void *stream) {
   if (!c) return AWFL_ERR_ARG;
   if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
+  if (dir == 0 && (c->xlo_ex || c->xhi_ex))
+    return fail(c, AWFL_ERR_ARG, "the x split of a slab needs its neighbours' columns (awfl_split_slab)");
   if (bad_ptr(d_state) || bad_ptr(d_tend)) return fail(c, AWFL_ERR_ARG, "state/tend pointer is NULL or misaligned");
   int rc = set_device(c);
   if (rc) return rc;
@@ -775,6 +783,8 @@ int awfl_apply_tendencies(awfl_ctx *c, void *d_state, const void *d_tend, double
 int awfl_split(awfl_ctx *c, void *d_state, double dt, int dir, void *stream) {
   if (!c) return AWFL_ERR_ARG;
   if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
+  if (dir == 0 && (c->xlo_ex || c->xhi_ex))
+    return fail(c, AWFL_ERR_ARG, "the x split of a slab needs its neighbours' columns (awfl_split_slab)");
   if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "state pointer is NULL or misaligned");
   int rc = set_device(c);
   if (rc) return rc;
@@ -790,6 +800,8 @@ int awfl_split(awfl_ctx *c, void *d_state, double dt, int dir, void *stream) {
 
 int awfl_step(awfl_ctx *c, void *d_state, double dt, void *stream) {
   if (!c) return AWFL_ERR_ARG;
+  if (c->xlo_ex || c->xhi_ex)
+    return fail(c, AWFL_ERR_ARG, "a slab's step exchanges columns between its x split's slabs (awfl_split_slab)");
   for (int spl = 0; spl < 3; spl++) {
     const int dir = c->dimswitch ? spl : 2 - spl;
     int rc = awfl_split(c, d_state, dt, dir, stream);
@@ -799,18 +811,94 @@ int awfl_step(awfl_ctx *c, void *d_state, double dt, void *stream) {
   return AWFL_OK;
 }
 
+int awfl_create_slab(const awfl_config *global, int nslabs, int slab, int device, awfl_ctx **out) {
+  if (!global || !out) return fail(nullptr, AWFL_ERR_ARG, "awfl_create_slab: NULL argument");
+  *out = nullptr;
+  if (global->ord != 5 && global->ord != 9) return fail(nullptr, AWFL_ERR_ARG, "ord must be 5 or 9 (got %d)", global->ord);
+  const int hs = (global->ord - 1) / 2;
+  if (nslabs < 1 || slab < 0 || slab >= nslabs)
+    return fail(nullptr, AWFL_ERR_ARG, "awfl_create_slab: slab %d of %d", slab, nslabs);
+  if (global->nx < (long)nslabs * (hs + 1))
+    return fail(nullptr, AWFL_ERR_ARG, "awfl_create_slab: nx = %d leaves a slab of %d slabs narrower than %d cells",
+                global->nx, nslabs, hs + 1);
+  const int base = global->nx / nslabs, extra = global->nx % nslabs;
+  awfl_config local = *global;
+  local.nx = base + (slab < extra ? 1 : 0);
+  int rc = awfl_create(&local, device, out);
+  if (rc) return rc;
+  awfl_ctx *c = *out;
+  c->nslabs = nslabs;
+  c->slab = slab;
+  c->xoff = slab * base + (slab < extra ? slab : extra);
+  c->nx_global = global->nx;
+  c->dx = global->xlen / global->nx;  // the grid's spacing, as the undivided grid computes it
+  if (nslabs > 1) {
+    const bool periodic = global->bc_x == AWFL_BC_PERIODIC;
+    c->xlo_ex = periodic || slab > 0;
+    c->xhi_ex = periodic || slab < nslabs - 1;
+  }
+  return AWFL_OK;
+}
+
+int awfl_slab_info(const awfl_ctx *c, int *nslabs, int *slab, int *xoff, int *nx_global, long *halo_elems) {
+  if (!c) return AWFL_ERR_ARG;
+  if (nslabs) *nslabs = c->nslabs;
+  if (slab) *slab = c->slab;
+  if (xoff) *xoff = c->xoff;
+  if (nx_global) *nx_global = c->nx_global > 0 ? c->nx_global : c->cfg.nx;
+  if (halo_elems) *halo_elems = 2L * 5 * c->cfg.nz * c->cfg.ny * (c->hs + 1);
+  return AWFL_OK;
+}
+
+int awfl_slab_pack(awfl_ctx *c, const void *d_state, void *d_send, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state) || (reinterpret_cast<uintptr_t>(d_send) & 7) != 0 || !d_send)
+    return fail(c, AWFL_ERR_ARG, "awfl_slab_pack: state or send pointer is NULL or misaligned");
+  if (c->cfg.nx < c->hs + 1) return fail(c, AWFL_ERR_ARG, "awfl_slab_pack: the slab is narrower than hs+1 cells");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaError_t e = launch_slab_pack(d_state, fp32(c) ? 4 : 8, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs, d_send,
+                                   (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "slab_pack");
+  return AWFL_OK;
+}
+
+int awfl_split_slab(awfl_ctx *c, void *d_state, const void *d_recv, double dt, void *stream) {
+  if (!c) return AWFL_ERR_ARG;
+  if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "state pointer is NULL or misaligned");
+  if ((c->xlo_ex || c->xhi_ex) && (!d_recv || (reinterpret_cast<uintptr_t>(d_recv) & 7) != 0))
+    return fail(c, AWFL_ERR_ARG, "awfl_split_slab: the received columns are NULL or misaligned");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const long side = 5L * c->cfg.nz * c->cfg.ny * (c->hs + 1);
+  cudaError_t e;
+  if (fp32(c)) {
+    SweepArgs32 A = sweep_args32(c, d_state, nullptr, dt, 0, MODE_APPLY);
+    A.xh[0] = c->xlo_ex ? (const float *)d_recv : nullptr;
+    A.xh[1] = c->xhi_ex ? (const float *)d_recv + side : nullptr;
+    e = launch_sweep_fp32(c->cfg.ord, 0, A, (cudaStream_t)stream);
+  } else {
+    SweepArgs A = sweep_args(c, d_state, nullptr, dt, 0, MODE_APPLY);
+    A.xh[0] = c->xlo_ex ? (const double *)d_recv : nullptr;
+    A.xh[1] = c->xhi_ex ? (const double *)d_recv + side : nullptr;
+    e = launch_sweep_fp64(c->cfg.ord, 0, A, (cudaStream_t)stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "split_slab");
+  return AWFL_OK;
+}
+
 int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
                        int dir, void *stream) {
   if (!c) return AWFL_ERR_ARG;
+  if (c->nslabs > 1) return fail(c, AWFL_ERR_ARG, "tracer transport is not available on a slab");
   if (fp32(c)) return fail(c, AWFL_ERR_ARG, "tracer transport needs an FP64 context");
   if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
   if (ntracers < 0 || ntracers > 64) return fail(c, AWFL_ERR_ARG, "ntracers must be in [0, 64]");
   if (ntracers == 0) return awfl_split(c, d_state, dt, dir, stream);
   if (bad_ptr(d_state) || bad_ptr(d_tracers)) return fail(c, AWFL_ERR_ARG, "state or tracer pointer is NULL or misaligned");
   if (!pos) return fail(c, AWFL_ERR_ARG, "pos (positive-definite flags) is NULL");
-  const int ext = dir == 0 ? c->cfg.nx : (dir == 1 ? c->cfg.ny : c->cfg.nz);
-  if (ext < c->hs && !(dir == 1 && c->sim2d))
-    return fail(c, AWFL_ERR_ARG, "tracer transport needs at least %d cells along direction %d", c->hs, dir);
+  // (every stencil index maps into the line for any length: a wall copies cell 0 or n-1;
+  // periodic directions shorter than hs are refused by awfl_create)
   int rc = set_device(c);
   if (rc) return rc;
   if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendencies (Spatial:572-575)
@@ -841,6 +929,7 @@ int awfl_step_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracer
 
 int awfl_step_tlm(awfl_ctx *c, void *d_state_tangent, double dt, void *stream) {
   if (!c) return AWFL_ERR_ARG;
+  if (c->nslabs > 1) return fail(c, AWFL_ERR_ARG, "the tangent-linear step is not available on a slab");
   if (fp32(c)) return fail(c, AWFL_ERR_ARG, "awfl_step_tlm needs an FP64 context");
   if (bad_ptr(d_state_tangent)) return fail(c, AWFL_ERR_ARG, "state pointer is NULL or misaligned");
   int rc = set_device(c);
@@ -871,6 +960,7 @@ int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
 }
 
 int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int nsteps, double dt, void *stream) {
+  if (c && c->nslabs > 1) return fail(c, AWFL_ERR_ARG, "the adjoint is not available on a slab");
   if (!c) return AWFL_ERR_ARG;
   if (fp32(c)) return fail(c, AWFL_ERR_ARG, "awfl_step_adjoint needs an FP64 context");
   if (bad_ptr(d_state_ckpt) || bad_ptr(d_lambda)) return fail(c, AWFL_ERR_ARG, "state or lambda pointer is NULL or misaligned");

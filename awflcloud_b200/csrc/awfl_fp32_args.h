@@ -29,6 +29,8 @@ struct SweepArgs32 {
   Bg32 bg;
   int tma;             // interior chunks' stencil rows arrive by TMA through tmap
   unsigned int *err;   // set to nonzero if a bounded wait of the sweep gave up
+  // x sweeps of a slab: the neighbouring slabs' halo columns (values), as SweepArgs::xh
+  const float *xh[2];
 };
 
 // Encodes *m as the tiled tensor map of an FP32 state with halo-inclusive extents

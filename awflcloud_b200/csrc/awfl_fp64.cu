@@ -115,6 +115,7 @@ struct InitArgs {
   double *state;
   float *state32, *comp32;
   int nx, ny, nz, hs, ord;
+  int xoff, nx_global;  // a slab of a larger grid: global x index of cell 0, the grid's nx
   double dx, dy, dz, xlen, ylen, zlen;
   int data_spec, sim2d;
   int kind, shape;
@@ -181,7 +182,7 @@ __global__ void init_state_kernel(InitArgs a) {
       for (int ii = 0; ii < a.ord; ii++) {
         const double zloc = (k + 0.5) * a.dz + a.pts[kk] * a.dz;
         double yloc = a.sim2d ? a.ylen / 2 : (j + 0.5) * a.dy + a.pts[jj] * a.dy;
-        const double xloc = (i + 0.5) * a.dx + a.pts[ii] * a.dx;
+        const double xloc = (a.xoff + i + 0.5) * a.dx + a.pts[ii] * a.dx;
         const double wt = a.wts[kk] * a.wts[jj] * a.wts[ii];
         if (a.kind == 1) {
           const double th = 300, rh = d_const_theta_density(th, zloc);
@@ -219,7 +220,7 @@ __global__ void init_state_kernel(InitArgs a) {
         }
       }
   if (a.noise_amp > 0) {
-    const unsigned long long cell = ((unsigned long long)k * a.ny + j) * a.nx + i;
+    const unsigned long long cell = ((unsigned long long)k * a.ny + j) * a.nx_global + (a.xoff + i);
     const unsigned long long base = a.seed * 0x100000001B3ULL;
     double nz_;
     if (a.noise_kind == 1) {  // Box-Muller: u1 in (0, 1], u2 in [0, 1)
@@ -250,6 +251,7 @@ cudaError_t launch_init_state_fp64(const InitLaunch &L, cudaStream_t st) {
   a.state32 = L.state32;
   a.comp32 = L.comp32;
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.hs = L.hs; a.ord = L.ord;
+  a.xoff = L.xoff; a.nx_global = L.nx_global > 0 ? L.nx_global : L.nx;
   a.dx = L.dx; a.dy = L.dy; a.dz = L.dz; a.xlen = L.xlen; a.ylen = L.ylen; a.zlen = L.zlen;
   a.data_spec = L.data_spec; a.sim2d = L.sim2d; a.kind = L.kind; a.shape = L.shape;
   a.x0 = L.x0; a.y0 = L.y0; a.z0 = L.z0; a.xrad = L.xrad; a.yrad = L.yrad; a.zrad = L.zrad;
@@ -276,7 +278,8 @@ __global__ void init_tracers_kernel(InitArgs a, int ntr) {
   const int hs = a.hs;
   const long sy = a.nx + 2 * hs, sz = (long)(a.ny + 2 * hs) * sy, sv = (long)(a.nz + 2 * hs) * sz;
   const long s = (hs + k) * sz + (hs + j) * sy + hs + i;
-  bool inside = k >= 1 * a.nz / 10 && k < 3 * a.nz / 10 && i >= 4 * a.nx / 10 && i < 6 * a.nx / 10;
+  const int ig = a.xoff + i;
+  bool inside = k >= 1 * a.nz / 10 && k < 3 * a.nz / 10 && ig >= 4 * a.nx_global / 10 && ig < 6 * a.nx_global / 10;
   if (!a.sim2d) inside = inside && j >= 4 * a.ny / 10 && j < 6 * a.ny / 10;
   for (int l = 0; l < ntr; l++) {
     double acc = 0;
@@ -286,7 +289,7 @@ __global__ void init_tracers_kernel(InitArgs a, int ntr) {
           for (int ii = 0; ii < a.ord; ii++) {
             const double zloc = (k + 0.5) * a.dz + a.pts[kk] * a.dz;
             const double yloc = a.sim2d ? a.ylen / 2 : (j + 0.5) * a.dy + a.pts[jj] * a.dy;
-            const double xloc = (i + 0.5) * a.dx + a.pts[ii] * a.dx;
+            const double xloc = (a.xoff + i + 0.5) * a.dx + a.pts[ii] * a.dx;
             const double wt = a.wts[kk] * a.wts[jj] * a.wts[ii];
             const double rh = d_const_theta_density(300, zloc);
             double tval;
@@ -305,6 +308,7 @@ cudaError_t launch_init_tracers_fp64(const InitLaunch &L, int ntr, cudaStream_t 
   memset(&a, 0, sizeof a);
   a.state = (double *)L.state;
   a.nx = L.nx; a.ny = L.ny; a.nz = L.nz; a.hs = L.hs; a.ord = L.ord;
+  a.xoff = L.xoff; a.nx_global = L.nx_global > 0 ? L.nx_global : L.nx;
   a.dx = L.dx; a.dy = L.dy; a.dz = L.dz; a.xlen = L.xlen; a.ylen = L.ylen; a.zlen = L.zlen;
   a.sim2d = L.sim2d;
   for (int m = 0; m < 9; m++) { a.pts[m] = m < L.ord ? L.pts[m] : 0; a.wts[m] = m < L.ord ? L.wts[m] : 0; }
@@ -456,6 +460,33 @@ cudaError_t launch_tracer_fields(const void *state, int fp32, long plane, const 
   if (blocks > (long)nsm * 8) blocks = (long)nsm * 8;
   tracer_fields_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, tracers, ntr, nx, ny, nz, hs,
                                                          out);
+  return cudaGetLastError();
+}
+
+// Halo columns a slab sends to its neighbours before an x split: the hs+1 first (side 0)
+// and last (side 1) interior columns of each variable, [2][5][nz][ny][hs+1].
+template <class T>
+__global__ void slab_pack_kernel(const T *state, int nx, int ny, int nz, int hs, T *send) {
+  const int w = hs + 1;
+  const long n = 2L * 5 * nz * ny * w;
+  const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % w);
+    long r = t / w;
+    const int j = (int)(r % ny); r /= ny;
+    const int k = (int)(r % nz); r /= nz;
+    const int v = (int)(r % 5);
+    const int side = (int)(r / 5);
+    const int i = side == 0 ? c : nx - w + c;
+    send[t] = state[v * sv + (hs + k) * sz + (hs + j) * sy + hs + i];
+  }
+}
+
+cudaError_t launch_slab_pack(const void *state, int esz, int nx, int ny, int nz, int hs, void *send, cudaStream_t st) {
+  const long n = 2L * 5 * nz * ny * (hs + 1);
+  const unsigned blocks = (unsigned)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  if (esz == 8) slab_pack_kernel<double><<<blocks, 256, 0, st>>>((const double *)state, nx, ny, nz, hs, (double *)send);
+  else slab_pack_kernel<float><<<blocks, 256, 0, st>>>((const float *)state, nx, ny, nz, hs, (float *)send);
   return cudaGetLastError();
 }
 

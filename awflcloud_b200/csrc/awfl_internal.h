@@ -53,6 +53,11 @@ struct SweepArgs {
   double dt;
   const double *dens_c, *denstheta_c;             // hyDensCells, hyDensThetaCells (nz+2hs)
   const double *dens_g, *denstheta_g, *pres_g;    // hyDensGLL, hyDensThetaGLL, hyPressureGLL (nz*ngll)
+  // x sweeps of a slab of a larger grid: the halo columns of a slab end that borders
+  // another slab, [5][nz][ny][hs+1] values per side (side 0: positions -(hs+1)..-1, the
+  // lower neighbour's last columns; side 1: positions nx..nx+hs, the upper neighbour's
+  // first); nullptr for an end with the grid's own boundary condition
+  const double *xh[2];
 };
 
 
@@ -60,6 +65,7 @@ struct InitLaunch {
   void *state;
   float *state32, *comp32;  // FP32 contexts: value and Kahan planes (state unused)
   int nx, ny, nz, hs, ord;
+  int xoff, nx_global;  // a slab: its first cell's global x index; the grid's nx (0: not a slab)
   double dx, dy, dz, xlen, ylen, zlen;
   int data_spec, sim2d, kind, shape;
   double x0, y0, z0, xrad, yrad, zrad, amp, pwr, noise_amp;
@@ -131,5 +137,8 @@ cudaError_t launch_output_fields(const void *state, int fp32, long plane, const 
                                  const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
                                  int nsm, double *out, cudaStream_t st);
 cudaError_t launch_selftest_pow(const double *x, double y, double *out, long n, int mode, cudaStream_t st);
+// The hs+1 first and last interior x columns of every variable of a state (value plane)
+// into send = [2][5][nz][ny][hs+1] elements of the state's type (esz 8 or 4).
+cudaError_t launch_slab_pack(const void *state, int esz, int nx, int ny, int nz, int hs, void *send, cudaStream_t st);
 
 }  // namespace awfl

@@ -15,7 +15,7 @@ namespace awfl {
 struct P64 {
   using Real = double;
   static constexpr int kWdiv = 1;
-  static constexpr bool kAsyncRing = false;
+  static constexpr bool kAsyncRing = true;
   static constexpr bool kTmaRing = false;
   // ord 5: 4 CTAs per SM (<= 128 registers), more warps to hide the FP64 latency
   // (measured +17%); ord 9 would spill heavily at that budget

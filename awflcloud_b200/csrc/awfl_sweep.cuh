@@ -23,6 +23,10 @@
 // 1557-1578): periodic wraps; a wall copies the edge cell with zero normal momentum, and
 // its boundary face uses the interior state on both sides. The halo values are also
 // written to the state's halo cells, as the reference does in place.
+// An x sweep of a slab of a larger grid (A.xh[side] != nullptr) takes an end's halo
+// values from the neighbouring slab's columns instead (hs+1 of them: the neighbour's edge
+// cell is reconstructed here, so the face between the slabs gets the same left and right
+// states, hence the same flux, as in the undivided grid).
 //
 // The physics policy P supplies the element type, the per-cell reconstruction (+ADER +
 // time average), the face flux, the tendency and the in-place update:
@@ -216,6 +220,18 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   }
   const long tv = (long)nz * ny * nx;
   const bool periodic = A.bc == BC_PERIODIC;
+  // x sweep of a slab: the ends bordering another slab, and that slab's columns
+  // ([5][nz][ny][HS+1] per side: side 0 holds positions -(HS+1)..-1, side 1 L..L+HS)
+  bool xlo = false, xhi = false;
+  int jline = 0;
+  if constexpr (DIR == 0) {
+    xlo = A.xh[0] != nullptr;
+    xhi = A.xh[1] != nullptr;
+    jline = bx * W + w;
+  }
+  auto XH = [&](int side, int v, int col) -> Real {
+    return Real(A.xh[side][(((long)v * nz + kline) * ny + jline) * (HS + 1) + col]);
+  };
 
   auto G = [&](int v, int p) -> Real { return P::load(A, lb + v * sv + p * sd); };
   // ring slot of position p: the async ring counts from p = HS so that a chunk's rows
@@ -235,6 +251,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   auto topval = [&](int v, int p, bool first) -> Real {  // p >= L
     const int q = p - L;
     if (q >= HS) return Real(0);  // beyond the last cell's stencil: never read
+    if (xhi) return XH(1, v, q);
     if (periodic) return first ? G(v, q) : sWrap[v][q * W + w];
     return v == NM ? Real(0) : G(v, L - 1);
   };
@@ -278,9 +295,12 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   if (valid && c < HS) {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-      const Real bot = periodic ? G(v, L + c - HS) : (v == NM ? Real(0) : G(v, 0));
-      const Real orig = G(v, c);
-      const Real top = periodic ? orig : (v == NM ? Real(0) : G(v, L - 1));
+      const Real bot = xlo ? XH(0, v, c + 1) : (periodic ? G(v, L + c - HS) : (v == NM ? Real(0) : G(v, 0)));
+      const Real top = xhi ? XH(1, v, c) : (periodic ? G(v, c) : (v == NM ? Real(0) : G(v, L - 1)));
+      // position c of a wall line shorter than HS is a top halo cell: its stencil value is
+      // the wall copy (read from the interior, never from a halo cell another thread of
+      // this prologue is writing); periodic lines are at least HS long (awfl_create)
+      const Real orig = c < L ? G(v, c) : top;
       ringAt(v, c - HS) = bot;
       ringAt(v, c) = orig;
       sWrap[v][c * W + w] = orig;
@@ -308,9 +328,14 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       for (int v = 0; v < 5; v++) pre[v] = p < L ? G(v, p) : topval(v, p, true);
     }
   }
-  // periodic: the left state of face 0 is the right edge of cell L-1
-  if (valid && periodic && c == 0) {
+  // periodic: the left state of face 0 is the right edge of cell L-1; a slab bordering
+  // another below: the right edge of that slab's last cell (position -1)
+  if (valid && (periodic || xlo) && c == 0) {
     auto wrapSten = [&](int v, int m) -> Real {
+      if (xlo) {
+        const int p = -1 - HS + m;
+        return p < 0 ? XH(0, v, p + HS + 1) : G(v, p);
+      }
       int p = L - 1 - HS + m;
       p %= L;
       if (p < 0) p += L;
@@ -400,7 +425,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
         qL[v] = c == 0 ? sER[v][E(0)] : up;
       }
       if (act) {
-        if (base + c == 0 && !periodic) {
+        if (base + c == 0 && !periodic && !xlo) {
 #pragma unroll
           for (int v = 0; v < 5; v++) qL[v] = eL[v];
         }
@@ -447,7 +472,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 #pragma unroll
       for (int v = 0; v < 5; v++) qR[v] = sEL[v][E(c)];
 #pragma unroll
-      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic) ? qR[v] : sER[v][E(c)];
+      for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic && !xlo) ? qR[v] : sER[v][E(c)];
       P::template flux<DIR, NG>(qL, qR, DIR == 2 ? f : kline, A, F);
 #pragma unroll
       for (int v = 0; v < 5; v++) sF[v][E(c + 1)] = F[v];
@@ -488,6 +513,16 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       qL[v] = sER[v][E(0)];
       qR[v] = periodic ? sEL0[v][w] : qL[v];
       Fl[v] = sF[v][E(0)];
+    }
+    if (xhi) {  // a slab bordering another above: the left edge of that slab's first cell
+      auto hiSten = [&](int v, int m) -> Real {
+        const int p = L - HS + m;
+        return p >= L ? XH(1, v, p - L) : ringAt(v, p);
+      };
+      Real hL[5], hR[5], hs_;
+      P::template recon<ORD, DIR>(hiSten, kline, A, hL, hR, hs_, -1L);
+#pragma unroll
+      for (int v = 0; v < 5; v++) qR[v] = hL[v];
     }
     P::template flux<DIR, NG>(qL, qR, DIR == 2 ? L : kline, A, F);
     typename P::Aux aux;

@@ -12,16 +12,16 @@
 //   tracer_face_kernel    per face: edge BCs (Spatial:826-835), the state's Riemann flux
 //                         (riemann) and the upwind tracer fluxes (Spatial:891-901,
 //                         1249-1259, 1633-1643)
-//   tracer_limit_kernel   per face: the positivity limiter (Spatial:904-935, 1262-1293,
-//                         1646-1677) from the unscaled fluxes
+//   tracer_limit_kernel   per line: the positivity limiter (Spatial:904-935, 1262-1293,
+//                         1646-1677), faces in the reference's serial order, in place
 //   tracer_update_kernel  per cell: tendency, density multiplied back, apply
 //                         (Spatial:948-955; Temporal_ader.h:67-69), and the halo cells of
 //                         this direction left holding tracer/density, as the reference's
 //                         in-place halo fill leaves them
 //
-// Decisions where the reference's code is not well defined: the limiter reads unscaled
-// fluxes (the reference scales tracerFlux in place while other iterations read it); the
-// y branch for v < 0 reads the faces along y (the reference indexes tracerFlux(tr,k,j,ind_j),
+// Decisions where the reference's code is not well defined: the limiter follows the
+// reference's serial loop order (it scales tracerFlux in place while other iterations of
+// its parallel_for read it, so only the serial order gives one result); the y branch for v < 0 reads the faces along y (the reference indexes tracerFlux(tr,k,j,ind_j),
 // Spatial:1285-1286); a periodic z wraps like x and y (the reference reads outside the
 // array there). Stencil halos are computed from the boundary conditions (periodic wrap;
 // wall: the edge cell, the state's normal momentum zero), as the reference's halo fill
@@ -264,39 +264,79 @@ __global__ void __launch_bounds__(128) tracer_face_kernel(TracerArgs T, int hs) 
   }
 }
 
+// Positivity limiter (Spatial:904-935, 1262-1293, 1646-1677) in the reference's serial
+// loop order: one thread per line visits the faces in increasing order and scales each in
+// place by its upwind cell's factor, computed from that cell's two faces as they stand at
+// that moment (the face behind already scaled, the face itself and the ones ahead not
+// yet) -- the one defined result of the reference's in-place parallel_for, the one its
+// CPU build gives when the loop runs in order. Faces of other lines are never read.
 template <int DIR>
 __global__ void __launch_bounds__(128) tracer_limit_kernel(TracerArgs T, int hs) {
   const SweepArgs &A = T.A;
   const Geo<DIR> G(A, hs);
-  const long nf = G.nface();
-  const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (f >= nf) return;
-  const int fx = G.nx + (DIR == 0), fy = G.ny + (DIR == 1);
-  const int i = (int)(f % fx), j = (int)((f / fx) % fy), k = (int)(f / ((long)fx * fy));
-  const int pf = DIR == 0 ? i : (DIR == 1 ? j : k);
   const int n = G.n();
-  const double un = T.UN[f];
-  int ind = -1;
-  if (un > 0) { ind = pf - 1; if (ind == -1) ind = n - 1; }
-  else if (un < 0) { ind = pf; if (ind == n) ind = 0; }
-  int ck, cj, ci, fk, fj, fi;
-  if (ind >= 0) {
-    G.at(k, j, i, ind, ck, cj, ci);
-    G.at(k, j, i, ind + 1, fk, fj, fi);
-  }
+  const long nlines = DIR == 0 ? (long)G.nz * G.ny : (DIR == 1 ? (long)G.nz * G.nx : (long)G.ny * G.nx);
+  const long line = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (line >= nlines) return;
+  int k0, j0, i0;  // the line's cell 0
+  if (DIR == 0) { i0 = 0; j0 = (int)(line % G.ny); k0 = (int)(line / G.ny); }
+  else if (DIR == 1) { j0 = 0; i0 = (int)(line % G.nx); k0 = (int)(line / G.nx); }
+  else { k0 = 0; i0 = (int)(line % G.nx); j0 = (int)(line / G.nx); }
+  const long nf = G.nface();
+  auto face = [&](int p) {
+    int kk, jj, ii;
+    G.at(k0, j0, i0, p, kk, jj, ii);
+    return G.face(kk, jj, ii);
+  };
   const double eps = 1.e-10;
   for (int l = 0; l < T.ntr; l++) {
-    const double F = T.TF[l * nf + f];
-    double out = F;
-    if (ind >= 0 && ((T.pos >> l) & 1ull)) {
-      const double f1 = dmin(T.TF[l * nf + G.face(ck, cj, ci)], 0.);
-      const double f2 = dmax(T.TF[l * nf + G.face(fk, fj, fi)], 0.);
-      const double fluxOut = A.dt * (f2 - f1) / A.dxd;
-      const double dens = T.D[G.cell(ck, cj, ci)] + A.dens_c[hs + ck];
-      const double q = T.tr[l * G.sv + G.g(ck, cj, ci)] / dens;  // the divided tracer (Spatial:624-627)
-      out = F * dmin(1., q * dens / (fluxOut + eps));
+    const double *TF = T.TF + l * nf;
+    double *TF2 = T.TF2 + l * nf;
+    const bool posdef = (T.pos >> l) & 1ull;
+    double prev = 0., s0 = 0., s1 = 0.;  // scaled fluxes of the face behind, faces 0 and 1
+    for (int f = 0; f <= n; f++) {
+      const long fi = face(f);
+      const double F = TF[fi];
+      double out = F;
+      if (posdef) {
+        const double un = T.UN[fi];
+        int c = -1;
+        double f1 = 0., f2 = 0.;
+        if (un > 0) {
+          if (f == 0) {  // upwind cell n-1: faces n-1 and n, not reached yet
+            c = n - 1;
+            f1 = dmin(n == 1 ? F : TF[face(n - 1)], 0.);
+            f2 = dmax(TF[face(n)], 0.);
+          } else {       // upwind cell f-1: face f-1 scaled already, face f not yet
+            c = f - 1;
+            f1 = dmin(prev, 0.);
+            f2 = dmax(F, 0.);
+          }
+        } else if (un < 0) {
+          if (f == n) {  // upwind cell 0: faces 0 and 1, scaled already (face 1 is this one when n == 1)
+            c = 0;
+            f1 = dmin(s0, 0.);
+            f2 = dmax(n == 1 ? F : s1, 0.);
+          } else {       // upwind cell f: this face and the next, not yet scaled
+            c = f;
+            f1 = dmin(F, 0.);
+            f2 = dmax(TF[face(f + 1)], 0.);
+          }
+        }
+        if (c >= 0) {
+          int ck, cj, ci;
+          G.at(k0, j0, i0, c, ck, cj, ci);
+          const double fluxOut = A.dt * (f2 - f1) / A.dxd;
+          const double dens = T.D[G.cell(ck, cj, ci)] + A.dens_c[hs + ck];
+          const double q = T.tr[l * G.sv + G.g(ck, cj, ci)] / dens;  // the divided tracer (Spatial:624-627)
+          out = F * dmin(1., q * dens / (fluxOut + eps));
+        }
+      }
+      TF2[fi] = out;
+      prev = out;
+      if (f == 0) s0 = out;
+      if (f == 1) s1 = out;
     }
-    T.TF2[l * nf + f] = out;
   }
 }
 
@@ -351,7 +391,8 @@ cudaError_t run(const TracerArgs &T, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   tracer_cell_kernel<ORD, DIR><<<gc, 128, 0, st>>>(T);
   tracer_face_kernel<DIR, NG><<<gf, 128, 0, st>>>(T, HS);
-  tracer_limit_kernel<DIR><<<gf, 128, 0, st>>>(T, HS);
+  const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
+  tracer_limit_kernel<DIR><<<(unsigned)((nlines + 127) / 128), 128, 0, st>>>(T, HS);
   tracer_update_kernel<DIR><<<gc, 128, 0, st>>>(T, HS);
   return cudaGetLastError();
 }

@@ -164,9 +164,11 @@ int awfl_write_netcdf_fields_tracers(awfl_ctx *ctx, const char *path, const doub
  * cells along dir are left holding tracer/rho, as the reference's in-place halo fill leaves
  * them. Allocates (once per context, grown when ntracers grows) a scratch buffer of
  * (2*ngll^2 + 11 + 2*ntracers) doubles per cell and (2*ntracers + 1) per face. Decisions
- * where the reference's code is not well defined: the limiter scales each face by its
- * upwind cell's factor computed from unscaled fluxes; the y limiter's v < 0 branch reads
- * the y faces; a periodic z wraps. */
+ * where the reference's code is not well defined: the limiter scales the faces of a line
+ * in place in increasing order, as the reference's loop does when it runs serially (it
+ * scales in place while other iterations read, Spatial:904-935); the y limiter's v < 0
+ * branch reads the y faces (the reference swaps j and i there, :1285-1286); a periodic z
+ * wraps (the reference reads outside its flux array there). */
 int awfl_split_tracers(awfl_ctx *ctx, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
                        int dir, void *stream);
 /* One time step with tracers (Temporal_ader::timeStep with the tracer code compiled in):
@@ -197,6 +199,35 @@ int awfl_split(awfl_ctx *ctx, void *d_state, double dt, int dir, void *stream);
  * flipped after every step). sim2d (ny == 1) skips the Y split, whose tendency the
  * reference sets to zero. */
 int awfl_step(awfl_ctx *ctx, void *d_state, double dt, void *stream);
+
+/* ---- x-slab decomposition of one grid over several GPUs: no counterpart in the active
+ * reference, whose single domain lives in one process; its legacy model decomposes x/y
+ * with MPI halo exchanges (qjrmsCode/Exchange.cpp:106-176) and an MPI_Allreduce(MIN) of dt
+ * (qjrmsCode/Initializer.cpp:263). Slab s of n owns the x cells [xoff, xoff + nx_s) of the
+ * grid `global` (nx split as evenly as possible, every slab at least hs+1 cells) with the
+ * whole y and z extent; its context works on its own state (awfl_sizes: nx_s in x) with
+ * the grid's dx, places initial data by global cell (awfl_init_state), and runs y and z
+ * splits alone (awfl_split). Before each x split the slabs trade hs+1 columns:
+ *   awfl_slab_pack   copies the slab's first and last hs+1 interior columns of every
+ *                    variable into d_send = [2][5][nz][ny][hs+1] (side 0: first columns,
+ *                    for the slab below; side 1: last columns, for the slab above);
+ *   (the caller moves side 1 of slab s to side 0 of d_recv of slab s+1, and side 0 of
+ *   slab s to side 1 of d_recv of slab s-1: NCCL send/recv, a copy, ...; a periodic x
+ *   wraps from the last slab to the first);
+ *   awfl_split_slab  the fused x split with the neighbours' columns (d_recv, same layout:
+ *                    side 0 = the slab below's last columns, side 1 = the slab above's
+ *                    first); an end at a wall of the grid ignores its side.
+ * The interior cells then advance bit for bit as in the undivided grid. The CFL time step
+ * of the grid is the minimum of the slabs' awfl_cfl. Tracer transport, the tangent-linear
+ * step and the adjoint refuse slab contexts, and so do awfl_step, awfl_split and
+ * awfl_compute_tendencies for the x direction when an end borders another slab. */
+int awfl_create_slab(const awfl_config *global, int nslabs, int slab, int device, awfl_ctx **out);
+/* The slab's place: slab count, index, global x index of its first cell, the grid's nx,
+ * and the elements of one d_send / d_recv buffer (2*5*nz*ny*(hs+1)). Any pointer may be
+ * NULL; a context made by awfl_create is slab 0 of 1. */
+int awfl_slab_info(const awfl_ctx *ctx, int *nslabs, int *slab, int *xoff, int *nx_global, long *halo_elems);
+int awfl_slab_pack(awfl_ctx *ctx, const void *d_state, void *d_send, void *stream);
+int awfl_split_slab(awfl_ctx *ctx, void *d_state, const void *d_recv, double dt, void *stream);
 
 /* Tangent-linear time step (FP64 contexts): d_state_tangent holds two FP64 state planes,
  * the state then a perturbation direction. The state advances exactly like awfl_step

@@ -71,7 +71,9 @@ static const oreal C0 = 27.5629410929725921310572974482;
 static const oreal GAMMA = 1.40027894002789400278940027894;
 
 enum { idR = 0, idU = 1, idV = 2, idW = 3, idT = 4 };
-enum { BC_PERIODIC = 0, BC_WALL = 1 };
+/* BC_GIVEN (x only; test infrastructure for slab decompositions): the caller supplies the
+ * x halos (no halo fill); the line ends' edge values are copied as at a wall. */
+enum { BC_PERIODIC = 0, BC_WALL = 1, BC_GIVEN = 2 };
 enum { DATA_THERMAL = 1, DATA_COLLISION = 2, DATA_STRAKA = 3, DATA_IGW = 4 };
 
 struct oracle_ctx {
@@ -330,6 +332,7 @@ static void time_avg_full(oreal dts[NADER][NGLL], oreal dt) {
 /* Spatial:631-662 (x), 994-1025 (y), 1351-1382 (z). */
 static void fill_halos(const oracle_ctx *c, oreal *st, int dir) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
+  if (dir == 0 && c->bc[0] == BC_GIVEN) return;
   if (dir == 0) {
 #pragma omp parallel for collapse(2)
     for (int k = 0; k < nz; k++)
@@ -624,40 +627,50 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
         }
   }
 
-  /* Positivity limiter of the tracer fluxes (Spatial:904-935, 1262-1293, 1646-1677). Each
-   * face's flux is scaled by the factor of its upwind cell, computed from that cell's
-   * UNSCALED face fluxes: the reference scales tracerFlux in place while other iterations
-   * read it (a data race under its parallel_for), so the read-before-any-scaling order is
-   * taken. The y branch for v < 0 reads the faces along y (the reference indexes
-   * tracerFlux(tr,k,j,ind_j) there, Spatial:1285-1286, with j and i swapped), and a
-   * periodic z wraps like x and y (the reference reads outside the array there). */
+  /* Positivity limiter of the tracer fluxes (Spatial:904-935, 1262-1293, 1646-1677), in the
+   * reference's serial loop order: the reference scales tracerFlux in place inside a
+   * parallel_for whose other iterations read it, so its one defined result is the serial
+   * one (its CPU build run in order), which this restates: along each line the faces are
+   * visited in increasing order and each is scaled in place by its upwind cell's factor,
+   * computed from that cell's two faces as they stand at that moment (the face behind
+   * already scaled, the face itself and the ones ahead not yet). The y branch for v < 0
+   * reads the faces along y (the reference indexes tracerFlux(tr,k,j,ind_j) there,
+   * Spatial:1285-1286, with j and i swapped), and a periodic z wraps like x and y (the
+   * reference reads outside the array there). */
   if (ntr > 0) {
     const int n = dir == 0 ? nx : (dir == 1 ? ny : nz);
     const oreal eps = 1.e-10;
-    int ek = nz + (dir == 2), ej = ny + (dir == 1), ei = nx + (dir == 0);
+    const int la = dir == 2 ? ny : nz, lb = dir == 0 ? ny : nx;  /* the lines: (la, lb) */
+    const long nflim = (long)ntr * (nz + 1) * (ny + 1) * (nx + 1);
+    memcpy(c->tflux_lim, c->tflux, sizeof(oreal) * (size_t)nflim);
 #pragma omp parallel for collapse(3)
-    for (int k = 0; k < ek; k++)
-      for (int j = 0; j < ej; j++)
-        for (int i = 0; i < ei; i++)
-          for (int l = 0; l < ntr; l++) {
-            long fi = fidx(c, l, k, j, i);
-            oreal F = c->tflux[fi];
-            c->tflux_lim[fi] = F;
-            if (!c->trpos[l]) continue;
-            oreal un = 0.5 * (c->limits[lidx(c, nm, 0, k, j, i)] + c->limits[lidx(c, nm, 1, k, j, i)]);
-            int f = dir == 0 ? i : (dir == 1 ? j : k);
+    for (int l = 0; l < ntr; l++)
+      for (int a = 0; a < la; a++)
+        for (int b = 0; b < lb; b++) {
+          if (!c->trpos[l]) continue;
+          /* the line's cell at index p along dir */
+#define LK(p) (dir == 2 ? (p) : a)
+#define LJ(p) (dir == 1 ? (p) : (dir == 2 ? a : b))
+#define LI(p) (dir == 0 ? (p) : b)
+          oreal *TF = c->tflux_lim;
+          for (int f = 0; f <= n; f++) {
+            const long fi = fidx(c, l, LK(f), LJ(f), LI(f));
+            const oreal un = 0.5 * (c->limits[lidx(c, nm, 0, LK(f), LJ(f), LI(f))] +
+                                    c->limits[lidx(c, nm, 1, LK(f), LJ(f), LI(f))]);
             int ind;
             if (un > 0) { ind = f - 1; if (ind == -1) ind = n - 1; }
             else if (un < 0) { ind = f; if (ind == n) ind = 0; }
             else continue;
-            int ck = dir == 2 ? ind : k, cj = dir == 1 ? ind : j, ci = dir == 0 ? ind : i;
-            int fk1 = dir == 2 ? ind + 1 : k, fj1 = dir == 1 ? ind + 1 : j, fi1 = dir == 0 ? ind + 1 : i;
-            oreal f1 = dmin(c->tflux[fidx(c, l, ck, cj, ci)], 0.);
-            oreal f2 = dmax(c->tflux[fidx(c, l, fk1, fj1, fi1)], 0.);
-            oreal fluxOut = dt * (f2 - f1) / dxd;
-            oreal dens = st[sidx(c, idR, HS + ck, HS + cj, HS + ci)] + c->hyDensCells[HS + ck];
-            c->tflux_lim[fi] = F * dmin(1., tr[sidx(c, l, HS + ck, HS + cj, HS + ci)] * dens / (fluxOut + eps));
+            const oreal f1 = dmin(TF[fidx(c, l, LK(ind), LJ(ind), LI(ind))], 0.);
+            const oreal f2 = dmax(TF[fidx(c, l, LK(ind + 1), LJ(ind + 1), LI(ind + 1))], 0.);
+            const oreal fluxOut = dt * (f2 - f1) / dxd;
+            const oreal dens = st[sidx(c, idR, HS + LK(ind), HS + LJ(ind), HS + LI(ind))] + c->hyDensCells[HS + LK(ind)];
+            TF[fi] *= dmin(1., tr[sidx(c, l, HS + LK(ind), HS + LJ(ind), HS + LI(ind))] * dens / (fluxOut + eps));
           }
+#undef LK
+#undef LJ
+#undef LI
+        }
   }
 
   /* Flux divergence (K5: Spatial:940-956, 1298-1310, 1680-1696). */
@@ -694,10 +707,10 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
         }
 }
 
-/* Temporal_ader::timeStep (Temporal_ader.h:48-72) with the tracer transport compiled in:
- * per split, computeTendencies on state and tracers, then state += dt*tend and
- * tracers += dt*tracerTend. sim2d's y split zeroes both tendencies (Spatial:572-575). */
-void oracle_time_step_tracers(oracle_ctx *c, oreal *st, oreal *tr, int ntr, const int *pos, oreal dt) {
+/* One split of Temporal_ader::timeStep (Temporal_ader.h:50-70) with the tracer transport
+ * compiled in: computeTendencies along dir on state and tracers, then state += dt*tend
+ * and tracers += dt*tracerTend. sim2d's y split zeroes both tendencies (Spatial:572-575). */
+void oracle_split_tracers(oracle_ctx *c, oreal *st, oreal *tr, int ntr, const int *pos, oreal dt, int dir) {
   const long nf = (long)(c->nz + 1) * (c->ny + 1) * (c->nx + 1);
   const long ncell = (long)c->nz * c->ny * c->nx;
   oreal *tend = (oreal *)calloc((size_t)NUMSTATE * ncell, sizeof(oreal));
@@ -708,27 +721,26 @@ void oracle_time_step_tracers(oracle_ctx *c, oreal *st, oreal *tr, int ntr, cons
   c->tlimits = (oreal *)calloc((size_t)ntr * 2 * nf + 1, sizeof(oreal));
   c->tflux = (oreal *)calloc((size_t)ntr * nf + 1, sizeof(oreal));
   c->tflux_lim = (oreal *)calloc((size_t)ntr * nf + 1, sizeof(oreal));
-  for (int split = 0; split < 3; split++) {
-    int dir;
-    if (c->dimswitch) dir = split;
-    else dir = 2 - split;
-    if (dir == 1 && c->sim2d) {
-      memset(tend, 0, sizeof(oreal) * NUMSTATE * ncell);
-      memset(c->ttend, 0, sizeof(oreal) * ntr * ncell);
-    } else {
-      oracle_compute_tendencies_dir(c, st, tend, dt, dir);
-    }
-    oracle_apply(c, st, tend, dt);
-    for (int k = 0; k < c->nz; k++)
-      for (int j = 0; j < c->ny; j++)
-        for (int i = 0; i < c->nx; i++)
-          for (int l = 0; l < ntr; l++)
-            tr[sidx(c, l, HS + k, HS + j, HS + i)] += dt * c->ttend[tidx(c, l, k, j, i)];
-  }
-  c->dimswitch = !c->dimswitch;
+  if (!(dir == 1 && c->sim2d)) oracle_compute_tendencies_dir(c, st, tend, dt, dir);
+  oracle_apply(c, st, tend, dt);
+  for (int k = 0; k < c->nz; k++)
+    for (int j = 0; j < c->ny; j++)
+      for (int i = 0; i < c->nx; i++)
+        for (int l = 0; l < ntr; l++)
+          tr[sidx(c, l, HS + k, HS + j, HS + i)] += dt * c->ttend[tidx(c, l, k, j, i)];
   free(tend); free(c->ttend); free(c->tlimits); free(c->tflux); free(c->tflux_lim);
   c->ntr = 0; c->trpos = NULL; c->tr = NULL; c->ttend = NULL;
   c->tlimits = c->tflux = c->tflux_lim = NULL;
+}
+
+/* Temporal_ader::timeStep (Temporal_ader.h:48-72) with the tracer transport compiled in:
+ * oracle_split_tracers for each split in the dimSwitch order. */
+void oracle_time_step_tracers(oracle_ctx *c, oreal *st, oreal *tr, int ntr, const int *pos, oreal dt) {
+  for (int split = 0; split < 3; split++) {
+    const int dir = c->dimswitch ? split : 2 - split;
+    oracle_split_tracers(c, st, tr, ntr, pos, dt, dir);
+  }
+  c->dimswitch = !c->dimswitch;
 }
 
 /* Spatial:565-594 */
@@ -1016,6 +1028,11 @@ static void matmul_cr(const oreal *A, int K, int R, const oreal *B, int C, oreal
       for (int k = 0; k < K; k++) tmp += A[k * R + r] * B[cc * K + k];
       out[cc * R + r] = tmp;
     }
+}
+
+/* Grid spacing set directly (a slab of a larger grid keeps the whole grid's dx). */
+void oracle_set_spacing(oracle_ctx *c, oreal dx, oreal dy, oreal dz) {
+  c->dx = dx; c->dy = dy; c->dz = dz;
 }
 
 oracle_ctx *oracle_create(int nx, int ny, int nz, oreal xlen, oreal ylen, oreal zlen,

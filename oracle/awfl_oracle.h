@@ -34,6 +34,8 @@ typedef struct oracle_ctx oracle_ctx;
 oracle_ctx *oracle_create(int nx, int ny, int nz, oreal xlen, oreal ylen, oreal zlen,
                           int bc_x, int bc_y, int bc_z, int weno_scalars, int weno_winds,
                           int data_spec);
+/* Grid spacing set directly (a slab of a larger grid keeps the whole grid's dx). */
+void oracle_set_spacing(oracle_ctx *c, oreal dx, oreal dy, oreal dz);
 void oracle_destroy(oracle_ctx *c);
 int oracle_ord(void);
 int oracle_ngll(void);
@@ -69,6 +71,8 @@ void oracle_time_step(oracle_ctx *c, oreal *state, oreal dt);
  * pos[l] != 0 marks a positive-definite tracer (limited). Decisions where the reference's
  * code is not well defined are stated at the limiter. */
 void oracle_time_step_tracers(oracle_ctx *c, oreal *state, oreal *tracers, int ntr, const int *pos, oreal dt);
+/* One split of that step along dir (0/1/2). */
+void oracle_split_tracers(oracle_ctx *c, oreal *state, oreal *tracers, int ntr, const int *pos, oreal dt, int dir);
 int oracle_get_dimswitch(const oracle_ctx *c);
 void oracle_set_dimswitch(oracle_ctx *c, int v);
 

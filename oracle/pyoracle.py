@@ -48,12 +48,13 @@ def oracle_path(ord_: int, crpow: bool = False) -> str:
     return os.path.join(HERE, "liboracle_o%d%s.so" % (ord_, "_crpow" if crpow else ""))
 
 
-def ref_path(ord_: int, crpow: bool = False) -> str:
-    return os.path.join(HERE, "_ref", "libawflref_o%d%s.so" % (ord_, "_crpow" if crpow else ""))
+def ref_path(ord_: int, crpow: bool = False, tracers: bool = False) -> str:
+    return os.path.join(HERE, "_ref", "libawflref_%so%d%s.so" % ("trc_" if tracers else "", ord_,
+                                                                 "_crpow" if crpow else ""))
 
 
-def ref_available(ord_: int = 5, crpow: bool = False) -> bool:
-    return os.path.exists(ref_path(ord_, crpow))
+def ref_available(ord_: int = 5, crpow: bool = False, tracers: bool = False) -> bool:
+    return os.path.exists(ref_path(ord_, crpow, tracers))
 
 
 class _Grid:
@@ -103,6 +104,8 @@ class Oracle(_Grid):
             L.oracle_add_theta_noise.argtypes = [_VP, _DP, ctypes.c_ulonglong, _D]
             L.oracle_init_tracers.argtypes = [_VP, _DP, _I]
             L.oracle_time_step_tracers.argtypes = [_VP, _DP, _DP, _I, ctypes.POINTER(_I), _D]
+            L.oracle_split_tracers.argtypes = [_VP, _DP, _DP, _I, ctypes.POINTER(_I), _D, _I]
+            L.oracle_set_spacing.argtypes = [_VP, _D, _D, _D]
             L.oracle_compute_dt.restype = _D
             L.oracle_compute_dt.argtypes = [_VP, _DP, _D]
             L.oracle_compute_tendencies_dir.argtypes = [_VP, _DP, _DP, _D, _I]
@@ -156,6 +159,16 @@ class Oracle(_Grid):
         pos = [1] * n if pos is None else pos
         flags = (_I * max(n, 1))(*[int(bool(p)) for p in pos])
         self.L.oracle_time_step_tracers(self.h, _ptr(st), _ptr(tr), n, flags, dt)
+
+    def set_spacing(self, dx, dy, dz):
+        self.L.oracle_set_spacing(self.h, dx, dy, dz)
+
+    def split_tracers(self, st, tr, dt, d, pos=None):
+        """One split (direction d) of state and tracers with the tracer code compiled in."""
+        n = tr.shape[0]
+        pos = [1] * n if pos is None else pos
+        flags = (_I * max(n, 1))(*[int(bool(p)) for p in pos])
+        self.L.oracle_split_tracers(self.h, _ptr(st), _ptr(tr), n, flags, dt, d)
 
     def compute_dt(self, st, cfl=0.8):
         return self.L.oracle_compute_dt(self.h, _ptr(st), cfl)
@@ -267,10 +280,10 @@ class RefHarness(_Grid):
     _libs: dict = {}
 
     @classmethod
-    def lib(cls, ord_, crpow=False):
-        key = (ord_, crpow)
+    def lib(cls, ord_, crpow=False, tracers=False):
+        key = (ord_, crpow, tracers)
         if key not in cls._libs:
-            path = ref_path(ord_, crpow)
+            path = ref_path(ord_, crpow, tracers)
             if not os.path.exists(path):
                 raise FileNotFoundError(path + " (build with: make -C oracle ref)")
             L = ctypes.CDLL(path)
@@ -301,17 +314,31 @@ class RefHarness(_Grid):
             L.awflref_coefs_to_tv.restype = _D
             L.awflref_coefs_to_tv.argtypes = [_DP, _I]
             L.awflref_weno_coefs.argtypes = [_VP, _DP, _DP]
+            L.awflref_set_tracer_pos.argtypes = [_I, ctypes.POINTER(_I)]
+            L.awflref_has_tracer_transport.restype = _I
+            L.awflref_set_tracers.argtypes = [_VP, _DP]
+            L.awflref_split.argtypes = [_VP, _D, _I]
+            L.awflref_output.argtypes = [_VP, _D]
+            L.awflref_output_size.restype = ctypes.c_long
+            L.awflref_output_size.argtypes = [ctypes.c_char_p]
+            L.awflref_output_get.argtypes = [ctypes.c_char_p, _DP]
             cls._libs[key] = L
         return cls._libs[key]
 
     def __init__(self, nx, ny, nz, xlen=20000.0, ylen=20000.0, zlen=10000.0, bc=(0, 0, 1),
-                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5, crpow=False, ntracers=0):
+                 weno_scalars=True, weno_winds=True, data="thermal", ord_=5, crpow=False, ntracers=0,
+                 tracer_transport=False, pos=None):
         """crpow: the reference's code with its pow/exp calls bound to a correctly rounded
         implementation instead of glibc's. ntracers: tracers registered with addTracer
-        before init (the driver's names: uniform, theta, block)."""
+        before init (the driver's names: uniform, theta, block), posDef flags `pos`
+        (default all true). tracer_transport: the build with the reference's tracer code
+        compiled in (its NO_TRACERS line blanked, serial loops)."""
         super().__init__(ord_, nx, ny, nz)
-        self.L = self.lib(ord_, crpow)
+        self.L = self.lib(ord_, crpow, tracer_transport)
         self.L.awflref_set_num_tracers(ntracers)
+        if pos is not None:
+            arr = (_I * len(pos))(*[int(p) for p in pos])
+            self.L.awflref_set_tracer_pos(len(pos), arr)
         self.ntracers = ntracers
         self.h = self.L.awflref_create(nx, ny, nz, xlen, ylen, zlen, bc[0], bc[1], bc[2],
                                        int(weno_scalars), int(weno_winds), data.encode())
@@ -335,6 +362,35 @@ class RefHarness(_Grid):
         assert tr.size == self.L.awflref_tracer_size(self.h)
         self.L.awflref_get_tracers(self.h, _ptr(tr))
         return tr
+
+    def set_tracers(self, tr):
+        tr = np.ascontiguousarray(tr, dtype=np.float64)
+        assert tr.size == self.L.awflref_tracer_size(self.h)
+        self.L.awflref_set_tracers(self.h, _ptr(tr))
+
+    def split(self, dt, spl):
+        """One split of Temporal_ader::timeStep: computeTendencies(spl) on state and
+        tracers, then both applies."""
+        self.L.awflref_split(self.h, dt, spl)
+
+    def output(self, etime):
+        """Spatial::output on the current state: {variable name: values} of everything it
+        wrote (the netCDF stand-in records them instead of writing a file)."""
+        self.L.awflref_output(self.h, etime)
+        names = ["x", "y", "z", "hyDens", "hyPressure", "hyTheta", "t", "dens_pert", "u", "v", "w",
+                 "pot_temp_pert", "pressure_pert"] + ["tracer_" + n for n in ("uniform", "theta", "block")]
+        out = {}
+        for n in names:
+            sz = self.L.awflref_output_size(n.encode())
+            if sz >= 0:
+                a = np.zeros(sz)
+                self.L.awflref_output_get(n.encode(), _ptr(a))
+                out[n] = a
+        return out
+
+    @property
+    def has_tracer_transport(self):
+        return bool(self.L.awflref_has_tracer_transport())
 
     def get_state(self):
         st = self.new_state()

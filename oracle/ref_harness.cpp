@@ -60,12 +60,32 @@ inline double unit_uniform(uint64_t seed, uint64_t i) {
 }  // namespace
 
 // Number of tracers the next awflref_create registers with addTracer before init, named
-// like the reference driver's three (driver.cpp:27-29); 0 by default.
+// like the reference driver's three (driver.cpp:27-29); 0 by default. Their posDef flags
+// (addTracer's second argument, Spatial...h:119-125): true unless set otherwise.
 int g_pending_tracers = 0;
+int g_pending_pos[64];
+bool g_pending_pos_set = false;
 
 extern "C" {
 
-void awflref_set_num_tracers(int n) { g_pending_tracers = n < 0 ? 0 : n; }
+void awflref_set_num_tracers(int n) {
+  g_pending_tracers = n < 0 ? 0 : (n > 64 ? 64 : n);
+  g_pending_pos_set = false;
+}
+// posDef flags of the tracers the next awflref_create registers (after set_num_tracers)
+void awflref_set_tracer_pos(int n, const int *pos) {
+  for (int i = 0; i < 64; i++) g_pending_pos[i] = i < n ? pos[i] : 1;
+  g_pending_pos_set = true;
+}
+// 1 when this build has the reference's tracer transport compiled in (NO_TRACERS not
+// defined in its Spatial header)
+int awflref_has_tracer_transport() {
+#ifdef NO_TRACERS
+  return 0;
+#else
+  return 1;
+#endif
+}
 
 int awflref_ord() { return ord; }
 int awflref_ngll() { return ngll; }
@@ -94,7 +114,8 @@ void *awflref_create(int nx, int ny, int nz, double xlen, double ylen, double zl
   RefHandle *h = new RefHandle();
   static const char *const names[3] = {"uniform", "theta", "block"};
   for (int t = 0; t < g_pending_tracers; t++)
-    h->model.spaceOp.addTracer(t < 3 ? names[t] : "tracer" + std::to_string(t), true, "");
+    h->model.spaceOp.addTracer(t < 3 ? names[t] : "tracer" + std::to_string(t),
+                               g_pending_pos_set ? g_pending_pos[t] != 0 : true, "");
   try {
     h->model.init(path);
   } catch (...) {
@@ -128,6 +149,54 @@ void awflref_get_tracers(void *p, double *out) {
   RefHandle *h = static_cast<RefHandle *>(p);
   size_t n = h->tracers.totElems();
   for (size_t i = 0; i < n; i++) out[i] = h->tracers.data()[i];
+}
+
+void awflref_set_tracers(void *p, const double *in) {
+  RefHandle *h = static_cast<RefHandle *>(p);
+  size_t n = h->tracers.totElems();
+  for (size_t i = 0; i < n; i++) h->tracers.data()[i] = in[i];
+}
+
+// One split of Temporal_ader::timeStep (Temporal_ader.h:50-70): computeTendencies on state
+// and tracers for split index spl, then state += dt*stateTend and tracers +=
+// dt*tracerTend over the interior (the reference's two apply loops).
+void awflref_split(void *p, double dt, int spl) {
+  RefHandle *h = static_cast<RefHandle *>(p);
+  Spatial &s = h->model.spaceOp;
+  int constexpr hs = Spatial::hs;
+  real dtloc = dt;
+  s.computeTendencies(h->state, h->model.stateTendArr, h->tracers, h->model.tracerTendArr, dtloc, spl);
+  auto &st = h->state;
+  auto &tr = h->tracers;
+  auto &tend = h->model.stateTendArr;
+  auto &ttend = h->model.tracerTendArr;
+  for (int l = 0; l < Spatial::numState; l++)
+    for (int k = 0; k < s.nz; k++)
+      for (int j = 0; j < s.ny; j++)
+        for (int i = 0; i < s.nx; i++) st(l, hs + k, hs + j, hs + i) += dtloc * tend(l, k, j, i);
+  for (int l = 0; l < s.numTracers; l++)
+    for (int k = 0; k < s.nz; k++)
+      for (int j = 0; j < s.ny; j++)
+        for (int i = 0; i < s.nx; i++) tr(l, hs + k, hs + j, hs + i) += dtloc * ttend(l, k, j, i);
+}
+
+// Spatial::output (Spatial...h:1705-1791) on the current state and tracers; the netCDF
+// stand-in keeps every variable it wrote (awflref_output_size / awflref_output_get).
+void awflref_output(void *p, double etime) {
+  RefHandle *h = static_cast<RefHandle *>(p);
+  yakl::netcdf_record().clear();
+  h->model.spaceOp.output(h->state, h->tracers, etime);
+}
+long awflref_output_size(const char *name) {
+  auto &m = yakl::netcdf_record();
+  auto it = m.find(name);
+  return it == m.end() ? -1 : (long)it->second.size();
+}
+void awflref_output_get(const char *name, double *out) {
+  auto &m = yakl::netcdf_record();
+  auto it = m.find(name);
+  if (it == m.end()) return;
+  for (size_t i = 0; i < it->second.size(); i++) out[i] = it->second[i];
 }
 
 long awflref_state_size(void *p) {

@@ -11,7 +11,11 @@ drives that build through ``oracle.pyoracle.RefHarness`` and stores:
 * ``case_<name>.npz``    -- per configuration: background, initial state, CFL dt,
                             tendencies of every split of steps 1-2, the state after
                             each split of step 1 and after every step;
-* ``tracers_init.npz``   -- initTracers of the driver's tracers on three grids.
+* ``tracers_init.npz``   -- initTracers of the driver's tracers on three grids;
+* ``tracer_transport.npz`` -- state and tracers after each split of the reference's own
+                            tracer transport (its NO_TRACERS code compiled in);
+* ``output_fields.npz``  -- everything the reference's output() writes (coordinates,
+                            hydrostatic profiles, the six fields, the tracer fields).
 
 Needs the reference's source tree (``--ref DIR`` or $AWFL_REFERENCE_DIR) and g++ with OpenMP.
 Run from the repository root:  python tests/golden/make_golden.py --ref DIR
@@ -47,6 +51,10 @@ CASES = {
     "o5_straka":         (5, 10, 8, 6, (0, 0, 1), True, True, "straka", None, None, 1),
     "o9_pw_thermal":     (9, 10, 8, 6, (0, 0, 1), True, True, "thermal", None, 0.01, 3),
     "o9_walls_mixed":    (9, 10, 8, 6, (1, 1, 1), True, False, "thermal", None, 0.01, 2),
+    # wall directions shorter than the halo width: the stencil reaches past the line's far
+    # end into halo cells that hold wall copies
+    "o5_thin_walls":     (5, 1, 8, 6, (1, 0, 1), True, True, "thermal", None, 0.01, 3),
+    "o5_flat_z":         (5, 10, 8, 1, (0, 1, 1), True, True, "thermal", None, 0.01, 3),
 }
 
 
@@ -133,6 +141,87 @@ def make_tracers():
     return path
 
 
+# Tracer transport by the reference's own tracer code (its Spatial header with NO_TRACERS
+# blanked, built serially: oracle/Makefile): name -> (ord, nx, ny, nz, bc, pos, splits,
+# crpow). Each case starts from the reference's state and tracers after two time steps of
+# the noisy thermal with the driver's three tracers (initTracers), then records every
+# split of `splits` (directions, in order). Positive-definite tracers are limited only in
+# x and z: the reference's y limiter indexes tracerFlux(tr,k,j,ind_j) for v < 0
+# (Spatial...h:1285-1286), faces of another direction that the y split never writes.
+TRANSPORT_CASES = {
+    "o5_pw_steps_nopos":  (5, 10, 8, 6, (0, 0, 1), (0, 0, 0), (0, 1, 2, 2, 1, 0), True),
+    "o5_walls_steps_nopos": (5, 10, 8, 6, (1, 1, 1), (0, 0, 0), (0, 1, 2, 2, 1, 0), True),
+    "o5_pw_xz_pos":       (5, 10, 8, 6, (0, 0, 1), (1, 1, 1), (0, 2, 2, 0), True),
+    "o5_walls_xz_pos":    (5, 10, 8, 6, (1, 1, 1), (1, 1, 1), (0, 2, 2, 0), True),
+    "o5_mixed_pos":       (5, 10, 8, 6, (0, 1, 1), (1, 0, 1), (0, 2), True),
+    "o5_sim2d_steps_pos": (5, 12, 1, 8, (0, 0, 1), (1, 1, 1), (0, 2, 2, 0), True),
+    "o9_pw_xz_pos":       (9, 10, 8, 6, (0, 0, 1), (1, 1, 1), (0, 2), True),
+    "o5_pw_glibc_pos":    (5, 10, 8, 6, (0, 0, 1), (1, 1, 1), (0, 2), False),
+}
+
+
+def make_transport():
+    out = {}
+    for name, (ord_, nx, ny, nz, bc, pos, splits, crpow) in TRANSPORT_CASES.items():
+        R = RefHarness(nx, ny, nz, bc=bc, ord_=ord_, crpow=crpow, ntracers=3, tracer_transport=True,
+                       pos=list(pos))
+        assert R.has_tracer_transport
+        R.init_state()
+        R.add_theta_noise(SEED, 0.01)
+        R.init_tracers()
+        dt = R.compute_dt(0.8 if ord_ == 5 else 0.4)
+        for _ in range(2):
+            R.time_step(dt)
+        out[name + "_config"] = np.array([ord_, nx, ny, nz, bc[0], bc[1], bc[2], int(crpow)])
+        out[name + "_pos"] = np.array(pos)
+        out[name + "_splits"] = np.array(splits)
+        out[name + "_dt"] = np.array(dt)
+        out[name + "_state0"] = R.get_state()
+        out[name + "_tracers0"] = R.get_tracers()
+        for s, d in enumerate(splits):
+            R.dimswitch = 1  # split index d is direction d
+            R.split(dt, d)
+            out[name + "_tracers%d" % (s + 1)] = R.get_tracers()
+        out[name + "_state_end"] = R.get_state()
+    path = os.path.join(OUT, "tracer_transport.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+# Spatial::output (Spatial...h:1705-1791) by the reference's own code, its netCDF writes
+# recorded by the stand-in (oracle/shim/YAKL_netcdf.h): name -> (ord, nx, ny, nz, bc,
+# crpow). For each case: the first record (etime 0: coordinates, hydrostatic profiles and
+# the fields of the initial state with the driver's three tracers) and a later one after
+# three time steps.
+OUTPUT_CASES = {
+    "o5_crpow": (5, 10, 8, 6, (0, 0, 1), True),
+    "o5_glibc": (5, 10, 8, 6, (0, 0, 1), False),
+    "o9_walls_crpow": (9, 12, 10, 8, (1, 1, 1), True),
+}
+
+
+def make_output():
+    out = {}
+    for name, (ord_, nx, ny, nz, bc, crpow) in OUTPUT_CASES.items():
+        R = RefHarness(nx, ny, nz, bc=bc, ord_=ord_, crpow=crpow, ntracers=3)
+        R.init_state()
+        R.add_theta_noise(SEED, 0.01)
+        R.init_tracers()
+        dt = R.compute_dt(0.8 if ord_ == 5 else 0.4)
+        out[name + "_config"] = np.array([ord_, nx, ny, nz, bc[0], bc[1], bc[2], int(crpow)])
+        for rec, nsteps in ((0, 0), (1, 3)):
+            for _ in range(nsteps):
+                R.time_step(dt)
+            etime = nsteps * dt
+            out["%s_r%d_state" % (name, rec)] = R.get_state()
+            out["%s_r%d_tracers" % (name, rec)] = R.get_tracers()
+            for var, val in R.output(etime).items():
+                out["%s_r%d_%s" % (name, rec, var)] = val
+    path = os.path.join(OUT, "output_fields.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
 def main():
     import argparse
     ap = argparse.ArgumentParser()
@@ -143,6 +232,8 @@ def main():
         ap.error("--ref or AWFL_REFERENCE_DIR is required")
     pyoracle.build(ref=True, ref_dir=a.ref)
     print("wrote", make_tracers())
+    print("wrote", make_transport())
+    print("wrote", make_output())
     for o in (5, 9):
         make_tables(o)
         make_probes(o)

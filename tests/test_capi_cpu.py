@@ -79,13 +79,17 @@ def test_wrapper_rejects_wrong_buffers_before_any_device_call():
 
 def test_split_tracers_argument_checks_before_any_device_call():
     """awfl_split_tracers refuses bad arguments on the host: FP32 contexts, more than 64
-    tracers, a NULL flag array, and a direction shorter than the stencil half-width."""
+    tracers, a NULL flag array, a bad direction. A wall direction shorter than the stencil
+    half-width is accepted (its stencil indices map to its cells); only the host-only
+    context stops it. Periodic ones that short are refused when the context is made."""
     import ctypes
     L = capi.lib()
     pos = (ctypes.c_int * 2)(1, 1)
-    short = capi.Context(1, 8, 6, bc=("wall", "periodic", "wall"), device=-1)  # periodic is refused at create
+    short = capi.Context(1, 8, 6, bc=("wall", "periodic", "wall"), device=-1)
     assert L.awfl_split_tracers(short.h, 8, 8, 2, pos, 0.1, 0, None) == -1
-    assert b"at least 2 cells" in L.awfl_last_error(short.h)
+    assert b"host-only" in L.awfl_last_error(short.h)
+    with pytest.raises(capi.AwflError):
+        capi.Context(1, 8, 6, bc=("periodic", "periodic", "wall"), device=-1)
     c = capi.Context(10, 8, 6, device=-1)
     assert L.awfl_split_tracers(c.h, 8, 8, 65, pos, 0.1, 0, None) == -1
     assert L.awfl_split_tracers(c.h, 8, 8, 2, None, 0.1, 0, None) == -1

@@ -1,7 +1,15 @@
 """The oracle's restatement of the reference's tracer transport (its code under
 #ifndef NO_TRACERS, Spatial_euler3d_cons_expl_cart_fv_Agrid.h:624-955 and the y/z
-equivalents). The reference defines NO_TRACERS unconditionally (:10), so no output of the
-reference pins this part; these are the properties the scheme has instead: the state is
+equivalents), which the reference compiles out (NO_TRACERS, :10).
+
+Pinned to the reference's own tracer code: tests/golden/tracer_transport.npz comes from
+the reference built with that one line blanked (oracle/Makefile, serially), and the
+restatement must reproduce every split of it bit for bit -- x, y and z splits, periodic
+and wall boundaries, ord 5 and 9, limited (positive-definite) tracers in x and z, glibc's
+and a correctly rounded pow. (The reference's y limiter reads faces of another direction
+for v < 0, :1285-1286; the y splits of the fixtures carry no positive-definite tracer.)
+
+The properties the scheme has are checked as well: the state is
 untouched by the tracers, a uniform mixing ratio stays uniform, tracer mass is conserved
 where the mass flux through the boundary is zero (periodic x/y; a z wall, where the
 reconstruction zeroes w -- an x or y wall copies the edge state without zeroing the normal
@@ -49,3 +57,27 @@ def test_tracer_transport_properties(ord_, bc, ws):
     for t in (1, 2):
         assert tr[t][I[1:]].min() > -1e-6 * tr[t][I[1:]].max()
     assert np.abs(tr[1][I[1:]] - O.new_tracers(4)[1][I[1:]]).max() > 0  # it moved
+
+
+def _transport_cases(golden_dir):
+    import os
+    z = np.load(os.path.join(golden_dir, "tracer_transport.npz"))
+    names = sorted({k[:-len("_config")] for k in z.files if k.endswith("_config")})
+    return z, names
+
+
+def test_restatement_equals_reference_tracer_transport(golden_dir):
+    z, names = _transport_cases(golden_dir)
+    assert len(names) >= 8
+    for name in names:
+        ord_, nx, ny, nz, bcx, bcy, bcz, crpow = (int(v) for v in z[name + "_config"])
+        pos = [int(p) for p in z[name + "_pos"]]
+        O = Oracle(nx, ny, nz, bc=(bcx, bcy, bcz), ord_=ord_, crpow=bool(crpow))
+        st = z[name + "_state0"].copy()
+        tr = z[name + "_tracers0"].copy()
+        dt = float(z[name + "_dt"])
+        for s, d in enumerate(z[name + "_splits"]):
+            O.split_tracers(st, tr, dt, int(d), pos=pos)
+            want = z[name + "_tracers%d" % (s + 1)]
+            assert np.array_equal(tr, want), (name, s, int(d), np.abs(tr - want).max())
+        assert np.array_equal(st, z[name + "_state_end"]), name

@@ -98,3 +98,28 @@ def test_tracer_record_variables(tmp_path):
     assert e.value.code == -7
     with pytest.raises(ValueError):
         c.write_netcdf_fields_tracers(path, f1[:8], names, 3.0)
+
+
+def test_file_fixed_variables_equal_reference_output(tmp_path, golden_dir):
+    """The coordinates and hydrostatic profiles the library writes are the ones the
+    reference's own output() writes (tests/golden/output_fields.npz: its first record,
+    recorded by the netCDF stand-in), bit for bit; the record fields written from the
+    reference's own values read back unchanged."""
+    import os
+    z = np.load(os.path.join(golden_dir, "output_fields.npz"))
+    names = sorted({k[:-len("_config")] for k in z.files if k.endswith("_config")})
+    assert len(names) >= 3
+    tr = ["uniform", "theta", "block"]
+    fields = ["dens_pert", "u", "v", "w", "pot_temp_pert", "pressure_pert"] + ["tracer_" + n for n in tr]
+    for name in names:
+        o, nx, ny, nz, bx, by, bz, _ = (int(v) for v in z[name + "_config"])
+        bcn = {0: "periodic", 1: "wall"}
+        c = capi.Context(nx, ny, nz, bc=(bcn[bx], bcn[by], bcn[bz]), ord_=o, device=-1)
+        path = str(tmp_path / (name + ".nc"))
+        f = np.stack([z["%s_r0_%s" % (name, v)].reshape(nz, ny, nx) for v in fields])
+        c.write_netcdf_fields_tracers(path, f, tr, 0.0)
+        with netcdf(path, "r", mmap=False) as nc:
+            for v in ("x", "y", "z", "hyDens", "hyPressure", "hyTheta"):
+                np.testing.assert_array_equal(nc.variables[v][:], z["%s_r0_%s" % (name, v)], err_msg=(name, v))
+            for i, v in enumerate(fields):
+                np.testing.assert_array_equal(nc.variables[v][0], f[i], err_msg=(name, v))

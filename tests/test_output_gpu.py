@@ -1,7 +1,13 @@
 """Output diagnostics of Spatial::output (Spatial:1744-1778) on the device and the netCDF
-file written from them, for both state forms: the fields against the same formulas in
-numpy FP64 on the copied state (bit for bit except pressure_pert, whose pow the device
-rounds correctly and libm may not: 1e-9 Pa on ~1e5 Pa), and the file against the fields."""
+file written from them, for both state forms.
+
+Pinned to the reference's own output(): tests/golden/output_fields.npz holds every field
+the reference computed (recorded by its netCDF stand-in) for two records of three
+configurations; the device fields from the same states are bit-identical to them where
+the reference's pow is correctly rounded, and within a few ulp of the ~1e5 Pa pressure in
+pressure_pert against its glibc build. Also: the fields against the same formulas in numpy
+FP64 on the copied state (bit for bit except pressure_pert, whose pow the device rounds
+correctly and libm may not: 1e-9 Pa on ~1e5 Pa), and the file against the fields."""
 import numpy as np
 import pytest
 
@@ -63,3 +69,29 @@ def test_output_fields_and_file(tmp_path, prec):
             for r, f in enumerate(recs):
                 np.testing.assert_array_equal(nc.variables[name][r + 1], f[i])
         assert np.abs(nc.variables["w"][2]).max() > 0  # the bubble has started to rise
+
+
+def test_output_fields_equal_reference_output(golden_dir):
+    import os
+    z = np.load(os.path.join(golden_dir, "output_fields.npz"))
+    names = sorted({k[:-len("_config")] for k in z.files if k.endswith("_config")})
+    fields = ["dens_pert", "u", "v", "w", "pot_temp_pert", "pressure_pert"]
+    tr = ["uniform", "theta", "block"]
+    bcn = {0: "periodic", 1: "wall"}
+    for name in names:
+        o, nx, ny, nz, bx, by, bz, crpow = (int(v) for v in z[name + "_config"])
+        c = capi.Context(nx, ny, nz, bc=(bcn[bx], bcn[by], bcn[bz]), ord_=o)
+        for rec in (0, 1):
+            st = torch.from_numpy(z["%s_r%d_state" % (name, rec)].copy()).cuda()
+            trs = torch.from_numpy(z["%s_r%d_tracers" % (name, rec)].copy()).cuda()
+            got = c.output_fields(st).cpu().numpy()
+            for i, v in enumerate(fields):
+                want = z["%s_r%d_%s" % (name, rec, v)].reshape(nz, ny, nx)
+                if crpow or v != "pressure_pert":
+                    np.testing.assert_array_equal(got[i], want, err_msg=(name, rec, v))
+                else:  # glibc's pow vs correctly rounded: a few ulp of the ~1e5 Pa pressure
+                    np.testing.assert_allclose(got[i], want, rtol=0, atol=4 * np.spacing(1.2e5))
+            gt = c.output_tracer_fields(st, trs).cpu().numpy()
+            for t, n in enumerate(tr):
+                np.testing.assert_array_equal(gt[t], z["%s_r%d_tracer_%s" % (name, rec, n)].reshape(nz, ny, nx),
+                                              err_msg=(name, rec, n))

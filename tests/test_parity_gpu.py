@@ -170,6 +170,32 @@ def test_rising_bubble_vs_glibc_build(o, n, steps, cfl):
         assert e <= RTOL, (v, e)
 
 
+@pytest.mark.parametrize("o,n,steps,cfl", [(5, (64, 64, 32), 50, 0.8), (9, (32, 32, 16), 10, 0.4)])
+def test_each_step_vs_glibc_build_same_inputs(o, n, steps, cfl):
+    """Against the reference's glibc build on the same inputs: every one of the run's steps
+    starts from the glibc build's own state (the oracle with glibc's pow, bit-identical to
+    the reference's CPU build) and must land within 1e-12 relative L2 per variable of that
+    build's next state. Only the rounding of glibc's pow separates the two; over many steps
+    the scheme amplifies it (test_rising_bubble_vs_glibc_build), one step from the same
+    input it stays far below the bar."""
+    O, st = _bubble_case(o, *n)
+    dt = O.compute_dt(st, cfl)
+    c = capi.Context(*n, ord_=o)
+    h = c.hs
+    d = torch.from_numpy(st.copy()).cuda()
+    worst = [0.0] * 5
+    for _ in range(steps):
+        d.copy_(torch.from_numpy(st))
+        c.dimswitch = O.dimswitch
+        O.time_step(st, dt)
+        c.step(d, dt)
+        got = d.cpu().numpy()
+        for v in range(5):
+            worst[v] = max(worst[v], rel_l2(got[v, h:-h, h:-h, h:-h], st[v, h:-h, h:-h, h:-h]))
+    print("worst per-step relative L2 vs the glibc build:", ["%.2e" % e for e in worst])
+    assert max(worst) <= 1e-12, worst
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_splits_bit_exact_vs_crpow_oracle(case):
     """Every split (tendencies, halos, states) of steps 1-2 and the fused steps, from the

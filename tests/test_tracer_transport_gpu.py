@@ -1,6 +1,8 @@
 """Tracer transport on the device (awfl_step_tracers / awfl_split_tracers; the reference's
-tracer code, compiled out there by NO_TRACERS, built in) against the oracle's restatement
-of the same code: bit for bit, tracers and their halos, for several configurations.
+tracer code, compiled out there by NO_TRACERS, built in): bit for bit against the
+reference's own tracer code (tests/golden/tracer_transport.npz, made by the reference built
+with NO_TRACERS blanked), and against the oracle's restatement of the same code, tracers
+and their halos, for several configurations.
 
 FP64 with no contracted multiply-add on both sides and the correctly rounded pow (the
 oracle's crpow build) in the state's reconstruction, so equality is exact. The state
@@ -29,6 +31,7 @@ CASES = [
     (5, 16, 12, 10, (0, 0, 0), False, True, 0.8, 3),
     (5, 24, 1, 16, (0, 0, 1), True, True, 0.8, 3),
     (9, 20, 18, 16, (0, 1, 1), True, False, 0.4, 2),
+    (5, 1, 12, 8, (1, 0, 1), True, True, 0.8, 2),   # a wall direction of one cell
 ]
 
 
@@ -62,11 +65,13 @@ def test_step_tracers_bit_exact(case):
     assert np.array_equal(dst.cpu().numpy(), dst_plain.cpu().numpy())
     for t in range(4):
         assert np.array_equal(got_tr[t], tr[t]), (t, np.abs(got_tr[t] - tr[t]).max())
-    # the block tracer has moved
+    # the theta and block tracers have moved (the block is empty on a grid of fewer than
+    # 3 cells in x: its x range is [4nx/10, 6nx/10))
     O0 = Oracle(nx, ny, nz, bc=bc, ord_=o)
     t0 = O0.new_tracers(3)
     O0.init_tracers(t0)
-    assert np.abs(got_tr[2] - t0[2])[h:h + nz, h:h + ny, h:h + nx].max() > 1e-6
+    for t in ((1, 2) if nx >= 3 else (1,)):
+        assert np.abs(got_tr[t] - t0[t])[h:h + nz, h:h + ny, h:h + nx].max() > 1e-6, t
 
 
 def test_split_tracers_rejects_fp32_and_bad_args():
@@ -79,3 +84,29 @@ def test_split_tracers_rejects_fp32_and_bad_args():
     st64 = c64.new_state()
     with pytest.raises(ValueError):
         c64.step_tracers(st64, tr, 0.5, pos=[1])
+
+
+def test_split_tracers_equal_reference_tracer_code(golden_dir):
+    """Every split of the reference-made cases that use the correctly rounded pow: tracers
+    (halos included) after each split and the final state, bit for bit."""
+    import os
+    z = np.load(os.path.join(golden_dir, "tracer_transport.npz"))
+    names = sorted({k[:-len("_config")] for k in z.files if k.endswith("_config")})
+    done = 0
+    for name in names:
+        o, nx, ny, nz, bcx, bcy, bcz, crpow = (int(v) for v in z[name + "_config"])
+        if not crpow:
+            continue  # glibc's pow: pinned through the oracle on the CPU
+        pos = [int(p) for p in z[name + "_pos"]]
+        c = capi.Context(nx, ny, nz, bc=(BCN[bcx], BCN[bcy], BCN[bcz]), ord_=o)
+        dst = torch.from_numpy(z[name + "_state0"].copy()).cuda()
+        dtr = torch.from_numpy(z[name + "_tracers0"].copy()).cuda()
+        dt = float(z[name + "_dt"])
+        for s, d in enumerate(z[name + "_splits"]):
+            c.split_tracers(dst, dtr, dt, int(d), pos=pos)
+            got = dtr.cpu().numpy()
+            want = z[name + "_tracers%d" % (s + 1)]
+            assert np.array_equal(got, want), (name, s, int(d), np.abs(got - want).max())
+        assert np.array_equal(dst.cpu().numpy(), z[name + "_state_end"]), name
+        done += 1
+    assert done >= 7
