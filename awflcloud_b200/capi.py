@@ -9,7 +9,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libawfl.so")
+# the in-tree build; AWFL_LIBRARY names another build of the same library (a variant
+# compiled with different options, for comparisons)
+LIB_PATH = os.environ.get("AWFL_LIBRARY") or os.path.join(HERE, "lib", "libawfl.so")
 
 AWFL_OK = 0
 STATUS = {0: "AWFL_OK", -1: "AWFL_ERR_ARG", -2: "AWFL_ERR_CUDA", -3: "AWFL_ERR_NOMEM",

@@ -12,6 +12,17 @@ namespace awfl {
 // ------------------------------------------------------------------------------------
 // FP64 physics policy of the line sweep (awfl_sweep.cuh): the reference's arithmetic.
 // ------------------------------------------------------------------------------------
+#ifdef AWFL_FP64_OUTLINE_RIEMANN
+struct Q5 {
+  double v[5];
+};
+template <int DIR, int NG> static __device__ __noinline__ Q5 riemann_call(Q5 qL, Q5 qR, int kf, const SweepArgs *A) {
+  Q5 F;
+  riemann<DIR, NG>(qL.v, qR.v, kf, *A, F.v);
+  return F;
+}
+#endif
+
 struct P64 {
   using Real = double;
   static constexpr int kWdiv = 1;
@@ -19,7 +30,10 @@ struct P64 {
   static constexpr bool kTmaRing = false;
   // ord 5: 4 CTAs per SM (<= 128 registers), more warps to hide the FP64 latency
   // (measured +17%); ord 9 would spill heavily at that budget
-  static constexpr int min_blocks(int ord) { return ord == 5 ? 4 : 1; }
+#ifndef AWFL_P64_MIN_BLOCKS_ORD5
+#define AWFL_P64_MIN_BLOCKS_ORD5 4
+#endif
+  static constexpr int min_blocks(int ord) { return ord == 5 ? AWFL_P64_MIN_BLOCKS_ORD5 : 1; }
   using Args = SweepArgs;
   struct Aux {};
   static __device__ __forceinline__ void load_aux(const Args &, long, long, Aux &) {}
@@ -33,7 +47,19 @@ struct P64 {
   template <int DIR, int NG>
   static __device__ __forceinline__ void flux(const double (&qL)[5], const double (&qR)[5], int kf, const Args &A,
                                               double (&F)[5]) {
+#ifdef AWFL_FP64_OUTLINE_RIEMANN
+    Q5 a, b;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      a.v[v] = qL[v];
+      b.v[v] = qR[v];
+    }
+    const Q5 f = riemann_call<DIR, NG>(a, b, kf, &A);
+#pragma unroll
+    for (int v = 0; v < 5; v++) F[v] = f.v[v];
+#else
     riemann<DIR, NG>(qL, qR, kf, A, F);
+#endif
   }
 
   // K5 divergence (Spatial:940-956, 1298-1310, 1680-1696): z adds onto the gravity source.

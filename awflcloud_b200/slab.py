@@ -104,18 +104,20 @@ class SlabDomain:
         dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
         return t.item()
 
-    def split(self, state, dt, d, stream=None):
+    def split(self, state, dt, d):
+        """One split on torch's current stream (the stream the process group's NCCL
+        operations are ordered with; enter another one with torch.cuda.stream(...))."""
         if d != 0 or self.nslabs == 1:
-            self.ctx.split(state, dt, d, stream=stream)
+            self.ctx.split(state, dt, d)
             return
-        self.ctx.slab_pack(state, self.send, stream=stream)
+        self.ctx.slab_pack(state, self.send)
         exchange_columns(self.send, self.recv, self.rank, self.nslabs, self.periodic, self.group)
-        self.ctx.split_slab(state, self.recv, dt, stream=stream)
+        self.ctx.split_slab(state, self.recv, dt)
 
-    def step(self, state, dt, stream=None):
+    def step(self, state, dt):
         """Temporal_ader::timeStep on this slab: three splits in the dimSwitch order, the x
         split after the column exchange."""
         ds = self.dimswitch
         for spl in range(3):
-            self.split(state, dt, spl if ds else 2 - spl, stream=stream)
+            self.split(state, dt, spl if ds else 2 - spl)
         self.dimswitch = 1 - ds

@@ -90,8 +90,9 @@ def max_over_ranks(x, world):
 
 
 def job_throughput(world, cells, steps, max_ms):
-    """Whole-job Mcell-steps/s of N replicas of one grid (weak scaling): every rank advances
-    its own grid `steps` times; the job takes the slowest rank's time."""
+    """Whole-job Mcell-steps/s at N GPUs (weak scaling): every rank advances its `cells`
+    cells `steps` times (its slab of the N-slab grid); the job takes the slowest rank's
+    time."""
     return world * cells * steps / (max_ms * 1e-3) / 1e6
 
 
@@ -253,16 +254,33 @@ def run_reference(a):
 
 
 # ----------------------------------------------------------------------------- our arm
+def make_domain(a, prec, local, world):
+    """N = 1: the workload's grid on this GPU. N > 1: slab `rank` of one grid N times as
+    long in x (a.nx cells of it per GPU, x extent and dx scaled alike), decomposed over the
+    ranks with the halo-column exchange before every x split (SlabDomain)."""
+    from awflcloud_b200 import capi
+    if world == 1:
+        ctx = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=prec, device=local)
+        st = ctx.new_state()
+        ctx.init_state(st, **BUBBLE)
+        dt = ctx.cfl(st, cfl_for(a.ord))
+        return ctx, st, dt, ctx.split, ctx.step, lambda: ctx.dimswitch, lambda v: setattr(ctx, "dimswitch", v)
+    from awflcloud_b200.slab import SlabDomain
+    dom = SlabDomain(a.nx * world, a.ny, a.nz, device=local, xlen=20000.0 * world, ord_=a.ord, precision=prec)
+    st = dom.new_state()
+    dom.ctx.init_state(st, **BUBBLE)
+    dt = dom.cfl(st, cfl_for(a.ord))
+    return (dom.ctx, st, dt, lambda s, dt_, d: dom.split(s, dt_, d), lambda s, dt_: dom.step(s, dt_),
+            lambda: dom.dimswitch, lambda v: setattr(dom, "dimswitch", v))
+
+
 def time_form(a, prec, local, world, clocks=None):
     """Time K fused steps of one precision form; per-launch CUDA events on the stream."""
     import torch
     import torch.distributed as dist
     from awflcloud_b200 import capi, flops
     cells = a.nx * a.ny * a.nz
-    ctx = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=prec, device=local)
-    st = ctx.new_state()
-    ctx.init_state(st, **BUBBLE)
-    dt = ctx.cfl(st, cfl_for(a.ord))
+    ctx, st, dt, split, step, get_ds, set_ds = make_domain(a, prec, local, world)
     stream = torch.cuda.current_stream()
     peak = capi.measure_fma_peak(prec, local)
     peaks = {"peak_scalar": round(peak, 3)}
@@ -273,7 +291,7 @@ def time_form(a, prec, local, world, clocks=None):
         peaks["peak_paired"] = round(paired, 3)
         peak = max(peak, paired)
     for _ in range(a.warmup):
-        ctx.step(st, dt)
+        step(st, dt)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -281,15 +299,16 @@ def time_form(a, prec, local, world, clocks=None):
     if clocks is not None:
         clocks.start()
     # Events between the three split launches of every step give the per-launch time of
-    # the sweep kernel (the only kernel in the step).
+    # the sweep kernel (the only kernel in the step at N = 1; at N > 1 the x split's
+    # interval also holds the column packing and exchange).
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * a.steps + 1)]
     ev[0].record(stream)
     for s in range(a.steps):
-        ds = ctx.dimswitch
+        ds = get_ds()
         for spl in range(3):
-            ctx.split(st, dt, spl if ds else 2 - spl)
+            split(st, dt, spl if ds else 2 - spl)
             ev[3 * s + spl + 1].record(stream)
-        ctx.dimswitch = 1 - ds
+        set_ds(1 - ds)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -314,7 +333,7 @@ def time_form(a, prec, local, world, clocks=None):
                 "ops_executed_source": EXECUTED_OPS.get((prec, a.ord), {}).get("source"),
                 "launch_ms_avg": round(avg_launch_s * 1e3, 4),
                 "bytes_algorithmic_per_launch": cells * 10 * esz * (1 if prec == capi.FP64 else 2)}
-    return {"ctx": ctx, "state": st, "dt": dt, "value": job_throughput(world, cells, a.steps, max_ms),
+    return {"ctx": ctx, "state": st, "dt": dt, "step": step, "value": job_throughput(world, cells, a.steps, max_ms),
             "ms_per_step": max_ms / a.steps, "roofline": roofline, "clocks": clk, "flops": fl,
             "finite": bool(torch.isfinite(st).all().item())}
 
@@ -617,11 +636,11 @@ def run_ours(a):
     main_prec = capi.FP32 if a.precision == "fp32" else capi.FP64
     main = time_form(a, main_prec, local, world, clocks=ClockSampler(local))
     other = time_form(a, capi.FP64, local, world) if (main_prec == capi.FP32 and not a.no_compare) else None
-    e2e = None if a.no_e2e else e2e_leg(a, main["ctx"], main["state"], main["dt"], torch.cuda.current_stream(), world)
+    e2e = None if a.no_e2e else e2e_leg(a, main, torch.cuda.current_stream(), world)
     # the precision-matched end-to-end figure: the FP64 path through the same C ABI calls
     e2e64 = None
     if other is not None and not a.no_e2e:
-        e2e64 = e2e_leg(a, other["ctx"], other["state"], other["dt"], torch.cuda.current_stream(), world)
+        e2e64 = e2e_leg(a, other, torch.cuda.current_stream(), world)
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(main["value"], 3), "unit": UNIT, "n_gpus": world,
@@ -629,8 +648,10 @@ def run_ours(a):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if main_prec == capi.FP64 else "f32", "data": DATA,
                 "config": bench_config(a),
-                "parallelism": "replicas (one domain per GPU, no collective)" if world > 1 else "single GPU",
-                "roofline": main["roofline"], "gpu_launches": 3 * a.steps, "finite": main["finite"],
+                "parallelism": ("x slabs of one %dx%dx%d grid, %d cells wide per GPU; NCCL send/recv of "
+                                "hs+1 halo columns per side before every x split, dt by all-reduce MIN"
+                                % (a.nx * world, a.ny, a.nz, a.nx)) if world > 1 else "single GPU",
+                "roofline": main["roofline"], "gpu_launches": (4 if world > 1 else 3) * a.steps, "finite": main["finite"],
                 "clocks": main["clocks"], "flops_per_cell_step": main["flops"]}
         if other is not None:
             line["fp64"] = {"value": round(other["value"], 3), "ms_per_step": round(other["ms_per_step"], 4),
@@ -662,7 +683,7 @@ def run_ours(a):
     return 0
 
 
-def e2e_leg(a, ctx, st, dt, stream, world):
+def e2e_leg(a, form, stream, world):
     """The same metric through the C ABI with HOST buffers: every step copies its input
     state from pinned host memory to the device, advances it one time step and copies the
     result back. Steps rotate over three device buffers on three streams, so that the
@@ -674,9 +695,12 @@ def e2e_leg(a, ctx, st, dt, stream, world):
     import torch.distributed as dist
     from awflcloud_b200 import capi
     L = capi.lib()
+    ctx, st, dt, step = form["ctx"], form["state"], form["dt"], form["step"]
     nbytes = st.numel() * st.element_size()
     host_in = torch.empty_like(st, device="cpu").pin_memory()
-    nbuf = 3
+    # N > 1: the slabs' column exchange orders its NCCL operations with one stream, so
+    # the steps run on that one stream (no overlap of copies and compute across steps)
+    nbuf = 3 if world == 1 else 1
     host_out = [torch.empty_like(st, device="cpu").pin_memory() for _ in range(nbuf)]
     host_in.copy_(st)
     dev = [st] + [torch.empty_like(st) for _ in range(nbuf - 1)]
@@ -684,10 +708,11 @@ def e2e_leg(a, ctx, st, dt, stream, world):
 
     def one(n):
         k = n % nbuf
-        s = streams[k].cuda_stream
-        assert L.awfl_copy_h2d(dev[k].data_ptr(), host_in.data_ptr(), nbytes, s) == 0
-        ctx.step(dev[k], dt, stream=s)
-        assert L.awfl_copy_d2h(host_out[k].data_ptr(), dev[k].data_ptr(), nbytes, s) == 0
+        with torch.cuda.stream(streams[k]):
+            s = streams[k].cuda_stream
+            assert L.awfl_copy_h2d(dev[k].data_ptr(), host_in.data_ptr(), nbytes, s) == 0
+            step(dev[k], dt)
+            assert L.awfl_copy_d2h(host_out[k].data_ptr(), dev[k].data_ptr(), nbytes, s) == 0
 
     for s_ in streams:
         s_.wait_stream(stream)
