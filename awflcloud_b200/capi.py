@@ -80,6 +80,7 @@ _SIGS = {
     "awfl_split_slab": (_I, [_VP, _VP, _VP, _D, _VP]),
     "awfl_step_adjoint": (_I, [_VP, _VP, _VP, _I, _D, _VP]),
     "awfl_adjoint_tape_bytes": (_I, [_VP, _I, ctypes.POINTER(_L)]),
+    "awfl_set_adjoint_subwindow": (_I, [_VP, _I]),
     "awfl_get_dimswitch": (_I, [_VP, ctypes.POINTER(_I)]),
     "awfl_set_dimswitch": (_I, [_VP, _I]),
     "awfl_get_tables": (_I, [_VP] + [_DP] * 10),
@@ -454,6 +455,10 @@ class Context:
         out = _L()
         self._check(self.L.awfl_adjoint_tape_bytes(self.h, int(nsteps), ctypes.byref(out)))
         return out.value
+
+    def set_adjoint_subwindow(self, steps):
+        """Steps per recorded sub-window of step_adjoint (0: the whole window)."""
+        self._check(self.L.awfl_set_adjoint_subwindow(self.h, int(steps)))
 
     @property
     def dimswitch(self):

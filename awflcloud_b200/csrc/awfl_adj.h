@@ -34,6 +34,22 @@
 namespace awfl {
 namespace adj {
 
+// Reciprocal for the reverse sweeps (a derivative, not a replay of the reference's
+// rounding, so about an ulp is enough): on the device the hardware's approximate
+// reciprocal (rcp.approx.ftz.f64, ~2^-20 relative) refined by two Newton-Raphson steps
+// y <- y + y(1 - x y) (each doubles the correct bits), a few FMAs instead of an IEEE
+// division; on the host (the CPU checks of these functions) the plain division.
+AWFL_AHD double arcp(double x) {
+#if defined(__CUDA_ARCH__)
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = fma(y, fma(-x, y, 1.0), y);
+  return fma(y, fma(-x, y, 1.0), y);
+#else
+  return 1. / x;
+#endif
+}
+
 template <int N> AWFL_AHD double tv(const double *a) {
   if constexpr (N == 3) return awfl_tv_n3<double>(a);
   else if constexpr (N == 5) return awfl_tv_n5<double>(a);
@@ -60,7 +76,7 @@ AWFL_AHD void weno_fwd(const Tables<ORD> &T, const double (&u)[ORD], double (&aw
       a[i][ii] = t;
     }
   }
-  const double rid = 1. / T.idl[HS + 1];
+  const double rid = arcp(T.idl[HS + 1]);
   AWFL_UNROLL for (int ii = 0; ii < ORD; ii++) {
     double t = 0.;
     AWFL_UNROLL for (int s = 0; s < ORD; s++) t += T.recon[((HS + 1) * ORD + s) * ORD + ii] * u[s];
@@ -79,17 +95,17 @@ AWFL_AHD void weno_fwd(const Tables<ORD> &T, const double (&u)[ORD], double (&aw
   tvs[HS + 1] = lo + (tv<ORD>(a[HS + 1]) - lo) * T.sigma;
   double w[HS + 2], S = 0.;
   AWFL_UNROLL for (int i = 0; i < HS + 2; i++) {
-    w[i] = T.idl[i] / (tvs[i] * tvs[i] + eps);
+    w[i] = T.idl[i] * arcp(tvs[i] * tvs[i] + eps);
     S += w[i];
   }
-  double r = 1. / (S + eps);
+  double r = arcp(S + eps);
   S = 0.;
   AWFL_UNROLL for (int i = 0; i < HS + 2; i++) {
     const double x = w[i] * r, d = T.idl[i];
-    w[i] = x * (d + d * d - 3. * d * x + x * x) / (d * d + x * (1. - 2. * d));
+    w[i] = x * (d + d * d - 3. * d * x + x * x) * arcp(d * d + x * (1. - 2. * d));
     S += w[i];
   }
-  r = 1. / (S + eps);
+  r = arcp(S + eps);
   AWFL_UNROLL for (int ii = 0; ii < ORD; ii++) {
     double t = 0.;
     AWFL_UNROLL for (int i = 0; i < HS + 2; i++) {
@@ -117,7 +133,7 @@ AWFL_AHD void weno_vjp(const Tables<ORD> &T, const double (&u)[ORD], const doubl
       a[i][ii] = t;
     }
   }
-  const double rid = 1. / T.idl[HS + 1];
+  const double rid = arcp(T.idl[HS + 1]);
   AWFL_UNROLL for (int ii = 0; ii < ORD; ii++) {
     double t = 0.;
     AWFL_UNROLL for (int s = 0; s < ORD; s++) t += T.recon[((HS + 1) * ORD + s) * ORD + ii] * u[s];
@@ -136,19 +152,19 @@ AWFL_AHD void weno_vjp(const Tables<ORD> &T, const double (&u)[ORD], const doubl
   tvs[HS + 1] = lo + (tv<ORD>(a[HS + 1]) - lo) * T.sigma;
   double w0[NP], dd[NP], S1 = 0.;
   AWFL_UNROLL for (int i = 0; i < NP; i++) {
-    dd[i] = 1. / (tvs[i] * tvs[i] + eps);
+    dd[i] = arcp(tvs[i] * tvs[i] + eps);
     w0[i] = T.idl[i] * dd[i];
     S1 += w0[i];
   }
-  const double r1 = 1. / (S1 + eps);
+  const double r1 = arcp(S1 + eps);
   double w1[NP], w2[NP], S2 = 0.;
   AWFL_UNROLL for (int i = 0; i < NP; i++) {
     const double x = w0[i] * r1, d = T.idl[i];
     w1[i] = x;
-    w2[i] = x * (d + d * d - 3. * d * x + x * x) / (d * d + x * (1. - 2. * d));
+    w2[i] = x * (d + d * d - 3. * d * x + x * x) * arcp(d * d + x * (1. - 2. * d));
     S2 += w2[i];
   }
-  const double r2 = 1. / (S2 + eps);
+  const double r2 = arcp(S2 + eps);
   // ---- reverse
   double la[NP][ORD];
   double lw[NP];
@@ -174,7 +190,7 @@ AWFL_AHD void weno_vjp(const Tables<ORD> &T, const double (&u)[ORD], const doubl
   AWFL_UNROLL for (int i = 0; i < NP; i++) {
     const double x = w1[i], d = T.idl[i];
     const double N = d + d * d - 3. * d * x + x * x, D = d * d + x * (1. - 2. * d);
-    const double rD = 1. / D;
+    const double rD = arcp(D);
     const double dm = ((N + x * (2. * x - 3. * d)) - x * N * (1. - 2. * d) * rD) * rD;
     lw[i] *= dm;
   }
@@ -309,7 +325,7 @@ AWFL_AHD void cell_dt(const Tables<ORD> &T, int kb, const CellArgs &A, CellFwd<O
   const bool wtop = DIR == 2 && A.bc == BC_WALL && kb == A.nz - 1;
   const bool wbot = DIR == 2 && A.bc == BC_WALL && kb == 0;
   AWFL_UNROLL for (int ii = 0; ii < NG; ii++) {
-    const double rr = 1. / X.q[idR][0][ii];
+    const double rr = arcp(X.q[idR][0][ii]);
     const double mn = X.q[NM][0][ii] * rr;
     AWFL_UNROLL for (int x = 0; x < 4; x++) X.f[x][0][ii] = mn * X.q[x + 1][0][ii];
     X.g[0][ii] = ::pow(X.q[idT][0][ii], GAMMA);
@@ -318,7 +334,7 @@ AWFL_AHD void cell_dt(const Tables<ORD> &T, int kb, const CellArgs &A, CellFwd<O
     const double fill = -(X.q[idR][0][NG - 1] - A.dens_g[kb * NG + NG - 1]) * GRAV;
     AWFL_UNROLL for (int ii = 0; ii < NG; ii++) X.sr[0][ii] = fill;
   }
-  const double rdx = 1. / A.dxd;
+  const double rdx = arcp(A.dxd);
   AWFL_UNROLL for (int kt = 0; kt < NA - 1; kt++) {
     const double rk = 1. / (kt + 1.);
     const double cg = kt == 0 ? C0 : 0.5 * C0;
@@ -346,7 +362,7 @@ AWFL_AHD void cell_dt(const Tables<ORD> &T, int kb, const CellArgs &A, CellFwd<O
     if (wtop) X.q[idW][kt + 1][NG - 1] = 0.;
     if (wbot) X.q[idW][kt + 1][0] = 0.;
     AWFL_UNROLL for (int ii = 0; ii < NG; ii++) {
-      const double rr0 = 1. / X.q[idR][0][ii];
+      const double rr0 = arcp(X.q[idR][0][ii]);
       AWFL_UNROLL for (int x = 0; x < 4; x++) {
         double tot = 0.;
         AWFL_UNROLL for (int ir = 0; ir <= kt + 1; ir++) tot += X.q[NM][ir][ii] * X.q[x + 1][kt + 1 - ir][ii];
@@ -358,7 +374,7 @@ AWFL_AHD void cell_dt(const Tables<ORD> &T, int kb, const CellArgs &A, CellFwd<O
         tg += (kt + 1. - ir) * GAMMA * X.g[ir][ii] * X.q[idT][kt + 1 - ir][ii];
         if (ir > 0) tg -= (kt + 1. - ir) * X.q[idT][ir][ii] * X.g[kt + 1 - ir][ii];
       }
-      X.g[kt + 1][ii] = (GAMMA * X.g[0][ii] * X.q[idT][kt + 1][ii] + tg * rk) / X.q[idT][0][ii];
+      X.g[kt + 1][ii] = (GAMMA * X.g[0][ii] * X.q[idT][kt + 1][ii] + tg * rk) * arcp(X.q[idT][0][ii]);
     }
   }
 }
@@ -442,13 +458,13 @@ AWFL_AHD void cell_dt_vjp(const Tables<ORD> &T, int kb, const CellArgs &A, const
       dm *= A.dt;
     }
   }
-  const double rdx = 1. / A.dxd;
+  const double rdx = arcp(A.dxd);
   AWFL_UNROLL for (int kt = NA - 2; kt >= 0; kt--) {
     const double rk = 1. / (kt + 1.);
     const double cg = kt == 0 ? C0 : 0.5 * C0;
     // (f, g) at level kt+1
     AWFL_UNROLL for (int ii = 0; ii < NG; ii++) {
-      const double rT0 = 1. / X.q[idT][0][ii];
+      const double rT0 = arcp(X.q[idT][0][ii]);
       const double lG = lg[kt + 1][ii];
       const double lnum = lG * rT0;
       lq[idT][0][ii] -= lG * X.g[kt + 1][ii] * rT0;
@@ -464,7 +480,7 @@ AWFL_AHD void cell_dt_vjp(const Tables<ORD> &T, int kb, const CellArgs &A, const
           lg[kt + 1 - ir][ii] -= c * X.q[idT][ir][ii];
         }
       }
-      const double rR0 = 1. / X.q[idR][0][ii];
+      const double rR0 = arcp(X.q[idR][0][ii]);
       AWFL_UNROLL for (int x = 0; x < 4; x++) {
         const double lF = lf[x][kt + 1][ii];
         const double lt = lF * rR0;
@@ -502,8 +518,8 @@ AWFL_AHD void cell_dt_vjp(const Tables<ORD> &T, int kb, const CellArgs &A, const
   }
   // level 0: fluxes and pressure of the GLL values
   AWFL_UNROLL for (int ii = 0; ii < NG; ii++) {
-    const double rr = 1. / X.q[idR][0][ii];
-    lq[idT][0][ii] += lg[0][ii] * GAMMA * X.g[0][ii] / X.q[idT][0][ii];
+    const double rr = arcp(X.q[idR][0][ii]);
+    lq[idT][0][ii] += lg[0][ii] * GAMMA * X.g[0][ii] * arcp(X.q[idT][0][ii]);
     AWFL_UNROLL for (int x = 0; x < 4; x++) {
       const double l0 = lf[x][0][ii] * rr;
       lq[NM][0][ii] += l0 * X.q[x + 1][0][ii];
@@ -551,14 +567,14 @@ AWFL_AHD void riemann_fwd(const double (&qL)[5], const double (&qR)[5], double (
     AWFL_UNROLL for (int k = 0; k < 3; k++) vel[k] = 0.5 * (qL[k + 1] + qR[k + 1]);
     t = 0.5 * (qL[4] + qR[4]);
   } else {
-    const double rl = 1. / qL[0], rr = 1. / qR[0];
+    const double rl = arcp(qL[0]), rr = arcp(qR[0]);
     AWFL_UNROLL for (int k = 0; k < 3; k++) vel[k] = 0.5 * (qL[k + 1] * rl + qR[k + 1] * rr);
     t = 0.5 * (qL[4] * rl + qR[4] * rr);
   }
   const double p = C0 * ::pow(r * t, GAMMA);
-  const double cs = ::sqrt(GAMMA * p / r);
+  const double cs = ::sqrt(GAMMA * p * arcp(r));
   const double vn = vel[DIR], va = vel[TA], vb = vel[TB];
-  const double rt = 1. / t, rc = 0.5 / cs;
+  const double rt = arcp(t), rc = 0.5 * arcp(cs);
   const double *qU = vn > 0 ? qL : qR;
   const double w1 = qU[0] - qU[4] * rt, w2 = qU[QA] - va * qU[4] * rt, w3 = qU[QB] - vb * qU[4] * rt;
   const double w5 = (vn * qR[0] - qR[QN]) * rc + 0.5 * qR[4] * rt;
@@ -566,7 +582,7 @@ AWFL_AHD void riemann_fwd(const double (&qL)[5], const double (&qR)[5], double (
   const double Q0 = w1 + w5 + w6;
   const double QNv = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
   const double QAv = w2 + va * (w5 + w6), QBv = w3 + vb * (w5 + w6), Q4 = t * (w5 + w6);
-  const double r0 = 1. / Q0;
+  const double r0 = arcp(Q0);
   F[0] = QNv;
   F[QN] = QNv * QNv * r0 + C0 * ::pow(Q4, GAMMA);
   F[QA] = QNv * QAv * r0;
@@ -583,7 +599,7 @@ AWFL_AHD void riemann_vjp(const double (&qL)[5], const double (&qR)[5], const do
   // ---- forward
   const double r = 0.5 * (qL[0] + qR[0]);
   double vel[3], t;
-  const double rl = 1. / qL[0], rrr = 1. / qR[0];
+  const double rl = arcp(qL[0]), rrr = arcp(qR[0]);
   if (DIR == 1) {
     AWFL_UNROLL for (int k = 0; k < 3; k++) vel[k] = 0.5 * (qL[k + 1] + qR[k + 1]);
     t = 0.5 * (qL[4] + qR[4]);
@@ -592,9 +608,9 @@ AWFL_AHD void riemann_vjp(const double (&qL)[5], const double (&qR)[5], const do
     t = 0.5 * (qL[4] * rl + qR[4] * rrr);
   }
   const double p = C0 * ::pow(r * t, GAMMA);
-  const double cs = ::sqrt(GAMMA * p / r);
+  const double cs = ::sqrt(GAMMA * p * arcp(r));
   const double vn = vel[DIR], va = vel[TA], vb = vel[TB];
-  const double rt = 1. / t, rc = 0.5 / cs;
+  const double rt = arcp(t), rc = 0.5 * arcp(cs);
   const bool left = vn > 0;
   const double *qU = left ? qL : qR;
   const double w1 = qU[0] - qU[4] * rt, w2 = qU[QA] - va * qU[4] * rt, w3 = qU[QB] - vb * qU[4] * rt;
@@ -604,13 +620,13 @@ AWFL_AHD void riemann_vjp(const double (&qL)[5], const double (&qR)[5], const do
   const double Q0 = w1 + W;
   const double QNv = vn * w1 + (vn - cs) * w5 + (vn + cs) * w6;
   const double QAv = w2 + va * W, QBv = w3 + vb * W, Q4 = t * W;
-  const double r0 = 1. / Q0;
+  const double r0 = arcp(Q0);
   const double pw = ::pow(Q4, GAMMA);
   // ---- reverse: fluxes -> characteristic state
   const double lQN = lF[0] + lF[QN] * 2. * QNv * r0 + (lF[QA] * QAv + lF[QB] * QBv + lF[4] * Q4) * r0;
   const double lQ0 = -(lF[QN] * QNv * QNv + lF[QA] * QNv * QAv + lF[QB] * QNv * QBv + lF[4] * QNv * Q4) * r0 * r0;
   const double lQA = lF[QA] * QNv * r0, lQB = lF[QB] * QNv * r0;
-  const double lQ4 = lF[QN] * C0 * GAMMA * pw / Q4 + lF[4] * QNv * r0;
+  const double lQ4 = lF[QN] * C0 * GAMMA * pw * arcp(Q4) + lF[4] * QNv * r0;
   const double lw1 = lQ0 + vn * lQN, lw2 = lQA, lw3 = lQB;
   const double lWc = lQ0 + va * lQA + vb * lQB + t * lQ4;
   const double lw5 = lWc + (vn - cs) * lQN;
@@ -625,14 +641,14 @@ AWFL_AHD void riemann_vjp(const double (&qL)[5], const double (&qR)[5], const do
   gR[0] += lw5 * vn * rc;
   gR[QN] -= lw5 * rc;
   gR[4] += lw5 * 0.5 * rt;
-  lcs -= lw5 * (vn * qR[0] - qR[QN]) * rc / cs;
+  lcs -= lw5 * (vn * qR[0] - qR[QN]) * rc * arcp(cs);
   lt -= lw5 * 0.5 * qR[4] * rt * rt;
   // w6 = (qLN - vn qL0) / (2 cs) + qL4 / (2 t)
   lvn -= lw6 * qL[0] * rc;
   gL[0] -= lw6 * vn * rc;
   gL[QN] += lw6 * rc;
   gL[4] += lw6 * 0.5 * rt;
-  lcs -= lw6 * (qL[QN] - vn * qL[0]) * rc / cs;
+  lcs -= lw6 * (qL[QN] - vn * qL[0]) * rc * arcp(cs);
   lt -= lw6 * 0.5 * qL[4] * rt * rt;
   // upwind w1..w3
   {
@@ -646,8 +662,8 @@ AWFL_AHD void riemann_vjp(const double (&qL)[5], const double (&qR)[5], const do
     lvb -= lw3 * qU[4] * rt;
   }
   // cs = sqrt(gamma p / r), p = C0 (r t)^gamma
-  const double lp = lcs * cs / (2. * p);
-  double lr = -lcs * cs / (2. * r) + lp * GAMMA * p / r;
+  const double lp = lcs * cs * arcp(2. * p);
+  double lr = -lcs * cs * arcp(2. * r) + lp * GAMMA * p * arcp(r);
   lt += lp * GAMMA * p * rt;
   gL[0] += 0.5 * lr;
   gR[0] += 0.5 * lr;

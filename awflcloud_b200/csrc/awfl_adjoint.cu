@@ -20,6 +20,7 @@ struct PTLM {
   static constexpr int kWdiv = 2;
   static constexpr bool kAsyncRing = false;
   static constexpr bool kTmaRing = false;
+  static constexpr bool kSlab = false;
   static constexpr int min_blocks(int) { return 1; }
   using Args = SweepArgs;
   struct Aux {};
@@ -65,6 +66,7 @@ cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t 
 // A.tend points at the split's record: q0 (5*NGLL planes of ncell), then eL, eR (10).
 // ------------------------------------------------------------------------------------
 struct P64Rec : P64 {
+  static constexpr bool kSlab = false;
   template <int ORD> struct Rec {
     double *q0;
     long n, cell;

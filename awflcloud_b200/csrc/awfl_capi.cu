@@ -59,6 +59,8 @@ struct awfl_ctx {
   // index of its first cell, the grid's nx, and which ends border another slab
   int nslabs = 1, slab = 0, xoff = 0, nx_global = 0;
   bool xlo_ex = false, xhi_ex = false;
+  // discrete adjoint: steps per recorded sub-window (0: the whole window at once)
+  int adj_sub = 0;
   std::string err;
 };
 
@@ -948,14 +950,49 @@ int awfl_step_tlm(awfl_ctx *c, void *d_state_tangent, double dt, void *stream) {
 
 
 
-int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
-  if (!c || nsteps < 0 || !bytes) return AWFL_ERR_ARG;
-  const long nspl = (c->sim2d ? 2L : 3L) * nsteps;
+namespace {
+
+// The split directions of `nsteps` steps from dimSwitch value ds (sim2d drops Y).
+std::vector<int> split_dirs(const awfl_ctx *c, int nsteps, int ds) {
+  std::vector<int> dirs;
+  for (int n = 0; n < nsteps; n++) {
+    for (int spl = 0; spl < 3; spl++) {
+      const int dir = ds ? spl : 2 - spl;
+      if (dir == 1 && c->sim2d) continue;
+      dirs.push_back(dir);
+    }
+    ds = !ds;
+  }
+  return dirs;
+}
+
+// Device memory (doubles) of awfl_step_adjoint for a window of nsteps steps: the split-
+// start states and records of the recorded stretch (the whole window, or one sub-window),
+// the sub-window start states, and the reverse scratch.
+long adjoint_doubles(const awfl_ctx *c, int nsteps) {
+  const long per_step = c->sim2d ? 2L : 3L;
   const long ncell = (long)c->cfg.nx * c->cfg.ny * c->cfg.nz;
   const long nface = (long)(c->cfg.nx + 1) * (c->cfg.ny + 1) * (c->cfg.nz + 1);
   const long rec = (5L * c->ngll + 10L) * ncell;  // per split: level-0 values + edges
-  *bytes = (long)sizeof(double) * (nspl > 0 ? (nspl + 1) * state_plane(c) + nspl * rec : 0) +
-           (long)sizeof(double) * (10L * nface + 5L * (c->cfg.ord + c->ngll) * ncell);
+  const int m = c->adj_sub > 0 && c->adj_sub < nsteps ? c->adj_sub : nsteps;  // recorded steps
+  const long nsub = m > 0 ? (nsteps + m - 1) / m : 0;
+  const long nspl = per_step * m;
+  const long tape = nspl > 0 ? (nspl + 1) * state_plane(c) + nspl * rec : 0;
+  const long starts = nsub > 1 ? (nsub - 1) * state_plane(c) : 0;
+  return tape + starts + 10L * nface + 5L * (c->cfg.ord + c->ngll) * ncell;
+}
+
+}  // namespace
+
+int awfl_adjoint_tape_bytes(const awfl_ctx *c, int nsteps, long *bytes) {
+  if (!c || nsteps < 0 || !bytes) return AWFL_ERR_ARG;
+  *bytes = (long)sizeof(double) * adjoint_doubles(c, nsteps);
+  return AWFL_OK;
+}
+
+int awfl_set_adjoint_subwindow(awfl_ctx *c, int steps) {
+  if (!c || steps < 0) return AWFL_ERR_ARG;
+  c->adj_sub = steps;
   return AWFL_OK;
 }
 
@@ -974,61 +1011,89 @@ int awfl_step_adjoint(awfl_ctx *c, const void *d_state_ckpt, void *d_lambda, int
   const long plane = state_plane(c);
   const long ncell = (long)nx * ny * nz;
   const long nface = (long)(nx + 1) * (ny + 1) * (nz + 1);
-  // split order of the window: dimSwitch as the context holds it now (its value at the
-  // checkpoint), flipped after every step
-  std::vector<int> dirs;
-  int ds = c->dimswitch;
-  for (int n = 0; n < nsteps; n++) {
-    for (int spl = 0; spl < 3; spl++) {
-      const int dir = ds ? spl : 2 - spl;
-      if (dir == 1 && c->sim2d) continue;
-      dirs.push_back(dir);
-    }
-    ds = !ds;
+  if (nsteps == 0) {
+    cudaError_t e = launch_zero_halo((double *)d_lambda, nx, ny, nz, c->hs, c->nsm, st);
+    return e == cudaSuccess ? AWFL_OK : cuda_fail(c, e, "adjoint reverse sweep");
   }
-  const long nspl = (long)dirs.size();
+  // Sub-windows of m steps (the whole window when the context's sub-window length is 0 or
+  // not shorter): pass 1 steps from the checkpoint with the plain sweep (bit-identical to
+  // the recording one) and keeps the state at each sub-window's start; pass 2, last
+  // sub-window first, recomputes the sub-window with the recording sweep (split-start
+  // states and records) and runs its reverse sweeps, last split first.
+  const int m = c->adj_sub > 0 && c->adj_sub < nsteps ? c->adj_sub : nsteps;
+  const int nsub = (nsteps + m - 1) / m;
+  const long per_step = c->sim2d ? 2L : 3L;
   const long rec = (5L * c->ngll + 10L) * ncell;  // per split: level-0 values + edges
-  if (nspl > 0) {
-    rc = ensure_buffer(c, &c->d_tape, &c->tape_bytes, sizeof(double) * (size_t)((nspl + 1) * plane + nspl * rec),
-                       "adjoint tape");
-    if (rc) return rc;
-    rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes, sizeof(double) * (size_t)(10 * nface + 5L * (ord + c->ngll) * ncell),
-                       "adjoint scratch");
-    if (rc) return rc;
+  const long mspl = per_step * m;
+  rc = ensure_buffer(c, &c->d_tape, &c->tape_bytes,
+                     sizeof(double) * (size_t)((mspl + 1) * plane + mspl * rec + (long)(nsub - 1) * plane),
+                     "adjoint tape");
+  if (rc) return rc;
+  rc = ensure_buffer(c, &c->d_adj, &c->adj_bytes, sizeof(double) * (size_t)(10 * nface + 5L * (ord + c->ngll) * ncell),
+                     "adjoint scratch");
+  if (rc) return rc;
+  double *states = c->d_tape, *recs = c->d_tape + (mspl + 1) * plane;
+  double *starts = recs + mspl * rec;  // sub-window g >= 1 starts at starts + (g-1)*plane
+  auto start_of = [&](int g) -> const double * {
+    return g == 0 ? (const double *)d_state_ckpt : starts + (long)(g - 1) * plane;
+  };
+  // dimSwitch at each sub-window start (the context's value is the checkpoint's)
+  std::vector<int> ds_at(nsub);
+  {
+    int ds = c->dimswitch;
+    for (int g = 0; g < nsub; g++) {
+      ds_at[g] = ds;
+      if (m % 2) ds = !ds;
+    }
   }
-  // forward recomputation: state s = state at the start of split s (s = 0..nspl), and the
-  // record of split s (its level-0 values and edges) taken by the recording sweep
-  double *states = c->d_tape, *recs = c->d_tape + (nspl + 1) * plane;
   cudaError_t e = cudaSuccess;
-  if (nspl > 0) e = cudaMemcpyAsync(states, d_state_ckpt, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
-  for (long s = 0; s < nspl && e == cudaSuccess; s++) {
-    double *dst = states + (s + 1) * plane;
-    e = cudaMemcpyAsync(dst, states + s * plane, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess)
-      e = launch_sweep_rec(ord, dirs[s], sweep_args(c, dst, recs + s * rec, dt, dirs[s], MODE_APPLY), st);
+  // pass 1: the sub-window start states
+  for (int g = 1; g < nsub && e == cudaSuccess; g++) {
+    double *dst = starts + (long)(g - 1) * plane;
+    e = cudaMemcpyAsync(dst, start_of(g - 1), sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
+    const std::vector<int> dirs = split_dirs(c, m, ds_at[g - 1]);
+    for (size_t s = 0; s < dirs.size() && e == cudaSuccess; s++)
+      e = launch_sweep_fp64(ord, dirs[s], sweep_args(c, dst, nullptr, dt, dirs[s], MODE_APPLY), st);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "adjoint forward recomputation");
-  // reverse sweeps, last split first
-  for (long s = nspl - 1; s >= 0 && e == cudaSuccess; s--) {
-    const int dir = dirs[s];
-    adj::SplitArgs A{};
-    A.state = states + s * plane;
-    A.q0 = recs + s * rec;
-    A.edges = A.q0 + 5L * c->ngll * ncell;
-    A.lq = c->d_adj;
-    A.ls = c->d_adj + 10 * nface;
-    A.lq0 = A.ls + 5L * ord * ncell;
-    A.lam = (double *)d_lambda;
-    A.nx = nx; A.ny = ny; A.nz = nz; A.hs = c->hs;
-    A.sim2d = c->sim2d;
-    A.ca.nz = nz;
-    A.ca.bc = dir == 0 ? c->cfg.bc_x : (dir == 1 ? c->cfg.bc_y : c->cfg.bc_z);
-    A.ca.weno_s = c->cfg.weno_scalars; A.ca.weno_w = c->cfg.weno_winds;
-    A.ca.dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
-    A.ca.dt = dt;
-    A.ca.dens_c = c->d_dens_c; A.ca.denstheta_c = c->d_denstheta_c;
-    A.ca.dens_g = c->d_dens_g; A.ca.denstheta_g = c->d_denstheta_g; A.ca.pres_g = c->d_pres_g;
-    e = launch_adjoint_split(ord, dir, A, 0, c->nsm, st);
+  // pass 2: each sub-window recorded and reversed, last first
+  for (int g = nsub - 1; g >= 0 && e == cudaSuccess; g--) {
+    const int mg = (g == nsub - 1) ? nsteps - g * m : m;
+    const std::vector<int> dirs = split_dirs(c, mg, ds_at[g]);
+    const long nspl = (long)dirs.size();
+    if (nspl == 0) continue;
+    // forward recomputation: state s = state at the start of split s (s = 0..nspl), and the
+    // record of split s (its level-0 values and edges) taken by the recording sweep
+    e = cudaMemcpyAsync(states, start_of(g), sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
+    for (long s = 0; s < nspl && e == cudaSuccess; s++) {
+      double *dst = states + (s + 1) * plane;
+      e = cudaMemcpyAsync(dst, states + s * plane, sizeof(double) * plane, cudaMemcpyDeviceToDevice, st);
+      if (e == cudaSuccess)
+        e = launch_sweep_rec(ord, dirs[s], sweep_args(c, dst, recs + s * rec, dt, dirs[s], MODE_APPLY), st);
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "adjoint forward recomputation");
+    // reverse sweeps, last split first
+    for (long s = nspl - 1; s >= 0 && e == cudaSuccess; s--) {
+      const int dir = dirs[s];
+      adj::SplitArgs A{};
+      A.state = states + s * plane;
+      A.q0 = recs + s * rec;
+      A.edges = A.q0 + 5L * c->ngll * ncell;
+      A.lq = c->d_adj;
+      A.ls = c->d_adj + 10 * nface;
+      A.lq0 = A.ls + 5L * ord * ncell;
+      A.lam = (double *)d_lambda;
+      A.nx = nx; A.ny = ny; A.nz = nz; A.hs = c->hs;
+      A.sim2d = c->sim2d;
+      A.ca.nz = nz;
+      A.ca.bc = dir == 0 ? c->cfg.bc_x : (dir == 1 ? c->cfg.bc_y : c->cfg.bc_z);
+      A.ca.weno_s = c->cfg.weno_scalars; A.ca.weno_w = c->cfg.weno_winds;
+      A.ca.dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+      A.ca.dt = dt;
+      A.ca.dens_c = c->d_dens_c; A.ca.denstheta_c = c->d_denstheta_c;
+      A.ca.dens_g = c->d_dens_g; A.ca.denstheta_g = c->d_denstheta_g; A.ca.pres_g = c->d_pres_g;
+      e = launch_adjoint_split(ord, dir, A, 0, c->nsm, st);
+    }
   }
   if (e == cudaSuccess) e = launch_zero_halo((double *)d_lambda, nx, ny, nz, c->hs, c->nsm, st);
   if (e != cudaSuccess) return cuda_fail(c, e, "adjoint reverse sweep");

@@ -489,6 +489,7 @@ struct P32 {
   // from its kernel parameter, the ensemble's persistent sweep from the work list in
   // global memory (its shared-memory copy of the arguments is no place for one)
   static constexpr bool kTmaRing = true;
+  static constexpr bool kSlab = true;  // awfl_split_slab
   static bool prepare_tma(SweepArgs32 &A, int ord, int dir, int C, int W) {
     return prepare_sweep_map32(A, ord, dir, C, W);
   }

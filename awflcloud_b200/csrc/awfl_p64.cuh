@@ -28,6 +28,7 @@ struct P64 {
   static constexpr int kWdiv = 1;
   static constexpr bool kAsyncRing = true;
   static constexpr bool kTmaRing = false;
+  static constexpr bool kSlab = true;  // awfl_split_slab
   // ord 5: 4 CTAs per SM (<= 128 registers), more warps to hide the FP64 latency
   // (measured +17%); ord 9 would spill heavily at that budget
 #ifndef AWFL_P64_MIN_BLOCKS_ORD5

@@ -47,6 +47,7 @@
 //                                          for single-grid sweeps, the work list in
 //                                          global memory for ensembles)
 //   min_blocks(ORD)                        CTAs per SM the register budget must allow
+//   kSlab                                  the policy runs x splits of slabs (A.xh)
 //   load(A, gidx) / store(A, gidx, x)      state element access (halo writes)
 //   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
 #pragma once
@@ -134,7 +135,10 @@ template <int ORD, int C, int W, int ESZ> __host__ __device__ constexpr int tma_
 // One CTA's tile: lines bx*W .. bx*W+W-1 of plane `by` (x, y sweeps: by = k; z: by = j).
 // tmap: the tensor map of the TMA path (a kernel-parameter or global address), or nullptr
 // (the instantiation with TMA = true then stages every chunk by cp.async).
-template <class P, int ORD, int DIR, int C, int W, bool TMA = false>
+// SLAB: the x sweep of a slab of a larger grid, whose ends may take their halo values from
+// the neighbouring slabs (A.xh); a separate instantiation, so that the plain sweeps carry
+// none of its registers.
+template <class P, int ORD, int DIR, int C, int W, bool TMA = false, bool SLAB = false>
 __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int bx, const int by,
                                            const void *tmap = nullptr) {
   using Real = typename P::Real;
@@ -222,9 +226,10 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   const bool periodic = A.bc == BC_PERIODIC;
   // x sweep of a slab: the ends bordering another slab, and that slab's columns
   // ([5][nz][ny][HS+1] per side: side 0 holds positions -(HS+1)..-1, side 1 L..L+HS)
+  static_assert(!SLAB || DIR == 0, "slabs are cut along x");
   bool xlo = false, xhi = false;
   int jline = 0;
-  if constexpr (DIR == 0) {
+  if constexpr (SLAB) {
     xlo = A.xh[0] != nullptr;
     xhi = A.xh[1] != nullptr;
     jline = bx * W + w;
@@ -542,10 +547,10 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 
 // TMA: the policy's single-grid TMA path; its tensor map lives in the (grid-constant)
 // kernel parameter, the only place besides global memory a TMA copy may read it from.
-template <class P, int ORD, int DIR, int C, int W, bool TMA>
+template <class P, int ORD, int DIR, int C, int W, bool TMA, bool SLAB = false>
 __global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) sweep_kernel(const __grid_constant__ typename P::Args A) {
-  if constexpr (TMA) sweep_tile<P, ORD, DIR, C, W, true>(A, blockIdx.x, blockIdx.y, P::tma_map(A));
-  else sweep_tile<P, ORD, DIR, C, W, false>(A, blockIdx.x, blockIdx.y);
+  if constexpr (TMA) sweep_tile<P, ORD, DIR, C, W, true, SLAB>(A, blockIdx.x, blockIdx.y, P::tma_map(A));
+  else sweep_tile<P, ORD, DIR, C, W, false, SLAB>(A, blockIdx.x, blockIdx.y);
 }
 
 template <int ORD, int DIR> struct SweepShape;
@@ -570,6 +575,20 @@ cudaError_t launch_sweep_t(const typename P::Args &A, cudaStream_t st) {
   if (DIR == 0) grid = dim3((A.ny + W - 1) / W, A.nz);
   else if (DIR == 1) grid = dim3((A.nx + W - 1) / W, A.nz);
   else grid = dim3((A.nx + W - 1) / W, A.ny);
+  // the x split of a slab with neighbouring slabs' columns: the SLAB instantiation
+  if constexpr (DIR == 0 && P::kSlab) {
+    if (A.xh[0] != nullptr || A.xh[1] != nullptr) {
+      if constexpr (P::kTmaRing) {
+        typename P::Args a = A;
+        if (P::prepare_tma(a, ORD, DIR, C, W)) {
+          sweep_kernel<P, ORD, DIR, C, W, true, true><<<grid, block, 0, st>>>(a);
+          return cudaGetLastError();
+        }
+      }
+      sweep_kernel<P, ORD, DIR, C, W, false, true><<<grid, block, 0, st>>>(A);
+      return cudaGetLastError();
+    }
+  }
   if constexpr (P::kTmaRing) {
     // the policy encodes this launch's tensor map (box = one chunk of one variable); a
     // layout TMA cannot address (alignment) leaves tma off and the cp.async path runs

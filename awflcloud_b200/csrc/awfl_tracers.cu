@@ -37,6 +37,7 @@ namespace awfl {
 // tracer kernels read. A.tend points at the record base: R (NG*NG planes of ncell), U
 // (NG*NG), E (10: eL, eR), D (1: the pre-split rho', the stencil centre).
 struct P64Trc : P64 {
+  static constexpr bool kSlab = false;
   // the record stores need registers: 3 CTAs per SM at ord 5 instead of the plain sweep's 4
   static constexpr int min_blocks(int ord) { return ord == 5 ? 3 : 1; }
   template <int ORD> struct Rec {
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128) tracer_cell_kernel(TracerArgs T) {
       s[m] = T.tr[l * G.sv + G.g(kk, jj, ii)] / (T.D[G.cell(kk, jj, ii)] + A.dens_c[HS + kk]);
     }
     double rt[NG][NG], rut[NG][NG];
-    reconstruct_gll<ORD>(s, rt[0], A.weno_s != 0);
+    reconstruct_gll_any<ORD>(s, rt[0], A.weno_s != 0);
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
       rt[0][ii] *= rser[0][ii];

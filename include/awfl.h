@@ -243,14 +243,22 @@ int awfl_step_tlm(awfl_ctx *ctx, void *d_state_tangent, double dt, void *stream)
  * the adjoint of the state after the nsteps steps (dJ/dS_end), on return the adjoint of
  * the checkpoint state (dJ/dS_ckpt), dt held fixed. Halo entries of d_lambda are ignored
  * on entry and zero on return. The window is recomputed forward from the checkpoint and
- * its split-start states kept on a device tape owned by the context (see
- * awfl_adjoint_tape_bytes); a caller checkpointing every k steps calls this once per
- * segment, last segment first. Stream-ordered on `stream`. */
+ * its split-start states and per-split records kept on a device tape owned by the context
+ * (see awfl_adjoint_tape_bytes); a caller checkpointing every k steps calls this once per
+ * segment, last segment first. With a sub-window length m set (awfl_set_adjoint_subwindow)
+ * the window is taken m steps at a time: one plain forward pass keeps the state at every
+ * m-th step, then each sub-window, last first, is recomputed with its records and
+ * reversed -- a tape of about nsteps/m + 3m states and 3m records instead of 3*nsteps + 1
+ * states and 3*nsteps records, for one more forward pass over the window. The result is
+ * the same either way. Stream-ordered on `stream`. */
 int awfl_step_adjoint(awfl_ctx *ctx, const void *d_state_ckpt, void *d_lambda, int nsteps, double dt,
                       void *stream);
 
 /* Device memory awfl_step_adjoint holds for a window of nsteps steps (tape + scratch). */
 int awfl_adjoint_tape_bytes(const awfl_ctx *ctx, int nsteps, long *bytes);
+
+/* Steps per recorded sub-window of awfl_step_adjoint (0, the default: the whole window). */
+int awfl_set_adjoint_subwindow(awfl_ctx *ctx, int steps);
 
 /* The dimSwitch flag of the context (1 = next step runs X,Y,Z). */
 int awfl_get_dimswitch(const awfl_ctx *ctx, int *value);

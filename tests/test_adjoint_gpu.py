@@ -133,6 +133,32 @@ def test_adjoint_is_the_transpose_of_the_tlm(ord_, bc):
     assert abs(lhs - rhs) <= 1e-11 * scale, (lhs, rhs, scale)
 
 
+@pytest.mark.parametrize("m", [1, 3, 7])
+def test_two_level_window_equals_one_level(m):
+    """Sub-windows of m steps (one plain forward pass keeping every m-th state, then each
+    sub-window recorded and reversed) give exactly the one-level adjoint of the 20-step
+    window -- odd m included, whose sub-windows start with the other dimSwitch -- on a
+    smaller tape."""
+    c = capi.Context(*N)
+    s0 = base_state(c)
+    dt = c.cfl(s0, 0.8)
+    g = torch.Generator().manual_seed(13)
+    lam = unit_direction(c, g)
+    a = lam.clone()
+    c.dimswitch = 1
+    c.step_adjoint(s0, a, 20, dt)
+    one_level = c.adjoint_tape_bytes(20)
+    c.set_adjoint_subwindow(m)
+    b = lam.clone()
+    c.dimswitch = 1
+    c.step_adjoint(s0, b, 20, dt)
+    torch.cuda.synchronize()
+    assert c.dimswitch == 1
+    assert torch.equal(a, b)
+    assert c.adjoint_tape_bytes(20) < one_level / 2
+    c.set_adjoint_subwindow(0)
+
+
 def test_adjoint_segments_equal_one_window():
     """Two 10-step windows (the second from the recomputed checkpoint) give exactly the
     adjoint of one 20-step window."""
@@ -164,11 +190,15 @@ def test_gradient_matches_central_finite_differences():
     awfl_step_adjoint (checkpoint every 10 steps) against FP64 central differences,
     eps = 1e-6, 16 seeded unit directions.
 
-    The finite difference itself is only good to ~1.5e-6 here: its rounding part grows as
-    1/eps (1.1e-5 at eps = 1e-7; the fluxes carry the full ~1e5 Pa pressure, so every
-    step leaves ~1e-13 of rounding noise in the state) and its truncation part as eps^2
-    (1e-4 at eps = 1e-5). Hence the 3e-6 bound; the adjoint agrees with the FP64
-    tangent-linear model to ~1e-12 (test_adjoint_is_the_transpose_of_the_tlm)."""
+    This test meets 2e-6 (measured 1.6e-6), not the north star's 1e-6, and the shortfall is
+    the FP64 finite difference's own error, not the adjoint's: the difference's rounding
+    part grows as 1/eps (1.1e-5 at eps = 1e-7; the fluxes carry the full ~1e5 Pa
+    pressure, so every step leaves ~1e-13 of rounding noise in the state) and its
+    truncation part as eps^2 (9.7e-5 at eps = 1e-5); directions scaled to the state's own
+    magnitudes do no better (1.1e-6 at best). The 1e-6 bar is met against the same
+    differences taken in extended precision (test_gradient_matches_extended_precision_
+    finite_differences: ~1e-8), and the adjoint agrees with the FP64 tangent-linear model
+    to ~1e-12 (test_adjoint_is_the_transpose_of_the_tlm)."""
     c = capi.Context(*N)
     s0 = base_state(c)
     dt = c.cfl(s0, 0.8)
@@ -193,7 +223,7 @@ def test_gradient_matches_central_finite_differences():
         fd.append((J(s0 + eps * v) - J(s0 - eps * v)) / (2 * eps))
     gv, fd = np.array(gv), np.array(fd)
     err = np.linalg.norm(gv - fd) / np.linalg.norm(fd)
-    assert err <= 3e-6, (err, gv, fd)
+    assert err <= 2e-6, (err, gv, fd)
 
 
 def test_gradient_matches_extended_precision_finite_differences():
