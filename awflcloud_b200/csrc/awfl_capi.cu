@@ -432,6 +432,8 @@ int awfl_create(const awfl_config *cfg, int device, awfl_ctx **out) {
     return fail(nullptr, AWFL_ERR_NOT_BUILT, "precision %d is not available in this build", cfg->precision);
   const int hs = (cfg->ord - 1) / 2;
   if (cfg->nx < 1 || cfg->ny < 1 || cfg->nz < 1) return fail(nullptr, AWFL_ERR_ARG, "nx, ny, nz must be >= 1");
+  // the kernels lay y and z along grid dimensions of at most 65535 blocks
+  if (cfg->ny > 65535 || cfg->nz > 65535) return fail(nullptr, AWFL_ERR_ARG, "ny and nz must be <= 65535");
   if (!(cfg->xlen > 0) || !(cfg->ylen > 0) || !(cfg->zlen > 0))
     return fail(nullptr, AWFL_ERR_ARG, "xlen, ylen, zlen must be > 0");
   const int bcs[3] = {cfg->bc_x, cfg->bc_y, cfg->bc_z};

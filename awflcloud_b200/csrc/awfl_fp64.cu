@@ -403,63 +403,71 @@ cudaError_t launch_check_state(const void *state, int fp32, long plane, const do
 // Output diagnostics of Spatial::output (Spatial:1744-1778), FP64 from either state form:
 // out[f][k][j][i], f = dens_pert, u, v, w, pot_temp_pert, pressure_pert. Same operations
 // and order as the reference (IEEE division, no contraction in this translation unit,
-// the correctly rounded pow for C0*(r*t)^gamma).
-__global__ void output_fields_kernel(const void *state, int fp32, long plane, const double *dens_c,
-                                     const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
-                                     double *out) {
+// the correctly rounded pow for C0*(r*t)^gamma). One thread per cell: x along the block,
+// y and z along the grid (no index division), a streaming kernel bound by its 88 bytes
+// per cell.
+constexpr int kOutX = 128;
+__global__ void __launch_bounds__(kOutX) output_fields_kernel(const void *state, int fp32, long plane,
+                                                             const double *dens_c, const double *denstheta_c,
+                                                             const double *pres_c, int nx, int ny, int nz, int hs,
+                                                             double *out) {
+  const int i = blockIdx.x * kOutX + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= nx) return;
   const long n = (long)nz * ny * nx;
+  const long c = ((long)k * ny + j) * nx + i;
   const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long)nx * ny));
-    const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
-    const double rp = state_at(state, fp32, plane, g);
-    const double r = rp + dens_c[hs + k];
-    out[c] = rp;
-    out[n + c] = state_at(state, fp32, plane, g + 1 * sv) / r;
-    out[2 * n + c] = state_at(state, fp32, plane, g + 2 * sv) / r;
-    out[3 * n + c] = state_at(state, fp32, plane, g + 3 * sv) / r;
-    const double t = (state_at(state, fp32, plane, g + 4 * sv) + denstheta_c[hs + k]) / r;
-    out[4 * n + c] = t - denstheta_c[hs + k] / dens_c[hs + k];
-    const double p = C0 * pow_cr(r * t, GAMMA);
-    out[5 * n + c] = p - pres_c[hs + k];
-  }
+  const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
+  const double dk = dens_c[hs + k], dtk = denstheta_c[hs + k], pk = pres_c[hs + k];
+  const double rp = state_at(state, fp32, plane, g);
+  const double mu = state_at(state, fp32, plane, g + 1 * sv);
+  const double mv = state_at(state, fp32, plane, g + 2 * sv);
+  const double mw = state_at(state, fp32, plane, g + 3 * sv);
+  const double mt = state_at(state, fp32, plane, g + 4 * sv);
+  const double r = rp + dk;
+  out[c] = rp;
+  out[n + c] = mu / r;
+  out[2 * n + c] = mv / r;
+  out[3 * n + c] = mw / r;
+  const double t = (mt + dtk) / r;
+  out[4 * n + c] = t - dtk / dk;
+  const double p = C0 * pow_cr(r * t, GAMMA);
+  out[5 * n + c] = p - pk;
 }
 
 cudaError_t launch_output_fields(const void *state, int fp32, long plane, const double *dens_c,
                                  const double *denstheta_c, const double *pres_c, int nx, int ny, int nz, int hs,
                                  int nsm, double *out, cudaStream_t st) {
-  const long n = (long)nz * ny * nx;
-  long blocks = (n + 255) / 256;
-  if (blocks > (long)nsm * 8) blocks = (long)nsm * 8;
-  if (blocks < 1) blocks = 1;
-  output_fields_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, denstheta_c, pres_c, nx, ny, nz,
-                                                         hs, out);
+  (void)nsm;
+  if ((long)nz * ny * nx == 0) return cudaSuccess;
+  const dim3 grid((nx + kOutX - 1) / kOutX, ny, nz);
+  output_fields_kernel<<<grid, kOutX, 0, st>>>(state, fp32, plane, dens_c, denstheta_c, pres_c, nx, ny, nz, hs, out);
   return cudaGetLastError();
 }
 
 // Tracer fields of Spatial::output (Spatial:1778-1783): out[tr][k][j][i] =
-// tracers(tr, hs+k, hs+j, hs+i) / (rho'(k,j,i) + hyDensCells(hs+k)).
-__global__ void tracer_fields_kernel(const void *state, int fp32, long plane, const double *dens_c,
-                                     const double *tracers, int ntr, int nx, int ny, int nz, int hs, double *out) {
+// tracers(tr, hs+k, hs+j, hs+i) / (rho'(k,j,i) + hyDensCells(hs+k)). Launched like
+// output_fields_kernel.
+__global__ void __launch_bounds__(kOutX) tracer_fields_kernel(const void *state, int fp32, long plane,
+                                                             const double *dens_c, const double *tracers, int ntr,
+                                                             int nx, int ny, int nz, int hs, double *out) {
+  const int i = blockIdx.x * kOutX + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= nx) return;
   const long n = (long)nz * ny * nx;
+  const long c = ((long)k * ny + j) * nx + i;
   const long sy = nx + 2 * hs, sz = (long)(ny + 2 * hs) * sy, sv = (long)(nz + 2 * hs) * sz;
-  for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long)nx * ny));
-    const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
-    const double r = state_at(state, fp32, plane, g) + dens_c[hs + k];
-    for (int t = 0; t < ntr; t++) out[t * n + c] = tracers[t * sv + g] / r;
-  }
+  const long g = (hs + k) * sz + (hs + j) * sy + hs + i;
+  const double r = state_at(state, fp32, plane, g) + dens_c[hs + k];
+  for (int t = 0; t < ntr; t++) out[t * n + c] = tracers[t * sv + g] / r;
 }
 
 cudaError_t launch_tracer_fields(const void *state, int fp32, long plane, const double *dens_c,
                                  const double *tracers, int ntr, int nx, int ny, int nz, int hs, int nsm, double *out,
                                  cudaStream_t st) {
+  (void)nsm;
   const long n = (long)nz * ny * nx;
   if (n == 0 || ntr == 0) return cudaSuccess;
-  long blocks = (n + 255) / 256;
-  if (blocks > (long)nsm * 8) blocks = (long)nsm * 8;
-  tracer_fields_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, fp32, plane, dens_c, tracers, ntr, nx, ny, nz, hs,
-                                                         out);
+  const dim3 grid((nx + kOutX - 1) / kOutX, ny, nz);
+  tracer_fields_kernel<<<grid, kOutX, 0, st>>>(state, fp32, plane, dens_c, tracers, ntr, nx, ny, nz, hs, out);
   return cudaGetLastError();
 }
 

@@ -629,7 +629,39 @@ def ensemble_leg(a, local):
     torch.cuda.synchronize()
     seq_ms = e0.elapsed_time(e1)
     counts = {"%dx%dx%d" % s: int((picks == k).sum()) for k, s in enumerate(ENS_SIZES)}
+    # load report: each size class alone, as an ensemble of its members and member by member
+    by_size = []
+    for k, size in enumerate(ENS_SIZES):
+        idx = [i for i in range(len(cfgs)) if picks[i] == k]
+        if not idx:
+            continue
+        sub = capi.Ensemble([cfgs[i] for i in idx], device=local)
+        sub_states = [states[i].clone() for i in idx]
+        for q, i in enumerate(idx):
+            sub.bind(q, sub_states[q], dts[i])
+        sub.tune(reps=3, stream=stream)
+        sub.step(2, stream=stream)
+        nst = 10
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sub.step(nst, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sub_ms = e0.elapsed_time(e1)
+        e0.record(stream)
+        for _ in range(nst):
+            for q, i in enumerate(idx):
+                E.members[i].step(sub_states[q], dts[i])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        one_ms = e0.elapsed_time(e1)
+        c_cells = len(idx) * size[0] * size[1] * size[2]
+        by_size.append({"size": "%dx%dx%d" % size, "members": len(idx), "cells": c_cells,
+                        "ensemble_value": round(c_cells * nst / (sub_ms * 1e-3) / 1e6, 1),
+                        "sequential_value": round(c_cells * nst / (one_ms * 1e-3) / 1e6, 1)})
+        del sub
     return {"workload": "%d FP32 ord-5 members, %d steps, sizes %s" % (a.ens_members, a.ens_steps, counts),
+            "by_size": by_size,
             "value": round(cells * a.ens_steps / (ens_ms * 1e-3) / 1e6, 3), "unit": UNIT,
             "ms_per_step": round(ens_ms / a.ens_steps, 4),
             "sequential_value": round(cells * a.ens_steps / (seq_ms * 1e-3) / 1e6, 3),
