@@ -49,6 +49,12 @@ __device__ __forceinline__ double div_markstein(double a, double b, double y) {
 // a / r.b, correctly rounded
 template <class Sc> __device__ __forceinline__ Sc divr(const Sc &a, const Rcp<Sc> &r) { return a / r.b; }
 __device__ __forceinline__ double divr(const double &a, const Rcp<double> &r) { return div_markstein(a, r.b, r.y); }
+// a / r.b, correctly rounded for every dividend: those below 2^-900 in magnitude (where
+// the quotient or the remainder could leave the normal range, as transported tracer
+// values that decay towards zero can) take the IEEE division itself
+__device__ __forceinline__ double divr_any(double a, const Rcp<double> &r) {
+  return fabs(a) < 0x1p-900 ? a / r.b : div_markstein(a, r.b, r.y);
+}
 // any scalar divided by a double divisor with a known reciprocal
 template <class Sc> __device__ __forceinline__ Sc divd(const Sc &a, const Rcp<double> &r) { return a / r.b; }
 __device__ __forceinline__ double divd(const double &a, const Rcp<double> &r) { return div_markstein(a, r.b, r.y); }
@@ -59,6 +65,13 @@ template <class Sc> __device__ __forceinline__ Sc divk(const Sc &a, int k) {
   if (k == 1) return a;
   if ((k & (k - 1)) == 0) return a * (1.0 / k);
   return divd(a, rcp_known((double)k, 1.0 / k));
+}
+
+// divk for dividends of any magnitude (divr_any's range)
+__device__ __forceinline__ double divk_any(double a, int k) {
+  if (k == 1) return a;
+  if ((k & (k - 1)) == 0) return a * (1.0 / k);
+  return divr_any(a, rcp_known((double)k, 1.0 / k));
 }
 
 // the reciprocal of 2b from that of b (exact: a power-of-two scaling)

@@ -101,6 +101,9 @@ struct oracle_ctx {
   const int *trpos;
   oreal *tr, *ttend;        /* (ntr,nz+2hs,ny+2hs,nx+2hs), (ntr,nz,ny,nx) */
   oreal *tlimits, *tflux, *tflux_lim;  /* (ntr,2,...), (ntr,...), (ntr,...) */
+  /* faces of the last tracer split whose limited flux differs from the one computed with
+   * every face read unscaled (the serial order's chains; oracle_limiter_chained_faces) */
+  long lim_chained;
 };
 
 /* ---------------------------------------------------------------- indexing */
@@ -653,6 +656,7 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
 #define LJ(p) (dir == 1 ? (p) : (dir == 2 ? a : b))
 #define LI(p) (dir == 0 ? (p) : b)
           oreal *TF = c->tflux_lim;
+          long chained = 0;
           for (int f = 0; f <= n; f++) {
             const long fi = fidx(c, l, LK(f), LJ(f), LI(f));
             const oreal un = 0.5 * (c->limits[lidx(c, nm, 0, LK(f), LJ(f), LI(f))] +
@@ -665,8 +669,15 @@ void oracle_compute_tendencies_dir(oracle_ctx *c, oreal *st, oreal *tend, oreal 
             const oreal f2 = dmax(TF[fidx(c, l, LK(ind + 1), LJ(ind + 1), LI(ind + 1))], 0.);
             const oreal fluxOut = dt * (f2 - f1) / dxd;
             const oreal dens = st[sidx(c, idR, HS + LK(ind), HS + LJ(ind), HS + LI(ind))] + c->hyDensCells[HS + LK(ind)];
-            TF[fi] *= dmin(1., tr[sidx(c, l, HS + LK(ind), HS + LJ(ind), HS + LI(ind))] * dens / (fluxOut + eps));
+            const oreal q = tr[sidx(c, l, HS + LK(ind), HS + LJ(ind), HS + LI(ind))];
+            TF[fi] *= dmin(1., q * dens / (fluxOut + eps));
+            /* the same face with both of its cell's faces read unscaled */
+            const oreal u1 = dmin(c->tflux[fidx(c, l, LK(ind), LJ(ind), LI(ind))], 0.);
+            const oreal u2 = dmax(c->tflux[fidx(c, l, LK(ind + 1), LJ(ind + 1), LI(ind + 1))], 0.);
+            if (!(c->tflux[fi] * dmin(1., q * dens / (dt * (u2 - u1) / dxd + eps)) == TF[fi])) chained++;
           }
+#pragma omp atomic
+          c->lim_chained += chained;
 #undef LK
 #undef LJ
 #undef LI
@@ -717,6 +728,7 @@ void oracle_split_tracers(oracle_ctx *c, oreal *st, oreal *tr, int ntr, const in
   c->ntr = ntr;
   c->trpos = pos;
   c->tr = tr;
+  c->lim_chained = 0;
   c->ttend = (oreal *)calloc((size_t)ntr * ncell + 1, sizeof(oreal));
   c->tlimits = (oreal *)calloc((size_t)ntr * 2 * nf + 1, sizeof(oreal));
   c->tflux = (oreal *)calloc((size_t)ntr * nf + 1, sizeof(oreal));
@@ -779,6 +791,7 @@ void oracle_time_step(oracle_ctx *c, oreal *st, oreal dt) {
 }
 
 int oracle_get_dimswitch(const oracle_ctx *c) { return c->dimswitch; }
+long oracle_limiter_chained_faces(const oracle_ctx *c) { return c->lim_chained; }
 void oracle_set_dimswitch(oracle_ctx *c, int v) { c->dimswitch = v != 0; }
 
 /* ---------------------------------------------------------------- CFL */

@@ -74,6 +74,10 @@ void oracle_time_step_tracers(oracle_ctx *c, oreal *state, oreal *tracers, int n
 /* One split of that step along dir (0/1/2). */
 void oracle_split_tracers(oracle_ctx *c, oreal *state, oreal *tracers, int ntr, const int *pos, oreal dt, int dir);
 int oracle_get_dimswitch(const oracle_ctx *c);
+/* Faces of the last oracle_split_tracers / oracle_time_step_tracers split whose limited
+ * flux differs from the value computed with every face read before scaling: the faces where
+ * the serial order of the limiter matters. */
+long oracle_limiter_chained_faces(const oracle_ctx *c);
 void oracle_set_dimswitch(oracle_ctx *c, int v);
 
 /* Derived tables and background, for pinning against the reference. */

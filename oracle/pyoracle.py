@@ -105,6 +105,8 @@ class Oracle(_Grid):
             L.oracle_init_tracers.argtypes = [_VP, _DP, _I]
             L.oracle_time_step_tracers.argtypes = [_VP, _DP, _DP, _I, ctypes.POINTER(_I), _D]
             L.oracle_split_tracers.argtypes = [_VP, _DP, _DP, _I, ctypes.POINTER(_I), _D, _I]
+            L.oracle_limiter_chained_faces.restype = ctypes.c_long
+            L.oracle_limiter_chained_faces.argtypes = [_VP]
             L.oracle_set_spacing.argtypes = [_VP, _D, _D, _D]
             L.oracle_compute_dt.restype = _D
             L.oracle_compute_dt.argtypes = [_VP, _DP, _D]
@@ -169,6 +171,11 @@ class Oracle(_Grid):
         pos = [1] * n if pos is None else pos
         flags = (_I * max(n, 1))(*[int(bool(p)) for p in pos])
         self.L.oracle_split_tracers(self.h, _ptr(st), _ptr(tr), n, flags, dt, d)
+
+    def limiter_chained_faces(self):
+        """Faces of the last tracer split whose limited flux depends on the serial order
+        (differs from the value with every face read unscaled)."""
+        return self.L.oracle_limiter_chained_faces(self.h)
 
     def compute_dt(self, st, cfl=0.8):
         return self.L.oracle_compute_dt(self.h, _ptr(st), cfl)

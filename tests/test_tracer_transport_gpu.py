@@ -74,6 +74,47 @@ def test_step_tracers_bit_exact(case):
         assert np.abs(got_tr[t] - t0[t])[h:h + nz, h:h + ny, h:h + nx].max() > 1e-6, t
 
 
+def _chained_case(nx, ny, nz, bc, d, seed):
+    """A state whose velocity along d changes sign cell by cell at random (many cells
+    empty through both faces) and positive tracers with nearly empty cells: there the
+    limiter scales a face that the next face reads, the places where the reference's
+    serial face order decides the result."""
+    O = Oracle(nx, ny, nz, bc=bc, weno_scalars=True, weno_winds=True, crpow=True)
+    st = O.new_state()
+    O.init_state(st)
+    rng = np.random.default_rng(seed)
+    h = O.hs
+    inner = (slice(h, h + nz), slice(h, h + ny), slice(h, h + nx))
+    sh = (nz, ny, nx)
+    st[(1 + d,) + inner] = rng.choice([-1., 1.], size=sh) * rng.uniform(10, 40, size=sh)
+    tr = O.new_tracers(3)
+    for t in range(3):
+        tr[(t,) + inner] = np.where(rng.uniform(size=sh) > 0.4, rng.uniform(0.5, 1.5, sh), rng.uniform(0, 1e-2, sh))
+    return O, st, tr
+
+
+@pytest.mark.parametrize("d", [0, 1, 2])
+@pytest.mark.parametrize("bc", [(0, 0, 1), (1, 1, 1)])
+def test_limiter_serial_chains(d, bc):
+    """The device limits every face at once and redoes in face order only the lines where
+    a scaled face feeds another: on a case with hundreds of such faces (counted by the
+    oracle) one split matches the oracle's serial limiter bit for bit."""
+    nx, ny, nz = 24, 20, 16
+    O, st, tr = _chained_case(nx, ny, nz, bc, d, 7 + d)
+    pos = [1, 1, 0]
+    dt = O.compute_dt(st, 0.8)
+    c = capi.Context(nx, ny, nz, bc=tuple(BCN[b] for b in bc), weno_scalars=True, weno_winds=True, ord_=5)
+    dst = torch.from_numpy(st).cuda()
+    dtr = torch.from_numpy(tr).cuda()
+    O.split_tracers(st, tr, dt, d, pos=pos)
+    assert O.limiter_chained_faces() > 100
+    c.split_tracers(dst, dtr, dt, d, pos=pos)
+    got = dtr.cpu().numpy()
+    for t in range(3):
+        assert np.array_equal(got[t], tr[t]), (t, np.abs(got[t] - tr[t]).max())
+    assert np.array_equal(dst.cpu().numpy(), st)
+
+
 def test_split_tracers_rejects_fp32_and_bad_args():
     c = capi.Context(16, 12, 10, precision=capi.FP32)
     st = c.new_state()
