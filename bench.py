@@ -322,6 +322,8 @@ def time_form(a, prec, local, world, clocks=None):
     avg_launch_s = statistics.mean(launch_ms) * 1e-3
     achieved = flops_launch / avg_launch_s / 1e12
     esz = 8 if prec == capi.FP64 else 4
+    per_cell = EXECUTED_OPS.get((prec, a.ord), {}).get("ops_per_cell")
+    ops_exec = per_cell * cells if per_cell else None
     roofline = {"bound": "fp64" if prec == capi.FP64 else "fp32",
                 "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
                 "frac": round(achieved / peak, 4), "traffic": TRAFFIC.get((prec, a.ord)),
@@ -329,7 +331,8 @@ def time_form(a, prec, local, world, clocks=None):
                                "FMA lane; FP32: the larger of scalar and paired FMA)",
                 **peaks,
                 "ops_algorithmic": flops_launch,
-                "ops_executed": EXECUTED_OPS.get((prec, a.ord), {}).get("ops_per_launch"),
+                "ops_executed": ops_exec,
+                "frac_executed": round(ops_exec / avg_launch_s / 1e12 / peak, 4) if ops_exec else None,
                 "ops_executed_source": EXECUTED_OPS.get((prec, a.ord), {}).get("source"),
                 "launch_ms_avg": round(avg_launch_s * 1e3, 4),
                 "bytes_algorithmic_per_launch": cells * 10 * esz * (1 if prec == capi.FP64 else 2)}
@@ -342,12 +345,17 @@ def time_form(a, prec, local, world, clocks=None):
 # dram__bytes_read.sum + dram__bytes_write.sum of the sweep kernels on this 256x256x128
 # workload (one capture of the same build; ncu cannot run inside the timed process).
 TRAFFIC = {(0, 5): 650_500_000, (1, 5): 635_700_000}
-# Floating-point operations the sweep kernels execute per launch (mean over x/y/z), from
-# ncu's per-opcode thread-instruction counters of the same capture: FP32 form: FADD + FMUL
-# + 2 x FFMA, paired instructions counted per lane; FP64: DADD + DMUL + 2 x DFMA (the
-# division and pow sequences included). The algorithmic count (flops.py) follows the
-# reference's loops instead.
-EXECUTED_OPS = {}
+# Floating-point operations the sweep kernels execute per cell and split (mean over x/y/z),
+# from ncu's per-opcode thread-instruction counters on 256x256x64 (4,194,304 cells): FP32
+# form: FADD + FMUL + 2 x FFMA, paired instructions counted per lane; FP64: DADD + DMUL +
+# 2 x DFMA (the division and pow sequences included). The algorithmic count (flops.py)
+# follows the reference's loops instead.
+EXECUTED_OPS = {
+    (1, 5): {"ops_per_cell": 1769, "source": "ncu sm__sass_thread_inst_executed_op_{fadd,fmul,ffma,fadd2,fmul2,"
+                                             "ffma2}_pred_on, sweep kernels at 256x256x64"},
+    (0, 5): {"ops_per_cell": 4766, "source": "ncu sm__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on, "
+                                             "sweep kernels at 256x256x64"},
+}
 
 
 def rel_l2_after(a, steps, local):
@@ -581,6 +589,67 @@ def precision_leg(a, local):
 ENS_SIZES = ((32, 32, 32), (64, 64, 32), (96, 96, 48), (128, 128, 64))
 
 
+def ensemble_members(a):
+    """The seeded members of the batching form: size picks, member configs and the
+    init_state arguments of each member, drawn in member order."""
+    import numpy as np
+    from awflcloud_b200 import capi
+    rng = np.random.default_rng(20261203)
+    picks = rng.integers(0, len(ENS_SIZES), size=a.ens_members)
+    cfgs = [dict(nx=ENS_SIZES[p][0], ny=ENS_SIZES[p][1], nz=ENS_SIZES[p][2], precision=capi.FP32, ord_=5)
+            for p in picks]
+    inits = []
+    for i in range(len(cfgs)):
+        r = float(rng.uniform(1000.0, 3000.0))
+        inits.append(dict(kind=1, shape=1, x0=float(rng.uniform(5e3, 15e3)), y0=float(rng.uniform(5e3, 15e3)),
+                          z0=float(rng.uniform(1.5e3, 3e3)), xrad=r, yrad=r, zrad=r, amp=float(rng.uniform(1, 4)),
+                          pwr=1.0, noise_amp=0.01, noise_seed=20261203 + i))
+    return picks, cfgs, inits
+
+
+def ensemble_ranks_leg(a, local, rank, world):
+    """The batching form over N GPUs: the one-GPU leg's seeded members spread over the ranks
+    by cell count (awflcloud_b200.members), each rank's share one ensemble on its own GPU,
+    no communication while stepping; the step loop timed on each rank's stream, maximum
+    over ranks. Total work is fixed as N grows (strong scaling)."""
+    import torch
+    import torch.distributed as dist
+    from awflcloud_b200.members import RankEnsemble, member_cells
+    picks, cfgs, inits = ensemble_members(a)
+    R = RankEnsemble(cfgs, rank, world, device=local)
+    states = []
+    for i in R.share:
+        m = R.member(i)
+        s = m.new_state()
+        m.init_state(s, **inits[i])
+        R.bind(i, s, m.cfl(s, 0.8))
+        states.append(s)
+    stream = torch.cuda.current_stream()
+    R.tune(reps=3, stream=stream)
+    R.step(2, stream=stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    R.step(a.ens_steps, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) if R.share else 0.0
+    dist.barrier()
+    max_ms = max_over_ranks(ms, world)
+    cells = sum(member_cells(cfgs))
+    finite = all(bool(torch.isfinite(s).all().item()) for s in states)
+    R.close()
+    return {"workload": "%d FP32 ord-5 members, %d steps, over %d GPUs" % (a.ens_members, a.ens_steps, world),
+            "value": round(cells * a.ens_steps / (max_ms * 1e-3) / 1e6, 3), "unit": UNIT,
+            "ms_per_step": round(max_ms / a.ens_steps, 4), "scaling": "strong",
+            "cells_per_rank": [sum(member_cells([cfgs[i] for i in sh])) for sh in R.shares],
+            "members_per_rank": [len(sh) for sh in R.shares],
+            "parallelism": "members assigned to ranks by cell count (largest first onto the least-loaded "
+                           "rank); one ensemble per GPU; no collective while stepping",
+            "finite_on_rank0": finite}
+
+
 def ensemble_leg(a, local):
     """Batching form: ens_members FP32 ord-5 members with seeded sizes from ENS_SIZES and
     seeded bubbles (centre x, y in [5, 15] km, z in [1.5, 3] km, amp in [1, 4] K, radius in
@@ -590,18 +659,12 @@ def ensemble_leg(a, local):
     import numpy as np
     import torch
     from awflcloud_b200 import capi
-    rng = np.random.default_rng(20261203)
-    picks = rng.integers(0, len(ENS_SIZES), size=a.ens_members)
-    cfgs = [dict(nx=ENS_SIZES[p][0], ny=ENS_SIZES[p][1], nz=ENS_SIZES[p][2], precision=capi.FP32, ord_=5)
-            for p in picks]
+    picks, cfgs, inits = ensemble_members(a)
     E = capi.Ensemble(cfgs, device=local)
     states, dts = [], []
     for i, m in enumerate(E.members):
         s = m.new_state()
-        r = float(rng.uniform(1000.0, 3000.0))
-        m.init_state(s, kind=1, shape=1, x0=float(rng.uniform(5e3, 15e3)), y0=float(rng.uniform(5e3, 15e3)),
-                     z0=float(rng.uniform(1.5e3, 3e3)), xrad=r, yrad=r, zrad=r, amp=float(rng.uniform(1, 4)),
-                     pwr=1.0, noise_amp=0.01, noise_seed=20261203 + i)
+        m.init_state(s, **inits[i])
         dt = m.cfl(s, 0.8)
         E.bind(i, s, dt)
         states.append(s)
@@ -691,6 +754,8 @@ def run_ours(a):
     e2e64 = None
     if other is not None and not a.no_e2e:
         e2e64 = e2e_leg(a, other, torch.cuda.current_stream(), world)
+    # the batching form over the ranks (every rank takes part); on one GPU the leg below
+    ens_ranks = ensemble_ranks_leg(a, local, rank, world) if (world > 1 and not a.no_ensemble) else None
 
     if rank == 0:
         line = {"metric": METRIC, "value": round(main["value"], 3), "unit": UNIT, "n_gpus": world,
@@ -717,7 +782,9 @@ def run_ours(a):
         line["output"] = output_leg(main["ctx"], main["state"])
         if not a.no_adjoint:
             line["adjoint"] = adjoint_leg(a, local)
-        if not a.no_ensemble:
+        if ens_ranks is not None:
+            line["ensemble"] = ens_ranks
+        elif not a.no_ensemble:
             line["ensemble"] = ensemble_leg(a, local)
         if not a.no_precision:
             line["precision"] = precision_leg(a, local)

@@ -143,3 +143,30 @@ def test_ensemble_rejects_bad_use():
         E.step(1)
     with pytest.raises(capi.AwflError):
         E.set_shape(0, 99)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_rank_shares_equal_single_steps(world):
+    """The members split over ranks (awflcloud_b200.members): each share is its own
+    ensemble -- here every rank's share held in this one process on one GPU, none waiting
+    on another -- and every member still equals stepping it alone, bit for bit (FP64)."""
+    from awflcloud_b200.members import RankEnsemble
+    cfgs = member_configs(capi.FP64, 5)
+    parts = [RankEnsemble(cfgs, r, world) for r in range(world)]
+    assert sorted(i for p in parts for i in p.share) == list(range(len(cfgs)))
+    states, dts = [None] * len(cfgs), [None] * len(cfgs)
+    for p in parts:
+        for i in p.share:
+            m = p.member(i)
+            states[i] = init_member(m, i)
+            dts[i] = m.cfl(states[i], 0.8)
+            p.bind(i, states[i], dts[i])
+    s0 = [s.clone() for s in states]
+    for p in parts:
+        p.step(3)
+    ref = alone(cfgs, s0, dts, 3)
+    torch.cuda.synchronize()
+    for p in parts:
+        for i in p.share:
+            assert mismatch(p.member(i), states[i], ref[i]) == 0.0, i
+        p.close()
