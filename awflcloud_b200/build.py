@@ -14,6 +14,7 @@ Translation units and their numerics flags:
   awfl_ensemble.cu ensemble host side: work lists, CUDA graph, autotuner (host code only)
   awfl_netcdf.cu   netCDF output file writer (host code only)
   awfl_tracers.cu  tracer transport of the FP64 path: --fmad=false
+  awfl_tracers32.cu  tracer transport of the FP32 form: the FP32 form's flags
 
 The library lands in-tree at awflcloud_b200/lib/libawfl.so so that it travels with the
 source tree. ``python -m awflcloud_b200.build [--force]``.
@@ -47,6 +48,7 @@ UNITS = {
     "awfl_ensemble.cu": [],
     "awfl_netcdf.cu": [],
     "awfl_tracers.cu": ["--fmad=false"],
+    "awfl_tracers32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
 }
 
 

@@ -262,6 +262,9 @@ int ensure_tables(awfl_ctx *c) {
   if (e == cudaSuccess)
     e = upload_tables_ens32(c->cfg.ord, c->recon.data(), c->c2g.data(), c->s2g.data(), c->deriv.data(),
                             c->idl.data(), c->sigma, c->wts_ngll.data());
+  if (e == cudaSuccess)
+    e = upload_tables_tracers32(c->cfg.ord, c->recon.data(), c->c2g.data(), c->s2g.data(), c->deriv.data(),
+                                c->idl.data(), c->sigma, c->wts_ngll.data());
   if (e != cudaSuccess) return cuda_fail(c, e, "upload of FP32 transform tables");
   if (c->device >= 0 && c->device < 256) g_tab_uploaded[c->device] |= bit;
   return AWFL_OK;
@@ -895,7 +898,6 @@ int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntrace
                        int dir, void *stream) {
   if (!c) return AWFL_ERR_ARG;
   if (c->nslabs > 1) return fail(c, AWFL_ERR_ARG, "tracer transport is not available on a slab");
-  if (fp32(c)) return fail(c, AWFL_ERR_ARG, "tracer transport needs an FP64 context");
   if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
   if (ntracers < 0 || ntracers > 64) return fail(c, AWFL_ERR_ARG, "ntracers must be in [0, 64]");
   if (ntracers == 0) return awfl_split(c, d_state, dt, dir, stream);
@@ -910,11 +912,19 @@ int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntrace
   for (int l = 0; l < ntracers; l++)
     if (pos[l]) mask |= 1ull << l;
   const size_t need =
-      sizeof(double) * (size_t)tracer_scratch_doubles(c->cfg.ord, c->cfg.nx, c->cfg.ny, c->cfg.nz, ntracers);
+      tracer_scratch_bytes(c->cfg.ord, c->cfg.nx, c->cfg.ny, c->cfg.nz, ntracers, fp32(c) ? 4 : 8);
   rc = ensure_buffer(c, &c->d_trc, &c->trc_bytes, need, "tracer scratch");
   if (rc) return rc;
-  SweepArgs A = sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY);
-  cudaError_t e = launch_split_tracers(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, (cudaStream_t)stream);
+  cudaError_t e;
+  if (fp32(c)) {
+    SweepArgs32 A = sweep_args32(c, d_state, nullptr, dt, dir, MODE_APPLY);
+    const double dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
+    e = launch_split_tracers32(c->cfg.ord, dir, A, c->d_dens_c, dt, dxd, d_tracers, ntracers, mask,
+                               reinterpret_cast<float *>(c->d_trc), (cudaStream_t)stream);
+  } else {
+    SweepArgs A = sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY);
+    e = launch_split_tracers(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, (cudaStream_t)stream);
+  }
   if (e != cudaSuccess) return cuda_fail(c, e, "split_tracers");
   return AWFL_OK;
 }

@@ -238,9 +238,16 @@ __device__ __forceinline__ void reconstruct_gll32(const T (&sten)[ORD], T (&out)
   }
 }
 
-template <int ORD, int DIR, class Sten>
+// A recorder that keeps nothing (the default of cell_recon32): rec.series32(q, rtot) sees
+// the whole ADER series q[v][kt][ii] (level 0 as perturbations) and the total density of
+// the GLL points before the edge time average, for the tracer transport.
+struct NoRecord32 {
+  template <class Q, class Rt> __device__ __forceinline__ void series32(const Q &, const Rt &) const {}
+};
+
+template <int ORD, int DIR, class Sten, class Rec = NoRecord32>
 __device__ __forceinline__ void cell_recon32(const Sten &sten, int kb, const SweepArgs32 &A, float (&eL)[5],
-                                             float (&eR)[5], float &src_avg) {
+                                             float (&eR)[5], float &src_avg, const Rec &rec = Rec()) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
   constexpr int NA = NG;
@@ -370,6 +377,7 @@ __device__ __forceinline__ void cell_recon32(const Sten &sten, int kb, const Swe
       }
     }
   }
+  rec.series32(q, rtot);
   // compute_timeAvg_edges on perturbations (Spatial:2153-2177)
 #pragma unroll
   for (int v = 0; v < 5; v++) {

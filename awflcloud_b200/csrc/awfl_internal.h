@@ -108,11 +108,19 @@ cudaError_t launch_sweep_tlm(int ord, int dir, const SweepArgs &A, cudaStream_t 
 cudaError_t launch_sweep_rec(int ord, int dir, const SweepArgs &A, cudaStream_t st);
 cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes);
 // Tracer transport of the FP64 path (awfl_tracers.cu): one split of state (fused, MODE_APPLY
-// arithmetic of awfl_split) and tracers; scratch holds tracer_scratch_doubles(...) doubles.
+// arithmetic of awfl_split) and tracers; scratch holds tracer_scratch_bytes(..., 8) bytes.
 cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
                                  unsigned long long pos, double *scratch, cudaStream_t st);
-long tracer_scratch_doubles(int ord, int nx, int ny, int nz, int ntr);
+// scratch of one tracer split: records and fluxes of elem bytes each, and the line flags
+size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem);
 cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes);
+// The same in the FP32 form (awfl_tracers32.cu): the FP32 state split with FP64 tracers;
+// scratch holds tracer_scratch_bytes(..., 4) bytes; dens_c: rho_h rows (FP64).
+cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &A, const double *dens_c, double dt,
+                                   double dxd, double *tracers, int ntr, unsigned long long pos, float *scratch,
+                                   cudaStream_t st);
+cudaError_t upload_tables_tracers32(int ord, const double *recon, const double *c2g, const double *s2g,
+                                    const double *deriv, const double *idl, double sigma, const double *wts);
 // Adjoint reverse sweeps (awfl_adjrev.cu)
 cudaError_t launch_adjoint_split(int ord, int dir, const adj::SplitArgs &A, int need_edges, int nsm, cudaStream_t st);
 cudaError_t launch_zero_halo(double *lam, int nx, int ny, int nz, int hs, int nsm, cudaStream_t st);

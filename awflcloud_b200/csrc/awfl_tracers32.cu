@@ -1,0 +1,337 @@
+// Tracer transport of the FP32 precision form: the reference's tracer code (Spatial:624-955
+// and the y/z equivalents, compiled out there by NO_TRACERS) in FP32 arithmetic beside the
+// FP32 form's state split, as the reference applies tracer tendencies in every precision
+// (Temporal_ader.h:67-69). The tracers stay FP64 arrays (rho*tracer, the layout of the FP64
+// path's), the way the FP32 state keeps a compensation plane beside its FP32 values: the
+// reconstruction, the ADER series, the fluxes and the limiter run in FP32, the division
+// by the density and the update in FP64. Per directional split:
+//
+//   tracer_divide_kernel   tracers /= (rho' + rho_h), in place (awfl_trc.cuh)
+//   sweep_kernel<P32Trc>   the FP32 form's fused state split (the P32 arithmetic) that also
+//                          records, per cell, the total density and normal-momentum ADER
+//                          series, the time-averaged edge perturbations, the pre-split rho'
+//                          and the reciprocal densities of the GLL points
+//   tracer_cell32_kernel   per cell and tracer: reconstruction of tracer/density, the
+//                          rho*tracer ADER series (diffTransformTracer, Spatial:2095-2125)
+//                          and its edge time average (Spatial:760-809, 1123-1170, 1500-1548)
+//   tracer_face32_kernel   per face: edge BCs (Spatial:826-835), the FP32 form's Riemann
+//                          mass flux and the upwind tracer fluxes (Spatial:891-901,
+//                          1249-1259, 1633-1643)
+//   tracer_limit_*_kernel  the positivity limiter with the serial face order's result
+//   tracer_update_kernel   tendency, density multiplied back, apply; halos as the reference
+//                          leaves them (awfl_trc.cuh)
+// Compiled with the FP32 form's flags (multiply-add contraction, fast division).
+#include <cuda_runtime.h>
+
+#include "awfl_fp32.cuh"
+#include "awfl_internal.h"
+
+namespace awfl {
+
+// Recording FP32 policy: the P32 arithmetic plus, per interior cell, the records the
+// tracer kernels read. A.tend points at the record base (floats): R (NG*NG planes of
+// ncell: the total density series), U (NG*NG: normal momentum), E (10: eL, eR
+// perturbations), D (1: the pre-split rho'), Y (NG: 1/rho of the GLL points).
+struct P32Trc : P32 {
+  static constexpr bool kSlab = false;
+  template <int ORD> struct Rec {
+    float *base;
+    long n, cell;
+    int nm;
+    template <class Q, class Rt> __device__ __forceinline__ void series32(const Q &q, const Rt &rtot) const {
+      constexpr int NG = OrdTraits<ORD>::NGLL;
+#pragma unroll
+      for (int kt = 0; kt < NG; kt++)
+#pragma unroll
+        for (int ii = 0; ii < NG; ii++) {
+          base[(kt * NG + ii) * n + cell] = kt == 0 ? rtot[ii] : q[idR][kt][ii];
+          base[(NG * NG + kt * NG + ii) * n + cell] = q[nm][kt][ii];
+        }
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 11 + ii) * n + cell] = frcp(rtot[ii]);
+    }
+  };
+  template <int ORD, int DIR, class S>
+  static __device__ __forceinline__ void recon(const S &sten, int kb, const Args &A, float (&eL)[5], float (&eR)[5],
+                                               float &src, long cell) {
+    if (cell < 0) {  // the periodic prologue's repeat of cell L-1: recorded in its chunk
+      cell_recon32<ORD, DIR>(sten, kb, A, eL, eR, src);
+      return;
+    }
+    constexpr int NG = OrdTraits<ORD>::NGLL;
+    constexpr int HS = (ORD - 1) / 2;
+    const long n = (long)A.nx * A.ny * A.nz;
+    cell_recon32<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell, 1 + DIR});
+    float *e = A.tend + 2L * NG * NG * n;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      e[v * n + cell] = eL[v];
+      e[(5 + v) * n + cell] = eR[v];
+    }
+    e[10 * n + cell] = sten(idR, HS);
+  }
+};
+
+template <int ORD, int DIR> struct PolicyShape<P32Trc, ORD, DIR> : PolicyShape<P32, ORD, DIR> {};
+
+namespace {
+
+struct TracerArgs32 {
+  using Flux = float;
+  SweepArgs32 A;             // the FP32 split's arguments (background, grid, bc, dt)
+  const double *dens_c;      // (nz+2hs): rho_h of the cell rows, FP64
+  double dt, dxd;            // FP64 time step and spacing of the update
+  double *tr;                // (ntr, nz+2hs, ny+2hs, nx+2hs), rho*tracer, FP64
+  int ntr;
+  unsigned long long pos;    // bit l: tracer l is positive definite (limited)
+  const float *R, *U;        // (ngll*ngll, ncell): recorded total density / normal-momentum series
+  const float *D;            // (ncell): recorded pre-split rho'
+  const float *Y;            // (ngll, ncell): recorded 1/rho of the GLL points
+  float *E;                  // (10, ncell): the state's time-averaged edge perturbations eL, eR
+  float *TE;                 // (ntr, 2, ncell): the tracers' edges (left, right)
+  float *TF, *TF2, *UN;      // (ntr, nface) unscaled / limited fluxes, (nface) limiter velocity
+  int *flag;                 // (nlines): the limiter's lines to redo in serial order
+};
+
+// The FP32 form's arithmetic of the shared kernels (awfl_trc.cuh): the division by the
+// density and the update in FP64 on the FP64 tracers, the limiter in FP32.
+__device__ __forceinline__ double trc_divisor(const TracerArgs32 &T, int hs, int k, long g) {
+  return (double)T.A.state[g] + T.dens_c[hs + k];
+}
+__device__ __forceinline__ float trc_dens(const TracerArgs32 &T, int hs, int k) { return T.A.bg.rho_c[hs + k]; }
+__device__ __forceinline__ float limit_face(const TracerArgs32 &T, float F, float f1, float f2, double q, float dens) {
+  const float eps = 1.e-10f;
+  const float fluxOut = T.A.dt * (f2 - f1) * T.A.inv_dxd;
+  const float r = (float)q * dens / (fluxOut + eps);
+  return F * (1.f < r ? 1.f : r);  // F * min(1, r)
+}
+__device__ __forceinline__ double trc_update(const TracerArgs32 &T, double q, int hs, int k, long c, float Fl,
+                                             float Fr) {
+  const double dens = (double)T.D[c] + T.dens_c[hs + k];  // the divisor of tracer_divide_kernel
+  const double tend = (double)((Fl - Fr) * T.A.inv_dxd);
+  return q * dens + T.dt * tend;
+}
+
+}  // namespace
+}  // namespace awfl
+
+#include "awfl_trc.cuh"
+
+namespace awfl {
+namespace {
+
+// One thread per cell and tracer; the blocks of one run of 128 cells are consecutive for
+// the tracers (block b: cells (b / ntr) * 128 .., tracer b % ntr), so the recorded series
+// that they share is read from DRAM once.
+template <int ORD, int DIR>
+__global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  const SweepArgs32 &A = T.A;
+  const Geo<DIR> G(A, HS);
+  const unsigned ncell = (unsigned)G.nz * G.ny * G.nx;
+  const unsigned cb = blockIdx.x / (unsigned)T.ntr;
+  const int l = (int)(blockIdx.x - cb * (unsigned)T.ntr);
+  const unsigned c = cb * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int i, j, k;
+  unflat(c, G.nx, G.ny, k, j, i);
+  const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  const bool posdef = (T.pos >> l) & 1ull;
+  // the stencil of tracer / density; halo positions read the interior cell whose value
+  // the boundary condition copies there
+  const double *tr = T.tr + l * G.sv;
+  float s[ORD];
+#pragma unroll
+  for (int m = 0; m < ORD; m++) {
+    bool wall;
+    const int p = halo_src(p0 - HS + m, n, A.bc, wall);
+    int kk, jj, ii;
+    G.at(k, j, i, p, kk, jj, ii);
+    s[m] = (float)tr[G.g(kk, jj, ii)];
+  }
+  float rt[NG][NG], rut[NG][NG];
+  reconstruct_gll32<ORD>(s, rt[0], A.weno_s != 0);
+  float rser[NG][NG], ruser[NG][NG], ry[NG];
+#pragma unroll
+  for (int kt = 0; kt < NG; kt++)
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      rser[kt][ii] = T.R[(kt * NG + ii) * (long)ncell + c];
+      ruser[kt][ii] = T.U[(kt * NG + ii) * (long)ncell + c];
+    }
+#pragma unroll
+  for (int ii = 0; ii < NG; ii++) ry[ii] = T.Y[ii * (long)ncell + c];
+  const Tables32<ORD> &TB = tab32<ORD>();
+#pragma unroll
+  for (int ii = 0; ii < NG; ii++) {
+    rt[0][ii] *= rser[0][ii];
+    if (posdef) rt[0][ii] = fmaxf(0.f, rt[0][ii]);
+  }
+#pragma unroll
+  for (int ii = 0; ii < NG; ii++) rut[0][ii] = rt[0][ii] * ruser[0][ii] * ry[ii];
+  // diffTransformTracer (Spatial:2095-2125)
+#pragma unroll
+  for (int kt = 0; kt < NG - 1; kt++) {
+    const float sc = -A.inv_dxd * (1.0f / (kt + 1));
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      float df = 0.f;
+#pragma unroll
+      for (int q = 0; q < NG; q++) df = fmaf(TB.deriv[q * NG + ii], rut[kt][q], df);
+      rt[kt + 1][ii] = df * sc;
+    }
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) {
+      float tot = 0.f;
+#pragma unroll
+      for (int ir = 0; ir <= kt + 1; ir++) {
+        tot = fmaf(ruser[ir][ii], rt[kt + 1 - ir][ii], tot);
+        if (ir != 0) tot = fmaf(-rser[ir][ii], rut[kt + 1 - ir][ii], tot);  // rut[kt+1] is not known yet
+      }
+      rut[kt + 1][ii] = tot * ry[ii];
+    }
+  }
+  // compute_timeAvg_edges (Spatial:2153-2177), then the positivity clamp of the edges
+  float tl = rt[0][0], trr = rt[0][NG - 1];
+  float dtmult = A.dt;
+#pragma unroll
+  for (int kt = 1; kt < NG; kt++) {
+    const float cf = dtmult * (1.0f / (kt + 1));
+    tl = fmaf(rt[kt][0], cf, tl);
+    trr = fmaf(rt[kt][NG - 1], cf, trr);
+    dtmult *= A.dt;
+  }
+  if (posdef) {
+    tl = fmaxf(0.f, tl);
+    trr = fmaxf(0.f, trr);
+  }
+  T.TE[(2L * l) * ncell + c] = tl;
+  T.TE[(2L * l + 1) * ncell + c] = trr;
+}
+
+// The left (side 0) and right (side 1) values at face f along a line, with the edge BCs:
+// periodic faces 0 and n both see (right edge of cell n-1, left edge of cell 0); at a wall
+// the outside value copies the inside one (Spatial:816-837). The mass flux is the FP32
+// form's Riemann flux of the state (riemann32), the one the state's own split uses.
+template <int DIR, int NG>
+__global__ void __launch_bounds__(128) tracer_face32_kernel(TracerArgs32 T, int hs) {
+  const SweepArgs32 &A = T.A;
+  const Geo<DIR> G(A, hs);
+  const long nf = G.nface();
+  const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  if (f < G.nlines()) T.flag[f] = 0;  // the limiter's per-line flags (nf > nlines)
+  const int fx = G.nx + (DIR == 0), fy = G.ny + (DIR == 1);
+  int i, j, k;
+  unflat((unsigned)f, fx, fy, k, j, i);
+  const int pf = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  const long ncell = (long)G.nz * G.ny * G.nx;
+  int pl = pf - 1, pr = pf;  // cells whose right / left edges meet at the face
+  bool lside_from_right = false, rside_from_left = false;  // wall copies
+  if (pf == 0) {
+    if (A.bc == BC_PERIODIC) pl = n - 1;
+    else { pl = 0; lside_from_right = true; }
+  }
+  if (pf == n) {
+    if (A.bc == BC_PERIODIC) pr = 0;
+    else { pr = n - 1; rside_from_left = true; }
+  }
+  int kl, jl, il, kr, jr, ir;
+  G.at(k, j, i, pl, kl, jl, il);
+  G.at(k, j, i, pr, kr, jr, ir);
+  const long cl = G.cell(kl, jl, il), cr = G.cell(kr, jr, ir);
+  float qL[5], qR[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    qL[v] = lside_from_right ? T.E[v * ncell + cl] : T.E[(5 + v) * ncell + cl];
+    qR[v] = rside_from_left ? T.E[(5 + v) * ncell + cr] : T.E[v * ncell + cr];
+  }
+  float F[5];
+  riemann32<DIR, NG>(qL, qR, k, A, F);  // k: the face's k (z) or the line's k
+  // the sides' total densities: the background of the face's two sides (riemann32's)
+  float bL, bR;
+  if (DIR == 2) {
+    bL = A.bg.rho_f[(k == 0 && A.bc == BC_PERIODIC) ? A.nz : k];
+    bR = A.bg.rho_f[(k == A.nz && A.bc == BC_PERIODIC) ? 0 : k];
+  } else {
+    bL = bR = A.bg.rho_c[hs + k];
+  }
+  const float rL = bL + qL[0], rR = bR + qR[0];
+  constexpr int NM = 1 + DIR;
+  const float vn = DIR == 1 ? 0.5f * (qL[NM] + qR[NM]) : 0.5f * (qL[NM] / rL + qR[NM] / rR);
+  T.UN[f] = 0.5f * (qL[NM] + qR[NM]);
+  for (int l = 0; l < T.ntr; l++) {
+    const float tL = lside_from_right ? T.TE[(2L * l) * ncell + cl] : T.TE[(2L * l + 1) * ncell + cl];
+    const float tR = rside_from_left ? T.TE[(2L * l + 1) * ncell + cr] : T.TE[(2L * l) * ncell + cr];
+    T.TF[l * nf + f] = vn > 0 ? F[0] * tL / rL : F[0] * tR / rR;
+  }
+}
+
+template <int ORD, int DIR>
+cudaError_t run32(const TracerArgs32 &T, cudaStream_t st) {
+  constexpr int HS = (ORD - 1) / 2;
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  const SweepArgs32 &A = T.A;
+  const long ncell = (long)A.nz * A.ny * A.nx;
+  const long nf = (long)(A.nz + (DIR == 2)) * (A.ny + (DIR == 1)) * (A.nx + (DIR == 0));
+  const unsigned gc = (unsigned)((ncell + 127) / 128), gf = (unsigned)((nf + 127) / 128);
+  tracer_divide_kernel<TracerArgs32><<<gc, 128, 0, st>>>(T, HS);
+  cudaError_t e = launch_sweep_t<P32Trc, ORD, DIR>(A, st);  // state split + records
+  if (e != cudaSuccess) return e;
+  tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
+  tracer_face32_kernel<DIR, NG><<<gf, 128, 0, st>>>(T, HS);
+  const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
+  tracer_limit_faces_kernel<TracerArgs32, DIR><<<gf, 128, 0, st>>>(T, HS);
+  tracer_limit_lines_kernel<TracerArgs32, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
+  tracer_update_kernel<TracerArgs32, DIR><<<gc, 128, 0, st>>>(T, HS);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &Ain, const double *dens_c, double dt,
+                                   double dxd, double *tracers, int ntr, unsigned long long pos, float *scratch,
+                                   cudaStream_t st) {
+  const int ng = ord == 5 ? 3 : 5;
+  const long ncell = (long)Ain.nz * Ain.ny * Ain.nx;
+  const long nfmax = (long)(Ain.nz + 1) * (Ain.ny + 1) * (Ain.nx + 1);
+  if (nfmax >= (1L << 31)) return cudaErrorInvalidValue;  // 32-bit cell and face indices
+  TracerArgs32 T;
+  T.A = Ain;
+  T.A.tend = scratch;  // the recording sweep's record base
+  T.A.mode = MODE_APPLY;
+  T.dens_c = dens_c;
+  T.dt = dt;
+  T.dxd = dxd;
+  T.tr = tracers;
+  T.ntr = ntr;
+  T.pos = pos;
+  T.R = scratch;
+  T.U = scratch + (long)ng * ng * ncell;
+  T.E = scratch + 2L * ng * ng * ncell;
+  T.D = T.E + 10 * ncell;
+  T.Y = T.E + 11 * ncell;
+  T.TE = T.E + (11L + ng) * ncell;
+  T.TF = T.TE + 2L * ntr * ncell;
+  T.TF2 = T.TF + (long)ntr * nfmax;
+  T.UN = T.TF2 + (long)ntr * nfmax;
+  T.flag = reinterpret_cast<int *>(T.UN + nfmax);
+  if (ord == 5) {
+    if (dir == 0) return run32<5, 0>(T, st);
+    if (dir == 1) return run32<5, 1>(T, st);
+    return run32<5, 2>(T, st);
+  }
+  if (dir == 0) return run32<9, 0>(T, st);
+  if (dir == 1) return run32<9, 1>(T, st);
+  return run32<9, 2>(T, st);
+}
+
+cudaError_t upload_tables_tracers32(int ord, const double *recon, const double *c2g, const double *s2g,
+                                    const double *deriv, const double *idl, double sigma, const double *wts) {
+  return upload_tables32_here(ord, recon, c2g, s2g, deriv, idl, sigma, wts);
+}
+
+}  // namespace awfl

@@ -439,17 +439,12 @@ def ord9_leg(a, local):
 
 
 def tracers_leg(a, local, ntr=3, steps=5, warmup=2):
-    """Tracer transport (the reference's compiled-out tracer code, built in): the FP64 path on
-    the main grid with the driver's three positive-definite tracers, awfl_step_tracers vs
-    awfl_step, CUDA events on the launching stream."""
+    """Tracer transport (the reference's compiled-out tracer code, built in) on the main grid
+    with the driver's three positive-definite tracers, awfl_step_tracers vs awfl_step, CUDA
+    events on the launching stream: the FP64 path, and the FP32 form (FP32 reconstruction,
+    fluxes and limiter, FP64 tracer arrays)."""
     import torch
     from awflcloud_b200 import capi
-    c = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=capi.FP64, device=local)
-    st = c.new_state()
-    c.init_state(st, kind=capi.INIT_BUBBLE, noise_amp=0.01)
-    tr = c.new_tracers(ntr)
-    c.init_tracers(tr)
-    dt = c.cfl(st, cfl_for(a.ord))
     stream = torch.cuda.current_stream()
 
     def timed(fn):
@@ -464,17 +459,32 @@ def tracers_leg(a, local, ntr=3, steps=5, warmup=2):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
-    ms_tr = timed(lambda: c.step_tracers(st, tr, dt))
-    ms_plain = timed(lambda: c.step(st, dt))
+    def form(prec):
+        c = capi.Context(a.nx, a.ny, a.nz, ord_=a.ord, precision=prec, device=local)
+        st = c.new_state()
+        c.init_state(st, kind=capi.INIT_BUBBLE, noise_amp=0.01)
+        tr = c.new_tracers(ntr)
+        c.init_tracers(tr)
+        dt = c.cfl(st, cfl_for(a.ord))
+        ms_tr = timed(lambda: c.step_tracers(st, tr, dt))
+        ms_plain = timed(lambda: c.step(st, dt))
+        finite = bool(torch.isfinite(tr).all().item())
+        del c, st, tr
+        return ms_tr, ms_plain, finite
+
+    ms_tr, ms_plain, finite = form(capi.FP64)
+    ms_tr32, ms_plain32, finite32 = form(capi.FP32)
     cells = a.nx * a.ny * a.nz
     return {"workload": "%s, FP64, %d positive-definite tracers (uniform, theta, block)" % (workload_name(a), ntr),
             "steps": steps, "warmup": warmup, "ms_per_step_with_tracers": round(ms_tr, 4),
             "ms_per_step_without": round(ms_plain, 4), "tracer_ms_per_step": round(ms_tr - ms_plain, 4),
-            "value": round(cells / (ms_tr * 1e-3) / 1e6, 3), "unit": "Mcell-steps/s",
-            "finite": bool(torch.isfinite(tr).all().item()),
-            "note": "per split: the state's fused sweep recording the density / normal-momentum ADER "
-                    "series, edges and pre-split density, then four tracer launches (cell, face, "
-                    "limiter, update)"}
+            "value": round(cells / (ms_tr * 1e-3) / 1e6, 3), "unit": "Mcell-steps/s", "finite": finite,
+            "fp32": {"ms_per_step_with_tracers": round(ms_tr32, 4), "ms_per_step_without": round(ms_plain32, 4),
+                     "tracer_ms_per_step": round(ms_tr32 - ms_plain32, 4),
+                     "value": round(cells / (ms_tr32 * 1e-3) / 1e6, 3), "finite": finite32},
+            "note": "per split: tracers divided by the density, the state's fused sweep recording the density / "
+                    "normal-momentum ADER series, edges, pre-split density and reciprocal densities, then the "
+                    "tracer launches (cell, face, limiter faces, limiter lines, update)"}
 
 
 def adjoint_leg(a, local):

@@ -154,16 +154,19 @@ int awfl_write_netcdf_fields_tracers(awfl_ctx *ctx, const char *path, const doub
                                      const char *const *names, double etime);
 
 /* Tracer transport: the reference's tracer code (Spatial:624-955 and the y/z equivalents),
- * which the reference itself compiles out (NO_TRACERS, Spatial:10), built in. FP64
- * contexts only. One split (dir = 0/1/2) of state AND tracers: the state exactly as
- * awfl_split advances it, and the tracers -- divided by the pre-split density,
+ * which the reference itself compiles out (NO_TRACERS, Spatial:10), built in, for both
+ * precisions: an FP32 context reconstructs, fluxes and limits the tracers in FP32 beside
+ * its FP32 state split and keeps the tracers FP64 (division by the density and the update
+ * in FP64). One split (dir = 0/1/2) of state AND tracers: the state as awfl_split
+ * advances it (FP64: bit for bit), and the tracers -- divided by the pre-split density,
  * reconstructed, advanced by their ADER series along the state's density and normal
  * momentum, upwind fluxes from the state's Riemann mass flux, the positivity limiter for
  * tracers with pos[l] != 0, then tracers = (tracers/rho)*rho + dt*tend in place.
  * ntracers <= 64 (0: awfl_split); tracers as for awfl_init_tracers (rho*tracer). The halo
  * cells along dir are left holding tracer/rho, as the reference's in-place halo fill leaves
  * them. Allocates (once per context, grown when ntracers grows) a scratch buffer of
- * (2*ngll^2 + 11 + 2*ntracers) doubles per cell and (2*ntracers + 1) per face. Decisions
+ * (2*ngll^2 + ngll + 11 + 2*ntracers) values per cell and (2*ntracers + 1) per face
+ * (doubles; floats in an FP32 context) and one int per line. Decisions
  * where the reference's code is not well defined: the limiter scales the faces of a line
  * in place in increasing order, as the reference's loop does when it runs serially (it
  * scales in place while other iterations read, Spatial:904-935); the y limiter's v < 0

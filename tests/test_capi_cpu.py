@@ -94,6 +94,8 @@ def test_split_tracers_argument_checks_before_any_device_call():
     assert L.awfl_split_tracers(c.h, 8, 8, 65, pos, 0.1, 0, None) == -1
     assert L.awfl_split_tracers(c.h, 8, 8, 2, None, 0.1, 0, None) == -1
     assert L.awfl_split_tracers(c.h, 8, 8, 2, pos, 0.1, 3, None) == -1
+    # an FP32 context takes tracers too: its arguments pass, and the host-only context then
+    # refuses the device work
     c32 = capi.Context(10, 8, 6, precision=capi.FP32, device=-1)
     assert L.awfl_split_tracers(c32.h, 8, 8, 2, pos, 0.1, 0, None) == -1
-    assert b"FP64" in L.awfl_last_error(c32.h)
+    assert b"host-only" in L.awfl_last_error(c32.h)

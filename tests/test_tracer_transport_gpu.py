@@ -115,16 +115,16 @@ def test_limiter_serial_chains(d, bc):
     assert np.array_equal(dst.cpu().numpy(), st)
 
 
-def test_split_tracers_rejects_fp32_and_bad_args():
-    c = capi.Context(16, 12, 10, precision=capi.FP32)
-    st = c.new_state()
-    tr = c.new_tracers(2)
-    with pytest.raises(capi.AwflError):
-        c.step_tracers(st, tr, 0.5)
+def test_split_tracers_rejects_bad_args():
     c64 = capi.Context(16, 12, 10)
     st64 = c64.new_state()
+    tr = c64.new_tracers(2)
     with pytest.raises(ValueError):
         c64.step_tracers(st64, tr, 0.5, pos=[1])
+    with pytest.raises(ValueError):
+        c64.step_tracers(st64, tr.float(), 0.5)  # tracers are FP64 arrays in every precision
+    with pytest.raises(capi.AwflError):
+        c64.split_tracers(st64, tr, 0.5, 3)
 
 
 def test_split_tracers_equal_reference_tracer_code(golden_dir):
