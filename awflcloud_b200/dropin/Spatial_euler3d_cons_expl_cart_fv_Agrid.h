@@ -20,8 +20,8 @@
 //    awfl_write_netcdf_tracers; tracers are FP64 for either precision, halos zero). Their
 //    tendencies are zero, so they stay constant (the reference adds an uninitialised
 //    tendency array to them, Temporal_ader.h:67-69) -- unless the extra YAML key
-//    tracer_transport is true (FP64 only): the reference's compiled-out tracer code then
-//    runs (awfl_split_tracers per split; addTracer's posDef flags select the limited
+//    tracer_transport is true (either precision): the reference's compiled-out tracer code
+//    then runs (awfl_split_tracers per split; addTracer's posDef flags select the limited
 //    tracers).
 //  * Optional extra YAML keys (absent = reference behaviour): tracer_transport (bool),
 //    precision (fp64 | fp32),
