@@ -111,6 +111,12 @@ cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes);
 // arithmetic of awfl_split) and tracers; scratch holds tracer_scratch_bytes(..., 8) bytes.
 cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
                                  unsigned long long pos, double *scratch, cudaStream_t st);
+// Record layout of a tracer split (both precisions; planes of ncell cells, then of nfmax
+// faces): R (NG*NG: the density series), U (NG*NG: the normal-momentum series), D (1: the
+// pre-split rho', the stencil centre), Y (NG: 1/rho of the GLL points), then per face F0
+// (the Riemann mass flux), VN (the velocity that picks the upwind side), UN (the
+// limiter's velocity), RUP (the upwind side's density), YUP (1/RUP).
+template <int NG> __host__ __device__ constexpr long trc_cell_planes() { return 2L * NG * NG + 1 + NG; }
 // scratch of one tracer split: records and fluxes of elem bytes each, and the line flags
 size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem);
 cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes);

@@ -52,6 +52,8 @@
 //   store_tend(A, tidx, x)                 tendency output (MODE_TEND)
 #pragma once
 
+#include <type_traits>
+
 #include "awfl_internal.h"
 
 namespace awfl {
@@ -132,6 +134,13 @@ template <int ORD, int C, int W, int ESZ> __host__ __device__ constexpr int tma_
   return tma_ring_pitch_of(ORD, C, W, ESZ);
 }
 
+// A policy with `static constexpr bool kFaceRec = true` sees every face the sweep computes:
+// P::face_rec<ORD, DIR>(A, face, kf, qL, qR, F) with the face's index in the tracer path's
+// face numbering (faces along DIR: n+1 per line), the k passed to the flux, the face's two
+// states after the edge BCs and its flux (the tracer transport records them).
+template <class P, class = void> struct PolicyFaceRec : std::false_type {};
+template <class P> struct PolicyFaceRec<P, std::void_t<decltype(P::kFaceRec)>> : std::bool_constant<P::kFaceRec> {};
+
 // One CTA's tile: lines bx*W .. bx*W+W-1 of plane `by` (x, y sweeps: by = k; z: by = j).
 // tmap: the tensor map of the TMA path (a kernel-parameter or global address), or nullptr
 // (the instantiation with TMA = true then stages every chunk by cp.async).
@@ -206,21 +215,25 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
   long sd;  // stride along DIR
   long tb;  // tendency offset of position 0
   long tsd;
+  long fb, fsd;  // face index of position 0 and its stride along DIR (face records only)
   if (DIR == 0) {
     const int k = by, j = bx * W + w;
     L = nx; valid = j < ny; kline = k;
     lb = (HS + k) * sz + (HS + (valid ? j : 0)) * sy + HS * sx; sd = sx;
     tb = ((long)k * ny + (valid ? j : 0)) * nx; tsd = 1;
+    fb = ((long)k * ny + (valid ? j : 0)) * (nx + 1); fsd = 1;
   } else if (DIR == 1) {
     const int k = by, i = bx * W + w;
     L = ny; valid = i < nx; kline = k;
     lb = (HS + k) * sz + HS * sy + HS + (valid ? i : 0); sd = sy;
     tb = (long)k * ny * nx + (valid ? i : 0); tsd = nx;
+    fb = (long)k * (ny + 1) * nx + (valid ? i : 0); fsd = nx;
   } else {
     const int j = by, i = bx * W + w;
     L = nz; valid = i < nx;
     lb = HS * sz + (HS + j) * sy + HS + (valid ? i : 0); sd = sz;
     tb = (long)j * nx + (valid ? i : 0); tsd = (long)ny * nx;
+    fb = (long)j * nx + (valid ? i : 0); fsd = (long)ny * nx;
   }
   const long tv = (long)nz * ny * nx;
   const bool periodic = A.bc == BC_PERIODIC;
@@ -435,6 +448,8 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
           for (int v = 0; v < 5; v++) qL[v] = eL[v];
         }
         P::template flux<DIR, NG>(qL, eL, DIR == 2 ? base + c : kline, A, F);
+        if constexpr (PolicyFaceRec<P>::value)
+          P::template face_rec<ORD, DIR>(A, fb + (base + c) * fsd, DIR == 2 ? base + c : kline, qL, eL, F);
       } else {
 #pragma unroll
         for (int v = 0; v < 5; v++) F[v] = Real(0);
@@ -479,6 +494,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 #pragma unroll
       for (int v = 0; v < 5; v++) qL[v] = (f == 0 && !periodic && !xlo) ? qR[v] : sER[v][E(c)];
       P::template flux<DIR, NG>(qL, qR, DIR == 2 ? f : kline, A, F);
+      if constexpr (PolicyFaceRec<P>::value) P::template face_rec<ORD, DIR>(A, fb + f * fsd, DIR == 2 ? f : kline, qL, qR, F);
 #pragma unroll
       for (int v = 0; v < 5; v++) sF[v][E(c + 1)] = F[v];
     }
@@ -530,6 +546,7 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
       for (int v = 0; v < 5; v++) qR[v] = hL[v];
     }
     P::template flux<DIR, NG>(qL, qR, DIR == 2 ? L : kline, A, F);
+    if constexpr (PolicyFaceRec<P>::value) P::template face_rec<ORD, DIR>(A, fb + L * fsd, DIR == 2 ? L : kline, qL, qR, F);
     typename P::Aux aux;
     if (A.mode == MODE_APPLY) P::load_aux(A, lb + (L - 1) * sd, sv, aux);
     finish(L - 1, Fl, F, DIR == 2 ? sSrc[E(0)] : Real(0), aux);

@@ -4,15 +4,15 @@
 //   tracer_divide_kernel  tracers /= density, in place (Spatial:624-627)
 //   sweep_kernel<P64Trc>  the state's fused split (the P64 arithmetic, so the state is
 //                         bit-identical to awfl_split's) that also records, per cell, the
-//                         density and normal-momentum ADER series, the time-averaged edge
-//                         states and the pre-split density perturbation
+//                         density and normal-momentum ADER series, the pre-split density
+//                         perturbation and, per face, the Riemann mass flux, the upwind
+//                         velocity and density and the limiter's velocity
 //   tracer_cell_kernel    per cell and tracer: the reconstruction of tracer/density, the
 //                         rho*tracer ADER series (diffTransformTracer, Spatial:2095-2125)
-//                         along the recorded series and its edge time average
-//                         (Spatial:760-809, 1123-1170, 1500-1548)
-//   tracer_face_kernel    per face: edge BCs (Spatial:826-835), the state's Riemann flux
-//                         (riemann) and the upwind tracer fluxes (Spatial:891-901,
-//                         1249-1259, 1633-1643)
+//                         along the recorded series, its edge time average
+//                         (Spatial:760-809, 1123-1170, 1500-1548) and the upwind tracer
+//                         fluxes of the faces the cell is upwind of (Spatial:891-901, with
+//                         the edge BCs of Spatial:816-837) from the recorded face values
 //   tracer_limit_faces_kernel / tracer_limit_lines_kernel
 //                         the positivity limiter (Spatial:904-935, 1262-1293, 1646-1677)
 //                         with the result of the reference's serial face order: per face,
@@ -36,12 +36,12 @@
 
 namespace awfl {
 
-// Recording FP64 policy: the P64 arithmetic plus, per interior cell, the records the
-// tracer kernels read. A.tend points at the record base: R (NG*NG planes of ncell), U
-// (NG*NG), E (10: eL, eR), D (1: the pre-split rho', the stencil centre), Y (NG: RN(1/rho)
-// of the GLL points).
+// Recording FP64 policy: the P64 arithmetic plus the records above, written by the sweep
+// itself (A.tend points at the record base): the cell records from cell_recon's series,
+// the face records from every face flux it computes.
 struct P64Trc : P64 {
   static constexpr bool kSlab = false;
+  static constexpr bool kFaceRec = true;
   // the record stores need registers: 3 CTAs per SM at ord 5 instead of the plain sweep's 4
   static constexpr int min_blocks(int ord) { return ord == 5 ? 3 : 1; }
   template <int ORD> struct Rec {
@@ -60,7 +60,7 @@ struct P64Trc : P64 {
         }
       // RN(1 / density) of the GLL points (the sweep's own reciprocals, rr in cell_recon)
 #pragma unroll
-      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 11 + ii) * n + cell] = 1.0 / q[idR][0][ii];
+      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 1 + ii) * n + cell] = 1.0 / q[idR][0][ii];
     }
   };
   template <int ORD, int DIR, class S>
@@ -74,13 +74,24 @@ struct P64Trc : P64 {
     constexpr int HS = (ORD - 1) / 2;
     const long n = (long)A.nx * A.ny * A.nz;
     cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell, 1 + DIR});
-    double *e = A.tend + 2L * NG * NG * n;
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      e[v * n + cell] = eL[v];
-      e[(5 + v) * n + cell] = eR[v];
-    }
-    e[10 * n + cell] = sten(idR, HS);
+    A.tend[2L * NG * NG * n + cell] = sten(idR, HS);
+  }
+  // the face records: the tracer face flux's inputs (Spatial:891-901), from the states the
+  // sweep's own Riemann flux saw
+  template <int ORD, int DIR>
+  static __device__ __forceinline__ void face_rec(const Args &A, long face, int, const double (&qL)[5],
+                                                  const double (&qR)[5], const double (&F)[5]) {
+    constexpr int NG = OrdTraits<ORD>::NGLL;
+    constexpr int NM = 1 + DIR;
+    const long n = (long)A.nx * A.ny * A.nz, nfm = (long)(A.nx + 1) * (A.ny + 1) * (A.nz + 1);
+    double *fr = A.tend + trc_cell_planes<NG>() * n + face;
+    const double vn = DIR == 1 ? 0.5 * (qL[NM] + qR[NM]) : 0.5 * (qL[NM] / qL[0] + qR[NM] / qR[0]);
+    fr[0] = F[0];
+    fr[nfm] = vn;
+    fr[2 * nfm] = 0.5 * (qL[NM] + qR[NM]);
+    const double rup = vn > 0 ? qL[0] : qR[0];
+    fr[3 * nfm] = rup;
+    fr[4 * nfm] = 1.0 / rup;  // RN(1/rup): the tracer fluxes' shared divisor
   }
 };
 
@@ -97,9 +108,8 @@ struct TracerArgs {
   const double *R, *U;       // (ngll*ngll, ncell): recorded density / normal-momentum series
   const double *D;           // (ncell): recorded pre-split rho'
   const double *Y;           // (ngll, ncell): recorded RN(1 / rho) of the GLL points
-  double *E;                 // (10, ncell): the state's time-averaged edges eL[5], eR[5]
-  double *TE;                // (ntr, 2, ncell): the tracers' edges (left, right)
-  double *TF, *TF2, *UN;     // (ntr, nface) unscaled / limited fluxes, (nface) limiter velocity
+  const double *F0, *VN, *UN, *RUP, *YUP;  // (nface) each: the recorded face values
+  double *TF, *TF2;          // (ntr, nface): unscaled / limited tracer fluxes
   int *flag;                 // (nlines): the limiter's lines to redo in serial order
 };
 
@@ -109,6 +119,10 @@ __device__ __forceinline__ double trc_divisor(const TracerArgs &T, int hs, int k
   return T.A.state[g] + T.A.dens_c[hs + k];
 }
 __device__ __forceinline__ double trc_dens(const TracerArgs &T, int hs, int k) { return T.A.dens_c[hs + k]; }
+// a / (the upwind density of face fi), correctly rounded through its recorded reciprocal
+__device__ __forceinline__ double trc_div_up(const TracerArgs &T, double a, long fi) {
+  return divr_any(a, rcp_known(T.RUP[fi], T.YUP[fi]));
+}
 // factor and scaled flux of one face from its upwind cell's two faces (f1 = min(., 0) of
 // the left one, f2 = max(., 0) of the right one; q: the cell's tracer / density)
 __device__ __forceinline__ double limit_face(const TracerArgs &T, double F, double f1, double f2, double q,
@@ -152,6 +166,7 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
   const int l = (int)(blockIdx.x - cb * (unsigned)T.ntr);
   const unsigned c = cb * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
+  if (l == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
   int i, j, k;
   unflat(c, G.nx, G.ny, k, j, i);
   const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
@@ -228,58 +243,9 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
     tl = dmax(0., tl);
     trr = dmax(0., trr);
   }
-  T.TE[(2L * l) * ncell + c] = tl;
-  T.TE[(2L * l + 1) * ncell + c] = trr;
-}
-
-// The left (side 0) and right (side 1) values at face f along a line, with the edge BCs:
-// periodic faces 0 and n both see (right edge of cell n-1, left edge of cell 0); at a wall
-// the outside value copies the inside one (Spatial:816-837).
-template <int DIR, int NG>
-__global__ void __launch_bounds__(128) tracer_face_kernel(TracerArgs T, int hs) {
-  const SweepArgs &A = T.A;
-  const Geo<DIR> G(A, hs);
-  const long nf = G.nface();
-  const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (f >= nf) return;
-  const long nlines = DIR == 0 ? (long)G.nz * G.ny : (DIR == 1 ? (long)G.nz * G.nx : (long)G.ny * G.nx);
-  if (f < nlines) T.flag[f] = 0;  // the limiter's per-line flags (nf > nlines)
-  const int fx = G.nx + (DIR == 0), fy = G.ny + (DIR == 1);
-  int i, j, k;
-  unflat((unsigned)f, fx, fy, k, j, i);
-  const int pf = DIR == 0 ? i : (DIR == 1 ? j : k);
-  const int n = G.n();
-  const long ncell = (long)G.nz * G.ny * G.nx;
-  int pl = pf - 1, pr = pf;  // cells whose right / left edges meet at the face
-  bool lside_from_right = false, rside_from_left = false;  // wall copies
-  if (pf == 0) {
-    if (A.bc == BC_PERIODIC) pl = n - 1;
-    else { pl = 0; lside_from_right = true; }
-  }
-  if (pf == n) {
-    if (A.bc == BC_PERIODIC) pr = 0;
-    else { pr = n - 1; rside_from_left = true; }
-  }
-  int kl, jl, il, kr, jr, ir;
-  G.at(k, j, i, pl, kl, jl, il);
-  G.at(k, j, i, pr, kr, jr, ir);
-  const long cl = G.cell(kl, jl, il), cr = G.cell(kr, jr, ir);
-  double qL[5], qR[5];
-#pragma unroll
-  for (int v = 0; v < 5; v++) {
-    qL[v] = lside_from_right ? T.E[v * ncell + cl] : T.E[(5 + v) * ncell + cl];
-    qR[v] = rside_from_left ? T.E[(5 + v) * ncell + cr] : T.E[v * ncell + cr];
-  }
-  double F[5];
-  riemann<DIR, NG>(qL, qR, k, A, F);  // k: the face's k (z) or the line's k
-  constexpr int NM = 1 + DIR;
-  const double vn = DIR == 1 ? 0.5 * (qL[NM] + qR[NM]) : 0.5 * (qL[NM] / qL[0] + qR[NM] / qR[0]);
-  T.UN[f] = 0.5 * (qL[NM] + qR[NM]);
-  for (int l = 0; l < T.ntr; l++) {
-    const double tL = lside_from_right ? T.TE[(2L * l) * ncell + cl] : T.TE[(2L * l + 1) * ncell + cl];
-    const double tR = rside_from_left ? T.TE[(2L * l + 1) * ncell + cr] : T.TE[(2L * l) * ncell + cr];
-    T.TF[l * nf + f] = vn > 0 ? F[0] * tL / qL[0] : F[0] * tR / qR[0];
-  }
+  // the fluxes of the faces this cell is upwind of
+  const long fs = DIR == 0 ? 1 : (DIR == 1 ? G.nx : (long)G.nx * G.ny), fl = G.face(k, j, i);
+  write_upwind_fluxes<double>(T, T.TF + (long)l * G.nface(), p0, n, A.bc == BC_PERIODIC, fl, fs, fl - p0 * fs, tl, trr);
 }
 
 template <int ORD, int DIR>
@@ -294,7 +260,6 @@ cudaError_t run(const TracerArgs &T, cudaStream_t st) {
   cudaError_t e = launch_sweep_t<P64Trc, ORD, DIR>(A, st);  // state split + records
   if (e != cudaSuccess) return e;
   tracer_cell_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
-  tracer_face_kernel<DIR, NG><<<gf, 128, 0, st>>>(T, HS);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs, DIR><<<gf, 128, 0, st>>>(T, HS);
   tracer_limit_lines_kernel<TracerArgs, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
@@ -317,16 +282,19 @@ cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &Ain, double 
   T.tr = tracers;
   T.ntr = ntr;
   T.pos = pos;
+  const long ncp = 2L * ng * ng + 1 + ng;  // trc_cell_planes
   T.R = scratch;
   T.U = scratch + (long)ng * ng * ncell;
-  T.E = scratch + 2L * ng * ng * ncell;
-  T.D = T.E + 10 * ncell;
-  T.Y = T.E + 11 * ncell;
-  T.TE = T.E + (11L + ng) * ncell;
-  T.TF = T.TE + 2L * ntr * ncell;
+  T.D = scratch + 2L * ng * ng * ncell;
+  T.Y = T.D + ncell;
+  T.F0 = scratch + ncp * ncell;
+  T.VN = T.F0 + nfmax;
+  T.UN = T.VN + nfmax;
+  T.RUP = T.UN + nfmax;
+  T.YUP = T.RUP + nfmax;
+  T.TF = scratch + ncp * ncell + 5 * nfmax;
   T.TF2 = T.TF + (long)ntr * nfmax;
-  T.UN = T.TF2 + (long)ntr * nfmax;
-  T.flag = reinterpret_cast<int *>(T.UN + nfmax);
+  T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);
   if (ord == 5) {
     if (dir == 0) return run<5, 0>(T, st);
     if (dir == 1) return run<5, 1>(T, st);
@@ -344,7 +312,7 @@ size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem) 
   long lines = (long)nz * ny;  // the most lines of one direction: the limiter's int flags
   if ((long)nz * nx > lines) lines = (long)nz * nx;
   if ((long)ny * nx > lines) lines = (long)ny * nx;
-  const long elems = (2L * ng * ng + 11 + ng) * ncell + 2L * ntr * ncell + 2L * ntr * nfmax + nfmax;
+  const long elems = (2L * ng * ng + 1 + ng) * ncell + 5 * nfmax + 2L * ntr * nfmax;
   return (size_t)elem * (size_t)elems + sizeof(int) * (size_t)lines;
 }
 

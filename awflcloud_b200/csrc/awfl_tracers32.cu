@@ -9,14 +9,14 @@
 //   tracer_divide_kernel   tracers /= (rho' + rho_h), in place (awfl_trc.cuh)
 //   sweep_kernel<P32Trc>   the FP32 form's fused state split (the P32 arithmetic) that also
 //                          records, per cell, the total density and normal-momentum ADER
-//                          series, the time-averaged edge perturbations, the pre-split rho'
-//                          and the reciprocal densities of the GLL points
+//                          series, the pre-split rho' and the reciprocal densities of the
+//                          GLL points, and per face the FP32 form's Riemann mass flux, the
+//                          upwind velocity and density and the limiter's velocity
 //   tracer_cell32_kernel   per cell and tracer: reconstruction of tracer/density, the
-//                          rho*tracer ADER series (diffTransformTracer, Spatial:2095-2125)
-//                          and its edge time average (Spatial:760-809, 1123-1170, 1500-1548)
-//   tracer_face32_kernel   per face: edge BCs (Spatial:826-835), the FP32 form's Riemann
-//                          mass flux and the upwind tracer fluxes (Spatial:891-901,
-//                          1249-1259, 1633-1643)
+//                          rho*tracer ADER series (diffTransformTracer, Spatial:2095-2125),
+//                          its edge time average (Spatial:760-809, 1123-1170, 1500-1548) and
+//                          the upwind tracer fluxes of the faces the cell is upwind of
+//                          (Spatial:891-901, 1249-1259, 1633-1643)
 //   tracer_limit_*_kernel  the positivity limiter with the serial face order's result
 //   tracer_update_kernel   tendency, density multiplied back, apply; halos as the reference
 //                          leaves them (awfl_trc.cuh)
@@ -28,12 +28,12 @@
 
 namespace awfl {
 
-// Recording FP32 policy: the P32 arithmetic plus, per interior cell, the records the
-// tracer kernels read. A.tend points at the record base (floats): R (NG*NG planes of
-// ncell: the total density series), U (NG*NG: normal momentum), E (10: eL, eR
-// perturbations), D (1: the pre-split rho'), Y (NG: 1/rho of the GLL points).
+// Recording FP32 policy: the P32 arithmetic plus the tracer split's records (floats; the
+// layout of trc_cell_planes: R is the total density series, U the normal momentum), A.tend
+// pointing at the record base.
 struct P32Trc : P32 {
   static constexpr bool kSlab = false;
+  static constexpr bool kFaceRec = true;
   template <int ORD> struct Rec {
     float *base;
     long n, cell;
@@ -48,7 +48,7 @@ struct P32Trc : P32 {
           base[(NG * NG + kt * NG + ii) * n + cell] = q[nm][kt][ii];
         }
 #pragma unroll
-      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 11 + ii) * n + cell] = frcp(rtot[ii]);
+      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 1 + ii) * n + cell] = frcp(rtot[ii]);
     }
   };
   template <int ORD, int DIR, class S>
@@ -62,13 +62,34 @@ struct P32Trc : P32 {
     constexpr int HS = (ORD - 1) / 2;
     const long n = (long)A.nx * A.ny * A.nz;
     cell_recon32<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell, 1 + DIR});
-    float *e = A.tend + 2L * NG * NG * n;
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      e[v * n + cell] = eL[v];
-      e[(5 + v) * n + cell] = eR[v];
+    A.tend[2L * NG * NG * n + cell] = sten(idR, HS);
+  }
+  // the face records, from the perturbation states the sweep's own Riemann flux saw: the
+  // sides' total densities with the background riemann32 gives them (z: the face's own
+  // rows, a periodic face 0 taking the top face's)
+  template <int ORD, int DIR>
+  static __device__ __forceinline__ void face_rec(const Args &A, long face, int kf, const float (&qL)[5],
+                                                  const float (&qR)[5], const float (&F)[5]) {
+    constexpr int NG = OrdTraits<ORD>::NGLL;
+    constexpr int HS = (ORD - 1) / 2;
+    constexpr int NM = 1 + DIR;
+    const long n = (long)A.nx * A.ny * A.nz, nfm = (long)(A.nx + 1) * (A.ny + 1) * (A.nz + 1);
+    float bL, bR;
+    if (DIR == 2) {
+      bL = A.bg.rho_f[(kf == 0 && A.bc == BC_PERIODIC) ? A.nz : kf];
+      bR = A.bg.rho_f[(kf == A.nz && A.bc == BC_PERIODIC) ? 0 : kf];
+    } else {
+      bL = bR = A.bg.rho_c[HS + kf];
     }
-    e[10 * n + cell] = sten(idR, HS);
+    const float rL = bL + qL[0], rR = bR + qR[0];
+    const float vn = DIR == 1 ? 0.5f * (qL[NM] + qR[NM]) : 0.5f * (qL[NM] / rL + qR[NM] / rR);
+    float *fr = A.tend + trc_cell_planes<NG>() * n + face;
+    fr[0] = F[0];
+    fr[nfm] = vn;
+    fr[2 * nfm] = 0.5f * (qL[NM] + qR[NM]);
+    const float rup = vn > 0 ? rL : rR;
+    fr[3 * nfm] = rup;
+    fr[4 * nfm] = frcp(rup);
   }
 };
 
@@ -87,9 +108,8 @@ struct TracerArgs32 {
   const float *R, *U;        // (ngll*ngll, ncell): recorded total density / normal-momentum series
   const float *D;            // (ncell): recorded pre-split rho'
   const float *Y;            // (ngll, ncell): recorded 1/rho of the GLL points
-  float *E;                  // (10, ncell): the state's time-averaged edge perturbations eL, eR
-  float *TE;                 // (ntr, 2, ncell): the tracers' edges (left, right)
-  float *TF, *TF2, *UN;      // (ntr, nface) unscaled / limited fluxes, (nface) limiter velocity
+  const float *F0, *VN, *UN, *RUP, *YUP;  // (nface) each: the recorded face values
+  float *TF, *TF2;           // (ntr, nface): unscaled / limited tracer fluxes
   int *flag;                 // (nlines): the limiter's lines to redo in serial order
 };
 
@@ -99,6 +119,7 @@ __device__ __forceinline__ double trc_divisor(const TracerArgs32 &T, int hs, int
   return (double)T.A.state[g] + T.dens_c[hs + k];
 }
 __device__ __forceinline__ float trc_dens(const TracerArgs32 &T, int hs, int k) { return T.A.bg.rho_c[hs + k]; }
+__device__ __forceinline__ float trc_div_up(const TracerArgs32 &T, float a, long fi) { return a * T.YUP[fi]; }
 __device__ __forceinline__ float limit_face(const TracerArgs32 &T, float F, float f1, float f2, double q, float dens) {
   const float eps = 1.e-10f;
   const float fluxOut = T.A.dt * (f2 - f1) * T.A.inv_dxd;
@@ -134,6 +155,7 @@ __global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
   const int l = (int)(blockIdx.x - cb * (unsigned)T.ntr);
   const unsigned c = cb * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
+  if (l == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
   int i, j, k;
   unflat(c, G.nx, G.ny, k, j, i);
   const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
@@ -207,67 +229,9 @@ __global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
     tl = fmaxf(0.f, tl);
     trr = fmaxf(0.f, trr);
   }
-  T.TE[(2L * l) * ncell + c] = tl;
-  T.TE[(2L * l + 1) * ncell + c] = trr;
-}
-
-// The left (side 0) and right (side 1) values at face f along a line, with the edge BCs:
-// periodic faces 0 and n both see (right edge of cell n-1, left edge of cell 0); at a wall
-// the outside value copies the inside one (Spatial:816-837). The mass flux is the FP32
-// form's Riemann flux of the state (riemann32), the one the state's own split uses.
-template <int DIR, int NG>
-__global__ void __launch_bounds__(128) tracer_face32_kernel(TracerArgs32 T, int hs) {
-  const SweepArgs32 &A = T.A;
-  const Geo<DIR> G(A, hs);
-  const long nf = G.nface();
-  const long f = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (f >= nf) return;
-  if (f < G.nlines()) T.flag[f] = 0;  // the limiter's per-line flags (nf > nlines)
-  const int fx = G.nx + (DIR == 0), fy = G.ny + (DIR == 1);
-  int i, j, k;
-  unflat((unsigned)f, fx, fy, k, j, i);
-  const int pf = DIR == 0 ? i : (DIR == 1 ? j : k);
-  const int n = G.n();
-  const long ncell = (long)G.nz * G.ny * G.nx;
-  int pl = pf - 1, pr = pf;  // cells whose right / left edges meet at the face
-  bool lside_from_right = false, rside_from_left = false;  // wall copies
-  if (pf == 0) {
-    if (A.bc == BC_PERIODIC) pl = n - 1;
-    else { pl = 0; lside_from_right = true; }
-  }
-  if (pf == n) {
-    if (A.bc == BC_PERIODIC) pr = 0;
-    else { pr = n - 1; rside_from_left = true; }
-  }
-  int kl, jl, il, kr, jr, ir;
-  G.at(k, j, i, pl, kl, jl, il);
-  G.at(k, j, i, pr, kr, jr, ir);
-  const long cl = G.cell(kl, jl, il), cr = G.cell(kr, jr, ir);
-  float qL[5], qR[5];
-#pragma unroll
-  for (int v = 0; v < 5; v++) {
-    qL[v] = lside_from_right ? T.E[v * ncell + cl] : T.E[(5 + v) * ncell + cl];
-    qR[v] = rside_from_left ? T.E[(5 + v) * ncell + cr] : T.E[v * ncell + cr];
-  }
-  float F[5];
-  riemann32<DIR, NG>(qL, qR, k, A, F);  // k: the face's k (z) or the line's k
-  // the sides' total densities: the background of the face's two sides (riemann32's)
-  float bL, bR;
-  if (DIR == 2) {
-    bL = A.bg.rho_f[(k == 0 && A.bc == BC_PERIODIC) ? A.nz : k];
-    bR = A.bg.rho_f[(k == A.nz && A.bc == BC_PERIODIC) ? 0 : k];
-  } else {
-    bL = bR = A.bg.rho_c[hs + k];
-  }
-  const float rL = bL + qL[0], rR = bR + qR[0];
-  constexpr int NM = 1 + DIR;
-  const float vn = DIR == 1 ? 0.5f * (qL[NM] + qR[NM]) : 0.5f * (qL[NM] / rL + qR[NM] / rR);
-  T.UN[f] = 0.5f * (qL[NM] + qR[NM]);
-  for (int l = 0; l < T.ntr; l++) {
-    const float tL = lside_from_right ? T.TE[(2L * l) * ncell + cl] : T.TE[(2L * l + 1) * ncell + cl];
-    const float tR = rside_from_left ? T.TE[(2L * l + 1) * ncell + cr] : T.TE[(2L * l) * ncell + cr];
-    T.TF[l * nf + f] = vn > 0 ? F[0] * tL / rL : F[0] * tR / rR;
-  }
+  // the fluxes of the faces this cell is upwind of
+  const long fs = DIR == 0 ? 1 : (DIR == 1 ? G.nx : (long)G.nx * G.ny), fl = G.face(k, j, i);
+  write_upwind_fluxes<float>(T, T.TF + (long)l * G.nface(), p0, n, A.bc == BC_PERIODIC, fl, fs, fl - p0 * fs, tl, trr);
 }
 
 template <int ORD, int DIR>
@@ -282,7 +246,6 @@ cudaError_t run32(const TracerArgs32 &T, cudaStream_t st) {
   cudaError_t e = launch_sweep_t<P32Trc, ORD, DIR>(A, st);  // state split + records
   if (e != cudaSuccess) return e;
   tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
-  tracer_face32_kernel<DIR, NG><<<gf, 128, 0, st>>>(T, HS);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs32, DIR><<<gf, 128, 0, st>>>(T, HS);
   tracer_limit_lines_kernel<TracerArgs32, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
@@ -309,16 +272,19 @@ cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &Ain, con
   T.tr = tracers;
   T.ntr = ntr;
   T.pos = pos;
+  const long ncp = 2L * ng * ng + 1 + ng;  // trc_cell_planes
   T.R = scratch;
   T.U = scratch + (long)ng * ng * ncell;
-  T.E = scratch + 2L * ng * ng * ncell;
-  T.D = T.E + 10 * ncell;
-  T.Y = T.E + 11 * ncell;
-  T.TE = T.E + (11L + ng) * ncell;
-  T.TF = T.TE + 2L * ntr * ncell;
+  T.D = scratch + 2L * ng * ng * ncell;
+  T.Y = T.D + ncell;
+  T.F0 = scratch + ncp * ncell;
+  T.VN = T.F0 + nfmax;
+  T.UN = T.VN + nfmax;
+  T.RUP = T.UN + nfmax;
+  T.YUP = T.RUP + nfmax;
+  T.TF = scratch + ncp * ncell + 5 * nfmax;
   T.TF2 = T.TF + (long)ntr * nfmax;
-  T.UN = T.TF2 + (long)ntr * nfmax;
-  T.flag = reinterpret_cast<int *>(T.UN + nfmax);
+  T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);
   if (ord == 5) {
     if (dir == 0) return run32<5, 0>(T, st);
     if (dir == 1) return run32<5, 1>(T, st);

@@ -11,13 +11,16 @@
 //   tr               double*, (ntr, nz+2hs, ny+2hs, nx+2hs): the tracers,
 //   ntr, pos         the tracer count and the positive-definite bits,
 //   D                const Flux*, (ncell): the recorded pre-split rho',
-//   TF, TF2, UN      Flux*, (ntr, nface), (ntr, nface), (nface): unscaled and limited
-//                    tracer fluxes, the limiter's velocity,
+//   F0, VN, UN       const Flux*, (nface) each: per face, recorded by the state's sweep, the
+//                    Riemann mass flux, the velocity that picks the upwind side and the
+//                    limiter's velocity,
+//   TF, TF2          Flux*, (ntr, nface): the unscaled and the limited tracer fluxes,
 //   flag             int*, (nlines): the limiter's lines to redo in serial order,
 // and these overloads for it:
 //   trc_divisor(T, hs, k, g)        the divisor of the division: rho' + rho_h (double)
 //   trc_dens(T, hs, k)              rho_h of row k as the limiter adds it to a recorded rho'
 //   limit_face(T, F, f1, f2, q, d)  a face's scaled flux from its upwind cell's two faces
+//   trc_div_up(T, a, fi)            a divided by the upwind density of face fi (recorded)
 //   trc_update(T, q, hs, k, c, Fl, Fr)
 //                                   the updated tracer of cell c (row k) from its divided
 //                                   value q and its limited face fluxes: q*rho + dt*tend
@@ -90,6 +93,27 @@ __device__ __forceinline__ void unflat(unsigned x, unsigned ex, unsigned ey, int
 
 template <int DIR> __device__ __forceinline__ long line_of(int k, int j, int i, int ny, int nx) {
   return DIR == 0 ? (long)k * ny + j : (DIR == 1 ? (long)k * nx + i : (long)j * nx + i);
+}
+
+// The tracer fluxes (Spatial:891-901, 1249-1259, 1633-1643) of the faces cell p of a line
+// is upwind of, from its time-averaged tracer edges tl (left) and tr (right): face flux =
+// the state's mass flux F0 times the upwind edge over the upwind density RUP, both recorded
+// by the sweep at the face; VN > 0 makes the left cell upwind. Edge BCs (Spatial:816-837):
+// periodic faces 0 and n both see (right edge of cell n-1, left edge of cell 0); at a wall
+// both sides of face 0 see cell 0's left edge, of face n cell n-1's right edge. Every face
+// of the line is written by exactly one cell (face 0 and face n of a periodic line by one
+// cell each). fl: this cell's left face, fs: the face stride along the line, f0: face 0.
+template <class Fx, class TA>
+__device__ __forceinline__ void write_upwind_fluxes(const TA &T, Fx *TF, int p, int n, bool periodic, long fl,
+                                                    long fs, long f0, Fx tl, Fx tr) {
+  auto put = [&](long fi, Fx t) { TF[fi] = trc_div_up(T, T.F0[fi] * t, fi); };
+  const long fr = fl + fs;
+  if ((p == 0 && !periodic) || !(T.VN[fl] > 0)) put(fl, tl);
+  if ((p == n - 1 && !periodic) || T.VN[fr] > 0) put(fr, tr);
+  if (periodic) {
+    if (p == n - 1 && T.VN[f0] > 0) put(f0, tr);                        // face 0, across the wrap
+    if (p == 0 && !(T.VN[f0 + (long)n * fs] > 0)) put(f0 + (long)n * fs, tl);  // face n, likewise
+  }
 }
 
 // tracers /= (rho' + rho_h) on the interior cells, with the state before the split
