@@ -894,8 +894,12 @@ int awfl_split_slab(awfl_ctx *c, void *d_state, const void *d_recv, double dt, v
   return AWFL_OK;
 }
 
-int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
-                       int dir, void *stream) {
+// One tracer split; io: TRC_IN_DIVIDED -- the tracers arrive divided by the current
+// density (the previous split of the same step left them so); TRC_OUT_DIVIDED -- leave
+// the interior divided by the post-split density for the next split. Either way the
+// values are the ones the undivided round trip gives, bit for bit.
+static int split_tracers_io(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
+                            int dir, int io, void *stream) {
   if (!c) return AWFL_ERR_ARG;
   if (c->nslabs > 1) return fail(c, AWFL_ERR_ARG, "tracer transport is not available on a slab");
   if (dir < 0 || dir > 2) return fail(c, AWFL_ERR_ARG, "dir must be 0, 1 or 2");
@@ -920,21 +924,30 @@ int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntrace
     SweepArgs32 A = sweep_args32(c, d_state, nullptr, dt, dir, MODE_APPLY);
     const double dxd = dir == 0 ? c->dx : (dir == 1 ? c->dy : c->dz);
     e = launch_split_tracers32(c->cfg.ord, dir, A, c->d_dens_c, dt, dxd, d_tracers, ntracers, mask,
-                               reinterpret_cast<float *>(c->d_trc), (cudaStream_t)stream);
+                               reinterpret_cast<float *>(c->d_trc), io, (cudaStream_t)stream);
   } else {
     SweepArgs A = sweep_args(c, d_state, nullptr, dt, dir, MODE_APPLY);
-    e = launch_split_tracers(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, (cudaStream_t)stream);
+    e = launch_split_tracers(c->cfg.ord, dir, A, d_tracers, ntracers, mask, c->d_trc, io, (cudaStream_t)stream);
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "split_tracers");
   return AWFL_OK;
 }
 
+int awfl_split_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
+                       int dir, void *stream) {
+  return split_tracers_io(c, d_state, d_tracers, ntracers, pos, dt, dir, 0, stream);
+}
+
 int awfl_step_tracers(awfl_ctx *c, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
                       void *stream) {
   if (!c) return AWFL_ERR_ARG;
+  // the tracers stay divided by the density from one split to the next (the division the
+  // next split would start with is done by the previous one's update); the y split of a
+  // sim2d context changes neither state nor tracers, and it is never the last
   for (int spl = 0; spl < 3; spl++) {
     const int dir = c->dimswitch ? spl : 2 - spl;
-    int rc = awfl_split_tracers(c, d_state, d_tracers, ntracers, pos, dt, dir, stream);
+    const int io = (spl > 0 ? TRC_IN_DIVIDED : 0) | (spl < 2 ? TRC_OUT_DIVIDED : 0);
+    int rc = split_tracers_io(c, d_state, d_tracers, ntracers, pos, dt, dir, io, stream);
     if (rc) return rc;
   }
   c->dimswitch = !c->dimswitch;

@@ -109,8 +109,12 @@ cudaError_t launch_sweep_rec(int ord, int dir, const SweepArgs &A, cudaStream_t 
 cudaError_t upload_tables_adj(int ord, const void *tab, size_t bytes);
 // Tracer transport of the FP64 path (awfl_tracers.cu): one split of state (fused, MODE_APPLY
 // arithmetic of awfl_split) and tracers; scratch holds tracer_scratch_bytes(..., 8) bytes.
+// io: TRC_IN_DIVIDED, the tracers arrive divided by the current density (no division at
+// the start); TRC_OUT_DIVIDED, the update leaves the interior divided by the post-split
+// density (for the next split of the same step).
+enum { TRC_IN_DIVIDED = 1, TRC_OUT_DIVIDED = 2 };
 cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
-                                 unsigned long long pos, double *scratch, cudaStream_t st);
+                                 unsigned long long pos, double *scratch, int io, cudaStream_t st);
 // Record layout of a tracer split (both precisions; planes of ncell cells, then of nfmax
 // faces): R (NG*NG: the density series), U (NG*NG: the normal-momentum series), D (1: the
 // pre-split rho', the stencil centre), Y (NG: 1/rho of the GLL points), then per face F0
@@ -124,7 +128,7 @@ cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes);
 // scratch holds tracer_scratch_bytes(..., 4) bytes; dens_c: rho_h rows (FP64).
 cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &A, const double *dens_c, double dt,
                                    double dxd, double *tracers, int ntr, unsigned long long pos, float *scratch,
-                                   cudaStream_t st);
+                                   int io, cudaStream_t st);
 cudaError_t upload_tables_tracers32(int ord, const double *recon, const double *c2g, const double *s2g,
                                     const double *deriv, const double *idl, double sigma, const double *wts);
 // Adjoint reverse sweeps (awfl_adjrev.cu)

@@ -249,28 +249,28 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
 }
 
 template <int ORD, int DIR>
-cudaError_t run(const TracerArgs &T, cudaStream_t st) {
+cudaError_t run(const TracerArgs &T, int io, cudaStream_t st) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
   const SweepArgs &A = T.A;
   const long ncell = (long)A.nz * A.ny * A.nx;
   const long nf = (long)(A.nz + (DIR == 2)) * (A.ny + (DIR == 1)) * (A.nx + (DIR == 0));
   const unsigned gc = (unsigned)((ncell + 127) / 128), gf = (unsigned)((nf + 127) / 128);
-  tracer_divide_kernel<TracerArgs><<<gc, 128, 0, st>>>(T, HS);
+  if (!(io & TRC_IN_DIVIDED)) tracer_divide_kernel<TracerArgs><<<gc, 128, 0, st>>>(T, HS);
   cudaError_t e = launch_sweep_t<P64Trc, ORD, DIR>(A, st);  // state split + records
   if (e != cudaSuccess) return e;
   tracer_cell_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs, DIR><<<gf, 128, 0, st>>>(T, HS);
   tracer_limit_lines_kernel<TracerArgs, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
-  tracer_update_kernel<TracerArgs, DIR><<<gc, 128, 0, st>>>(T, HS);
+  tracer_update_kernel<TracerArgs, DIR><<<gc, 128, 0, st>>>(T, HS, (io & TRC_OUT_DIVIDED) != 0);
   return cudaGetLastError();
 }
 
 }  // namespace
 
 cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &Ain, double *tracers, int ntr,
-                                 unsigned long long pos, double *scratch, cudaStream_t st) {
+                                 unsigned long long pos, double *scratch, int io, cudaStream_t st) {
   const int ng = ord == 5 ? 3 : 5;
   const long ncell = (long)Ain.nz * Ain.ny * Ain.nx;
   const long nfmax = (long)(Ain.nz + 1) * (Ain.ny + 1) * (Ain.nx + 1);
@@ -296,13 +296,13 @@ cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &Ain, double 
   T.TF2 = T.TF + (long)ntr * nfmax;
   T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);
   if (ord == 5) {
-    if (dir == 0) return run<5, 0>(T, st);
-    if (dir == 1) return run<5, 1>(T, st);
-    return run<5, 2>(T, st);
+    if (dir == 0) return run<5, 0>(T, io, st);
+    if (dir == 1) return run<5, 1>(T, io, st);
+    return run<5, 2>(T, io, st);
   }
-  if (dir == 0) return run<9, 0>(T, st);
-  if (dir == 1) return run<9, 1>(T, st);
-  return run<9, 2>(T, st);
+  if (dir == 0) return run<9, 0>(T, io, st);
+  if (dir == 1) return run<9, 1>(T, io, st);
+  return run<9, 2>(T, io, st);
 }
 
 size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem) {

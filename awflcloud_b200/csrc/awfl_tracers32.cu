@@ -235,21 +235,21 @@ __global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
 }
 
 template <int ORD, int DIR>
-cudaError_t run32(const TracerArgs32 &T, cudaStream_t st) {
+cudaError_t run32(const TracerArgs32 &T, int io, cudaStream_t st) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
   const SweepArgs32 &A = T.A;
   const long ncell = (long)A.nz * A.ny * A.nx;
   const long nf = (long)(A.nz + (DIR == 2)) * (A.ny + (DIR == 1)) * (A.nx + (DIR == 0));
   const unsigned gc = (unsigned)((ncell + 127) / 128), gf = (unsigned)((nf + 127) / 128);
-  tracer_divide_kernel<TracerArgs32><<<gc, 128, 0, st>>>(T, HS);
+  if (!(io & TRC_IN_DIVIDED)) tracer_divide_kernel<TracerArgs32><<<gc, 128, 0, st>>>(T, HS);
   cudaError_t e = launch_sweep_t<P32Trc, ORD, DIR>(A, st);  // state split + records
   if (e != cudaSuccess) return e;
   tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs32, DIR><<<gf, 128, 0, st>>>(T, HS);
   tracer_limit_lines_kernel<TracerArgs32, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
-  tracer_update_kernel<TracerArgs32, DIR><<<gc, 128, 0, st>>>(T, HS);
+  tracer_update_kernel<TracerArgs32, DIR><<<gc, 128, 0, st>>>(T, HS, (io & TRC_OUT_DIVIDED) != 0);
   return cudaGetLastError();
 }
 
@@ -257,7 +257,7 @@ cudaError_t run32(const TracerArgs32 &T, cudaStream_t st) {
 
 cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &Ain, const double *dens_c, double dt,
                                    double dxd, double *tracers, int ntr, unsigned long long pos, float *scratch,
-                                   cudaStream_t st) {
+                                   int io, cudaStream_t st) {
   const int ng = ord == 5 ? 3 : 5;
   const long ncell = (long)Ain.nz * Ain.ny * Ain.nx;
   const long nfmax = (long)(Ain.nz + 1) * (Ain.ny + 1) * (Ain.nx + 1);
@@ -286,13 +286,13 @@ cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &Ain, con
   T.TF2 = T.TF + (long)ntr * nfmax;
   T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);
   if (ord == 5) {
-    if (dir == 0) return run32<5, 0>(T, st);
-    if (dir == 1) return run32<5, 1>(T, st);
-    return run32<5, 2>(T, st);
+    if (dir == 0) return run32<5, 0>(T, io, st);
+    if (dir == 1) return run32<5, 1>(T, io, st);
+    return run32<5, 2>(T, io, st);
   }
-  if (dir == 0) return run32<9, 0>(T, st);
-  if (dir == 1) return run32<9, 1>(T, st);
-  return run32<9, 2>(T, st);
+  if (dir == 0) return run32<9, 0>(T, io, st);
+  if (dir == 1) return run32<9, 1>(T, io, st);
+  return run32<9, 2>(T, io, st);
 }
 
 cudaError_t upload_tables_tracers32(int ord, const double *recon, const double *c2g, const double *s2g,

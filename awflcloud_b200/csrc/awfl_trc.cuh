@@ -266,9 +266,11 @@ __global__ void __launch_bounds__(128) tracer_limit_lines_kernel(TA T, int hs) {
 
 // Per cell: the tendency of the limited fluxes, density multiplied back and the update
 // (Spatial:948-955; Temporal_ader.h:67-69), and the halo cells of this direction left
-// holding tracer/density, as the reference's in-place halo fill leaves them.
+// holding tracer/density, as the reference's in-place halo fill leaves them. out_divided:
+// the interior is left divided by the post-split density (the state's split is done), as
+// the next split's tracer_divide_kernel would divide it.
 template <class TA, int DIR>
-__global__ void __launch_bounds__(128) tracer_update_kernel(TA T, int hs) {
+__global__ void __launch_bounds__(128) tracer_update_kernel(TA T, int hs, bool out_divided) {
   const Geo<DIR> G(T.A, hs);
   const long ncell = (long)G.nz * G.ny * G.nx;
   const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -291,7 +293,8 @@ __global__ void __launch_bounds__(128) tracer_update_kernel(TA T, int hs) {
   for (int l = 0; l < T.ntr; l++) {
     double *t = T.tr + l * G.sv;
     const double q = t[gg];  // tracer / density (tracer_divide_kernel)
-    t[gg] = trc_update(T, q, hs, k, c, T.TF2[l * nf + fl], T.TF2[l * nf + fr]);
+    const double tn = trc_update(T, q, hs, k, c, T.TF2[l * nf + fl], T.TF2[l * nf + fr]);
+    t[gg] = out_divided ? tn / trc_divisor(T, hs, k, idR * G.sv + gg) : tn;
     if (T.A.bc == BC_PERIODIC) {
       if (p >= n - hs) t[halo(p - n)] = q;   // low halo (index p - n in [-hs, 0))
       if (p < hs) t[halo(n + p)] = q;        // high halo

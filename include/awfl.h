@@ -175,7 +175,10 @@ int awfl_write_netcdf_fields_tracers(awfl_ctx *ctx, const char *path, const doub
 int awfl_split_tracers(awfl_ctx *ctx, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
                        int dir, void *stream);
 /* One time step with tracers (Temporal_ader::timeStep with the tracer code compiled in):
- * awfl_split_tracers for each split in the dimSwitch order. */
+ * awfl_split_tracers for each split in the dimSwitch order; between two splits the
+ * tracers' interior stays divided by the density (each split's update does the division
+ * the next would start with), which gives the same values bit for bit. After an error the
+ * tracer array may be left divided. */
 int awfl_step_tracers(awfl_ctx *ctx, void *d_state, double *d_tracers, int ntracers, const int *pos, double dt,
                       void *stream);
 
