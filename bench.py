@@ -482,9 +482,10 @@ def tracers_leg(a, local, ntr=3, steps=5, warmup=2):
             "fp32": {"ms_per_step_with_tracers": round(ms_tr32, 4), "ms_per_step_without": round(ms_plain32, 4),
                      "tracer_ms_per_step": round(ms_tr32 - ms_plain32, 4),
                      "value": round(cells / (ms_tr32 * 1e-3) / 1e6, 3), "finite": finite32},
-            "note": "per split: tracers divided by the density, the state's fused sweep recording the density / "
-                    "normal-momentum ADER series, edges, pre-split density and reciprocal densities, then the "
-                    "tracer launches (cell, face, limiter faces, limiter lines, update)"}
+            "note": "per split: the state's fused sweep recording the density / normal-momentum ADER series, "
+                    "the pre-split density, reciprocal densities and per face the Riemann mass flux, upwind velocity "
+                    "and density; then the tracer launches (cell with the upwind fluxes, limiter faces, limiter "
+                    "lines, update); tracers divided by the density once per step, kept divided between splits"}
 
 
 def adjoint_leg(a, local):
