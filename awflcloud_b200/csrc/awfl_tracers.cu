@@ -110,7 +110,7 @@ struct TracerArgs {
   const double *Y;           // (ngll, ncell): recorded RN(1 / rho) of the GLL points
   const double *F0, *VN, *UN, *RUP, *YUP;  // (nface) each: the recorded face values
   double *TF, *TF2;          // (ntr, nface): unscaled / limited tracer fluxes
-  int *flag;                 // (nlines): the limiter's lines to redo in serial order
+  int *flag, *list, *count;  // the limiter's lines to redo in serial order: flags, list, length
 };
 
 // The FP64 path's arithmetic of the shared kernels (awfl_trc.cuh): the reference's
@@ -167,6 +167,7 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
   const unsigned c = cb * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   if (l == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
+  if (l == 0 && c == 0) *T.count = 0;
   int i, j, k;
   unflat(c, G.nx, G.ny, k, j, i);
   const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
@@ -262,7 +263,8 @@ cudaError_t run(const TracerArgs &T, int io, cudaStream_t st) {
   tracer_cell_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs, DIR><<<gf, 128, 0, st>>>(T, HS);
-  tracer_limit_lines_kernel<TracerArgs, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
+  const long lw = (nlines * T.ntr + 3) / 4;  // one warp per flagged line and tracer, grid-strided
+  tracer_limit_lines_kernel<TracerArgs, DIR><<<(unsigned)(lw < 148 * 8 ? lw : 148 * 8), 128, 0, st>>>(T, HS);
   tracer_update_kernel<TracerArgs, DIR><<<gc, 128, 0, st>>>(T, HS, (io & TRC_OUT_DIVIDED) != 0);
   return cudaGetLastError();
 }
@@ -295,6 +297,11 @@ cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &Ain, double 
   T.TF = scratch + ncp * ncell + 5 * nfmax;
   T.TF2 = T.TF + (long)ntr * nfmax;
   T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);
+  long lines = (long)Ain.nz * Ain.ny;  // as tracer_scratch_bytes
+  if ((long)Ain.nz * Ain.nx > lines) lines = (long)Ain.nz * Ain.nx;
+  if ((long)Ain.ny * Ain.nx > lines) lines = (long)Ain.ny * Ain.nx;
+  T.list = T.flag + lines;
+  T.count = T.list + lines;
   if (ord == 5) {
     if (dir == 0) return run<5, 0>(T, io, st);
     if (dir == 1) return run<5, 1>(T, io, st);
@@ -309,11 +316,11 @@ size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem) 
   const int ng = ord == 5 ? 3 : 5;
   const long ncell = (long)nz * ny * nx;
   const long nfmax = (long)(nz + 1) * (ny + 1) * (nx + 1);
-  long lines = (long)nz * ny;  // the most lines of one direction: the limiter's int flags
+  long lines = (long)nz * ny;  // the most lines of one direction: the limiter's flags and list
   if ((long)nz * nx > lines) lines = (long)nz * nx;
   if ((long)ny * nx > lines) lines = (long)ny * nx;
   const long elems = (2L * ng * ng + 1 + ng) * ncell + 5 * nfmax + 2L * ntr * nfmax;
-  return (size_t)elem * (size_t)elems + sizeof(int) * (size_t)lines;
+  return (size_t)elem * (size_t)elems + sizeof(int) * (2 * (size_t)lines + 1);
 }
 
 cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes) {

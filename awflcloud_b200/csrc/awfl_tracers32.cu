@@ -110,7 +110,7 @@ struct TracerArgs32 {
   const float *Y;            // (ngll, ncell): recorded 1/rho of the GLL points
   const float *F0, *VN, *UN, *RUP, *YUP;  // (nface) each: the recorded face values
   float *TF, *TF2;           // (ntr, nface): unscaled / limited tracer fluxes
-  int *flag;                 // (nlines): the limiter's lines to redo in serial order
+  int *flag, *list, *count;  // the limiter's lines to redo in serial order: flags, list, length
 };
 
 // The FP32 form's arithmetic of the shared kernels (awfl_trc.cuh): the division by the
@@ -156,6 +156,7 @@ __global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
   const unsigned c = cb * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   if (l == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
+  if (l == 0 && c == 0) *T.count = 0;
   int i, j, k;
   unflat(c, G.nx, G.ny, k, j, i);
   const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
@@ -248,7 +249,8 @@ cudaError_t run32(const TracerArgs32 &T, int io, cudaStream_t st) {
   tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs32, DIR><<<gf, 128, 0, st>>>(T, HS);
-  tracer_limit_lines_kernel<TracerArgs32, DIR><<<(unsigned)((nlines * T.ntr + 127) / 128), 128, 0, st>>>(T, HS);
+  const long lw = (nlines * T.ntr + 3) / 4;  // one warp per flagged line and tracer, grid-strided
+  tracer_limit_lines_kernel<TracerArgs32, DIR><<<(unsigned)(lw < 148 * 8 ? lw : 148 * 8), 128, 0, st>>>(T, HS);
   tracer_update_kernel<TracerArgs32, DIR><<<gc, 128, 0, st>>>(T, HS, (io & TRC_OUT_DIVIDED) != 0);
   return cudaGetLastError();
 }
@@ -285,6 +287,11 @@ cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &Ain, con
   T.TF = scratch + ncp * ncell + 5 * nfmax;
   T.TF2 = T.TF + (long)ntr * nfmax;
   T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);
+  long lines = (long)Ain.nz * Ain.ny;  // as tracer_scratch_bytes
+  if ((long)Ain.nz * Ain.nx > lines) lines = (long)Ain.nz * Ain.nx;
+  if ((long)Ain.ny * Ain.nx > lines) lines = (long)Ain.ny * Ain.nx;
+  T.list = T.flag + lines;
+  T.count = T.list + lines;
   if (ord == 5) {
     if (dir == 0) return run32<5, 0>(T, io, st);
     if (dir == 1) return run32<5, 1>(T, io, st);

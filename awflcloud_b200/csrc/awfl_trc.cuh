@@ -15,7 +15,9 @@
 //                    Riemann mass flux, the velocity that picks the upwind side and the
 //                    limiter's velocity,
 //   TF, TF2          Flux*, (ntr, nface): the unscaled and the limited tracer fluxes,
-//   flag             int*, (nlines): the limiter's lines to redo in serial order,
+//   flag, list, count  int*: per line, whether the limiter redoes it in serial order; the
+//                    list of those lines and its length (zeroed with the flags before
+//                    the limiter runs),
 // and these overloads for it:
 //   trc_divisor(T, hs, k, g)        the divisor of the division: rho' + rho_h (double)
 //   trc_dens(T, hs, k)              rho_h of row k as the limiter adds it to a recorded rho'
@@ -197,70 +199,88 @@ __global__ void __launch_bounds__(128) tracer_limit_faces_kernel(TA T, int hs) {
     }
     T.TF2[(long)l * nf + fi] = out;
   }
-  if (chained) T.flag[line_of<DIR>(k, j, i, G.ny, G.nx)] = 1;
+  if (chained) {
+    const long line = line_of<DIR>(k, j, i, G.ny, G.nx);
+    if (atomicExch(&T.flag[line], 1) == 0) T.list[atomicAdd(T.count, 1)] = (int)line;
+  }
 }
 
-// The flagged lines in the serial order, one thread per line and tracer: walking the faces
+// The flagged lines in the serial order, one warp per line and tracer: walking the faces
 // in order, a face keeps the first pass's value unless a face it reads (min of face f-1 for
 // un > 0; min of face 0 and max of face 1 for face n with un < 0) now holds a value other
-// than the unscaled one the first pass read; only those faces are limited again. The walk
-// reads three words per face and recomputes only along the chains.
+// than the unscaled one the first pass read; only those faces are limited again. The warp
+// loads 32 faces at a time (one per lane) and runs the walk over them uniformly, the
+// values coming by shuffle: the loads of a chunk overlap instead of one chain of
+// dependent loads per face.
 template <class TA, int DIR>
 __global__ void __launch_bounds__(128) tracer_limit_lines_kernel(TA T, int hs) {
   using Fx = typename TA::Flux;
   const Geo<DIR> G(T.A, hs);
   const int n = G.n();
-  const long nlines = G.nlines();
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long line = t / T.ntr;
-  const int l = (int)(t - line * T.ntr);
-  if (line >= nlines || !T.flag[line] || !((T.pos >> l) & 1ull)) return;
-  int k0, j0, i0;  // the line's cell 0
-  const unsigned ln = (unsigned)line;
-  if (DIR == 0) { i0 = 0; j0 = (int)(ln % (unsigned)G.ny); k0 = (int)(ln / (unsigned)G.ny); }
-  else if (DIR == 1) { j0 = 0; i0 = (int)(ln % (unsigned)G.nx); k0 = (int)(ln / (unsigned)G.nx); }
-  else { k0 = 0; i0 = (int)(ln % (unsigned)G.nx); j0 = (int)(ln / (unsigned)G.nx); }
+  const int lane = threadIdx.x & 31;
+  const long nwarps = (long)gridDim.x * (blockDim.x / 32);
+  const long items = (long)(*T.count) * T.ntr;
   const long nf = G.nface();
-  auto face = [&](int p) {
-    int kk, jj, ii;
-    G.at(k0, j0, i0, p, kk, jj, ii);
-    return G.face(kk, jj, ii);
-  };
-  const Fx *TF = T.TF + l * nf;
-  Fx *TF2 = T.TF2 + l * nf;
-  Fx sprev = 0, uprev = 0;              // the face behind: serial (scaled) and unscaled values
-  Fx s0 = 0, u0 = 0, s1 = 0, u1 = 0;   // faces 0 and 1, likewise
-#pragma unroll 4
-  for (int f = 0; f <= n; f++) {
-    const long fi = face(f);
-    const Fx F = TF[fi];
-    Fx out = TF2[fi];
-    const Fx un = T.UN[fi];
-    int c = -1;
-    Fx f1 = 0, f2 = 0;
-    if (un > 0 && f > 0) {
-      if (!(dmin(sprev, Fx(0)) == dmin(uprev, Fx(0)))) {  // upwind cell f-1 reads face f-1
-        c = f - 1;
-        f1 = dmin(sprev, Fx(0));
-        f2 = dmax(F, Fx(0));
+  for (long item = (blockIdx.x * (long)blockDim.x + threadIdx.x) / 32; item < items; item += nwarps) {
+    const int l = (int)(item % T.ntr);
+    if (!((T.pos >> l) & 1ull)) continue;  // unlimited: the first pass copied the fluxes
+    const unsigned ln = (unsigned)T.list[item / T.ntr];
+    int k0, j0, i0;  // the line's cell 0
+    if (DIR == 0) { i0 = 0; j0 = (int)(ln % (unsigned)G.ny); k0 = (int)(ln / (unsigned)G.ny); }
+    else if (DIR == 1) { j0 = 0; i0 = (int)(ln % (unsigned)G.nx); k0 = (int)(ln / (unsigned)G.nx); }
+    else { k0 = 0; i0 = (int)(ln % (unsigned)G.nx); j0 = (int)(ln / (unsigned)G.nx); }
+    auto face = [&](int p) {
+      int kk, jj, ii;
+      G.at(k0, j0, i0, p, kk, jj, ii);
+      return G.face(kk, jj, ii);
+    };
+    const Fx *TF = T.TF + l * nf;
+    Fx *TF2 = T.TF2 + l * nf;
+    Fx sprev = 0, uprev = 0;              // the face behind: serial (scaled) and unscaled values
+    Fx s0 = 0, u0 = 0, s1 = 0, u1 = 0;   // faces 0 and 1, likewise
+    for (int base = 0; base <= n; base += 32) {
+      const int fme = base + lane;
+      long fim = 0;
+      Fx Fm = 0, Tm = 0, Um = 0;
+      if (fme <= n) {
+        fim = face(fme);
+        Fm = TF[fim];
+        Tm = TF2[fim];
+        Um = T.UN[fim];
       }
-    } else if (un < 0 && f == n) {
-      if (!(dmin(s0, Fx(0)) == dmin(u0, Fx(0))) || (n >= 2 && !(dmax(s1, Fx(0)) == dmax(u1, Fx(0))))) {
-        c = 0;  // upwind cell 0
-        f1 = dmin(s0, Fx(0));
-        f2 = dmax(n == 1 ? F : s1, Fx(0));
+      const int cnt = n + 1 - base < 32 ? n + 1 - base : 32;
+      for (int i = 0; i < cnt; i++) {
+        const int f = base + i;
+        const Fx F = __shfl_sync(0xffffffffu, Fm, i);
+        Fx out = __shfl_sync(0xffffffffu, Tm, i);
+        const Fx un = __shfl_sync(0xffffffffu, Um, i);
+        int c = -1;
+        Fx f1 = 0, f2 = 0;
+        if (un > 0 && f > 0) {
+          if (!(dmin(sprev, Fx(0)) == dmin(uprev, Fx(0)))) {  // upwind cell f-1 reads face f-1
+            c = f - 1;
+            f1 = dmin(sprev, Fx(0));
+            f2 = dmax(F, Fx(0));
+          }
+        } else if (un < 0 && f == n) {
+          if (!(dmin(s0, Fx(0)) == dmin(u0, Fx(0))) || (n >= 2 && !(dmax(s1, Fx(0)) == dmax(u1, Fx(0))))) {
+            c = 0;  // upwind cell 0
+            f1 = dmin(s0, Fx(0));
+            f2 = dmax(n == 1 ? F : s1, Fx(0));
+          }
+        }
+        if (c >= 0) {
+          int ck, cj, ci;
+          G.at(k0, j0, i0, c, ck, cj, ci);
+          out = limit_face(T, F, f1, f2, T.tr[l * G.sv + G.g(ck, cj, ci)], T.D[G.cell(ck, cj, ci)] + trc_dens(T, hs, ck));
+          if (lane == i) TF2[fim] = out;
+        }
+        sprev = out;
+        uprev = F;
+        if (f == 0) { s0 = out; u0 = F; }
+        if (f == 1) { s1 = out; u1 = F; }
       }
     }
-    if (c >= 0) {
-      int ck, cj, ci;
-      G.at(k0, j0, i0, c, ck, cj, ci);
-      out = limit_face(T, F, f1, f2, T.tr[l * G.sv + G.g(ck, cj, ci)], T.D[G.cell(ck, cj, ci)] + trc_dens(T, hs, ck));
-      TF2[fi] = out;
-    }
-    sprev = out;
-    uprev = F;
-    if (f == 0) { s0 = out; u0 = F; }
-    if (f == 1) { s1 = out; u1 = F; }
   }
 }
 
