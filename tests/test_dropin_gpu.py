@@ -188,3 +188,35 @@ def test_reference_driver_tracer_transport(tmp_path):
             assert _rel(got, want) <= 1e-12, (name, _rel(got, want))
             # transported: differs from the initial field
             assert np.abs(got - t0[i, h:-h, h:-h, h:-h] / r).max() > 1e-8 or name == "uniform"
+
+
+def test_reference_driver_tracer_transport_fp32(tmp_path):
+    """The same driver run in the FP32 form (precision: fp32): its tracer transport (FP32
+    reconstruction, fluxes and limiter, FP64 tracer arrays) against the oracle's FP64
+    restatement, to the precision form's accuracy."""
+    from scipy.io import netcdf_file
+    from awflcloud_b200 import capi
+    O = Oracle(32, 24, 16, bc=(0, 1, 1), crpow=True)
+    st = O.new_state()
+    O.init_state(st)
+    tr = O.new_tracers(3)
+    O.init_tracers(tr)
+    dt0 = O.compute_dt(st, 0.8)
+    sim_time = 3.5 * dt0
+    inp, out = str(tmp_path / "in.yaml"), str(tmp_path / "out.nc")
+    _yaml(inp, out, sim_time, extra="tracer_transport : true\nprecision : fp32\n")
+    p = subprocess.run([BIN, inp], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr
+    etime = 0.0
+    while etime < sim_time:
+        dt = dt0 if etime + dt0 <= sim_time else sim_time - etime
+        O.time_step_tracers(st, tr, dt)
+        etime += dt
+    c = capi.Context(32, 24, 16, bc=("periodic", "wall", "wall"), device=-1)
+    h = c.hs
+    r = st[0, h:-h, h:-h, h:-h] + c.background()["hyDensCells"][h:-h, None, None]
+    with netcdf_file(out, "r", mmap=False) as nc:
+        for i, name in enumerate(["uniform", "theta", "block"]):
+            got = nc.variables["tracer_" + name][-1]
+            want = tr[i, h:-h, h:-h, h:-h] / r
+            assert _rel(got, want) <= 1e-6, (name, _rel(got, want))
