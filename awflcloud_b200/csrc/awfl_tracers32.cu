@@ -23,6 +23,8 @@
 // Compiled with the FP32 form's flags (multiply-add contraction, fast division).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "awfl_fp32.cuh"
 #include "awfl_internal.h"
 
@@ -141,40 +143,48 @@ __device__ __forceinline__ double trc_update(const TracerArgs32 &T, double q, in
 namespace awfl {
 namespace {
 
-// One thread per cell and tracer; the blocks of one run of 128 cells are consecutive for
-// the tracers (block b: cells (b / ntr) * 128 .., tracer b % ntr), so the recorded series
-// that they share is read from DRAM once.
-template <int ORD, int DIR>
-__global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
+// One lane or a pair of lanes (two tracers on the paired FP32 instructions: one
+// instruction, two results, each rounded like the scalar operation).
+__device__ __forceinline__ float lane_of(float x, int) { return x; }
+__device__ __forceinline__ float lane_of(F2 x, int w) { return w ? x.v.y : x.v.x; }
+template <class TT> __device__ __forceinline__ TT pair_of(float a, float b);
+template <> __device__ __forceinline__ float pair_of<float>(float a, float) { return a; }
+template <> __device__ __forceinline__ F2 pair_of<F2>(float a, float b) { return F2(a, b); }
+// max(0, x) on the lanes whose tracer is positive definite
+__device__ __forceinline__ float clamp_pos(float x, bool p0, bool) { return p0 ? fmaxf(0.f, x) : x; }
+__device__ __forceinline__ F2 clamp_pos(F2 x, bool p0, bool p1) {
+  return F2(p0 ? fmaxf(0.f, x.v.x) : x.v.x, p1 ? fmaxf(0.f, x.v.y) : x.v.y);
+}
+
+// Tracers l0 (TT = float) or l0 and l0+1 (TT = F2) of cell c: reconstruction of
+// tracer/density, times the recorded density, the rho*u*tracer series and
+// diffTransformTracer (Spatial:2095-2125) along the recorded series, the edge time average
+// (Spatial:2153-2177) and the fluxes of the faces the cell is upwind of.
+template <int ORD, int DIR, class TT>
+__device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const Geo<DIR> &G, unsigned c, int l0,
+                                                   int k, int j, int i) {
   constexpr int HS = (ORD - 1) / 2;
   constexpr int NG = OrdTraits<ORD>::NGLL;
+  constexpr int NL = std::is_same<TT, F2>::value ? 2 : 1;
   const SweepArgs32 &A = T.A;
-  const Geo<DIR> G(A, HS);
   const unsigned ncell = (unsigned)G.nz * G.ny * G.nx;
-  const unsigned cb = blockIdx.x / (unsigned)T.ntr;
-  const int l = (int)(blockIdx.x - cb * (unsigned)T.ntr);
-  const unsigned c = cb * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  if (l == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
-  if (l == 0 && c == 0) *T.count = 0;
-  int i, j, k;
-  unflat(c, G.nx, G.ny, k, j, i);
   const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
   const int n = G.n();
-  const bool posdef = (T.pos >> l) & 1ull;
-  // the stencil of tracer / density; halo positions read the interior cell whose value
-  // the boundary condition copies there
-  const double *tr = T.tr + l * G.sv;
-  float s[ORD];
+  const bool pos0 = (T.pos >> l0) & 1ull, pos1 = NL == 2 && ((T.pos >> (l0 + 1)) & 1ull);
+  // the stencil of tracer / density; halo positions read the interior cell whose value the
+  // boundary condition copies there
+  const double *tr0 = T.tr + l0 * G.sv, *tr1 = T.tr + (l0 + NL - 1) * G.sv;
+  TT s[ORD];
 #pragma unroll
   for (int m = 0; m < ORD; m++) {
     bool wall;
     const int p = halo_src(p0 - HS + m, n, A.bc, wall);
     int kk, jj, ii;
     G.at(k, j, i, p, kk, jj, ii);
-    s[m] = (float)tr[G.g(kk, jj, ii)];
+    const long g = G.g(kk, jj, ii);
+    s[m] = pair_of<TT>((float)tr0[g], (float)tr1[g]);
   }
-  float rt[NG][NG], rut[NG][NG];
+  TT rt[NG][NG], rut[NG][NG];
   reconstruct_gll32<ORD>(s, rt[0], A.weno_s != 0);
   float rser[NG][NG], ruser[NG][NG], ry[NG];
 #pragma unroll
@@ -188,51 +198,68 @@ __global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
   for (int ii = 0; ii < NG; ii++) ry[ii] = T.Y[ii * (long)ncell + c];
   const Tables32<ORD> &TB = tab32<ORD>();
 #pragma unroll
-  for (int ii = 0; ii < NG; ii++) {
-    rt[0][ii] *= rser[0][ii];
-    if (posdef) rt[0][ii] = fmaxf(0.f, rt[0][ii]);
-  }
+  for (int ii = 0; ii < NG; ii++) rt[0][ii] = clamp_pos(rt[0][ii] * rser[0][ii], pos0, pos1);
 #pragma unroll
-  for (int ii = 0; ii < NG; ii++) rut[0][ii] = rt[0][ii] * ruser[0][ii] * ry[ii];
-  // diffTransformTracer (Spatial:2095-2125)
+  for (int ii = 0; ii < NG; ii++) rut[0][ii] = (rt[0][ii] * ruser[0][ii]) * ry[ii];
 #pragma unroll
   for (int kt = 0; kt < NG - 1; kt++) {
     const float sc = -A.inv_dxd * (1.0f / (kt + 1));
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      float df = 0.f;
+      TT df = TT(0.f);
 #pragma unroll
-      for (int q = 0; q < NG; q++) df = fmaf(TB.deriv[q * NG + ii], rut[kt][q], df);
+      for (int q = 0; q < NG; q++) df = fmaT(TB.deriv[q * NG + ii], rut[kt][q], df);
       rt[kt + 1][ii] = df * sc;
     }
 #pragma unroll
     for (int ii = 0; ii < NG; ii++) {
-      float tot = 0.f;
+      TT tot = TT(0.f);
 #pragma unroll
       for (int ir = 0; ir <= kt + 1; ir++) {
-        tot = fmaf(ruser[ir][ii], rt[kt + 1 - ir][ii], tot);
-        if (ir != 0) tot = fmaf(-rser[ir][ii], rut[kt + 1 - ir][ii], tot);  // rut[kt+1] is not known yet
+        tot = fmaT(ruser[ir][ii], rt[kt + 1 - ir][ii], tot);
+        if (ir != 0) tot = fmaT(-rser[ir][ii], rut[kt + 1 - ir][ii], tot);  // rut[kt+1] is not known yet
       }
       rut[kt + 1][ii] = tot * ry[ii];
     }
   }
-  // compute_timeAvg_edges (Spatial:2153-2177), then the positivity clamp of the edges
-  float tl = rt[0][0], trr = rt[0][NG - 1];
+  TT tl = rt[0][0], trr = rt[0][NG - 1];
   float dtmult = A.dt;
 #pragma unroll
   for (int kt = 1; kt < NG; kt++) {
     const float cf = dtmult * (1.0f / (kt + 1));
-    tl = fmaf(rt[kt][0], cf, tl);
-    trr = fmaf(rt[kt][NG - 1], cf, trr);
+    tl = fmaT(rt[kt][0], cf, tl);
+    trr = fmaT(rt[kt][NG - 1], cf, trr);
     dtmult *= A.dt;
   }
-  if (posdef) {
-    tl = fmaxf(0.f, tl);
-    trr = fmaxf(0.f, trr);
-  }
+  tl = clamp_pos(tl, pos0, pos1);
+  trr = clamp_pos(trr, pos0, pos1);
   // the fluxes of the faces this cell is upwind of
   const long fs = DIR == 0 ? 1 : (DIR == 1 ? G.nx : (long)G.nx * G.ny), fl = G.face(k, j, i);
-  write_upwind_fluxes<float>(T, T.TF + (long)l * G.nface(), p0, n, A.bc == BC_PERIODIC, fl, fs, fl - p0 * fs, tl, trr);
+#pragma unroll
+  for (int w = 0; w < NL; w++)
+    write_upwind_fluxes<float>(T, T.TF + (long)(l0 + w) * G.nface(), p0, n, A.bc == BC_PERIODIC, fl, fs,
+                               fl - p0 * fs, lane_of(tl, w), lane_of(trr, w));
+}
+
+// One thread per cell and pair of tracers (a last single tracer on one lane); the blocks of
+// one run of 128 cells are consecutive for the pairs (block b: cells (b / npairs) * 128 ..,
+// pair b % npairs), so the recorded series that they share is read from DRAM once.
+template <int ORD, int DIR>
+__global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
+  constexpr int HS = (ORD - 1) / 2;
+  const Geo<DIR> G(T.A, HS);
+  const unsigned ncell = (unsigned)G.nz * G.ny * G.nx;
+  const unsigned npairs = (unsigned)(T.ntr + 1) / 2;
+  const unsigned cb = blockIdx.x / npairs;
+  const int g = (int)(blockIdx.x - cb * npairs);
+  const unsigned c = cb * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  if (g == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
+  if (g == 0 && c == 0) *T.count = 0;
+  int i, j, k;
+  unflat(c, G.nx, G.ny, k, j, i);
+  if (2 * g + 1 < T.ntr) tracer_cell32_body<ORD, DIR, F2>(T, G, c, 2 * g, k, j, i);
+  else tracer_cell32_body<ORD, DIR, float>(T, G, c, 2 * g, k, j, i);
 }
 
 template <int ORD, int DIR>
@@ -246,7 +273,7 @@ cudaError_t run32(const TracerArgs32 &T, int io, cudaStream_t st) {
   if (!(io & TRC_IN_DIVIDED)) tracer_divide_kernel<TracerArgs32><<<gc, 128, 0, st>>>(T, HS);
   cudaError_t e = launch_sweep_t<P32Trc, ORD, DIR>(A, st);  // state split + records
   if (e != cudaSuccess) return e;
-  tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)T.ntr, 128, 0, st>>>(T);
+  tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)((T.ntr + 1) / 2), 128, 0, st>>>(T);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs32, DIR><<<gf, 128, 0, st>>>(T, HS);
   const long lw = (nlines * T.ntr + 3) / 4;  // one warp per flagged line and tracer, grid-strided
