@@ -81,10 +81,23 @@ struct P64 {
   static __device__ __forceinline__ void store_tend(const Args &A, long g, double x) { A.tend[g] = x; }
 };
 
-// Single-grid sweep shapes of the FP64 path, ord 5 (measured at 256x256x128):
-// x 16 x 8, y and z 8 x 16.
-template <> struct PolicyShape<P64, 5, 0> { static constexpr int C = 16, W = 8; };
-template <> struct PolicyShape<P64, 5, 1> { static constexpr int C = 8, W = 16; };
-template <> struct PolicyShape<P64, 5, 2> { static constexpr int C = 8, W = 16; };
+// Single-grid sweep shapes of the FP64 path, ord 5 (chunk x lines; measured at
+// 256x256x128 with the current kernel against x 32 x 4 / 8 x 16 and y, z 4 x 32 / 16 x 8,
+// which took 1-2% longer): x 16 x 8, y and z 8 x 16. The macros let a build try others.
+#ifndef AWFL_P64_XC
+#define AWFL_P64_XC 16
+#define AWFL_P64_XW 8
+#endif
+#ifndef AWFL_P64_YC
+#define AWFL_P64_YC 8
+#define AWFL_P64_YW 16
+#endif
+#ifndef AWFL_P64_ZC
+#define AWFL_P64_ZC 8
+#define AWFL_P64_ZW 16
+#endif
+template <> struct PolicyShape<P64, 5, 0> { static constexpr int C = AWFL_P64_XC, W = AWFL_P64_XW; };
+template <> struct PolicyShape<P64, 5, 1> { static constexpr int C = AWFL_P64_YC, W = AWFL_P64_YW; };
+template <> struct PolicyShape<P64, 5, 2> { static constexpr int C = AWFL_P64_ZC, W = AWFL_P64_ZW; };
 
 }  // namespace awfl
