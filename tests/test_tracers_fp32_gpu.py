@@ -32,12 +32,15 @@ def inner(x, hs):
     return x[..., hs:-hs, hs:-hs, hs:-hs]
 
 
-@pytest.mark.parametrize("ord_,cfl,bc", [(5, 0.8, ("periodic", "periodic", "wall")), (5, 0.8, ("wall", "wall", "wall")),
-                                         (9, 0.4, ("periodic", "periodic", "wall"))])
-def test_fp32_tracers_follow_fp64(ord_, cfl, bc):
-    n, steps = (64, 64, 32), 20
-    c64 = capi.Context(*n, ord_=ord_, bc=bc)
-    c32 = capi.Context(*n, ord_=ord_, bc=bc, precision=capi.FP32)
+@pytest.mark.parametrize("ord_,cfl,bc,n", [(5, 0.8, ("periodic", "periodic", "wall"), (64, 64, 32)),
+                                           (5, 0.8, ("wall", "wall", "wall"), (64, 64, 32)),
+                                           (9, 0.4, ("periodic", "periodic", "wall"), (64, 64, 32)),
+                                           (5, 0.8, ("periodic", "periodic", "wall"), (64, 1, 32))])  # sim2d
+def test_fp32_tracers_follow_fp64(ord_, cfl, bc, n):
+    steps = 20
+    kw = dict(ylen=20000.0 / 64) if n[1] == 1 else {}
+    c64 = capi.Context(*n, ord_=ord_, bc=bc, **kw)
+    c32 = capi.Context(*n, ord_=ord_, bc=bc, precision=capi.FP32, **kw)
     s64, s32 = c64.new_state(), c32.new_state()
     c64.init_state(s64, **BUBBLE)
     c32.init_state(s32, **BUBBLE)
@@ -46,7 +49,7 @@ def test_fp32_tracers_follow_fp64(ord_, cfl, bc):
     c32.init_tracers(t32)
     assert torch.equal(t64, t32)
     plain = s32.clone()
-    cp = capi.Context(*n, ord_=ord_, bc=bc, precision=capi.FP32)  # its own split order (dimSwitch)
+    cp = capi.Context(*n, ord_=ord_, bc=bc, precision=capi.FP32, **kw)  # its own split order (dimSwitch)
     dt = c64.cfl(s64, cfl)
     for _ in range(steps):
         c64.step_tracers(s64, t64, dt)
