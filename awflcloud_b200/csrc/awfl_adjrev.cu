@@ -25,6 +25,12 @@ template <> __device__ __forceinline__ const Tables<5> &atab<5>() { return a_tab
 template <> __device__ __forceinline__ const Tables<9> &atab<9>() { return a_tab9; }
 
 constexpr int kAdjThreads = 128;
+// CTAs per SM requested of the two largest reverse kernels at ord 5 (register bound; the
+// compiler's 243-254 registers give 2; measured at 128x128x64: 3 CTAs at 168 registers with
+// spills no faster, 4 at 128 registers 12% slower)
+#ifndef AWFL_ADJ_MINB
+#define AWFL_ADJ_MINB 1
+#endif
 
 template <int ORD, int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_edges_kernel(adj::SplitArgs A) {
   const long n = adj::ncell_of(A);
@@ -38,13 +44,15 @@ template <int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_face_kerne
     adj::split_face<DIR>(A, f);
 }
 
-template <int ORD, int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_cell_kernel(adj::SplitArgs A) {
+template <int ORD, int DIR>
+__global__ void __launch_bounds__(kAdjThreads, ORD == 5 ? AWFL_ADJ_MINB : 1) adj_cell_kernel(adj::SplitArgs A) {
   const long n = adj::ncell_of(A);
   for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
     adj::split_cell_dt<ORD, DIR>(atab<ORD>(), A, c);
 }
 
-template <int ORD, int DIR> __global__ void __launch_bounds__(kAdjThreads) adj_weno_kernel(adj::SplitArgs A) {
+template <int ORD, int DIR>
+__global__ void __launch_bounds__(kAdjThreads, ORD == 5 ? AWFL_ADJ_MINB : 1) adj_weno_kernel(adj::SplitArgs A) {
   const long n = 5 * adj::ncell_of(A);
   for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < n; x += (long)gridDim.x * blockDim.x)
     adj::split_weno<ORD, DIR>(atab<ORD>(), A, x);
