@@ -175,31 +175,43 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
   const bool posdef = (T.pos >> l) & 1ull;
   // the stencil of tracer / density (divided by tracer_divide_kernel); halo positions
   // read the interior cell whose value the boundary condition copies there
-  const double *tr = T.tr + l * G.sv;
+  const double *tr = T.tr + l * G.sv + G.g(k, j, i);  // this cell's tracer
+  const long gsd = DIR == 0 ? 1 : (DIR == 1 ? G.sy : G.sz);  // state stride along the line
   double s[ORD];
+  if (p0 >= HS && p0 < n - HS) {  // the whole stencil inside the line
 #pragma unroll
-  for (int m = 0; m < ORD; m++) {
-    bool wall;
-    const int p = halo_src(p0 - HS + m, n, A.bc, wall);
-    int kk, jj, ii;
-    G.at(k, j, i, p, kk, jj, ii);
-    s[m] = tr[G.g(kk, jj, ii)];
+    for (int m = 0; m < ORD; m++) s[m] = tr[(m - HS) * gsd];
+  } else {
+#pragma unroll
+    for (int m = 0; m < ORD; m++) {
+      bool wall;
+      const int p = halo_src(p0 - HS + m, n, A.bc, wall);
+      s[m] = tr[(p - p0) * gsd];
+    }
   }
   double rt[NG][NG], rut[NG][NG];
   reconstruct_gll_any<ORD>(s, rt[0], A.weno_s != 0);
   double rser[NG][NG], ruser[NG][NG];
+  {
+    const double *r = T.R + c, *u = T.U + c;  // plane by plane, ncell apart
 #pragma unroll
-  for (int kt = 0; kt < NG; kt++)
+    for (int kt = 0; kt < NG; kt++)
 #pragma unroll
-    for (int ii = 0; ii < NG; ii++) {
-      rser[kt][ii] = T.R[(kt * NG + ii) * (long)ncell + c];
-      ruser[kt][ii] = T.U[(kt * NG + ii) * (long)ncell + c];
-    }
+      for (int ii = 0; ii < NG; ii++) {
+        rser[kt][ii] = *r;
+        ruser[kt][ii] = *u;
+        r += ncell;
+        u += ncell;
+      }
+  }
   // the divisors through their correctly rounded reciprocals (IEEE quotients bit for bit):
   // the GLL points' densities (reciprocals recorded by the sweep) and dx
   Rcp<double> rr[NG];
+  {
+    const double *y = T.Y + c;
 #pragma unroll
-  for (int ii = 0; ii < NG; ii++) rr[ii] = rcp_known(rser[0][ii], T.Y[ii * (long)ncell + c]);
+    for (int ii = 0; ii < NG; ii++) rr[ii] = rcp_known(rser[0][ii], y[ii * (long)ncell]);
+  }
   const Rcp<double> rdx = rcp_known(A.dxd, A.rdxd);
   const Tables<ORD> &TB = tab<ORD>();
 #pragma unroll
