@@ -33,26 +33,28 @@ def exchange_columns(send, recv, slab, nslabs, periodic, group=None):
     """Trade halo columns with the neighbouring slabs: send[1] (this slab's last columns)
     goes to the slab above and arrives there as its recv[0]; send[0] (its first columns)
     goes to the slab below as its recv[1]. send and recv are [2, n] tensors on the
-    process group's device. Every rank posts its operations in the same order (upward
-    send, receive from below, downward send, receive from above), so that two slabs that
-    are each other's neighbour on both sides (a periodic pair) match their messages in
-    order on any backend; tags 0 (upward) and 1 (downward) separate them where the backend
-    honours tags."""
+    process group's device. Every rank posts its operations as one batch
+    (batch_isend_irecv) in the same order (upward send, receive from below, downward
+    send, receive from above), so that two slabs that are each other's neighbour on both
+    sides (a periodic pair) match their messages in order on any backend; tags 0 (upward)
+    and 1 (downward) separate them where the backend honours tags."""
     import torch.distributed as dist
     lo, hi = neighbours(slab, nslabs, periodic)
     if lo is None and hi is None:
         return
     ranks = dist.get_process_group_ranks(group) if group is not None else list(range(nslabs))
-    reqs = []
+    ops = []
     if hi is not None:
-        reqs.append(dist.isend(send[1], ranks[hi], group=group, tag=0))
+        ops.append(dist.P2POp(dist.isend, send[1], ranks[hi], group=group, tag=0))
     if lo is not None:
-        reqs.append(dist.irecv(recv[0], ranks[lo], group=group, tag=0))
+        ops.append(dist.P2POp(dist.irecv, recv[0], ranks[lo], group=group, tag=0))
     if lo is not None:
-        reqs.append(dist.isend(send[0], ranks[lo], group=group, tag=1))
+        ops.append(dist.P2POp(dist.isend, send[0], ranks[lo], group=group, tag=1))
     if hi is not None:
-        reqs.append(dist.irecv(recv[1], ranks[hi], group=group, tag=1))
-    for r in reqs:
+        ops.append(dist.P2POp(dist.irecv, recv[1], ranks[hi], group=group, tag=1))
+    # one batch (one NCCL group): no rank's send waits for a receive that its peer has
+    # queued behind a send of its own
+    for r in dist.batch_isend_irecv(ops):
         r.wait()
 
 
