@@ -49,11 +49,12 @@ __device__ __forceinline__ double div_markstein(double a, double b, double y) {
 // a / r.b, correctly rounded
 template <class Sc> __device__ __forceinline__ Sc divr(const Sc &a, const Rcp<Sc> &r) { return a / r.b; }
 __device__ __forceinline__ double divr(const double &a, const Rcp<double> &r) { return div_markstein(a, r.b, r.y); }
-// a / r.b, correctly rounded for every dividend: those below 2^-900 in magnitude (where
-// the quotient or the remainder could leave the normal range, as transported tracer
-// values that decay towards zero can) take the IEEE division itself
+// a / r.b, correctly rounded for every dividend: nonzero ones below 2^-900 in magnitude
+// (where the quotient or the remainder could leave the normal range, as transported
+// tracer values that decay towards zero can) take the IEEE division itself; a zero
+// dividend stays on the short path, whose RN(a*y) is IEEE's signed zero
 __device__ __forceinline__ double divr_any(double a, const Rcp<double> &r) {
-  return fabs(a) < 0x1p-900 ? a / r.b : div_markstein(a, r.b, r.y);
+  return (fabs(a) < 0x1p-900 && a != 0.0) ? a / r.b : div_markstein(a, r.b, r.y);
 }
 // any scalar divided by a double divisor with a known reciprocal
 template <class Sc> __device__ __forceinline__ Sc divd(const Sc &a, const Rcp<double> &r) { return a / r.b; }

@@ -190,7 +190,18 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
     }
   }
   double rt[NG][NG], rut[NG][NG];
-  reconstruct_gll_any<ORD>(s, rt[0], A.weno_s != 0);
+  // a stencil of zeros (a tracer absent from this part of the domain) reconstructs to +0
+  // at every GLL point, WENO or not: every sum of the reconstruction starts at +0 and adds
+  // products with a zero factor, and its weights stay finite (eps keeps them off 1/0)
+  bool zero = true;
+#pragma unroll
+  for (int m = 0; m < ORD; m++) zero = zero && s[m] == 0.;
+  if (zero) {
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) rt[0][ii] = 0.;
+  } else {
+    reconstruct_gll_any<ORD>(s, rt[0], A.weno_s != 0);
+  }
   double rser[NG][NG], ruser[NG][NG];
   {
     const double *r = T.R + c, *u = T.U + c;  // plane by plane, ncell apart

@@ -150,6 +150,8 @@ __device__ __forceinline__ float lane_of(F2 x, int w) { return w ? x.v.y : x.v.x
 template <class TT> __device__ __forceinline__ TT pair_of(float a, float b);
 template <> __device__ __forceinline__ float pair_of<float>(float a, float) { return a; }
 template <> __device__ __forceinline__ F2 pair_of<F2>(float a, float b) { return F2(a, b); }
+__device__ __forceinline__ bool is_zero(float x) { return x == 0.f; }
+__device__ __forceinline__ bool is_zero(F2 x) { return x.v.x == 0.f && x.v.y == 0.f; }
 // max(0, x) on the lanes whose tracer is positive definite
 __device__ __forceinline__ float clamp_pos(float x, bool p0, bool) { return p0 ? fmaxf(0.f, x) : x; }
 __device__ __forceinline__ F2 clamp_pos(F2 x, bool p0, bool p1) {
@@ -185,7 +187,18 @@ __device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const 
     s[m] = pair_of<TT>((float)tr0[g], (float)tr1[g]);
   }
   TT rt[NG][NG], rut[NG][NG];
-  reconstruct_gll32<ORD>(s, rt[0], A.weno_s != 0);
+  // stencils of zeros (tracers absent from this part of the domain) reconstruct to +0 at
+  // every GLL point, WENO or not: every sum starts at +0 and adds products with a zero
+  // factor, and the weights stay finite (eps keeps them off 1/0)
+  bool zero = true;
+#pragma unroll
+  for (int m = 0; m < ORD; m++) zero = zero && is_zero(s[m]);
+  if (zero) {
+#pragma unroll
+    for (int ii = 0; ii < NG; ii++) rt[0][ii] = TT(0.f);
+  } else {
+    reconstruct_gll32<ORD>(s, rt[0], A.weno_s != 0);
+  }
   float rser[NG][NG], ruser[NG][NG], ry[NG];
 #pragma unroll
   for (int kt = 0; kt < NG; kt++)
