@@ -116,11 +116,15 @@ enum { TRC_IN_DIVIDED = 1, TRC_OUT_DIVIDED = 2 };
 cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &A, double *tracers, int ntr,
                                  unsigned long long pos, double *scratch, int io, cudaStream_t st);
 // Record layout of a tracer split (both precisions; planes of ncell cells, then of nfmax
-// faces): R (NG*NG: the density series), U (NG*NG: the normal-momentum series), D (1: the
-// pre-split rho', the stencil centre), Y (NG: 1/rho of the GLL points), then per face F0
-// (the Riemann mass flux), VN (the velocity that picks the upwind side), UN (the
-// limiter's velocity), RUP (the upwind side's density), YUP (1/RUP).
-template <int NG> __host__ __device__ constexpr long trc_cell_planes() { return 2L * NG * NG + 1 + NG; }
+// faces): R (NG*(NG-1): levels 0..NG-2 of the density series), U (NG*(NG-1): the same of
+// the normal-momentum series), D (1: the pre-split rho', the stencil centre), Y (NG: 1/rho
+// of the GLL points), then per face F0 (the Riemann mass flux), VN (the velocity that
+// picks the upwind side), UN (the limiter's velocity), RUP (the upwind side's density),
+// YUP (1/RUP). The series' last level only enters the tracer series' last momentum-flux
+// level, which no edge reads, so it is not recorded. The FP32 form recomputes Y and YUP
+// (its reciprocals are single fast-reciprocal instructions) and leaves their planes unused.
+template <int NG> __host__ __device__ constexpr long trc_series_planes() { return (long)NG * (NG - 1); }
+template <int NG> __host__ __device__ constexpr long trc_cell_planes() { return 2 * trc_series_planes<NG>() + 1 + NG; }
 // scratch of one tracer split: records and fluxes of elem bytes each, and the line flags
 size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem);
 cudaError_t upload_tables_tracers(int ord, const void *tab, size_t bytes);

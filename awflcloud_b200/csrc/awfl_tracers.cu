@@ -51,16 +51,17 @@ struct P64Trc : P64 {
     __device__ __forceinline__ void level0(int, int, const double &) const {}
     template <class Q> __device__ __forceinline__ void series(const Q &q) const {
       constexpr int NG = OrdTraits<ORD>::NGLL;
+      constexpr long NS = trc_series_planes<NG>();
 #pragma unroll
-      for (int kt = 0; kt < NG; kt++)
+      for (int kt = 0; kt < NG - 1; kt++)
 #pragma unroll
         for (int ii = 0; ii < NG; ii++) {
           base[(kt * NG + ii) * n + cell] = q[idR][kt][ii];
-          base[(NG * NG + kt * NG + ii) * n + cell] = q[nm][kt][ii];
+          base[(NS + kt * NG + ii) * n + cell] = q[nm][kt][ii];
         }
       // RN(1 / density) of the GLL points (the sweep's own reciprocals, rr in cell_recon)
 #pragma unroll
-      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 1 + ii) * n + cell] = 1.0 / q[idR][0][ii];
+      for (int ii = 0; ii < NG; ii++) base[(2 * NS + 1 + ii) * n + cell] = 1.0 / q[idR][0][ii];
     }
   };
   template <int ORD, int DIR, class S>
@@ -74,7 +75,7 @@ struct P64Trc : P64 {
     constexpr int HS = (ORD - 1) / 2;
     const long n = (long)A.nx * A.ny * A.nz;
     cell_recon<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell, 1 + DIR});
-    A.tend[2L * NG * NG * n + cell] = sten(idR, HS);
+    A.tend[2 * trc_series_planes<NG>() * n + cell] = sten(idR, HS);
   }
   // the face records: the tracer face flux's inputs (Spatial:891-901), from the states the
   // sweep's own Riemann flux saw
@@ -105,7 +106,7 @@ struct TracerArgs {
   double *tr;                // (ntr, nz+2hs, ny+2hs, nx+2hs), rho*tracer
   int ntr;
   unsigned long long pos;    // bit l: tracer l is positive definite (limited)
-  const double *R, *U;       // (ngll*ngll, ncell): recorded density / normal-momentum series
+  const double *R, *U;       // (ngll*(ngll-1), ncell): recorded density / normal-momentum series
   const double *D;           // (ncell): recorded pre-split rho'
   const double *Y;           // (ngll, ncell): recorded RN(1 / rho) of the GLL points
   const double *F0, *VN, *UN, *RUP, *YUP;  // (nface) each: the recorded face values
@@ -202,11 +203,11 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
   } else {
     reconstruct_gll_any<ORD>(s, rt[0], A.weno_s != 0);
   }
-  double rser[NG][NG], ruser[NG][NG];
+  double rser[NG - 1][NG], ruser[NG - 1][NG];
   {
     const double *r = T.R + c, *u = T.U + c;  // plane by plane, ncell apart
 #pragma unroll
-    for (int kt = 0; kt < NG; kt++)
+    for (int kt = 0; kt < NG - 1; kt++)
 #pragma unroll
       for (int ii = 0; ii < NG; ii++) {
         rser[kt][ii] = *r;
@@ -246,12 +247,15 @@ __global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC_CELL_MINB : 1) tracer
       for (int q = 0; q < NG; q++) df += TB.deriv[q * NG + ii] * rut[kt][q];
       rt[kt + 1][ii] = divk_any(divr_any(-df, rdx), kt + 1);
     }
+    if (kt + 1 < NG - 1) {  // the last level of rho*u*tracer reaches no edge
 #pragma unroll
-    for (int ii = 0; ii < NG; ii++) {
-      double tot = 0;
+      for (int ii = 0; ii < NG; ii++) {
+        double tot = 0;
 #pragma unroll
-      for (int ir = 0; ir <= kt + 1; ir++) tot += ruser[ir][ii] * rt[kt + 1 - ir][ii] - rser[ir][ii] * rut[kt + 1 - ir][ii];
-      rut[kt + 1][ii] = divr_any(tot, rr[ii]);
+        for (int ir = 0; ir <= kt + 1; ir++)
+          tot += ruser[ir][ii] * rt[kt + 1 - ir][ii] - rser[ir][ii] * rut[kt + 1 - ir][ii];
+        rut[kt + 1][ii] = divr_any(tot, rr[ii]);
+      }
     }
   }
   // compute_timeAvg_edges (Spatial:2153-2177), then the positivity clamp of the edges
@@ -307,10 +311,10 @@ cudaError_t launch_split_tracers(int ord, int dir, const SweepArgs &Ain, double 
   T.tr = tracers;
   T.ntr = ntr;
   T.pos = pos;
-  const long ncp = 2L * ng * ng + 1 + ng;  // trc_cell_planes
+  const long ns = (long)ng * (ng - 1), ncp = 2 * ns + 1 + ng;  // trc_series_planes, trc_cell_planes
   T.R = scratch;
-  T.U = scratch + (long)ng * ng * ncell;
-  T.D = scratch + 2L * ng * ng * ncell;
+  T.U = scratch + ns * ncell;
+  T.D = scratch + 2 * ns * ncell;
   T.Y = T.D + ncell;
   T.F0 = scratch + ncp * ncell;
   T.VN = T.F0 + nfmax;
@@ -342,7 +346,7 @@ size_t tracer_scratch_bytes(int ord, int nx, int ny, int nz, int ntr, int elem) 
   long lines = (long)nz * ny;  // the most lines of one direction: the limiter's flags and list
   if ((long)nz * nx > lines) lines = (long)nz * nx;
   if ((long)ny * nx > lines) lines = (long)ny * nx;
-  const long elems = (2L * ng * ng + 1 + ng) * ncell + 5 * nfmax + 2L * ntr * nfmax;
+  const long elems = (2L * ng * (ng - 1) + 1 + ng) * ncell + 5 * nfmax + 2L * ntr * nfmax;
   return (size_t)elem * (size_t)elems + sizeof(int) * (2 * (size_t)lines + 1);
 }
 

@@ -31,7 +31,8 @@
 namespace awfl {
 
 // Recording FP32 policy: the P32 arithmetic plus the tracer split's records (floats; the
-// layout of trc_cell_planes: R is the total density series, U the normal momentum), A.tend
+// layout of trc_cell_planes: R is the total density series, U the normal momentum; the
+// reciprocal planes Y and YUP stay unused, recomputed where they are needed), A.tend
 // pointing at the record base.
 struct P32Trc : P32 {
   static constexpr bool kSlab = false;
@@ -42,15 +43,14 @@ struct P32Trc : P32 {
     int nm;
     template <class Q, class Rt> __device__ __forceinline__ void series32(const Q &q, const Rt &rtot) const {
       constexpr int NG = OrdTraits<ORD>::NGLL;
+      constexpr long NS = trc_series_planes<NG>();
 #pragma unroll
-      for (int kt = 0; kt < NG; kt++)
+      for (int kt = 0; kt < NG - 1; kt++)
 #pragma unroll
         for (int ii = 0; ii < NG; ii++) {
           base[(kt * NG + ii) * n + cell] = kt == 0 ? rtot[ii] : q[idR][kt][ii];
-          base[(NG * NG + kt * NG + ii) * n + cell] = q[nm][kt][ii];
+          base[(NS + kt * NG + ii) * n + cell] = q[nm][kt][ii];
         }
-#pragma unroll
-      for (int ii = 0; ii < NG; ii++) base[(2 * NG * NG + 1 + ii) * n + cell] = frcp(rtot[ii]);
     }
   };
   template <int ORD, int DIR, class S>
@@ -64,7 +64,7 @@ struct P32Trc : P32 {
     constexpr int HS = (ORD - 1) / 2;
     const long n = (long)A.nx * A.ny * A.nz;
     cell_recon32<ORD, DIR>(sten, kb, A, eL, eR, src, Rec<ORD>{A.tend, n, cell, 1 + DIR});
-    A.tend[2L * NG * NG * n + cell] = sten(idR, HS);
+    A.tend[2 * trc_series_planes<NG>() * n + cell] = sten(idR, HS);
   }
   // the face records, from the perturbation states the sweep's own Riemann flux saw: the
   // sides' total densities with the background riemann32 gives them (z: the face's own
@@ -89,9 +89,7 @@ struct P32Trc : P32 {
     fr[0] = F[0];
     fr[nfm] = vn;
     fr[2 * nfm] = 0.5f * (qL[NM] + qR[NM]);
-    const float rup = vn > 0 ? rL : rR;
-    fr[3 * nfm] = rup;
-    fr[4 * nfm] = frcp(rup);
+    fr[3 * nfm] = vn > 0 ? rL : rR;
   }
 };
 
@@ -107,10 +105,9 @@ struct TracerArgs32 {
   double *tr;                // (ntr, nz+2hs, ny+2hs, nx+2hs), rho*tracer, FP64
   int ntr;
   unsigned long long pos;    // bit l: tracer l is positive definite (limited)
-  const float *R, *U;        // (ngll*ngll, ncell): recorded total density / normal-momentum series
+  const float *R, *U;        // (ngll*(ngll-1), ncell): recorded total density / normal-momentum series
   const float *D;            // (ncell): recorded pre-split rho'
-  const float *Y;            // (ngll, ncell): recorded 1/rho of the GLL points
-  const float *F0, *VN, *UN, *RUP, *YUP;  // (nface) each: the recorded face values
+  const float *F0, *VN, *UN, *RUP;  // (nface) each: the recorded face values
   float *TF, *TF2;           // (ntr, nface): unscaled / limited tracer fluxes
   int *flag, *list, *count;  // the limiter's lines to redo in serial order: flags, list, length
 };
@@ -121,7 +118,7 @@ __device__ __forceinline__ double trc_divisor(const TracerArgs32 &T, int hs, int
   return (double)T.A.state[g] + T.dens_c[hs + k];
 }
 __device__ __forceinline__ float trc_dens(const TracerArgs32 &T, int hs, int k) { return T.A.bg.rho_c[hs + k]; }
-__device__ __forceinline__ float trc_div_up(const TracerArgs32 &T, float a, long fi) { return a * T.YUP[fi]; }
+__device__ __forceinline__ float trc_div_up(const TracerArgs32 &T, float a, long fi) { return a * frcp(T.RUP[fi]); }
 __device__ __forceinline__ float limit_face(const TracerArgs32 &T, float F, float f1, float f2, double q, float dens) {
   const float eps = 1.e-10f;
   const float fluxOut = T.A.dt * (f2 - f1) * T.A.inv_dxd;
@@ -158,34 +155,26 @@ __device__ __forceinline__ F2 clamp_pos(F2 x, bool p0, bool p1) {
   return F2(p0 ? fmaxf(0.f, x.v.x) : x.v.x, p1 ? fmaxf(0.f, x.v.y) : x.v.y);
 }
 
-// Tracers l0 (TT = float) or l0 and l0+1 (TT = F2) of cell c: reconstruction of
+// Tracers l0 (TT = float) or l0 and l0+1 (TT = F2) of one cell: reconstruction of
 // tracer/density, times the recorded density, the rho*u*tracer series and
 // diffTransformTracer (Spatial:2095-2125) along the recorded series, the edge time average
-// (Spatial:2153-2177) and the fluxes of the faces the cell is upwind of.
-template <int ORD, int DIR, class TT>
-__device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const Geo<DIR> &G, unsigned c, int l0,
-                                                   int k, int j, int i) {
-  constexpr int HS = (ORD - 1) / 2;
+// (Spatial:2153-2177) and the fluxes of the faces the cell is upwind of. t0, t1: the
+// tracers at this cell; off: the stencil's offsets from it; rser, ruser, ry: the cell's
+// recorded density and normal-momentum series and reciprocal densities.
+template <int ORD, class TT>
+__device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const double *t0, const double *t1,
+                                                   const long (&off)[ORD],
+                                                   const float (&rser)[OrdTraits<ORD>::NGLL - 1][OrdTraits<ORD>::NGLL],
+                                                   const float (&ruser)[OrdTraits<ORD>::NGLL - 1][OrdTraits<ORD>::NGLL],
+                                                   const float (&ry)[OrdTraits<ORD>::NGLL], int l0,
+                                                   const UpwindFaces &U, float *TF, long nface) {
   constexpr int NG = OrdTraits<ORD>::NGLL;
   constexpr int NL = std::is_same<TT, F2>::value ? 2 : 1;
   const SweepArgs32 &A = T.A;
-  const unsigned ncell = (unsigned)G.nz * G.ny * G.nx;
-  const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
-  const int n = G.n();
   const bool pos0 = (T.pos >> l0) & 1ull, pos1 = NL == 2 && ((T.pos >> (l0 + 1)) & 1ull);
-  // the stencil of tracer / density; halo positions read the interior cell whose value the
-  // boundary condition copies there
-  const double *tr0 = T.tr + l0 * G.sv, *tr1 = T.tr + (l0 + NL - 1) * G.sv;
   TT s[ORD];
 #pragma unroll
-  for (int m = 0; m < ORD; m++) {
-    bool wall;
-    const int p = halo_src(p0 - HS + m, n, A.bc, wall);
-    int kk, jj, ii;
-    G.at(k, j, i, p, kk, jj, ii);
-    const long g = G.g(kk, jj, ii);
-    s[m] = pair_of<TT>((float)tr0[g], (float)tr1[g]);
-  }
+  for (int m = 0; m < ORD; m++) s[m] = pair_of<TT>((float)t0[off[m]], (float)t1[off[m]]);
   TT rt[NG][NG], rut[NG][NG];
   // stencils of zeros (tracers absent from this part of the domain) reconstruct to +0 at
   // every GLL point, WENO or not: every sum starts at +0 and adds products with a zero
@@ -199,16 +188,6 @@ __device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const 
   } else {
     reconstruct_gll32<ORD>(s, rt[0], A.weno_s != 0);
   }
-  float rser[NG][NG], ruser[NG][NG], ry[NG];
-#pragma unroll
-  for (int kt = 0; kt < NG; kt++)
-#pragma unroll
-    for (int ii = 0; ii < NG; ii++) {
-      rser[kt][ii] = T.R[(kt * NG + ii) * (long)ncell + c];
-      ruser[kt][ii] = T.U[(kt * NG + ii) * (long)ncell + c];
-    }
-#pragma unroll
-  for (int ii = 0; ii < NG; ii++) ry[ii] = T.Y[ii * (long)ncell + c];
   const Tables32<ORD> &TB = tab32<ORD>();
 #pragma unroll
   for (int ii = 0; ii < NG; ii++) rt[0][ii] = clamp_pos(rt[0][ii] * rser[0][ii], pos0, pos1);
@@ -224,15 +203,17 @@ __device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const 
       for (int q = 0; q < NG; q++) df = fmaT(TB.deriv[q * NG + ii], rut[kt][q], df);
       rt[kt + 1][ii] = df * sc;
     }
+    if (kt + 1 < NG - 1) {  // the last level of rho*u*tracer reaches no edge
 #pragma unroll
-    for (int ii = 0; ii < NG; ii++) {
-      TT tot = TT(0.f);
+      for (int ii = 0; ii < NG; ii++) {
+        TT tot = TT(0.f);
 #pragma unroll
-      for (int ir = 0; ir <= kt + 1; ir++) {
-        tot = fmaT(ruser[ir][ii], rt[kt + 1 - ir][ii], tot);
-        if (ir != 0) tot = fmaT(-rser[ir][ii], rut[kt + 1 - ir][ii], tot);  // rut[kt+1] is not known yet
+        for (int ir = 0; ir <= kt + 1; ir++) {
+          tot = fmaT(ruser[ir][ii], rt[kt + 1 - ir][ii], tot);
+          if (ir != 0) tot = fmaT(-rser[ir][ii], rut[kt + 1 - ir][ii], tot);  // rut[kt+1] is not known yet
+        }
+        rut[kt + 1][ii] = tot * ry[ii];
       }
-      rut[kt + 1][ii] = tot * ry[ii];
     }
   }
   TT tl = rt[0][0], trr = rt[0][NG - 1];
@@ -246,33 +227,73 @@ __device__ __forceinline__ void tracer_cell32_body(const TracerArgs32 &T, const 
   }
   tl = clamp_pos(tl, pos0, pos1);
   trr = clamp_pos(trr, pos0, pos1);
-  // the fluxes of the faces this cell is upwind of
-  const long fs = DIR == 0 ? 1 : (DIR == 1 ? G.nx : (long)G.nx * G.ny), fl = G.face(k, j, i);
 #pragma unroll
-  for (int w = 0; w < NL; w++)
-    write_upwind_fluxes<float>(T, T.TF + (long)(l0 + w) * G.nface(), p0, n, A.bc == BC_PERIODIC, fl, fs,
-                               fl - p0 * fs, lane_of(tl, w), lane_of(trr, w));
+  for (int w = 0; w < NL; w++) put_upwind_fluxes<float>(T, TF + w * nface, U, lane_of(tl, w), lane_of(trr, w));
 }
 
-// One thread per cell and pair of tracers (a last single tracer on one lane); the blocks of
-// one run of 128 cells are consecutive for the pairs (block b: cells (b / npairs) * 128 ..,
-// pair b % npairs), so the recorded series that they share is read from DRAM once.
+// One thread per cell for all its tracers, two at a time on the paired FP32 instructions
+// (a last single tracer on one lane): the cell's records, stencil offsets and upwind faces
+// are read and worked out once.
+#ifndef AWFL_TRC32_CELL_MINB
+#define AWFL_TRC32_CELL_MINB 8
+#endif
 template <int ORD, int DIR>
-__global__ void __launch_bounds__(128) tracer_cell32_kernel(TracerArgs32 T) {
+__global__ void __launch_bounds__(128, ORD == 5 ? AWFL_TRC32_CELL_MINB : 1) tracer_cell32_kernel(TracerArgs32 T) {
   constexpr int HS = (ORD - 1) / 2;
-  const Geo<DIR> G(T.A, HS);
+  constexpr int NG = OrdTraits<ORD>::NGLL;
+  const SweepArgs32 &A = T.A;
+  const Geo<DIR> G(A, HS);
   const unsigned ncell = (unsigned)G.nz * G.ny * G.nx;
-  const unsigned npairs = (unsigned)(T.ntr + 1) / 2;
-  const unsigned cb = blockIdx.x / npairs;
-  const int g = (int)(blockIdx.x - cb * npairs);
-  const unsigned c = cb * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
-  if (g == 0 && c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
-  if (g == 0 && c == 0) *T.count = 0;
+  if (c < G.nlines()) T.flag[c] = 0;  // the limiter's per-line flags (ncell >= nlines)
+  if (c == 0) *T.count = 0;
   int i, j, k;
   unflat(c, G.nx, G.ny, k, j, i);
-  if (2 * g + 1 < T.ntr) tracer_cell32_body<ORD, DIR, F2>(T, G, c, 2 * g, k, j, i);
-  else tracer_cell32_body<ORD, DIR, float>(T, G, c, 2 * g, k, j, i);
+  const int p0 = DIR == 0 ? i : (DIR == 1 ? j : k);
+  const int n = G.n();
+  // the stencil's state offsets along the line; halo positions read the interior cell
+  // whose value the boundary condition copies there
+  const long gsd = DIR == 0 ? 1 : (DIR == 1 ? G.sy : G.sz);
+  long off[ORD];
+  if (p0 >= HS && p0 < n - HS) {
+#pragma unroll
+    for (int m = 0; m < ORD; m++) off[m] = (m - HS) * gsd;
+  } else {
+#pragma unroll
+    for (int m = 0; m < ORD; m++) {
+      bool wall;
+      off[m] = (halo_src(p0 - HS + m, n, A.bc, wall) - p0) * gsd;
+    }
+  }
+  float rser[NG - 1][NG], ruser[NG - 1][NG], ry[NG];
+  {
+    const float *r = T.R + c, *u = T.U + c;  // plane by plane, ncell apart
+#pragma unroll
+    for (int kt = 0; kt < NG - 1; kt++)
+#pragma unroll
+      for (int ii = 0; ii < NG; ii++) {
+        rser[kt][ii] = *r;
+        ruser[kt][ii] = *u;
+        r += ncell;
+        u += ncell;
+      }
+  }
+  // 1/rho of the GLL points: the recording sweep's own reciprocal of the same value
+#pragma unroll
+  for (int ii = 0; ii < NG; ii++) ry[ii] = frcp(rser[0][ii]);
+  const long fs = DIR == 0 ? 1 : (DIR == 1 ? G.nx : (long)G.nx * G.ny), fl = G.face(k, j, i);
+  const UpwindFaces U = upwind_faces(T, p0, n, A.bc == BC_PERIODIC, fl, fs, fl - p0 * fs);
+  const long nface = G.nface();
+  const double *t = T.tr + G.g(k, j, i);
+  for (int l = 0; l < T.ntr; l += 2) {
+    if (l + 1 < T.ntr)
+      tracer_cell32_body<ORD, F2>(T, t + l * G.sv, t + (l + 1) * G.sv, off, rser, ruser, ry, l, U, T.TF + l * nface,
+                                  nface);
+    else
+      tracer_cell32_body<ORD, float>(T, t + l * G.sv, t + l * G.sv, off, rser, ruser, ry, l, U, T.TF + l * nface,
+                                     nface);
+  }
 }
 
 template <int ORD, int DIR>
@@ -286,7 +307,7 @@ cudaError_t run32(const TracerArgs32 &T, int io, cudaStream_t st) {
   if (!(io & TRC_IN_DIVIDED)) tracer_divide_kernel<TracerArgs32><<<gc, 128, 0, st>>>(T, HS);
   cudaError_t e = launch_sweep_t<P32Trc, ORD, DIR>(A, st);  // state split + records
   if (e != cudaSuccess) return e;
-  tracer_cell32_kernel<ORD, DIR><<<gc * (unsigned)((T.ntr + 1) / 2), 128, 0, st>>>(T);
+  tracer_cell32_kernel<ORD, DIR><<<gc, 128, 0, st>>>(T);
   const long nlines = DIR == 0 ? (long)A.nz * A.ny : (DIR == 1 ? (long)A.nz * A.nx : (long)A.ny * A.nx);
   tracer_limit_faces_kernel<TracerArgs32, DIR><<<gf, 128, 0, st>>>(T, HS);
   const long lw = (nlines * T.ntr + 3) / 4;  // one warp per flagged line and tracer, grid-strided
@@ -314,16 +335,14 @@ cudaError_t launch_split_tracers32(int ord, int dir, const SweepArgs32 &Ain, con
   T.tr = tracers;
   T.ntr = ntr;
   T.pos = pos;
-  const long ncp = 2L * ng * ng + 1 + ng;  // trc_cell_planes
+  const long ns = (long)ng * (ng - 1), ncp = 2 * ns + 1 + ng;  // trc_series_planes, trc_cell_planes
   T.R = scratch;
-  T.U = scratch + (long)ng * ng * ncell;
-  T.D = scratch + 2L * ng * ng * ncell;
-  T.Y = T.D + ncell;
+  T.U = scratch + ns * ncell;
+  T.D = scratch + 2 * ns * ncell;
   T.F0 = scratch + ncp * ncell;
   T.VN = T.F0 + nfmax;
   T.UN = T.VN + nfmax;
   T.RUP = T.UN + nfmax;
-  T.YUP = T.RUP + nfmax;
   T.TF = scratch + ncp * ncell + 5 * nfmax;
   T.TF2 = T.TF + (long)ntr * nfmax;
   T.flag = reinterpret_cast<int *>(T.TF2 + (long)ntr * nfmax);

@@ -105,17 +105,39 @@ template <int DIR> __device__ __forceinline__ long line_of(int k, int j, int i, 
 // both sides of face 0 see cell 0's left edge, of face n cell n-1's right edge. Every face
 // of the line is written by exactly one cell (face 0 and face n of a periodic line by one
 // cell each). fl: this cell's left face, fs: the face stride along the line, f0: face 0.
+// Which faces those are, decided once per cell for all its tracers: the left face (fed by
+// tl), the right face (tr), and on a periodic line face 0 (tr of cell n-1) and face n
+// (tl of cell 0).
+struct UpwindFaces {
+  long fl, fr, f0, fn;
+  bool pl, pr, p0, pn;
+};
+template <class TA>
+__device__ __forceinline__ UpwindFaces upwind_faces(const TA &T, int p, int n, bool periodic, long fl, long fs,
+                                                    long f0) {
+  UpwindFaces U;
+  U.fl = fl;
+  U.fr = fl + fs;
+  U.f0 = f0;
+  U.fn = f0 + (long)n * fs;
+  U.pl = (p == 0 && !periodic) || !(T.VN[fl] > 0);
+  U.pr = (p == n - 1 && !periodic) || T.VN[U.fr] > 0;
+  U.p0 = periodic && p == n - 1 && T.VN[f0] > 0;      // face 0, across the wrap
+  U.pn = periodic && p == 0 && !(T.VN[U.fn] > 0);     // face n, likewise
+  return U;
+}
+template <class Fx, class TA>
+__device__ __forceinline__ void put_upwind_fluxes(const TA &T, Fx *TF, const UpwindFaces &U, Fx tl, Fx tr) {
+  auto put = [&](long fi, Fx t) { TF[fi] = trc_div_up(T, T.F0[fi] * t, fi); };
+  if (U.pl) put(U.fl, tl);
+  if (U.pr) put(U.fr, tr);
+  if (U.p0) put(U.f0, tr);
+  if (U.pn) put(U.fn, tl);
+}
 template <class Fx, class TA>
 __device__ __forceinline__ void write_upwind_fluxes(const TA &T, Fx *TF, int p, int n, bool periodic, long fl,
                                                     long fs, long f0, Fx tl, Fx tr) {
-  auto put = [&](long fi, Fx t) { TF[fi] = trc_div_up(T, T.F0[fi] * t, fi); };
-  const long fr = fl + fs;
-  if ((p == 0 && !periodic) || !(T.VN[fl] > 0)) put(fl, tl);
-  if ((p == n - 1 && !periodic) || T.VN[fr] > 0) put(fr, tr);
-  if (periodic) {
-    if (p == n - 1 && T.VN[f0] > 0) put(f0, tr);                        // face 0, across the wrap
-    if (p == 0 && !(T.VN[f0 + (long)n * fs] > 0)) put(f0 + (long)n * fs, tl);  // face n, likewise
-  }
+  put_upwind_fluxes<Fx>(T, TF, upwind_faces(T, p, n, periodic, fl, fs, f0), tl, tr);
 }
 
 // tracers /= (rho' + rho_h) on the interior cells, with the state before the split

@@ -165,7 +165,7 @@ int awfl_write_netcdf_fields_tracers(awfl_ctx *ctx, const char *path, const doub
  * ntracers <= 64 (0: awfl_split); tracers as for awfl_init_tracers (rho*tracer). The halo
  * cells along dir are left holding tracer/rho, as the reference's in-place halo fill leaves
  * them. Allocates (once per context, grown when ntracers grows) a scratch buffer of
- * (2*ngll^2 + ngll + 1) values per cell and (2*ntracers + 5) per face (doubles; floats in
+ * (2*ngll*(ngll-1) + ngll + 1) values per cell and (2*ntracers + 5) per face (doubles; floats in
  * an FP32 context) and two ints per line. Decisions
  * where the reference's code is not well defined: the limiter scales the faces of a line
  * in place in increasing order, as the reference's loop does when it runs serially (it
