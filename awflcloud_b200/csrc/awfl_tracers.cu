@@ -39,11 +39,16 @@ namespace awfl {
 // Recording FP64 policy: the P64 arithmetic plus the records above, written by the sweep
 // itself (A.tend points at the record base): the cell records from cell_recon's series,
 // the face records from every face flux it computes.
+// 4 CTAs per SM at ord 5, as the plain sweep: 40-72 bytes of spills, 4% faster per step
+// with tracers than 3 CTAs without spills (256x256x128, three tracers)
+#ifndef AWFL_TRC_SWEEP_MINB
+#define AWFL_TRC_SWEEP_MINB 4
+#endif
 struct P64Trc : P64 {
   static constexpr bool kSlab = false;
   static constexpr bool kFaceRec = true;
-  // the record stores need registers: 3 CTAs per SM at ord 5 instead of the plain sweep's 4
-  static constexpr int min_blocks(int ord) { return ord == 5 ? 3 : 1; }
+  // CTAs per SM (AWFL_TRC_SWEEP_MINB above)
+  static constexpr int min_blocks(int ord) { return ord == 5 ? AWFL_TRC_SWEEP_MINB : 1; }
   template <int ORD> struct Rec {
     double *base;
     long n, cell;
