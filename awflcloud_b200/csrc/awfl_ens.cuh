@@ -27,8 +27,17 @@ template <class Args> struct EnsList {
   long total;          // tiles
 };
 
+// CTAs per SM the register budget must allow: the policy's own figure, or, where the
+// including unit defines AWFL_ENS_THREADS_PER_SM_ORD5, that many threads per SM at ord 5
+#ifndef AWFL_ENS_THREADS_PER_SM_ORD5
+#define AWFL_ENS_THREADS_PER_SM_ORD5 0
+#endif
+template <class P, int ORD, int C, int W> constexpr int ens_min_blocks() {
+  return (ORD == 5 && AWFL_ENS_THREADS_PER_SM_ORD5 > 0) ? AWFL_ENS_THREADS_PER_SM_ORD5 / (C * W) : P::min_blocks(ORD);
+}
+
 template <class P, int ORD, int DIR, int C, int W>
-__global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) ens_sweep_kernel(EnsList<typename P::Args> E) {
+__global__ void __launch_bounds__(C *W, (ens_min_blocks<P, ORD, C, W>())) ens_sweep_kernel(EnsList<typename P::Args> E) {
   __shared__ typename P::Args sA;
   for (long t = blockIdx.x; t < E.total; t += gridDim.x) {
     int lo = 0, hi = E.n - 1;

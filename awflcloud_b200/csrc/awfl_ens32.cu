@@ -2,6 +2,12 @@
 // instantiated for the P32 policy, sm_100a. Same flags as awfl_fp32.cu.
 #include <cuda_runtime.h>
 
+// 512 threads' registers per SM at ord 5 (at most 128 a thread): the persistent sweeps then
+// hold 4 CTAs of 128 threads per SM like the single-grid FP32 sweep, instead of 3 at the
+// compiler's 142-150 registers
+#ifndef AWFL_ENS_THREADS_PER_SM_ORD5
+#define AWFL_ENS_THREADS_PER_SM_ORD5 512
+#endif
 #include "awfl_ens.cuh"
 #include "awfl_fp32.cuh"
 
