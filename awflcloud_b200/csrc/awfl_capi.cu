@@ -795,7 +795,14 @@ int awfl_split(awfl_ctx *c, void *d_state, double dt, int dir, void *stream) {
   if (bad_ptr(d_state)) return fail(c, AWFL_ERR_ARG, "state pointer is NULL or misaligned");
   int rc = set_device(c);
   if (rc) return rc;
-  if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendency: the state is unchanged
+  if (dir == 1 && c->sim2d) {  // zero tendencies (Spatial:572-575)
+    // FP64: state += dt*0 as the reference applies them (no value changes; a -0 becomes
+    // +0); the FP32 form's compensated update is left out, its state is unchanged
+    if (fp32(c)) return AWFL_OK;
+    cudaError_t e = launch_add_zero_fp64((double *)d_state, 5, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs, c->nsm,
+                                         (cudaStream_t)stream);
+    return e == cudaSuccess ? AWFL_OK : cuda_fail(c, e, "split");
+  }
   cudaError_t e = fp32(c)
                       ? launch_sweep_fp32(c->cfg.ord, dir, sweep_args32(c, d_state, nullptr, dt, dir, MODE_APPLY),
                                           (cudaStream_t)stream)
@@ -911,7 +918,18 @@ static int split_tracers_io(awfl_ctx *c, void *d_state, double *d_tracers, int n
   // periodic directions shorter than hs are refused by awfl_create)
   int rc = set_device(c);
   if (rc) return rc;
-  if (dir == 1 && c->sim2d) return AWFL_OK;  // zero tendencies (Spatial:572-575)
+  if (dir == 1 && c->sim2d) {  // zero tendencies (Spatial:572-575)
+    // FP64: state and tracers += dt*0 as the reference applies them (no value changes; a
+    // -0 becomes +0; tracers held divided between splits are -0 exactly where rho*tracer
+    // is); the FP32 form leaves both unchanged
+    if (fp32(c)) return AWFL_OK;
+    cudaError_t e = launch_add_zero_fp64((double *)d_state, 5, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs, c->nsm,
+                                         (cudaStream_t)stream);
+    if (e == cudaSuccess)
+      e = launch_add_zero_fp64(d_tracers, ntracers, c->cfg.nx, c->cfg.ny, c->cfg.nz, c->hs, c->nsm,
+                               (cudaStream_t)stream);
+    return e == cudaSuccess ? AWFL_OK : cuda_fail(c, e, "split_tracers");
+  }
   unsigned long long mask = 0;
   for (int l = 0; l < ntracers; l++)
     if (pos[l]) mask |= 1ull << l;

@@ -6,6 +6,7 @@
 //                          K4 Riemann + K5 divergence (+ K6 apply when fused), one direction
 //                          (Spatial:631-957 x, 994-1310 y, 1351-1696 z; Temporal_ader.h:63-65)
 //   apply_kernel           K6 apply alone (Temporal_ader.h:63-65)
+//   add_zero_kernel        the apply of a sim2d y split's zero tendencies
 //   cfl_kernel             K0 CFL time step (Spatial:169-183)
 //   init_state_kernel      K9 initial data quadrature (Spatial:428-485)
 #include <cuda_runtime.h>
@@ -47,6 +48,32 @@ cudaError_t launch_apply_fp64(double *state, const double *tend, double dt, int 
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   apply_kernel<<<(unsigned)blocks, 256, 0, st>>>(state, tend, dt, nx, ny, nz, hs);
+  return cudaGetLastError();
+}
+
+// x += dt*0 on the interior of nplanes planes of the state layout: what the apply
+// (Temporal_ader.h:63-69) does with the zero tendencies of a sim2d y split (Spatial:572-575).
+// It changes no value; a -0 becomes +0, as in the reference.
+__global__ void add_zero_kernel(double *p, int nplanes, int nx, int ny, int nz, int hs) {
+  const long n = (long)nplanes * nz * ny * nx;
+  for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+    long r = idx;
+    const int i = r % nx; r /= nx;
+    const int j = r % ny; r /= ny;
+    const int k = r % nz; r /= nz;
+    const int l = (int)r;
+    const long s = (((long)l * (nz + 2 * hs) + hs + k) * (ny + 2 * hs) + hs + j) * (nx + 2 * hs) + hs + i;
+    p[s] = __dadd_rn(p[s], 0.0);
+  }
+}
+
+cudaError_t launch_add_zero_fp64(double *p, int nplanes, int nx, int ny, int nz, int hs, int nsm, cudaStream_t st) {
+  const long n = (long)nplanes * nz * ny * nx;
+  long blocks = (n + 255) / 256;
+  const long cap = (long)nsm * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  add_zero_kernel<<<(unsigned)blocks, 256, 0, st>>>(p, nplanes, nx, ny, nz, hs);
   return cudaGetLastError();
 }
 

@@ -141,6 +141,8 @@ cudaError_t launch_zero_halo(double *lam, int nx, int ny, int nz, int hs, int ns
 cudaError_t upload_tables_adjrev(int ord, const void *tab, size_t bytes);
 cudaError_t launch_apply_fp64(double *state, const double *tend, double dt, int nx, int ny, int nz, int hs,
                               int nsm, cudaStream_t st);
+// x += dt*0 on the interior of nplanes planes (the sim2d y split's apply of zero tendencies)
+cudaError_t launch_add_zero_fp64(double *p, int nplanes, int nx, int ny, int nz, int hs, int nsm, cudaStream_t st);
 cudaError_t launch_cfl_fp64(const double *state, const double *dens_c, const double *denstheta_c, double cfl,
                             double dx, double dy, double dz, int nx, int ny, int nz, int hs, int nsm,
                             unsigned long long *d_out, cudaStream_t st);

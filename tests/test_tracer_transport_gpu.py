@@ -63,8 +63,11 @@ def test_step_tracers_bit_exact(case):
     got_tr = dtr.cpu().numpy()
     assert np.array_equal(dst.cpu().numpy(), st)
     assert np.array_equal(dst.cpu().numpy(), dst_plain.cpu().numpy())
+    assert np.array_equal(dst.cpu().numpy().view(np.int64), st.view(np.int64))
     for t in range(4):
         assert np.array_equal(got_tr[t], tr[t]), (t, np.abs(got_tr[t] - tr[t]).max())
+        # bit patterns too: the signs of zero (tracers absent from most cells) included
+        assert np.array_equal(got_tr[t].view(np.int64), tr[t].view(np.int64)), t
     # the theta and block tracers have moved (the block is empty on a grid of fewer than
     # 3 cells in x: its x range is [4nx/10, 6nx/10))
     O0 = Oracle(nx, ny, nz, bc=bc, ord_=o)
