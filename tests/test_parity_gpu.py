@@ -150,6 +150,7 @@ def test_rising_bubble_bit_exact(o, n, steps, cfl):
         O.time_step(st, dt)
         c.step(d, dt)
     assert np.array_equal(d.cpu().numpy(), st)
+    assert np.array_equal(d.cpu().numpy().view(np.int64), st.view(np.int64))  # signs of zero too
 
 
 @pytest.mark.parametrize("o,n,steps,cfl", [(5, (64, 64, 32), 50, 0.8)])
@@ -219,11 +220,14 @@ def test_splits_bit_exact_vs_crpow_oracle(case):
             c.compute_tendencies(d, tend, dt, dd)
             torch.cuda.synchronize()
             assert np.array_equal(tend.cpu().numpy(), t_o), (step, spl)
+            assert np.array_equal(tend.cpu().numpy().view(np.int64), t_o.view(np.int64)), (step, spl)
             O.apply(st, t_o, dt)
             c.apply_tendencies(d, tend, dt)
             assert np.array_equal(d.cpu().numpy(), st), (step, spl)
+            assert np.array_equal(d.cpu().numpy().view(np.int64), st.view(np.int64)), (step, spl)
         c.step(fused, dt)
         assert np.array_equal(fused.cpu().numpy(), st), step
+        assert np.array_equal(fused.cpu().numpy().view(np.int64), st.view(np.int64)), step
 
 
 def test_fused_equals_unfused_bitwise():

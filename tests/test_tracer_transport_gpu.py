@@ -151,6 +151,9 @@ def test_split_tracers_equal_reference_tracer_code(golden_dir):
             got = dtr.cpu().numpy()
             want = z[name + "_tracers%d" % (s + 1)]
             assert np.array_equal(got, want), (name, s, int(d), np.abs(got - want).max())
+            assert np.array_equal(got.view(np.int64), np.ascontiguousarray(want).view(np.int64)), (name, s, int(d))
         assert np.array_equal(dst.cpu().numpy(), z[name + "_state_end"]), name
+        assert np.array_equal(dst.cpu().numpy().view(np.int64),
+                              np.ascontiguousarray(z[name + "_state_end"]).view(np.int64)), name
         done += 1
     assert done >= 7
