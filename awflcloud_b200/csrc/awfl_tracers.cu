@@ -148,6 +148,19 @@ __device__ __forceinline__ double trc_update(const TracerArgs &T, double q, int 
 }  // namespace
 }  // namespace awfl
 
+// The limiter, update and division kernels are bound by memory latency, not bandwidth:
+// registers capped for 16 (limiter, division: 32 registers) and 12 (update: 40) CTAs of 128
+// threads per SM, a few bytes of spills, made the FP64 step with three tracers 10% faster
+// than the compiler's 36-72 registers (12 for the limiter, or 16 for the update: slower)
+#ifndef AWFL_TRC_LIMIT_MINB
+#define AWFL_TRC_LIMIT_MINB 16
+#endif
+#ifndef AWFL_TRC_UPDATE_MINB
+#define AWFL_TRC_UPDATE_MINB 12
+#endif
+#ifndef AWFL_TRC_DIVIDE_MINB
+#define AWFL_TRC_DIVIDE_MINB 16
+#endif
 #include "awfl_trc.cuh"
 
 namespace awfl {

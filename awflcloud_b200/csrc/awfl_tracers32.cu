@@ -141,6 +141,18 @@ __device__ __forceinline__ double trc_update(const TracerArgs32 &T, double q, in
 }  // namespace
 }  // namespace awfl
 
+// The limiter, update and division kernels are bound by memory latency, not bandwidth:
+// registers capped for 16 CTAs of 128 threads per SM (32) made the FP32 form's step with
+// three tracers 16% faster than the compiler's 36-64 registers (12 CTAs: slower)
+#ifndef AWFL_TRC_LIMIT_MINB
+#define AWFL_TRC_LIMIT_MINB 16
+#endif
+#ifndef AWFL_TRC_UPDATE_MINB
+#define AWFL_TRC_UPDATE_MINB 16
+#endif
+#ifndef AWFL_TRC_DIVIDE_MINB
+#define AWFL_TRC_DIVIDE_MINB 16
+#endif
 #include "awfl_trc.cuh"
 
 namespace awfl {

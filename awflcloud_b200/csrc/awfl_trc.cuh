@@ -143,8 +143,11 @@ __device__ __forceinline__ void write_upwind_fluxes(const TA &T, Fx *TF, int p, 
 // tracers /= (rho' + rho_h) on the interior cells, with the state before the split
 // (Spatial:624-627). The halos are not touched: every kernel of the split maps a halo
 // position to the interior cell whose value it holds.
+#ifndef AWFL_TRC_DIVIDE_MINB
+#define AWFL_TRC_DIVIDE_MINB 1
+#endif
 template <class TA>
-__global__ void __launch_bounds__(128) tracer_divide_kernel(TA T, int hs) {
+__global__ void __launch_bounds__(128, AWFL_TRC_DIVIDE_MINB) tracer_divide_kernel(TA T, int hs) {
   const Geo<0> G(T.A, hs);
   const long ncell = (long)G.nz * G.ny * G.nx;
   const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -171,8 +174,11 @@ __global__ void __launch_bounds__(128) tracer_divide_kernel(TA T, int hs) {
 // every read sees the value the serial loop would). tracer_limit_lines_kernel redoes the
 // flagged lines serially. Equal reads are compared as values: a read that differs only in
 // the sign of a zero leaves the factor unchanged (it enters as f2 - f1 + eps).
+#ifndef AWFL_TRC_LIMIT_MINB
+#define AWFL_TRC_LIMIT_MINB 1
+#endif
 template <class TA, int DIR>
-__global__ void __launch_bounds__(128) tracer_limit_faces_kernel(TA T, int hs) {
+__global__ void __launch_bounds__(128, AWFL_TRC_LIMIT_MINB) tracer_limit_faces_kernel(TA T, int hs) {
   using Fx = typename TA::Flux;
   const Geo<DIR> G(T.A, hs);
   const int nf = (int)G.nface();  // < 2^31 (the launchers check)
@@ -311,8 +317,11 @@ __global__ void __launch_bounds__(128) tracer_limit_lines_kernel(TA T, int hs) {
 // holding tracer/density, as the reference's in-place halo fill leaves them. out_divided:
 // the interior is left divided by the post-split density (the state's split is done), as
 // the next split's tracer_divide_kernel would divide it.
+#ifndef AWFL_TRC_UPDATE_MINB
+#define AWFL_TRC_UPDATE_MINB 1
+#endif
 template <class TA, int DIR>
-__global__ void __launch_bounds__(128) tracer_update_kernel(TA T, int hs, bool out_divided) {
+__global__ void __launch_bounds__(128, AWFL_TRC_UPDATE_MINB) tracer_update_kernel(TA T, int hs, bool out_divided) {
   const Geo<DIR> G(T.A, hs);
   const long ncell = (long)G.nz * G.ny * G.nx;
   const long c = blockIdx.x * (long)blockDim.x + threadIdx.x;
