@@ -564,8 +564,19 @@ __device__ __forceinline__ void sweep_tile(const typename P::Args &A, const int 
 
 // TMA: the policy's single-grid TMA path; its tensor map lives in the (grid-constant)
 // kernel parameter, the only place besides global memory a TMA copy may read it from.
+// CTAs per SM the register budget must allow: the policy's figure, or for the x-slab
+// sweeps of ord 5 at least AWFL_SLAB_MINB_ORD5 (4: the FP32 slab sweep drops from 142 to
+// 112 registers, no spills, and its x split of a 128x256x128 slab from 0.442 to 0.408 ms;
+// the same bound on the single-grid FP32 sweeps made them slower)
+#ifndef AWFL_SLAB_MINB_ORD5
+#define AWFL_SLAB_MINB_ORD5 4
+#endif
+template <class P, int ORD, bool SLAB> constexpr int sweep_min_blocks() {
+  return (SLAB && ORD == 5 && AWFL_SLAB_MINB_ORD5 > P::min_blocks(ORD)) ? AWFL_SLAB_MINB_ORD5 : P::min_blocks(ORD);
+}
+
 template <class P, int ORD, int DIR, int C, int W, bool TMA, bool SLAB = false>
-__global__ void __launch_bounds__(C *W, P::min_blocks(ORD)) sweep_kernel(const __grid_constant__ typename P::Args A) {
+__global__ void __launch_bounds__(C *W, (sweep_min_blocks<P, ORD, SLAB>())) sweep_kernel(const __grid_constant__ typename P::Args A) {
   if constexpr (TMA) sweep_tile<P, ORD, DIR, C, W, true, SLAB>(A, blockIdx.x, blockIdx.y, P::tma_map(A));
   else sweep_tile<P, ORD, DIR, C, W, false, SLAB>(A, blockIdx.x, blockIdx.y);
 }
